@@ -1,0 +1,604 @@
+"""Scene generator and reader/writer for the reference's text input formats.
+
+A *scene* is a plain dict of numpy arrays and scalars:
+
+    params   dict of the 38 ``world.par`` keys (``src/dem_subsphere_io.cu:83-128``)
+    sub      dict: clump_id int32[N], pos f64[N,3], local f64[N,3], mass f64[N],
+             radius f64[N]                       (ph columns, ``src/dem_subsphere_io.cu:174-175``)
+    clump    dict: pos, vel, angvel f64[K,3], quat f64[K,4] (x,y,z,w),
+             prop f64[K,4] = (Ixx, Iyy, Izz, M)  (ch columns, ``src/dem_clumpsphere_io.cu:46-48``)
+    cube     dict or None: half f64[3], centre, vel, angvel f64[3], quat f64[4]
+             (``src/dem_cube_wall_io.cu:43-48``)
+    cylinder dict or None: radius, half_height, axis f64[3], prop f64[4], centre, vel,
+             angvel f64[3], quat f64[4]          (``src/dem_cylind_wall_io.cu:41-49``)
+    intruder dict or None: shape 'sphere'|'cylinder', radius, half_height, axis f64[3],
+             prop f64[4], pos, vel, angvel f64[3], quat f64[4],
+             motion 'constant_velocity'|'gravity'|'gravity_after_contact'
+             (``src/dem_penetrator_io.cu:42-115``)
+
+The builders below produce the synthetic workloads the engine is measured on
+(monodisperse spheres, tetrahedral clumps, polydisperse clumps) with seeded
+numpy generators, so every scene is reproducible from its seed.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+# Parameter keys in the order the reference's world.par lists them.
+PAR_KEYS = [
+    "NumberBody", "ClumpNum", "BranchLmtLen", "BodyFileDir", "IniConFile",
+    "StepSize", "EndStep", "StartStep", "OutputInterval",
+    "Ymod", "Prat", "Frcoe", "NormRes", "Frvel", "Beta", "MU_T", "MU_R", "Cohesion",
+    "Gravity", "Thresh", "GridLevels", "Update",
+    "WorldSize_x", "WorldSize_y", "WorldSize_z",
+    "WorldOrigin_x", "WorldOrigin_y", "WorldOrigin_z",
+    "BoxUpLmt_x", "BoxUpLmt_y", "BoxUpLmt_z",
+    "BoxLowLmt_x", "BoxLowLmt_y", "BoxLowLmt_z",
+    "isIntruder", "isSelfGravity", "isWallForce", "isQuaternion",
+]
+assert len(PAR_KEYS) == 38
+
+PI_REF = 3.14159265359  # the reference's PI literal (src/dem_constant.h:14)
+
+
+def damping_from_restitution(e: float) -> float:
+    """Damping ratio derived from restitution, as the reference's
+    LoadParameters computes it (src/dem_subsphere_io.cu:143-145)."""
+    ln = math.log(e)
+    return 2.0 * math.sqrt(5.0 / 6.0) * ln / math.sqrt(ln * ln + PI_REF * PI_REF)
+
+
+def rayleigh_dt(r: float, rho: float, E: float, nu: float) -> float:
+    """Rayleigh time step pi r sqrt(rho/G) / (0.1631 nu + 0.8766)."""
+    G = E / (2.0 * (1.0 + nu))
+    return math.pi * r * math.sqrt(rho / G) / (0.1631 * nu + 0.8766)
+
+
+# ----------------------------------------------------------------------------
+# quaternion helpers (x, y, z, w) with w the scalar, the reference convention
+# ----------------------------------------------------------------------------
+
+def quat_to_body2world(q: np.ndarray) -> np.ndarray:
+    """Rotation matrices C_bn (body -> world) for quaternions q[...,4].
+
+    Same matrix as the reference's Quat2IvDCM (src/type.h:238-250)."""
+    x, y, z, w = q[..., 0], q[..., 1], q[..., 2], q[..., 3]
+    m = np.empty(q.shape[:-1] + (3, 3))
+    m[..., 0, 0] = x * x - y * y - z * z + w * w
+    m[..., 1, 0] = 2.0 * (x * y + z * w)
+    m[..., 2, 0] = 2.0 * (x * z - y * w)
+    m[..., 0, 1] = 2.0 * (x * y - z * w)
+    m[..., 1, 1] = -x * x + y * y - z * z + w * w
+    m[..., 2, 1] = 2.0 * (y * z + x * w)
+    m[..., 0, 2] = 2.0 * (x * z + y * w)
+    m[..., 1, 2] = 2.0 * (y * z - x * w)
+    m[..., 2, 2] = -x * x - y * y + z * z + w * w
+    return m
+
+
+def random_unit_quaternions(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Uniformly distributed unit quaternions (Shoemake's method)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+    q = np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2),
+                  b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)], axis=1)
+    return q
+
+
+# ----------------------------------------------------------------------------
+# clump templates
+# ----------------------------------------------------------------------------
+
+def tetra_template(r: float = 1.0, offset_ratio: float = 0.6) -> np.ndarray:
+    """Four subsphere centres on a regular tetrahedron at distance
+    offset_ratio*r from the centroid (body frame)."""
+    v = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], dtype=np.float64)
+    v /= np.linalg.norm(v[0])
+    return v * (offset_ratio * r)
+
+
+def union_mass_properties(centres: np.ndarray, radii: np.ndarray, rho: float,
+                          samples: int = 400_000, seed: int = 7):
+    """Mass, centre of mass and inertia tensor of a union of spheres by
+    seeded Monte Carlo over the bounding box."""
+    rng = np.random.default_rng(seed)
+    lo = (centres - radii[:, None]).min(0)
+    hi = (centres + radii[:, None]).max(0)
+    pts = lo + (hi - lo) * rng.random((samples, 3))
+    inside = np.zeros(samples, dtype=bool)
+    for c, rr in zip(centres, radii):
+        inside |= ((pts - c) ** 2).sum(1) <= rr * rr
+    vol = np.prod(hi - lo) * inside.mean()
+    p = pts[inside]
+    com = p.mean(0)
+    d = p - com
+    cov = (d[:, :, None] * d[:, None, :]).mean(0)
+    inertia = rho * vol * (np.trace(cov) * np.eye(3) - cov)
+    return rho * vol, com, inertia
+
+
+def _principal_frame(centres, radii, rho):
+    """Re-express a template in its principal frame; returns (centres', I_principal, M)."""
+    M, com, I = union_mass_properties(centres, radii, rho)
+    w, V = np.linalg.eigh(I)
+    if np.linalg.det(V) < 0:
+        V[:, 0] = -V[:, 0]
+    return (centres - com) @ V, w, M
+
+
+# ----------------------------------------------------------------------------
+# scene assembly
+# ----------------------------------------------------------------------------
+
+def default_params(**kw) -> dict:
+    p = {
+        "NumberBody": 0, "ClumpNum": 0, "BranchLmtLen": 64,
+        "BodyFileDir": "./Rocks/", "IniConFile": "ph.00000000.bt",
+        "StepSize": 1e-5, "EndStep": 1, "StartStep": 0, "OutputInterval": 1,
+        "Ymod": 1e7, "Prat": 0.3, "Frcoe": 0.5, "NormRes": 0.5, "Frvel": 5e-4,
+        "Beta": 0.5, "MU_T": 0.5, "MU_R": 0.5, "Cohesion": 0.0,
+        "Gravity": -9.81, "Thresh": 1e-4, "GridLevels": 1, "Update": 0,
+        "WorldSize_x": 0.1, "WorldSize_y": 0.1, "WorldSize_z": 0.1,
+        "WorldOrigin_x": 0.0, "WorldOrigin_y": 0.0, "WorldOrigin_z": 0.0,
+        "BoxUpLmt_x": 0.1, "BoxUpLmt_y": 0.1, "BoxUpLmt_z": 0.1,
+        "BoxLowLmt_x": 0.0, "BoxLowLmt_y": 0.0, "BoxLowLmt_z": 0.0,
+        "isIntruder": 0, "isSelfGravity": 0, "isWallForce": 1, "isQuaternion": 1,
+    }
+    p.update(kw)
+    return p
+
+
+def set_world_box(params: dict, lo, hi):
+    """World box = hashing box = [lo, hi] (the reference pads it by one cell itself)."""
+    lo = np.asarray(lo, float)
+    hi = np.asarray(hi, float)
+    for a, k in enumerate("xyz"):
+        params["WorldOrigin_" + k] = float(lo[a])
+        params["WorldSize_" + k] = float(hi[a] - lo[a])
+        params["BoxLowLmt_" + k] = float(lo[a])
+        params["BoxUpLmt_" + k] = float(hi[a])
+
+
+def assemble(params, clump_pos, clump_quat, clump_vel, clump_angvel, clump_prop,
+             members_local, members_radius, members_mass, cube=None, cylinder=None,
+             intruder=None) -> dict:
+    """Build a scene from per-clump poses and per-clump member lists.
+
+    members_local[k] is an (n_k, 3) array of body-frame offsets, members_radius[k]
+    and members_mass[k] are (n_k,) arrays.  Subsphere world positions are
+    X_c + C_bn(q) local, the pose the reference's UpdatePos computes."""
+    K = len(clump_pos)
+    counts = np.array([len(m) for m in members_local], dtype=np.int64)
+    cid = np.repeat(np.arange(K, dtype=np.int32), counts)
+    local = np.concatenate(members_local, axis=0)
+    radius = np.concatenate(members_radius)
+    mass = np.concatenate(members_mass)
+    R = quat_to_body2world(clump_quat)
+    pos = clump_pos[cid] + np.einsum("nij,nj->ni", R[cid], local)
+    params = dict(params)
+    params["NumberBody"] = int(len(cid))
+    params["ClumpNum"] = int(K)
+    params["isWallForce"] = 1 if (cube is not None or cylinder is not None) else 0
+    params["isIntruder"] = 1 if intruder is not None else 0
+    return {
+        "params": params,
+        "sub": {"clump_id": cid, "pos": pos, "local": local, "mass": mass, "radius": radius},
+        "clump": {"pos": np.ascontiguousarray(clump_pos, dtype=np.float64),
+                  "vel": np.ascontiguousarray(clump_vel, dtype=np.float64),
+                  "quat": np.ascontiguousarray(clump_quat, dtype=np.float64),
+                  "angvel": np.ascontiguousarray(clump_angvel, dtype=np.float64),
+                  "prop": np.ascontiguousarray(clump_prop, dtype=np.float64)},
+        "cube": cube, "cylinder": cylinder, "intruder": intruder,
+    }
+
+
+def make_cube(half, centre, vel=(0, 0, 0), angvel=(0, 0, 0), quat=(1.0, 0, 0, 0)):
+    return {"half": np.array(half, float), "centre": np.array(centre, float),
+            "vel": np.array(vel, float), "angvel": np.array(angvel, float),
+            "quat": np.array(quat, float)}
+
+
+def make_cylinder(radius, half_height, centre, axis=(0, 0, 1), prop=(1, 1, 1, 1),
+                  vel=(0, 0, 0), angvel=(0, 0, 0), quat=(0, 0, 0, 1.0)):
+    return {"radius": float(radius), "half_height": float(half_height),
+            "axis": np.array(axis, float), "prop": np.array(prop, float),
+            "centre": np.array(centre, float), "vel": np.array(vel, float),
+            "angvel": np.array(angvel, float), "quat": np.array(quat, float)}
+
+
+def make_intruder(shape, radius, pos, vel, half_height=None, axis=(0, 0, 1),
+                  prop=(1, 1, 1, 1), angvel=(0, 0, 0), quat=(0, 0, 0, 1.0),
+                  motion="constant_velocity"):
+    if half_height is None:
+        half_height = radius
+    return {"shape": shape, "radius": float(radius), "half_height": float(half_height),
+            "axis": np.array(axis, float), "prop": np.array(prop, float),
+            "pos": np.array(pos, float), "vel": np.array(vel, float),
+            "angvel": np.array(angvel, float), "quat": np.array(quat, float),
+            "motion": motion}
+
+
+def lattice_points(rng, n, spacing, lo, nx, ny, jitter):
+    """n points on a cubic lattice filling x, then y, then z layers."""
+    idx = np.arange(n)
+    ix, iy, iz = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+    pts = np.stack([ix, iy, iz], axis=1) * spacing + np.asarray(lo, float)
+    if jitter > 0:
+        pts = pts + rng.uniform(-jitter, jitter, size=pts.shape)
+    return pts
+
+
+# ----------------------------------------------------------------------------
+# the measured workloads
+# ----------------------------------------------------------------------------
+
+MATERIAL = {"Ymod": 1e7, "Prat": 0.3, "Frcoe": 0.5, "NormRes": 0.5, "rho": 2650.0}
+
+
+def make_cfg0(n: int = 2000, seed: int = 20260828, steps: int = 10000) -> dict:
+    """2,000 monodisperse one-sphere clumps (r = 1 mm) on a 2.2 r lattice with
+    +-0.1 r jitter settling in a 40 x 40 x 80 mm cube wall; dt = 0.2 dt_Rayleigh."""
+    rng = np.random.default_rng(seed)
+    r, rho = 1e-3, MATERIAL["rho"]
+    m = rho * 4.0 / 3.0 * math.pi * r ** 3
+    I = 0.4 * m * r * r
+    dt = 0.2 * rayleigh_dt(r, rho, MATERIAL["Ymod"], MATERIAL["Prat"])
+    sp = 2.2 * r
+    pts = lattice_points(rng, n, sp, (1.1 * r, 1.1 * r, 1.1 * r), 18, 18, 0.1 * r)
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=steps,
+                            Ymod=MATERIAL["Ymod"], Prat=MATERIAL["Prat"],
+                            Frcoe=MATERIAL["Frcoe"], NormRes=MATERIAL["NormRes"],
+                            Thresh=0.2 * r, BranchLmtLen=64)
+    set_world_box(params, (0, 0, 0), (0.04, 0.04, 0.08))
+    K = n
+    return assemble(params, pts, np.tile([0, 0, 0, 1.0], (K, 1)), np.zeros((K, 3)),
+                    np.zeros((K, 3)), np.tile([I, I, I, m], (K, 1)),
+                    [np.zeros((1, 3))] * K, [np.array([r])] * K, [np.array([m])] * K,
+                    cube=make_cube((0.02, 0.02, 0.04), (0.02, 0.02, 0.04)))
+
+
+def _tetra_members(scales, r, offset_ratio, rho):
+    base = tetra_template(1.0, offset_ratio)
+    cen, Ip, M1 = _principal_frame(base, np.ones(4), rho)  # unit-size template
+    locals_, radii, masses, props = [], [], [], []
+    for s in scales:
+        rr = r * s
+        M = M1 * rr ** 3
+        locals_.append(cen * rr)
+        radii.append(np.full(4, rr))
+        masses.append(np.full(4, M / 4.0))
+        props.append([Ip[0] * rr ** 5, Ip[1] * rr ** 5, Ip[2] * rr ** 5, M])
+    return locals_, radii, masses, np.array(props)
+
+
+def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000) -> dict:
+    """50,000 tetrahedral clumps (4 subspheres, r = 1 mm, centre offset 0.6 r,
+    log-normal(0, 0.2) size scale, random orientation) seeded on a lattice above
+    the floor of a closed cylinder wall (R = 60 mm, half-height 150 mm, axis z)."""
+    rng = np.random.default_rng(seed)
+    r, rho = 1e-3, MATERIAL["rho"]
+    scales = rng.lognormal(0.0, 0.2, n_clumps)
+    locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
+    rmax = max(rr.max() for rr in radii)
+    ext = 2.0 * (0.6 * rmax + rmax) * 1.05  # lattice spacing: clump diameter + 5 %
+    R, H = 0.06, 0.15
+    # square lattice inscribed in the cylinder cross-section
+    half = (R - ext) / math.sqrt(2.0)
+    nx = max(1, int(2 * half / ext))
+    pts = lattice_points(rng, n_clumps, ext, (-half + 0.5 * ext, -half + 0.5 * ext, -H + 0.6 * ext),
+                         nx, nx, 0.02 * ext)
+    q = random_unit_quaternions(rng, n_clumps)
+    rmin = min(rr.min() for rr in radii)
+    dt = 0.2 * rayleigh_dt(rmin, rho, MATERIAL["Ymod"], MATERIAL["Prat"])
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=steps,
+                            Ymod=MATERIAL["Ymod"], Prat=MATERIAL["Prat"],
+                            Frcoe=MATERIAL["Frcoe"], NormRes=MATERIAL["NormRes"],
+                            Thresh=0.2 * rmin, BranchLmtLen=96)
+    top = max(pts[:, 2].max() + ext, H)
+    set_world_box(params, (-R, -R, -H), (R, R, top))
+    K = n_clumps
+    return assemble(params, pts, q, np.zeros((K, 3)), np.zeros((K, 3)), props,
+                    locals_, radii, masses,
+                    cylinder=make_cylinder(R, H, (0, 0, 0)))
+
+
+# ----------------------------------------------------------------------------
+# small, contact-rich scenes for parity tests
+# ----------------------------------------------------------------------------
+
+def _place_intruder_on_bed(pos, radius, xy, shape, Ri, Hi, depth):
+    """z of an intruder centred above xy whose lowest point overlaps the
+    highest subsphere beneath it by `depth`."""
+    d2 = (pos[:, 0] - xy[0]) ** 2 + (pos[:, 1] - xy[1]) ** 2
+    if shape == "sphere":
+        reach = np.sqrt(np.maximum((Ri + radius) ** 2 - d2, 0.0))
+        cand = d2 < (Ri + radius) ** 2
+        z = (pos[cand, 2] + reach[cand] - depth)
+    else:
+        cand = d2 < (Ri + radius) ** 2
+        z = pos[cand, 2] + radius[cand] + Hi - depth
+    return float(z.max())
+
+
+def make_test_spheres(n=400, seed=1, r=1e-3, overlap=0.02, vel=0.5, angvel=200.0,
+                      intruder="sphere", motion="constant_velocity", thresh_ratio=0.0003,
+                      dt=2e-7, steps=30, wall="cube", bl=64):
+    """Compressed lattice of one-sphere clumps: every neighbour pair overlaps by
+    about `overlap`*r, random linear and angular velocities, walls and an
+    intruder in contact from the first step, and a small Thresh so the
+    contact list is rebuilt every few steps."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    nx = int(round(n ** (1 / 3))) + 1
+    sp = 2 * r * (1 - overlap)
+    lo = np.array([r * (1 - 2 * overlap)] * 3)
+    pts = lattice_points(rng, n, sp, lo, nx, nx, 0.2 * overlap * r)
+    hi = pts.max(0) + r * (1 - 2 * overlap)
+    K = n
+    m = rho * 4 / 3 * math.pi * r ** 3
+    I = 0.4 * m * r * r
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=1,
+                            Thresh=thresh_ratio * r, BranchLmtLen=bl)
+    params["Cohesion"] = 0.0
+    box_lo, box_hi = -0.5 * r * np.ones(3), hi + np.array([0.5 * r, 0.5 * r, 6 * r])
+    set_world_box(params, box_lo, box_hi)
+    cube = cyl = None
+    if wall == "cube":
+        cube = make_cube(0.5 * hi, 0.5 * hi)
+    elif wall == "cylinder":
+        c = 0.5 * hi
+        cyl = make_cylinder(0.5 * max(hi[0], hi[1]) * 1.0, 0.5 * hi[2], c)
+    intr = None
+    if intruder is not None:
+        xy = (0.5 * hi[0] + 0.3 * r, 0.5 * hi[1] - 0.2 * r)
+        Ri, Hi = 3 * r, 2 * r
+        rad = np.full(len(pts), r)
+        z = _place_intruder_on_bed(pts, rad, xy, intruder, Ri, Hi, 0.25 * r)
+        c = (xy[0], xy[1], z)
+        if intruder == "sphere":
+            intr = make_intruder("sphere", Ri, c, (0, 0, -0.5), prop=(1, 1, 1, 0.05),
+                                 motion=motion)
+        else:
+            intr = make_intruder("cylinder", Ri, c, (0, 0, -0.5), half_height=Hi,
+                                 prop=(1, 1, 1, 0.05), motion=motion)
+    return assemble(params, pts, random_unit_quaternions(rng, K),
+                    rng.uniform(-vel, vel, (K, 3)), rng.uniform(-angvel, angvel, (K, 3)),
+                    np.tile([I, I, I, m], (K, 1)),
+                    [np.zeros((1, 3))] * K, [np.array([r])] * K, [np.array([m])] * K,
+                    cube=cube, cylinder=cyl, intruder=intr)
+
+
+def make_test_tetra(n_clumps=120, seed=2, r=1e-3, squeeze=0.8, vel=0.5, angvel=200.0,
+                    intruder="cylinder", motion="constant_velocity", thresh_ratio=0.0003,
+                    dt=2e-7, steps=30, wall="cube", bl=96, sigma=0.15):
+    """Tetrahedral clumps with random orientations packed closer than their
+    extent (`squeeze` < 1) so many inter-clump pairs overlap."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    scales = rng.lognormal(0.0, sigma, n_clumps)
+    locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
+    rmed = r * float(np.median(scales))
+    ext = 2 * 1.6 * rmed * squeeze
+    nx = int(round(n_clumps ** (1 / 3))) + 1
+    lo = np.array([0.5 * ext] * 3)
+    pts = lattice_points(rng, n_clumps, ext, lo, nx, nx, 0.03 * ext)
+    hi = pts.max(0) + 0.5 * ext
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=1,
+                            Thresh=thresh_ratio * r, BranchLmtLen=bl)
+    set_world_box(params, -0.5 * r * np.ones(3), hi + np.array([0.5 * r, 0.5 * r, 8 * r]))
+    cube = cyl = None
+    if wall == "cube":
+        cube = make_cube(0.5 * hi, 0.5 * hi)
+    elif wall == "cylinder":
+        cyl = make_cylinder(0.5 * max(hi[0], hi[1]), 0.5 * hi[2], 0.5 * hi)
+    intr = None
+    K = n_clumps
+    quats = random_unit_quaternions(rng, K)
+    if intruder is not None:
+        cid = np.repeat(np.arange(K), [len(m) for m in locals_])
+        R = quat_to_body2world(quats)
+        sub_pos = pts[cid] + np.einsum("nij,nj->ni", R[cid], np.concatenate(locals_))
+        sub_r = np.concatenate(radii)
+        xy = (0.5 * hi[0] + 0.3 * r, 0.5 * hi[1] - 0.2 * r)
+        Ri, Hi = 3 * r, 2 * r
+        z = _place_intruder_on_bed(sub_pos, sub_r, xy, intruder, Ri, Hi, 0.25 * r)
+        c = (xy[0], xy[1], z)
+        if intruder == "sphere":
+            intr = make_intruder("sphere", Ri, c, (0, 0, -0.5), prop=(1, 1, 1, 0.05),
+                                 motion=motion)
+        else:
+            intr = make_intruder("cylinder", Ri, c, (0, 0, -0.5), half_height=Hi,
+                                 prop=(1, 1, 1, 0.05), motion=motion)
+    return assemble(params, pts, quats,
+                    rng.uniform(-vel, vel, (K, 3)), rng.uniform(-angvel, angvel, (K, 3)),
+                    props, locals_, radii, masses, cube=cube, cylinder=cyl, intruder=intr)
+
+
+# ----------------------------------------------------------------------------
+# text formats of the reference
+# ----------------------------------------------------------------------------
+
+def _g(x) -> str:
+    return repr(float(x))
+
+
+def write_world_par(params: dict, path: str):
+    with open(path, "w") as f:
+        f.write("# written by nbody-clump_b200 scenegen\n")
+        for k in PAR_KEYS:
+            v = params[k]
+            if isinstance(v, str):
+                f.write(f"{k} = {v}\n")
+            elif k in ("NumberBody", "ClumpNum", "BranchLmtLen", "EndStep", "StartStep",
+                       "OutputInterval", "Update", "isIntruder", "isSelfGravity",
+                       "isWallForce", "isQuaternion"):
+                f.write(f"{k} = {int(v)}\n")
+            else:
+                f.write(f"{k} = {_g(v)}\n")
+
+
+def write_reference_inputs(scene: dict, d: str):
+    """Write world.par, ph/ch .bt and Rocks/*.bt into directory d, in the
+    layouts the reference reads (src/dem_subsphere_io.cu:52-175,
+    src/dem_clumpsphere_io.cu:46-48, src/dem_cube_wall_io.cu:43-48,
+    src/dem_penetrator_io.cu:42-115, src/dem_cylind_wall_io.cu:41-49)."""
+    os.makedirs(os.path.join(d, "Rocks"), exist_ok=True)
+    p = scene["params"]
+    write_world_par(p, os.path.join(d, "world.par"))
+    s = scene["sub"]
+    N = len(s["radius"])
+    # per-clump local member index
+    cid = s["clump_id"]
+    first = np.zeros(N, dtype=np.int64)
+    order = np.argsort(cid, kind="stable")
+    starts = np.searchsorted(cid[order], cid[order])
+    first[order] = np.arange(N) - starts
+    with open(os.path.join(d, p["IniConFile"]), "w") as f:
+        for i in range(N):
+            f.write("%d %d %d %s %s %s %s %s %s %s %s\n" % (
+                i, first[i], cid[i], *map(_g, s["pos"][i]), *map(_g, s["local"][i]),
+                _g(s["mass"][i]), _g(s["radius"][i])))
+    c = scene["clump"]
+    with open(os.path.join(d, "ch.00000000.bt"), "w") as f:
+        for k in range(len(c["pos"])):
+            f.write("%d %s\n" % (k, " ".join(map(_g, np.concatenate(
+                [c["pos"][k], c["vel"][k], c["quat"][k], c["angvel"][k], c["prop"][k]])))))
+    cube = scene.get("cube")
+    if cube is None:  # the reference always reads a cube file; write an inert one
+        cube = make_cube((1e3, 1e3, 1e3), (0, 0, 0))
+    with open(os.path.join(d, "Rocks", "CubeWall.bt"), "w") as f:
+        f.write(" ".join(map(_g, cube["half"])) + "\n")
+        f.write(" ".join(map(_g, cube["centre"])) + "\n")
+        f.write(" ".join(map(_g, cube["vel"])) + "\n")
+        f.write(" ".join(map(_g, cube["quat"])) + "\n")
+        f.write(" ".join(map(_g, cube["angvel"])) + "\n")
+    cyl = scene.get("cylinder")
+    if cyl is not None:
+        with open(os.path.join(d, "Rocks", "CylindWall.bt"), "w") as f:
+            f.write(f"{_g(cyl['radius'])} {_g(cyl['half_height'])}\n")
+            f.write(" ".join(map(_g, cyl["axis"])) + "\n")
+            f.write(" ".join(map(_g, cyl["prop"])) + "\n")
+            f.write(" ".join(map(_g, cyl["centre"])) + "\n")
+            f.write(" ".join(map(_g, cyl["vel"])) + "\n")
+            f.write(" ".join(map(_g, cyl["quat"])) + "\n")
+            f.write(" ".join(map(_g, cyl["angvel"])) + "\n")
+    it = scene.get("intruder")
+    if it is None:  # inert intruder far away (the reference always reads one)
+        it = make_intruder("sphere", 1e-3, (1e3, 1e3, 1e3), (0, 0, 0))
+    with open(os.path.join(d, "Rocks", "Penetrator.bt"), "w") as f:
+        if it["shape"] == "sphere":
+            f.write(f"sphere {_g(it['radius'])}\n")
+        else:
+            f.write(f"cylinder {_g(it['radius'])} {_g(it['half_height'])} "
+                    + " ".join(map(_g, it["axis"])) + "\n")
+        f.write(" ".join(map(_g, it["prop"])) + "\n")
+        f.write(" ".join(map(_g, it["pos"])) + "\n")
+        f.write(" ".join(map(_g, it["vel"])) + "\n")
+        f.write(" ".join(map(_g, it["quat"])) + "\n")
+        f.write(" ".join(map(_g, it["angvel"])) + "\n")
+        f.write(f"motion {it['motion']}\n")
+
+
+def read_reference_inputs(d: str) -> dict:
+    """Read a reference working directory (world.par, ph/ch .bt, Rocks/) into
+    a scene dict; the inverse of write_reference_inputs."""
+    params = {}
+    with open(os.path.join(d, "world.par")) as f:
+        for line in f:
+            core = line.split("#", 1)[0].replace("\t", "").replace(" ", "").strip()
+            if not core:
+                continue
+            k, v = core.split("=", 1)
+            params[k] = v
+    for k in list(params):
+        if k not in ("BodyFileDir", "IniConFile"):
+            params[k] = float(params[k])
+    for k in ("NumberBody", "ClumpNum", "BranchLmtLen", "EndStep", "StartStep",
+              "OutputInterval", "Update", "isIntruder", "isSelfGravity", "isWallForce",
+              "isQuaternion"):
+        params[k] = int(params[k])
+    N, K = params["NumberBody"], params["ClumpNum"]
+    ph = np.loadtxt(os.path.join(d, params["IniConFile"]), ndmin=2)[:N]
+    ch = np.loadtxt(os.path.join(d, "ch.00000000.bt"), ndmin=2)[:K]
+    sub = {"clump_id": ph[:, 2].astype(np.int32), "pos": ph[:, 3:6].copy(),
+           "local": ph[:, 6:9].copy(), "mass": ph[:, 9].copy(), "radius": ph[:, 10].copy()}
+    clump = {"pos": ch[:, 1:4].copy(), "vel": ch[:, 4:7].copy(), "quat": ch[:, 7:11].copy(),
+             "angvel": ch[:, 11:14].copy(), "prop": ch[:, 14:18].copy()}
+    cw = np.array(open(os.path.join(d, "Rocks", "CubeWall.bt")).read().split(), float)
+    cube = make_cube(cw[0:3], cw[3:6], cw[6:9], cw[13:16], cw[9:13])
+    tok = open(os.path.join(d, "Rocks", "Penetrator.bt")).read().split()
+    shape = tok[0].lower()
+    if shape == "sphere":
+        radius, hh, axis, rest = float(tok[1]), float(tok[1]), (0, 0, 1.0), tok[2:]
+    else:
+        off = 1 if shape == "cylinder" else 0
+        vals = tok[off:]
+        radius, hh, axis, rest = float(vals[0]), float(vals[1]), tuple(map(float, vals[2:5])), vals[5:]
+        shape = "cylinder"
+    num = list(map(float, rest[:17]))  # property(4) pos(3) vel(3) quat(4) angvel(3)
+    motion = "constant_velocity"
+    if len(rest) > 18 and rest[17].lower() == "motion":
+        motion = rest[18].lower()
+        if motion in ("constant", "kinematic"):
+            motion = "constant_velocity"
+        elif motion == "dynamic":
+            motion = "gravity"
+    intr = make_intruder(shape, radius, num[4:7], num[7:10], half_height=hh, axis=axis,
+                         prop=num[0:4], quat=num[10:14], angvel=num[14:17], motion=motion)
+    cyl = None
+    cpath = os.path.join(d, "Rocks", "CylindWall.bt")
+    if os.path.exists(cpath):
+        cv = np.array(open(cpath).read().split(), float)
+        cyl = make_cylinder(cv[0], cv[1], cv[9:12], cv[2:5], cv[5:9], cv[12:15], cv[19:22], cv[15:19])
+    return {"params": params, "sub": sub, "clump": clump,
+            "cube": cube if params["isWallForce"] else cube,
+            "cylinder": None, "intruder": intr if params["isIntruder"] else None,
+            "cylinder_file": cyl}
+
+
+# ----------------------------------------------------------------------------
+# npz round trip of a scene (golden fixtures and bench inputs)
+# ----------------------------------------------------------------------------
+
+def scene_to_npz(scene: dict, path: str):
+    flat = {}
+    for k, v in scene["params"].items():
+        flat["par/" + k] = np.array(v)
+    for grp in ("sub", "clump"):
+        for k, v in scene[grp].items():
+            flat[f"{grp}/{k}"] = np.asarray(v)
+    for grp in ("cube", "cylinder", "intruder"):
+        if scene.get(grp) is not None:
+            for k, v in scene[grp].items():
+                flat[f"{grp}/{k}"] = np.asarray(v)
+    np.savez_compressed(path, **flat)
+
+
+def scene_from_npz(path: str) -> dict:
+    z = np.load(path, allow_pickle=False)
+    scene = {"params": {}, "sub": {}, "clump": {}, "cube": None, "cylinder": None,
+             "intruder": None}
+    for key in z.files:
+        grp, k = key.split("/", 1)
+        v = z[key]
+        if grp == "par":
+            v = v.item() if v.shape == () else v
+            if isinstance(v, (np.integer, int)):
+                v = int(v)
+            elif isinstance(v, (np.floating, float)):
+                v = float(v)
+            elif isinstance(v, (np.str_, str)):
+                v = str(v)
+            scene["params"][k] = v
+        else:
+            if scene.get(grp) is None:
+                scene[grp] = {}
+            if v.shape == ():
+                v = v.item()
+                if isinstance(v, np.str_):
+                    v = str(v)
+            scene[grp][k] = v
+    return scene

@@ -1,0 +1,2 @@
+// Empty stand-in: the reference includes this header but uses nothing from it.
+#pragma once
