@@ -1,0 +1,310 @@
+"""Benchmark: subsphere-steps/s of the NBodyClump step on a B200.
+
+Workload (one GPU): 50,000 tetrahedral clumps = 200,000 subspheres
+(r = 1 mm x LogNormal(0, 0.2), centre offset 0.6 r, random orientation)
+settling under gravity in a closed cylinder wall (R = 60 mm, half-height
+300 mm), contact law in FP32 with FP64 positions and quaternions, dt = 0.2 of
+the Rayleigh step, Thresh = 0.2 r_min.  One step = one pass of the clump step
+(kick/drift/attitude/pose, list rebuild when triggered, contacts, clump
+reduction).  The bed is generated by seeded numpy and settles from a loose
+layered packing; the timed steps are the first W+1..W+K steps of that settle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank runs its own independent scene (different seed):
+weak scaling, no collective on the data path; timing is the max over ranks.
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "nbody-clump_b200"))
+import scenegen as sg  # noqa: E402
+
+METRIC = "subsphere-steps/sec"
+WORKLOAD = "cfg1: 50,000 tetra clumps (200,000 subspheres) settling in a cylinder wall"
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6553.6), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reduce_max(value, world, backend):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if backend == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_b200(args, world, rank, local):
+    import nbc
+    backend = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        backend = "nccl"
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    seed = 20260828 + rank
+    scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
+    N, K = scene["params"]["NumberBody"], scene["params"]["ClumpNum"]
+
+    # ---- device-resident throughput -----------------------------------
+    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True, device=local)
+    eng.step(args.warmup)
+    eng.sync()
+    st0 = eng.stats()
+    eng.timing_enable(True)
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        eng.step(args.steps)      # returns after the device finished (stream synchronised)
+        t1 = time.perf_counter()
+    tm = eng.timing_read()
+    st1 = eng.stats()
+    barrier(world)
+    local_s = t1 - t0
+    secs = reduce_max(local_s, world, backend)
+    value = N * args.steps * world / secs
+
+    # ---- end to end through the C ABI with host buffers -----------------
+    # create (H2D of the scene from host arrays), K steps, sync, D2H of the
+    # clump state, all inside the timed region
+    host_in = sum(np.asarray(v).nbytes for v in scene["sub"].values()) + \
+        sum(np.asarray(v).nbytes for v in scene["clump"].values())
+    barrier(world)
+    te0 = time.perf_counter()
+    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True, device=local)
+    e2.step(args.warmup + args.steps)
+    e2.sync()
+    out = e2.clumps()
+    te1 = time.perf_counter()
+    e2.close()
+    host_out = sum(v.nbytes for v in out.values())
+    e2e_s = reduce_max(te1 - te0, world, backend)
+    e2e_steps = args.warmup + args.steps
+    e2e_value = N * e2e_steps * world / e2e_s
+
+    # ---- roofline of the contact kernel -----------------------------------
+    pk, pk_kind = peaks()
+    npairs = st1["npairs"]
+    alg = algorithmic_contact_bytes(N, K, npairs, args.precision)
+    avg_ms = tm["contact_ms"] / max(1, tm["contact_launches"])
+    achieved = alg / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "contact_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tj = json.load(open(tp))
+            traffic = tj["bytes_per_subsphere"] * N
+        except Exception:
+            traffic = None
+
+    cpu = cpu_baseline(args) if (rank == 0 and not args.no_cpu_baseline) else None
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "subsphere-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded numpy bed, no dataset)",
+            "config": {"workload": WORKLOAD, "subspheres": N, "clumps": K, "precision": args.precision,
+                       "lanes": args.lanes, "graph": True, "pairs_listed": npairs,
+                       "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
+                       "l2": "working set 60+ MB per step; not flushed between steps (state is resident by design)",
+                       "parallelism": f"replicas x{world} (independent scenes)"},
+            "e2e": {"value": e2e_value, "unit": "subsphere-steps/s", "h2d_bytes_per_step": host_in / e2e_steps,
+                    "d2h_bytes_per_step": host_out / e2e_steps, "steps": e2e_steps,
+                    "includes": "nbc_create (upload) + steps + sync + clump-state download"},
+            "gpu_launches": tm["kernel_launches"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
+                         "frac": achieved / pk if pk else None, "traffic": traffic,
+                         "kernel": "k_contact", "avg_launch_ms": avg_ms,
+                         "alg_bytes_per_launch": alg, "peak_kind": pk_kind},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def algorithmic_contact_bytes(N, K, npairs, precision):
+    """Unique bytes the contact kernel must move per launch.
+
+    Per listed pair (front + back entry): partner indices 4 + 8 B and the
+    contact flag written 1 B.  Per subsphere: FP64 position and radius 32 B,
+    contact kinematics 3 x Real4, list offsets 4 x 4 B, boundary bits 2 B,
+    force and torque out 2 x Real4.  History traffic (36 B per touching pair
+    each way in FP32) is excluded here because the touching fraction is not
+    known host-side; ncu's DRAM bytes are reported beside this figure."""
+    r4 = 16 if precision == "mixed" else 32
+    per_pair = 4 + 8 + 1
+    per_sub = 32 + 3 * r4 + 16 + 2 + 2 * r4
+    return per_pair * npairs + per_sub * N
+
+
+def cpu_baseline(args):
+    """The FP64 CPU oracle on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    scene = sg.make_cfg1(n_clumps=args.clumps, seed=20260828, steps=10)
+    threads = 1
+    o = oracle.OracleScene(scene, threads=threads)
+    o.step(1)  # first step includes the initial list build, like the GPU warm-up
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > args.cpu_seconds or n >= 200:
+            break
+    dt = time.perf_counter() - t0
+    N = scene["params"]["NumberBody"]
+    return {"value": N * n / dt, "unit": "subsphere-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} steps of the same 200,000-subsphere scene after its first step, single thread"}
+
+
+def run_reference(args, world, rank, local):
+    """The reference arm: the project's FP64 CPU restatement of the
+    reference's clump step (the reference itself has no CPU implementation),
+    with every host thread, on the same workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    scene = sg.make_cfg1(n_clumps=args.clumps, seed=20260828, steps=args.warmup + args.steps)
+    N = scene["params"]["NumberBody"]
+    o = oracle.OracleScene(scene, threads=threads)
+    t = time.perf_counter()
+    o.step(max(1, args.warmup))
+    warm = (time.perf_counter() - t) / max(1, args.warmup)
+    budget = 150.0
+    steps = max(1, min(args.steps, int(budget / max(warm, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    v = N * steps / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "subsphere-steps/s",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded numpy bed, no dataset)",
+        "config": {"workload": WORKLOAD, "subspheres": N, "precision": "f64",
+                   "note": "CPU restatement of the reference clump step (oracle/), OpenMP threads"},
+        "cpu_baseline": {"value": v, "unit": "subsphere-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} steps of the {N}-subsphere scene after {max(1, args.warmup)} warm-up steps"},
+        "e2e": {"value": v, "unit": "subsphere-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--lanes", type=int, default=16)
+    ap.add_argument("--clumps", type=int, default=50_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

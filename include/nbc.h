@@ -1,0 +1,173 @@
+/*
+ * nbc.h -- C ABI of the B200 DEM engine (libnbc.so).
+ *
+ * Drop-in boundary for the NBodyClump hot path: the reference exposes one
+ * entry point, DEMClumpMain::RunSimulationClump() (src/dem_clump.h:36-96,
+ * called from src/main.cpp:7-8), which reads world.par, the ph/ch .bt initial
+ * conditions and Rocks/ files from the working directory, advances the clump
+ * step loop (src/dem_simulation_clump.cu:110-259) and writes the binary
+ * snapshot files.  nbc_open/nbc_run replace that call; the scene-level calls
+ * below replace the reference's internal class interfaces for callers that
+ * hold their scenes in memory (tests, batching, serving).
+ *
+ * Conventions: plain pointers and sizes only; every call returns nbc_status
+ * (the reference calls exit() on every error, src/include/helper_cuda.h:
+ * 985-1010); arrays are host memory unless named *_dev; vectors are
+ * interleaved xyz (quaternions xyzw) in double precision.  The engine owns
+ * all device memory.  Calls on one engine are not reentrant; separate
+ * engines are independent.
+ */
+#ifndef NBC_H
+#define NBC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int nbc_status;
+#define NBC_OK 0
+#define NBC_ERR_ARG (-1)          /* invalid argument or inconsistent scene */
+#define NBC_ERR_CUDA (-2)         /* a CUDA call failed (message in nbc_last_error) */
+#define NBC_ERR_IO (-3)           /* missing or malformed input file (src/dem_subsphere_io.cu:40-141) */
+#define NBC_ERR_NONFINITE (-4)    /* non-finite subsphere force (src/dem_force_cube_wall_clump.cu:295-331) */
+#define NBC_ERR_NO_DEVICE (-5)    /* no CUDA device: the engine has no CPU fallback */
+#define NBC_ERR_MEMORY (-6)       /* device allocation failed or over the engine's budget */
+#define NBC_ERR_STATE (-7)        /* call not valid in the engine's state */
+
+#define NBC_PREC_F64 0            /* every quantity in FP64, like the reference */
+#define NBC_PREC_MIXED 1          /* contact law in FP32 (overlap and positions FP64) */
+
+#define NBC_WALL_NONE 0
+#define NBC_WALL_CUBE 1           /* Rocks/CubeWall.bt, src/dem_cube_wall_io.cu:21-53 */
+#define NBC_WALL_CYLINDER 2       /* Rocks/CylindWall.bt, src/dem_cylind_wall_io.cu:20-55 */
+
+#define NBC_INTR_NONE (-1)
+#define NBC_INTR_CYLINDER 0       /* PenetratorShape, src/dem_parameters.h:93 */
+#define NBC_INTR_SPHERE 1
+
+#define NBC_MOTION_CONSTANT_VELOCITY 0   /* src/dem_penetrator_io.cu:100-115 */
+#define NBC_MOTION_GRAVITY 1
+#define NBC_MOTION_GRAVITY_AFTER_CONTACT 2
+
+/* One scene: the contents of world.par, ph/ch .bt and Rocks/ files.
+ * Replaces Parameters/GlobalFlg (src/dem_parameters.h:7-79) plus the arrays
+ * loaded by DEMSubSphereIo::LoadPhase (src/dem_subsphere_io.cu:151-193) and
+ * DEMClumpSphereIo::LoadPhase (src/dem_clumpsphere_io.cu:24-62). */
+typedef struct {
+    int n_sub, n_clump, branch_len;          /* NumberBody, ClumpNum, BranchLmtLen */
+    int start_step, end_step, output_interval;
+    double dt, ymod, prat, frcoe, normres, beta, cohesion, gravity, thresh;
+    double world_origin[3], world_size[3], box_lo[3], box_hi[3];
+    int is_wall_force;                       /* isWallForce */
+    /* subspheres (ph columns 3-11) */
+    const int* clump_id;                     /* [n_sub], 0 .. n_clump-1 */
+    const double* pos;                       /* [n_sub][3] */
+    const double* local;                     /* [n_sub][3] body-frame offset */
+    const double* mass;                      /* [n_sub] */
+    const double* radius;                    /* [n_sub] */
+    /* clumps (ch columns 2-18) */
+    const double* clump_pos;                 /* [n_clump][3] */
+    const double* clump_vel;                 /* [n_clump][3] */
+    const double* clump_quat;                /* [n_clump][4] x y z w */
+    const double* clump_angvel;              /* [n_clump][3] */
+    const double* clump_prop;                /* [n_clump][4] Ixx Iyy Izz M */
+    /* wall */
+    int wall;                                /* NBC_WALL_* */
+    double cube_half[3], cube_centre[3], cube_vel[3], cube_angvel[3];
+    double cyl_radius, cyl_half_height, cyl_axis[3], cyl_centre[3], cyl_vel[3], cyl_angvel[3];
+    /* intruder (penetrator) */
+    int intruder;                            /* NBC_INTR_* */
+    int intr_motion;                         /* NBC_MOTION_* */
+    double intr_radius, intr_half_height, intr_axis[3], intr_prop[4];
+    double intr_pos[3], intr_vel[3], intr_angvel[3];
+    /* hierarchical grid: levels > 1 enables it */
+    int levels;
+    const int* level;                        /* [n_sub], 0 = coarsest */
+    const double* level_cell;                /* [levels] cell size per level */
+} nbc_scene_desc;
+
+typedef struct {
+    int precision;      /* NBC_PREC_* */
+    int lanes;          /* lanes per subsphere in the contact kernel: 0 = autotuned, 8, 16 or 32 */
+    int use_graph;      /* 1: one CUDA graph per step with a conditional rebuild node */
+    int device;         /* CUDA device ordinal */
+    double pair_slack;  /* pair capacity = slack * pairs of the first list (0 = 1.6) */
+} nbc_options;
+
+typedef struct nbc_engine nbc_engine;
+
+/* last error message of the calling thread */
+const char* nbc_last_error(void);
+void nbc_default_options(nbc_options* opt);
+
+/* --- drop-in entry point: DEMClumpMain::RunSimulationClump ------------- */
+/* Read world.par, IniConFile, ch.00000000.bt and Rocks/ from workdir
+ * (src/dem_simulation_clump.cu:3-72). */
+nbc_status nbc_open(const char* workdir, const nbc_options* opt, nbc_engine** out);
+/* Run StartStep..EndStep with the reference's outputs into workdir
+ * (OutPart, OutClump, OutForce, OutCnt; src/dem_simulation_clump.cu:74-259). */
+nbc_status nbc_run(nbc_engine* e);
+
+/* --- scene-level calls ---------------------------------------------------- */
+nbc_status nbc_create(const nbc_scene_desc* const* scenes, int n_scenes, const nbc_options* opt,
+                      nbc_engine** out);
+nbc_status nbc_destroy(nbc_engine* e);
+/* advance every scene by nsteps steps (the loop body of
+ * src/dem_simulation_clump.cu:110-225) */
+nbc_status nbc_step(nbc_engine* e, int nsteps);
+/* like nbc_step, and the last step also records per-contact export data
+ * (normal force and contact point per pair, force split per subsphere) */
+nbc_status nbc_step_export(nbc_engine* e, int nsteps);
+/* wait for the device; applies the pending second half-kick so the state
+ * read back is the state after the last completed step */
+nbc_status nbc_sync(nbc_engine* e);
+
+nbc_status nbc_num_scenes(const nbc_engine* e, int* n);
+/* steps, rebuilds, pairs in the current list, error bits */
+nbc_status nbc_scene_stats(nbc_engine* e, int scene, int* steps, int* rebuilds, int* npairs, int* err);
+/* subspheres in the engine's current (cell-sorted) order; part_fix is the
+ * original ph row (ParticleID of src/dem_clump.cu:170-171) */
+nbc_status nbc_get_subspheres(nbc_engine* e, int scene, int* part_fix, int* clump_id, double* pos,
+                              double* radius);
+/* body-frame offset and mass of every subsphere, current order */
+nbc_status nbc_get_subsphere_body(nbc_engine* e, int scene, double* local, double* mass);
+nbc_status nbc_get_clumps(nbc_engine* e, int scene, double* pos, double* vel, double* quat,
+                          double* angvel, double* force, double* torque);
+/* force and torque on every subsphere from the last step (pairs + walls +
+ * intruder, the reference's totF/totT, src/dem_clump.cu:89-101), current order */
+nbc_status nbc_get_sub_forces(nbc_engine* e, int scene, double* force, double* torque);
+/* after nbc_step_export: pair / wall / intruder parts [6][n_sub][3] */
+nbc_status nbc_get_force_parts(nbc_engine* e, int scene, double* parts);
+/* the half pair list in the reference's order (Lpa/Lpb, src/dem_grid.cu:
+ * 561-601), subsphere indices in the current order; *npairs in/out */
+nbc_status nbc_get_pairs(nbc_engine* e, int scene, int* npairs, int* lpa, int* lpb);
+/* rows in the reference's pitched layout (Anei: front entries from slot 0,
+ * back entries from slot bl-1 downwards, -1 elsewhere), [n_sub][bl] */
+nbc_status nbc_get_rows(nbc_engine* e, int scene, int bl, int* anei, int* ng, int* ni);
+/* after nbc_step_export: force-chain rows of the reference's OutCnt output
+ * (CalFcnChain_cuk, src/dem_force_particle.cu:238-268): normal force and
+ * contact point per row slot, [n_sub][bl][3] each */
+nbc_status nbc_get_chain(nbc_engine* e, int scene, int bl, double* fcn, double* cpt);
+/* intruder position, velocity, last reaction force/torque, contact state */
+nbc_status nbc_get_intruder(nbc_engine* e, int scene, double* pos, double* vel, double* reaction,
+                            double* torque, int* state);
+/* after nbc_step_export: per-subsphere intruder diagnostics Fcn, Fct, Tcn,
+ * Tct [4][n_sub][3] (src/dem_force_penetrator_clump.cu:127-177) */
+nbc_status nbc_get_intruder_diag(nbc_engine* e, int scene, double* diag);
+/* reaction force/torque recorded at each of the last `count` completed
+ * steps (CacheFc/CacheTc of src/dem_integrate_penetrator.cu:108-109), [count][6] */
+nbc_status nbc_get_intruder_history(nbc_engine* e, int scene, int count, double* out);
+/* CUDA-event timing of the contact kernel on the engine's stream (also
+ * inside graph launches): enable resets the totals; read returns the summed
+ * kernel time in ms, the number of timed contact launches, the number of
+ * engine kernels launched and the number of rebuilds since enabling */
+nbc_status nbc_timing_enable(nbc_engine* e, int enable);
+nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launches, long long* kernel_launches,
+                           int* rebuilds);
+/* device memory in use and wall time of the last nbc_step in ms */
+nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBC_H */

@@ -1,0 +1,71 @@
+"""Build libnbc.so (the engine and its C ABI) in-tree for sm_100a.
+
+    python nbody-clump_b200/build.py [--force] [--verbose]
+
+nvcc compiles the CUDA sources and the C++ host files with
+`-gencode arch=compute_100a,code=sm_100a`; the shared library lands next to
+this file so it travels with the source tree.  No GPU is needed to build.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libnbc.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+SOURCES = ["engine.cu", "capi.cpp", "io.cpp"]
+HEADERS = ["kernels.cuh", "nbc_dev.cuh", "nbc_math.cuh", "engine.h", "io.h"]
+
+
+def _stale() -> bool:
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "nbc.h"))
+    deps.append(os.path.abspath(__file__))
+    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return OUT
+    objs = []
+    common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+              "-I", os.path.join(os.path.dirname(HERE), "include")]
+    for src in SOURCES:
+        obj = os.path.join(CSRC, "_obj_" + src.replace(".", "_") + ".o")
+        lang = [] if src.endswith(".cu") else ["-x", "cu"] if src.endswith(".cu") else []
+        cmd = [NVCC, *ARCH, *common, *lang, "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"] if verbose else []
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {src}")
+        if verbose and r.stderr:
+            sys.stderr.write(r.stderr)
+        objs.append(obj)
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("link failed")
+    for o in objs:
+        os.remove(o)
+    return OUT
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(a.force, a.verbose))

@@ -1,0 +1,309 @@
+// capi.cpp -- the extern "C" entry points of include/nbc.h.
+//
+// Every call catches the engine's exceptions and returns a status code with
+// the message in nbc_last_error(); the reference instead exits the process on
+// any error (src/include/helper_cuda.h:985-1010, src/dem_grid.cu:710-719,
+// src/dem_force_cube_wall_clump.cu:322-331).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/nbc.h"
+#include "engine.h"
+#include "io.h"
+
+namespace nbc {
+extern thread_local std::string g_last_error;
+}
+
+struct nbc_engine {
+    std::unique_ptr<nbc::EngineBase> eng;
+    std::unique_ptr<nbc::Workdir> wd;  // set by nbc_open
+    nbc_options opt;
+};
+
+namespace {
+
+nbc_status fail(nbc_status code, const std::string& msg) {
+    nbc::g_last_error = msg;
+    return code;
+}
+
+template <typename F>
+nbc_status guard(F&& f) {
+    try {
+        f();
+        return NBC_OK;
+    } catch (const nbc::NonFinite& e) {
+        return fail(NBC_ERR_NONFINITE, e.what());
+    } catch (const std::bad_alloc& e) {
+        return fail(NBC_ERR_MEMORY, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(NBC_ERR_ARG, e.what());
+    } catch (const std::runtime_error& e) {
+        std::string m = e.what();
+        if (m.find("no CUDA device") != std::string::npos) return fail(NBC_ERR_NO_DEVICE, m);
+        if (m.find("cudaMalloc") != std::string::npos) return fail(NBC_ERR_MEMORY, m);
+        if (m.find("scene ") == 0 || m.find("buffer too small") != std::string::npos ||
+            m.find("longer than") != std::string::npos || m.find("too many") != std::string::npos)
+            return fail(NBC_ERR_ARG, m);
+        return fail(NBC_ERR_CUDA, m);
+    } catch (...) {
+        return fail(NBC_ERR_CUDA, "unknown error");
+    }
+}
+
+bool bad_scene(nbc_engine* e, int s) { return !e || !e->eng || s < 0 || s >= e->eng->num_scenes(); }
+
+}  // namespace
+
+extern "C" {
+
+const char* nbc_last_error(void) { return nbc::g_last_error.c_str(); }
+
+void nbc_default_options(nbc_options* o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->precision = NBC_PREC_MIXED;
+    o->lanes = 0;
+    o->use_graph = 1;
+    o->device = 0;
+    o->pair_slack = 1.6;
+}
+
+nbc_status nbc_create(const nbc_scene_desc* const* scenes, int n, const nbc_options* opt, nbc_engine** out) {
+    if (!scenes || n <= 0 || !out) return fail(NBC_ERR_ARG, "nbc_create: no scenes");
+    for (int s = 0; s < n; s++)
+        if (!scenes[s]) return fail(NBC_ERR_ARG, "nbc_create: null scene");
+    *out = nullptr;
+    nbc_options o;
+    if (opt) o = *opt; else nbc_default_options(&o);
+    std::unique_ptr<nbc_engine> h(new nbc_engine());
+    h->opt = o;
+    nbc_status st = guard([&] {
+        std::vector<const nbc_scene_desc*> v(scenes, scenes + n);
+        h->eng.reset(nbc::make_engine(v, o));
+    });
+    if (st == NBC_OK) *out = h.release();
+    return st;
+}
+
+nbc_status nbc_destroy(nbc_engine* e) {
+    delete e;
+    return NBC_OK;
+}
+
+nbc_status nbc_step(nbc_engine* e, int n) {
+    if (!e || !e->eng || n < 0) return fail(NBC_ERR_ARG, "nbc_step: bad arguments");
+    return guard([&] { e->eng->step(n, false); });
+}
+
+nbc_status nbc_step_export(nbc_engine* e, int n) {
+    if (!e || !e->eng || n < 1) return fail(NBC_ERR_ARG, "nbc_step_export: bad arguments");
+    return guard([&] { e->eng->step(n, true); });
+}
+
+nbc_status nbc_sync(nbc_engine* e) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "nbc_sync: null engine");
+    return guard([&] { e->eng->sync(); });
+}
+
+nbc_status nbc_num_scenes(const nbc_engine* e, int* n) {
+    if (!e || !e->eng || !n) return fail(NBC_ERR_ARG, "nbc_num_scenes: bad arguments");
+    *n = e->eng->num_scenes();
+    return NBC_OK;
+}
+
+nbc_status nbc_scene_stats(nbc_engine* e, int s, int* steps, int* rebuilds, int* npairs, int* err) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->stats(s, steps, rebuilds, npairs, err); });
+}
+
+nbc_status nbc_get_subspheres(nbc_engine* e, int s, int* fix, int* cid, double* pos, double* rad) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->get_subspheres(s, fix, cid, pos, rad); });
+}
+
+nbc_status nbc_get_subsphere_body(nbc_engine* e, int s, double* local, double* mass) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->get_body(s, local, mass); });
+}
+
+nbc_status nbc_get_clumps(nbc_engine* e, int s, double* pos, double* vel, double* quat, double* w, double* f,
+                          double* t) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->get_clumps(s, pos, vel, quat, w, f, t); });
+}
+
+nbc_status nbc_get_sub_forces(nbc_engine* e, int s, double* f, double* t) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->get_sub_forces(s, f, t); });
+}
+
+nbc_status nbc_get_force_parts(nbc_engine* e, int s, double* parts) {
+    if (bad_scene(e, s) || !parts) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_force_parts(s, parts); });
+}
+
+nbc_status nbc_get_pairs(nbc_engine* e, int s, int* np, int* lpa, int* lpb) {
+    if (bad_scene(e, s) || !np) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_pairs(s, np, lpa, lpb); });
+}
+
+nbc_status nbc_get_rows(nbc_engine* e, int s, int bl, int* anei, int* ng, int* ni) {
+    if (bad_scene(e, s) || bl <= 0) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_rows(s, bl, anei, ng, ni); });
+}
+
+nbc_status nbc_get_chain(nbc_engine* e, int s, int bl, double* fcn, double* cpt) {
+    if (bad_scene(e, s) || bl <= 0 || !fcn || !cpt) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_chain(s, bl, fcn, cpt); });
+}
+
+nbc_status nbc_get_intruder(nbc_engine* e, int s, double* pos, double* vel, double* reac, double* tq, int* state) {
+    if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
+    return guard([&] { e->eng->get_intruder(s, pos, vel, reac, tq, state); });
+}
+
+nbc_status nbc_get_intruder_diag(nbc_engine* e, int s, double* diag) {
+    if (bad_scene(e, s) || !diag) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_intruder_diag(s, diag); });
+}
+
+nbc_status nbc_get_intruder_history(nbc_engine* e, int s, int count, double* out) {
+    if (bad_scene(e, s) || count < 0 || !out) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_intruder_history(s, count, out); });
+}
+
+nbc_status nbc_timing_enable(nbc_engine* e, int on) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
+    return guard([&] { e->eng->timing_enable(on != 0); });
+}
+
+nbc_status nbc_timing_read(nbc_engine* e, double* ms, int* nc, long long* nk, int* nr) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
+    return guard([&] { e->eng->timing_read(ms, nc, nk, nr); });
+}
+
+nbc_status nbc_engine_info(nbc_engine* e, double* bytes, double* ms) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
+    return guard([&] { e->eng->info(bytes, ms); });
+}
+
+// --- drop-in entry point ----------------------------------------------------
+
+nbc_status nbc_open(const char* workdir, const nbc_options* opt, nbc_engine** out) {
+    if (!workdir || !out) return fail(NBC_ERR_ARG, "nbc_open: bad arguments");
+    *out = nullptr;
+    std::unique_ptr<nbc::Workdir> wd(new nbc::Workdir());
+    std::string err;
+    if (!nbc::load_workdir(workdir, *wd, err)) return fail(NBC_ERR_IO, err);
+    nbc_options o;
+    if (opt) o = *opt;
+    else { nbc_default_options(&o); o.precision = NBC_PREC_F64; }
+    const nbc_scene_desc* d = &wd->desc;
+    nbc_engine* e = nullptr;
+    nbc_status st = nbc_create(&d, 1, &o, &e);
+    if (st != NBC_OK) return st;
+    e->wd = std::move(wd);
+    *out = e;
+    return NBC_OK;
+}
+
+// RunSimulationClump's loop with its outputs (src/dem_simulation_clump.cu:74-259)
+nbc_status nbc_run(nbc_engine* e) {
+    if (!e || !e->eng || !e->wd) return fail(NBC_ERR_STATE, "nbc_run: engine not opened from a working directory");
+    nbc::Workdir& w = *e->wd;
+    const nbc_scene_desc& D = w.desc;
+    const std::string dir = w.dir;
+    const bool intr = w.is_intruder;
+    for (const char* sub : {"/OutPart/", "/OutClump/", "/OutCnt/"})
+        if (!nbc::make_dirs(dir + sub)) return fail(NBC_ERR_IO, std::string("cannot create ") + dir + sub);
+    if (intr) {
+        if (!nbc::make_dirs(dir + "/OutForce/")) return fail(NBC_ERR_IO, "cannot create OutForce");
+        std::ofstream shape(dir + "/OutClump/PenetratorShape.bt");
+        if (D.intruder == NBC_INTR_SPHERE) shape << "sphere " << D.intr_radius << std::endl;
+        else shape << "cylinder " << D.intr_radius << " " << D.intr_half_height << std::endl;
+    }
+    const int n = D.n_sub, k = D.n_clump, bl = D.branch_len, oi = D.output_interval;
+    std::vector<int> fix(n), cid(n), ident(n), nei;
+    std::vector<double> pos(3 * (size_t)n), local(3 * (size_t)n), mass(n), rad(n);
+    std::vector<double> cp(3 * (size_t)k), cv(3 * (size_t)k), cq(4 * (size_t)k), cw(3 * (size_t)k), prop(4 * (size_t)k);
+    std::vector<double> hist, diag, fcn, cpt;
+    for (int i = 0; i < n; i++) ident[i] = i;
+    int count = 0, count2 = 0;
+    for (int ii = D.start_step; ii < D.end_step;) {
+        // run up to the next output boundary; the step that ends on one
+        // records the per-contact export data its files need
+        int to_out = oi - count;
+        int to_cnt = 2 * oi - count2;
+        int chunk = std::min(std::min(to_out, to_cnt), D.end_step - ii);
+        bool exp = (chunk == to_out) || (chunk == to_cnt);
+        nbc_status st = exp ? nbc_step_export(e, chunk) : nbc_step(e, chunk);
+        if (st != NBC_OK) return st;
+        ii += chunk;
+        count += chunk;
+        count2 += chunk;
+        if (count == oi || count2 == 2 * oi) {
+            st = nbc_sync(e);
+            if (st != NBC_OK) return st;
+        }
+        if (count == oi) {
+            std::printf("StepSize = %d\n", ii);
+            st = guard([&] {
+                e->eng->get_subspheres(0, fix.data(), cid.data(), pos.data(), rad.data());
+                e->eng->get_body(0, local.data(), mass.data());
+                e->eng->get_clumps(0, cp.data(), cv.data(), cq.data(), cw.data(), nullptr, nullptr);
+                e->eng->get_clump_prop(0, prop.data());
+            });
+            if (st != NBC_OK) return st;
+            if (!nbc::write_ph(nbc::bin_name(dir + "/OutPart", "ph", ii), n, ident.data(), fix.data(), cid.data(),
+                               pos.data(), local.data(), mass.data(), rad.data()))
+                return fail(NBC_ERR_IO, "cannot write OutPart");
+            bool ok;
+            if (intr) {
+                double ip[3], iv[3], re[3], tq[3];
+                int state;
+                st = guard([&] { e->eng->get_intruder(0, ip, iv, re, tq, &state); });
+                if (st != NBC_OK) return st;
+                double iw[3] = {D.intr_angvel[0], D.intr_angvel[1], D.intr_angvel[2]};
+                ok = nbc::write_ch(nbc::bin_name(dir + "/OutClump", "ch", ii), k, cp.data(), cv.data(), cq.data(),
+                                   cw.data(), prop.data(), ip, iv, w.intr_quat, iw);
+                hist.resize(6 * (size_t)oi);
+                diag.resize(12 * (size_t)n);
+                st = guard([&] {
+                    e->eng->get_intruder_history(0, oi, hist.data());
+                    e->eng->get_intruder_diag(0, diag.data());
+                });
+                if (st != NBC_OK) return st;
+                ok = ok && nbc::write_fc(nbc::bin_name(dir + "/OutForce", "fc", ii), oi, hist.data());
+                ok = ok && nbc::write_yi(nbc::bin_name(dir + "/OutForce", "yi", ii), n, cid.data(), diag.data());
+            } else {
+                ok = nbc::write_ch(nbc::bin_name(dir + "/OutClump", "ch", ii), k, cp.data(), cv.data(), cq.data(),
+                                   cw.data(), prop.data(), nullptr, nullptr, nullptr, nullptr);
+            }
+            if (!ok) return fail(NBC_ERR_IO, "cannot write OutClump/OutForce");
+            count = 0;
+        }
+        if (count2 == 2 * oi) {
+            nei.resize((size_t)n * bl);
+            fcn.resize((size_t)n * bl * 3);
+            cpt.resize((size_t)n * bl * 3);
+            st = guard([&] {
+                e->eng->get_rows(0, bl, nei.data(), nullptr, nullptr);
+                e->eng->get_chain(0, bl, fcn.data(), cpt.data());
+            });
+            if (st != NBC_OK) return st;
+            if (!nbc::write_cnt(dir + "/OutCnt", ii, n, bl, nei.data(), fcn.data(), cpt.data()))
+                return fail(NBC_ERR_IO, "cannot write OutCnt");
+            count2 = 0;
+        }
+    }
+    return nbc_sync(e);
+}
+
+}  // extern "C"

@@ -1,0 +1,910 @@
+// engine.cu -- host side of the B200 DEM engine and its C ABI (include/nbc.h).
+//
+// The Engine owns every device buffer of a batch of scenes, launches the
+// kernels of kernels.cuh, captures one step as a CUDA graph whose rebuild
+// branch is a conditional node, and converts device data to the reference's
+// host layouts on request.  It replaces the host orchestration of
+// DEMClumpMain::RunSimulationClump (src/dem_simulation_clump.cu:3-259), which
+// synchronises with the device about 30 times per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nbc.h"
+#include "kernels.cuh"
+#include "engine.h"
+
+namespace nbc {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +   \
+                            __FILE__ + ":" + std::to_string(__LINE__));                      \
+    } while (0)
+
+__global__ void k_setcond(cudaGraphConditionalHandle h, const int* flag, const int* halt) {
+    cudaGraphSetConditional(h, (*flag && !*halt) ? 1u : 0u);
+}
+
+// after every contact pass: count it, and advance the spring-history
+// generation so the next pass reads what this one wrote
+__global__ void k_count_contact(int* gstep, int* hgen, const int* halt) {
+    if (!*halt) {
+        *gstep += 1;
+        *hgen += 1;
+    }
+}
+
+static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// device memory helper
+// ---------------------------------------------------------------------------
+struct DevMem {
+    std::vector<void*> ptrs;
+    double bytes = 0;
+    template <typename T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        size_t b = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) throw CudaError(std::string("cudaMalloc ") + std::to_string(b) + ": " + cudaGetErrorString(e));
+        CK(cudaMemset(p, 0, b));
+        ptrs.push_back(p);
+        bytes += (double)b;
+        return (T*)p;
+    }
+    void release(void* p, size_t b) {
+        for (auto& q : ptrs)
+            if (q == p) { cudaFree(p); q = nullptr; bytes -= (double)b; }
+    }
+    ~DevMem() {
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+    }
+};
+
+template <typename R>
+class EngineT final : public EngineBase {
+   public:
+    EngineT(const std::vector<const nbc_scene_desc*>& sc, const nbc_options& opt) : opt_(opt) { setup(sc); }
+    ~EngineT() override {
+        if (gexec_) cudaGraphExecDestroy(gexec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        if (stream_) cudaStreamDestroy(stream_);
+        if (hflag_) cudaFreeHost(hflag_);
+    }
+
+    void step(int n, bool exp) override {
+        auto t0 = std::chrono::steady_clock::now();
+        if (post_done_) {
+            // a sync applied the pending half-kick: the next pass must not repeat it
+            CK(cudaMemsetAsync(h_.post_pending, 0, sizeof(int), stream_));
+            post_done_ = false;
+        }
+        int left = n;
+        while (left > 0) {
+            bool last = left == 1;
+            if (exp && last) {
+                run_step_eager(true);
+                left -= 1;
+                continue;
+            }
+            if (!opt_.use_graph || steps_done_ < 1) {
+                run_step_eager(false);
+                left -= 1;
+                continue;
+            }
+            if (!gexec_) capture();
+            int chunk = exp ? left - 1 : left;
+            int before = read_gstep();
+            for (int i = 0; i < chunk; i++) launch_graph();
+            CK(cudaStreamSynchronize(stream_));
+            int done = read_gstep() - before;
+            steps_done_ += done;
+            left -= done;
+            if (done < chunk) recover_halt();
+        }
+        CK(cudaStreamSynchronize(stream_));
+        check_errors();
+        last_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void sync() override {
+        // apply the pending second half-kick so the state is that of the last step
+        int pending = 0;
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(&pending, h_.post_pending, sizeof(int), cudaMemcpyDeviceToHost));
+        if (pending && !post_done_) {
+            launch_clump(0);
+            post_done_ = true;
+        }
+        CK(cudaStreamSynchronize(stream_));
+        refresh_dev();
+    }
+
+    // ---- getters ----------------------------------------------------------
+    int num_scenes() const override { return S_; }
+    void stats(int s, int* steps, int* rebuilds, int* npairs, int* err) override {
+        SceneDyn y = read_dyn(s);
+        if (steps) *steps = y.step + start_step_[s];
+        if (rebuilds) *rebuilds = y.nrebuild;
+        if (npairs) *npairs = y.npairs;
+        if (err) *err = y.err;
+    }
+    void get_subspheres(int s, int* fix, int* cid, double* pos, double* rad) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        int n = P.nsub, o = P.sub_off;
+        if (fix) {
+            CK(cudaMemcpy(fix, h_.part_fix + o, n * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        if (cid) {
+            CK(cudaMemcpy(cid, h_.clump_id + o, n * sizeof(int), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) cid[i] -= P.clump_off;
+        }
+        if (pos || rad) {
+            std::vector<double4> tmp(n);
+            CK(cudaMemcpy(tmp.data(), h_.posr + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) {
+                if (pos) { pos[3 * i] = tmp[i].x; pos[3 * i + 1] = tmp[i].y; pos[3 * i + 2] = tmp[i].z; }
+                if (rad) rad[i] = tmp[i].w;
+            }
+        }
+    }
+    void get_body(int s, double* local, double* mass) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        std::vector<double4> tmp(P.nsub);
+        CK(cudaMemcpy(tmp.data(), h_.lom + P.sub_off, P.nsub * sizeof(double4), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < P.nsub; i++) {
+            if (local) { local[3 * i] = tmp[i].x; local[3 * i + 1] = tmp[i].y; local[3 * i + 2] = tmp[i].z; }
+            if (mass) mass[i] = tmp[i].w;
+        }
+    }
+    void get_clump_prop(int s, double* prop) override {
+        const ScenePar& P = hpar_[s];
+        std::vector<double4> tmp(P.nclump);
+        CK(cudaMemcpy(tmp.data(), h_.cprop + P.clump_off, P.nclump * sizeof(double4), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < P.nclump; i++) {
+            prop[4 * i] = tmp[i].x; prop[4 * i + 1] = tmp[i].y; prop[4 * i + 2] = tmp[i].z; prop[4 * i + 3] = tmp[i].w;
+        }
+    }
+    void get_clumps(int s, double* pos, double* vel, double* quat, double* w, double* f, double* t) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        int n = P.nclump, o = P.clump_off;
+        std::vector<double4> tmp(n);
+        auto pull3 = [&](double4* src, double* dst) {
+            if (!dst) return;
+            CK(cudaMemcpy(tmp.data(), src + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) { dst[3 * i] = tmp[i].x; dst[3 * i + 1] = tmp[i].y; dst[3 * i + 2] = tmp[i].z; }
+        };
+        pull3(h_.cpos, pos);
+        pull3(h_.cvel, vel);
+        pull3(h_.cw, w);
+        pull3(h_.cF, f);
+        pull3(h_.cT, t);
+        if (quat) {
+            CK(cudaMemcpy(tmp.data(), h_.cq + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) {
+                quat[4 * i] = tmp[i].x; quat[4 * i + 1] = tmp[i].y; quat[4 * i + 2] = tmp[i].z; quat[4 * i + 3] = tmp[i].w;
+            }
+        }
+    }
+    void get_sub_forces(int s, double* f, double* t) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        pull_r4(h_.fsum, P.sub_off, P.nsub, f);
+        pull_r4((char*)h_.fsum + (size_t)N_ * sizeof(R4<R>), P.sub_off, P.nsub, t);
+    }
+    void get_force_parts(int s, double* parts) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        for (int c = 0; c < 6; c++)
+            pull_r4((char*)h_.xparts + (size_t)c * N_ * sizeof(R4<R>), P.sub_off, P.nsub, parts + (size_t)c * P.nsub * 3);
+    }
+    void get_intruder_diag(int s, double* diag) override {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        for (int c = 0; c < 4; c++)
+            pull_r4((char*)h_.xintr + (size_t)c * N_ * sizeof(R4<R>), P.sub_off, P.nsub, diag + (size_t)c * P.nsub * 3);
+    }
+    void get_pairs(int s, int* np, int* lpa, int* lpb) override {
+        refresh_dev();
+        SceneDyn y = read_dyn(s);
+        const ScenePar& P = hpar_[s];
+        int cap_in = *np;
+        *np = y.npairs;
+        if (!lpa && !lpb) return;
+        if (cap_in < y.npairs) throw ArgError("pair buffer too small");
+        int lc = read_int(h_.lcur);
+        const PairList& Lc = h_.L[lc & 1];
+        std::vector<int> own(y.npairs), nbr(y.npairs);
+        CK(cudaMemcpy(own.data(), Lc.own + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(nbr.data(), Lc.nbr + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < y.npairs; p++) {
+            if (lpa) lpa[p] = own[p] - P.sub_off;
+            if (lpb) lpb[p] = (nbr[p] & IDX_MASK) - P.sub_off;
+        }
+    }
+    // the reference's pitched rows (Anei, src/dem_grid.cu:466-552)
+    void get_rows(int s, int bl, int* anei, int* ng, int* ni) override {
+        RowData rd = pull_rows(s);
+        const ScenePar& P = hpar_[s];
+        const int n = P.nsub;
+        if (anei) std::fill(anei, anei + (size_t)n * bl, -1);
+        for (int i = 0; i < n; i++) {
+            int nf = rd.row[i + 1] - rd.row[i], nb = rd.brow[i + 1] - rd.brow[i];
+            if (ng) ng[i] = nf;
+            if (ni) ni[i] = nb;
+            if (!anei) continue;
+            if (nf > bl / 2 || nb > bl / 2) throw ArgError("row longer than bl/2");
+            for (int g = 0; g < nf; g++) anei[(size_t)i * bl + g] = (rd.nbr[rd.row[i] - rd.row[0] + g] & IDX_MASK) - P.sub_off;
+            for (int c = 0; c < nb; c++)
+                anei[(size_t)i * bl + bl - 1 - c] = (rd.bnbr[rd.brow[i] - rd.brow[0] + c] & IDX_MASK) - P.sub_off;
+        }
+    }
+    // CalFcnChain_cuk (src/dem_force_particle.cu:238-268) on the export data
+    void get_chain(int s, int bl, double* fcn, double* cpt) override {
+        RowData rd = pull_rows(s);
+        const ScenePar& P = hpar_[s];
+        const int n = P.nsub;
+        SceneDyn y = read_dyn(s);
+        std::vector<R4<R>> xf(y.npairs);
+        std::vector<double4> xc(y.npairs);
+        CK(cudaMemcpy(xf.data(), (R4<R>*)h_.xfcn + y.pair_off, y.npairs * sizeof(R4<R>), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(xc.data(), (double4*)h_.xcpt + y.pair_off, y.npairs * sizeof(double4), cudaMemcpyDeviceToHost));
+        std::fill(fcn, fcn + (size_t)n * bl * 3, 0.0);
+        std::fill(cpt, cpt + (size_t)n * bl * 3, 0.0);
+        const int p0 = rd.row[0];
+        for (int i = 0; i < n; i++) {
+            for (int g = 0; g < rd.row[i + 1] - rd.row[i]; g++) {
+                int p = rd.row[i] - p0 + g;
+                double* F = fcn + ((size_t)i * bl + g) * 3;
+                double* C = cpt + ((size_t)i * bl + g) * 3;
+                if (rd.nbr[p] < 0) continue;
+                F[0] = xf[p].x; F[1] = xf[p].y; F[2] = xf[p].z;
+                C[0] = xc[p].x; C[1] = xc[p].y; C[2] = xc[p].z;
+            }
+            for (int c = 0; c < rd.brow[i + 1] - rd.brow[i]; c++) {
+                int k = rd.brow[i] - rd.brow[0] + c;
+                if (rd.bnbr[k] < 0) continue;
+                int p = rd.bpair[k] - y.pair_off;
+                double* F = fcn + ((size_t)i * bl + bl - 1 - c) * 3;
+                double* C = cpt + ((size_t)i * bl + bl - 1 - c) * 3;
+                F[0] = -(double)xf[p].x; F[1] = -(double)xf[p].y; F[2] = -(double)xf[p].z;
+                C[0] = xc[p].x; C[1] = xc[p].y; C[2] = xc[p].z;
+            }
+        }
+    }
+    void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) override {
+        SceneDyn y = read_dyn(s);
+        for (int c = 0; c < 3; c++) {
+            if (pos) pos[c] = y.intr_p[c];
+            if (vel) vel[c] = y.intr_v[c];
+            if (reac) reac[c] = y.reaction[c];
+            if (tq) tq[c] = y.reaction_t[c];
+        }
+        if (state) *state = y.intr_state;
+    }
+    void get_intruder_history(int s, int count, double* out) override {
+        SceneDyn y = read_dyn(s);
+        if (count > ring_len_) throw ArgError("history longer than the ring");
+        std::vector<double> ring((size_t)ring_len_ * 6);
+        CK(cudaMemcpy(ring.data(), h_.ring + (size_t)s * ring_len_ * 6, ring.size() * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+        for (int c = 0; c < count; c++) {
+            int st = y.step - count + c;
+            if (st < 0) { for (int q = 0; q < 6; q++) out[c * 6 + q] = 0; continue; }
+            int slot = st % ring_len_;
+            for (int q = 0; q < 6; q++) out[c * 6 + q] = ring[(size_t)slot * 6 + q];
+        }
+    }
+    void timing_enable(bool on) override {
+        CK(cudaStreamSynchronize(stream_));
+        timing_ = on;
+        t_contact_ms_ = 0;
+        t_contact_n_ = 0;
+        launches_ = 0;
+        rebuilds_at_enable_ = total_rebuilds();
+        ev_used_ = 0;
+    }
+    void timing_read(double* ms, int* nc, long long* nk, int* nr) override {
+        CK(cudaStreamSynchronize(stream_));
+        harvest_events();
+        if (ms) *ms = t_contact_ms_;
+        if (nc) *nc = t_contact_n_;
+        if (nk) *nk = launches_ + (long long)(total_rebuilds() - rebuilds_at_enable_) * rebuild_launches();
+        if (nr) *nr = total_rebuilds() - rebuilds_at_enable_;
+    }
+    void info(double* bytes, double* ms) override {
+        if (bytes) *bytes = mem_.bytes;
+        if (ms) *ms = last_ms_;
+    }
+
+   private:
+    nbc_options opt_;
+    DevMem mem_;
+    cudaStream_t stream_ = nullptr;
+    Dev h_{};            // host copy of the device table
+    Dev* d_ = nullptr;   // device table
+    int S_ = 0, N_ = 0, K_ = 0, lanes_ = 16, passes_ = 0, rs_blocks_ = 0;
+    int ring_len_ = 1;
+    std::vector<ScenePar> hpar_;
+    std::vector<int> start_step_;
+    int* hflag_ = nullptr;  // pinned
+    int steps_done_ = 0;
+    bool post_done_ = false;
+    double last_ms_ = 0;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t gexec_ = nullptr;
+    // kernel timing: event pairs around the contact kernel
+    bool timing_ = false;
+    double t_contact_ms_ = 0;
+    int t_contact_n_ = 0;
+    long long launches_ = 0;
+    int rebuilds_at_enable_ = 0;
+    std::vector<cudaEvent_t> ev_;   // pairs
+    int ev_used_ = 0;               // pairs recorded and not yet harvested
+    cudaEvent_t gev_[2] = {nullptr, nullptr};
+    cudaGraphNode_t gev_node_[2] = {nullptr, nullptr};
+
+    int total_rebuilds() {
+        std::vector<SceneDyn> y(S_);
+        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        int n = 0;
+        for (auto& v : y) n = std::max(n, v.nrebuild);
+        return n;
+    }
+    // kernels one rebuild launches (launch_rebuild)
+    int rebuild_launches() const { return 1 + passes_ * 5 + 2 + 1 + 1 + 1 + 6 + 1 + 4; }
+    std::pair<cudaEvent_t, cudaEvent_t> next_pair() {
+        if ((size_t)(2 * ev_used_ + 2) > ev_.size()) {
+            for (int k = 0; k < 64; k++) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                ev_.push_back(e);
+            }
+        }
+        auto p = std::make_pair(ev_[2 * ev_used_], ev_[2 * ev_used_ + 1]);
+        ev_used_++;
+        return p;
+    }
+    void harvest_events() {
+        for (int k = 0; k < ev_used_; k++) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev_[2 * k], ev_[2 * k + 1]));
+            t_contact_ms_ += ms;
+            t_contact_n_++;
+        }
+        ev_used_ = 0;
+    }
+
+    struct RowData { std::vector<int> row, brow, nbr, bnbr, bpair; };
+
+    // ---- setup --------------------------------------------------------------
+    void setup(const std::vector<const nbc_scene_desc*>& sc) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device");
+        CK(cudaSetDevice(opt_.device));
+        CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        CK(cudaMallocHost(&hflag_, 4 * sizeof(int)));
+        lanes_ = opt_.lanes == 8 || opt_.lanes == 16 || opt_.lanes == 32 ? opt_.lanes : 16;
+        const int spb = CT_THREADS / lanes_;
+        S_ = (int)sc.size();
+        hpar_.resize(S_);
+        start_step_.resize(S_);
+        std::vector<SceneDyn> hdyn(S_);
+        int cells = 0, cblk = 0;
+        for (int s = 0; s < S_; s++) {
+            const nbc_scene_desc& D = *sc[s];
+            if (D.n_sub <= 0 || D.n_clump <= 0 || !D.pos || !D.radius || !D.clump_id)
+                throw ArgError("scene " + std::to_string(s) + ": empty or missing arrays");
+            ScenePar& P = hpar_[s];
+            memset(&P, 0, sizeof(P));
+            P.dt = D.dt; P.E = D.ymod; P.nu = D.prat; P.mu = D.frcoe; P.gravity = D.gravity;
+            P.beta = D.beta; P.cohesion = D.cohesion; P.thresh = D.thresh;
+            // LoadParameters (src/dem_subsphere_io.cu:143-145)
+            const double lnCOR = std::log(D.normres), PI_REF = 3.14159265359;
+            P.damping = 2.0 * std::sqrt(5.0 / 6.0) * lnCOR / std::sqrt(lnCOR * lnCOR + PI_REF * PI_REF);
+            P.kn_fac = 2.0 * D.ymod / (3.0 * (1.0 - D.prat * D.prat));
+            P.ks_fac = 2.0 * D.ymod / (1.0 + D.prat) / (2.0 - D.prat);
+            P.bl = D.branch_len > 0 ? D.branch_len : 256;
+            // SetMeshSize (src/dem_subsphere_io.cu:195-230)
+            double rmax = 0;
+            for (int i = 0; i < D.n_sub; i++) rmax = std::max(rmax, D.radius[i]);
+            const double mesh = 3.0 * rmax;
+            for (int a = 0; a < 3; a++) {
+                P.cell[a] = mesh;
+                P.icell[a] = 1.0 / mesh;
+                P.origin[a] = D.world_origin[a] - mesh;
+                double ws = D.world_size[a] + 2 * mesh;
+                P.gdim[a] = (int)(unsigned)std::ceil(ws / mesh);
+                P.box_lo[a] = D.box_lo[a];
+                P.box_hi[a] = D.box_hi[a];
+            }
+            P.levels = D.levels > 1 ? D.levels : 1;
+            if (P.levels > MAX_LEVELS) throw ArgError("too many grid levels");
+            if (P.levels > 1) throw ArgError("scene " + std::to_string(s) + ": hierarchical grid not built yet");
+            if (P.levels == 1) {
+                P.cellnum = P.gdim[0] * P.gdim[1] * P.gdim[2];
+            } else {
+                int off = 0;
+                for (int l = 0; l < P.levels; l++) {
+                    P.lcell[l] = D.level_cell[l];
+                    for (int a = 0; a < 3; a++)
+                        P.ldim[l][a] = (int)std::ceil((D.world_size[a] + 2 * mesh) / P.lcell[l]);
+                    P.loff[l] = off;
+                    off += P.ldim[l][0] * P.ldim[l][1] * P.ldim[l][2];
+                }
+                P.cellnum = off + 1;
+            }
+            P.cell_off = cells;
+            cells += P.cellnum;
+            P.sub_off = N_;
+            P.nsub = D.n_sub;
+            P.clump_off = K_;
+            P.nclump = D.n_clump;
+            P.cblk_off = cblk;
+            P.cblk_n = cdiv(D.n_sub, spb);
+            cblk += P.cblk_n;
+            N_ += D.n_sub;
+            K_ += D.n_clump;
+            // walls
+            P.wall = D.is_wall_force ? D.wall : WALL_NONE;
+            if (P.wall == WALL_CUBE) {
+                for (int a = 0; a < 3; a++) {
+                    P.w_half[a] = D.cube_half[a]; P.w_c[a] = D.cube_centre[a];
+                    P.w_v[a] = D.cube_vel[a]; P.w_w[a] = D.cube_angvel[a];
+                }
+            } else if (P.wall == WALL_CYL) {
+                P.cyl_R = D.cyl_radius; P.cyl_H = D.cyl_half_height;
+                for (int a = 0; a < 3; a++) {
+                    P.cyl_axis[a] = D.cyl_axis[a]; P.w_c[a] = D.cyl_centre[a];
+                    P.w_v[a] = D.cyl_vel[a]; P.w_w[a] = D.cyl_angvel[a];
+                }
+            }
+            SceneDyn& Y = hdyn[s];
+            memset(&Y, 0, sizeof(Y));
+            Y.rebuild = 1;  // the first step always builds the list (src/dem_simulation_clump.cu:124)
+            P.has_intr = D.intruder == NBC_INTR_SPHERE || D.intruder == NBC_INTR_CYLINDER;
+            if (P.has_intr) {
+                P.intr_shape = D.intruder;
+                P.intr_motion = D.intr_motion == NBC_MOTION_CONSTANT_VELOCITY ? 0 : 1;
+                P.intr_wait = D.intr_motion == NBC_MOTION_GRAVITY_AFTER_CONTACT;
+                P.intr_R = D.intr_radius;
+                P.intr_H = D.intruder == NBC_INTR_SPHERE ? D.intr_radius : D.intr_half_height;
+                for (int a = 0; a < 3; a++) {
+                    P.intr_axis[a] = D.intr_axis[a];
+                    P.intr_w[a] = D.intr_angvel[a];
+                    Y.intr_p[a] = D.intr_pos[a];
+                    Y.intr_v[a] = D.intr_vel[a];
+                }
+                P.intr_mass = D.intr_prop[3];
+            }
+            start_step_[s] = D.start_step;
+            ring_len_ = std::max(ring_len_, std::max(1, D.output_interval));
+        }
+        ring_len_ = std::max(ring_len_, 1024);
+        h_.S = S_; h_.N = N_; h_.K = K_;
+        h_.cells = cells;
+        h_.cblocks = cblk;
+        int bits = 1;
+        while ((1LL << bits) < (long long)cells) bits++;
+        h_.sort_bits = bits;
+        passes_ = cdiv(bits, 8);
+        rs_blocks_ = cdiv(N_, RS_TILE);
+
+        // host arrays in the input order
+        std::vector<double4> posr(N_), lom(N_);
+        std::vector<int> cid(N_), fix(N_), lev(N_, 0), sid(N_), csid(K_), mstart(K_ + 1, 0), midx(N_);
+        std::vector<double4> cpos(K_), cvel(K_), cw(K_), cq(K_), cprop(K_);
+        std::vector<int> sblk(cblk);
+        for (int s = 0; s < S_; s++) {
+            const nbc_scene_desc& D = *sc[s];
+            const ScenePar& P = hpar_[s];
+            for (int i = 0; i < D.n_sub; i++) {
+                int g = P.sub_off + i;
+                if (D.clump_id[i] < 0 || D.clump_id[i] >= D.n_clump)
+                    throw ArgError("scene " + std::to_string(s) + ": clump id out of range at row " + std::to_string(i));
+                posr[g] = make_double4(D.pos[3 * i], D.pos[3 * i + 1], D.pos[3 * i + 2], D.radius[i]);
+                lom[g] = make_double4(D.local[3 * i], D.local[3 * i + 1], D.local[3 * i + 2], D.mass[i]);
+                cid[g] = P.clump_off + D.clump_id[i];
+                fix[g] = i;
+                sid[g] = s;
+                if (P.levels > 1) lev[g] = D.level[i];
+                mstart[cid[g] + 1]++;
+            }
+            for (int k = 0; k < D.n_clump; k++) {
+                int g = P.clump_off + k;
+                csid[g] = s;
+                cpos[g] = make_double4(D.clump_pos[3 * k], D.clump_pos[3 * k + 1], D.clump_pos[3 * k + 2], 0);
+                cvel[g] = make_double4(D.clump_vel[3 * k], D.clump_vel[3 * k + 1], D.clump_vel[3 * k + 2], 0);
+                cw[g] = make_double4(D.clump_angvel[3 * k], D.clump_angvel[3 * k + 1], D.clump_angvel[3 * k + 2], 0);
+                cq[g] = make_double4(D.clump_quat[4 * k], D.clump_quat[4 * k + 1], D.clump_quat[4 * k + 2], D.clump_quat[4 * k + 3]);
+                cprop[g] = make_double4(D.clump_prop[4 * k], D.clump_prop[4 * k + 1], D.clump_prop[4 * k + 2], D.clump_prop[4 * k + 3]);
+            }
+            for (int b = 0; b < P.cblk_n; b++) sblk[P.cblk_off + b] = s;
+        }
+        for (int k = 0; k < K_; k++) mstart[k + 1] += mstart[k];
+        {
+            std::vector<int> cur(mstart.begin(), mstart.end() - 1);
+            for (int i = 0; i < N_; i++) midx[cur[cid[i]]++] = i;
+        }
+
+        // device allocation
+        const size_t N = N_;
+        h_.par = mem_.alloc<ScenePar>(S_);
+        h_.dyn = mem_.alloc<SceneDyn>(S_);
+        h_.sid = mem_.alloc<int>(N);
+        h_.csid = mem_.alloc<int>(K_);
+        h_.posr = mem_.alloc<double4>(N); h_.posr2 = mem_.alloc<double4>(N);
+        h_.lom = mem_.alloc<double4>(N); h_.lom2 = mem_.alloc<double4>(N);
+        h_.cum = mem_.alloc<double4>(N); h_.cum2 = mem_.alloc<double4>(N);
+        h_.clump_id = mem_.alloc<int>(N); h_.clump_id2 = mem_.alloc<int>(N);
+        h_.part_fix = mem_.alloc<int>(N); h_.part_fix2 = mem_.alloc<int>(N);
+        h_.level = mem_.alloc<int>(N); h_.level2 = mem_.alloc<int>(N);
+        h_.key = mem_.alloc<int>(N); h_.key2 = mem_.alloc<int>(N);
+        h_.kin = mem_.alloc<R4<R>>(3 * N); h_.kin2 = mem_.alloc<R4<R>>(3 * N);
+        h_.bhist = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N); h_.bhist2 = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N);
+        h_.bbits = mem_.alloc<uint16_t>(N); h_.bbits2 = mem_.alloc<uint16_t>(N);
+        h_.fsum = mem_.alloc<R4<R>>(2 * N);
+        h_.cpos = mem_.alloc<double4>(K_); h_.cvel = mem_.alloc<double4>(K_); h_.cw = mem_.alloc<double4>(K_);
+        h_.cq = mem_.alloc<double4>(K_); h_.cprop = mem_.alloc<double4>(K_);
+        h_.cF = mem_.alloc<double4>(K_); h_.cT = mem_.alloc<double4>(K_);
+        h_.mem_start = mem_.alloc<int>(K_ + 1);
+        h_.mem_idx = mem_.alloc<int>(N);
+        int* flags = mem_.alloc<int>(16);
+        h_.post_pending = flags + 0;
+        h_.any_rebuild = flags + 1;
+        h_.halt = flags + 2;
+        h_.lcur = flags + 3;
+        h_.hgen = flags + 4;
+        h_.gstep = flags + 5;
+        h_.kA = mem_.alloc<int>(N); h_.vA = mem_.alloc<int>(N); h_.kB = mem_.alloc<int>(N); h_.vB = mem_.alloc<int>(N);
+        h_.hist = mem_.alloc<int>((size_t)256 * rs_blocks_);
+        h_.perm = mem_.alloc<int>(N);
+        h_.inv = mem_.alloc<int>(N);
+        h_.cell_beg = mem_.alloc<int>(cells);
+        h_.cell_end = mem_.alloc<int>(cells);
+        h_.cnt_f = mem_.alloc<int>(N + 1);
+        h_.cnt_b = mem_.alloc<int>(N + 1);
+        h_.scan_tmp = mem_.alloc<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
+        for (int l = 0; l < 2; l++) {
+            h_.L[l].row = mem_.alloc<int>(N + 1);
+            h_.L[l].brow = mem_.alloc<int>(N + 1);
+        }
+        alloc_pairs(std::max<long long>(1024, 24LL * N_));
+        h_.xparts = mem_.alloc<R4<R>>(6 * N);
+        h_.xintr = mem_.alloc<R4<R>>(4 * N);
+        h_.ring_len = ring_len_;
+        h_.ring = mem_.alloc<double>((size_t)S_ * ring_len_ * 6);
+        h_.sblk_scene = mem_.alloc<int>(cblk);
+        d_ = mem_.alloc<Dev>(1);
+
+        CK(cudaMemcpy(h_.par, hpar_.data(), S_ * sizeof(ScenePar), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.dyn, hdyn.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.sid, sid.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.csid, csid.data(), K_ * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.posr, posr.data(), N * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.lom, lom.data(), N * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.clump_id, cid.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.part_fix, fix.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.level, lev.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.cpos, cpos.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.cvel, cvel.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.cw, cw.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.cq, cq.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h_.sblk_scene, sblk.data(), cblk * sizeof(int), cudaMemcpyHostToDevice));
+        // the first list is empty: rows of zeros
+        CK(cudaMemset(h_.L[0].row, 0, (N + 1) * sizeof(int)));
+        CK(cudaMemset(h_.L[0].brow, 0, (N + 1) * sizeof(int)));
+        int one = 1;
+        CK(cudaMemcpy(h_.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+        push_dev();
+    }
+
+    void alloc_pairs(long long cap) {
+        if (cap > 2000000000LL) throw CudaError("pair capacity above 2^31");
+        h_.cap = (int)cap;
+        for (int l = 0; l < 2; l++) {
+            h_.L[l].nbr = mem_.alloc<int>(cap);
+            h_.L[l].own = mem_.alloc<int>(cap);
+            h_.L[l].bnbr = mem_.alloc<int>(cap);
+            h_.L[l].bpair = mem_.alloc<int>(cap);
+            h_.H[l] = mem_.alloc<char>(hist_bytes(cap));
+            h_.touch[l] = mem_.alloc<uint8_t>(cap);
+        }
+        h_.xfcn = mem_.alloc<R4<R>>(cap);
+        h_.xcpt = mem_.alloc<double4>(cap);
+    }
+    static size_t hist_bytes(long long cap) { return (size_t)cap * (2 * sizeof(R4<R>) + sizeof(R)); }
+
+    // grow the pair buffers, keeping the current list and history generation
+    void grow_pairs(long long need) {
+        refresh_dev();
+        const double slack = opt_.pair_slack > 1.0 ? opt_.pair_slack : 1.6;
+        long long cap = std::max<long long>((long long)(need * slack), (long long)h_.cap + 1024);
+        Dev old = h_;
+        int lc = read_int(h_.lcur), hg = read_int(h_.hgen);
+        const PairList& Lo = old.L[lc & 1];
+        int np_f = 0, np_b = 0;
+        CK(cudaMemcpy(&np_f, Lo.row + N_, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&np_b, Lo.brow + N_, sizeof(int), cudaMemcpyDeviceToHost));
+        alloc_pairs(cap);
+        PairList& Ln = h_.L[lc & 1];
+        CK(cudaMemcpy(Ln.nbr, Lo.nbr, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(Ln.own, Lo.own, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(Ln.bnbr, Lo.bnbr, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(Ln.bpair, Lo.bpair, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice));
+        const int g = hg & 1;
+        char* ho = (char*)old.H[g];
+        char* hn = (char*)h_.H[g];
+        CK(cudaMemcpy(hn, ho, (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(hn + (size_t)h_.cap * sizeof(R4<R>), ho + (size_t)old.cap * sizeof(R4<R>),
+                      (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(hn + (size_t)h_.cap * 2 * sizeof(R4<R>), ho + (size_t)old.cap * 2 * sizeof(R4<R>),
+                      (size_t)np_f * sizeof(R), cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(h_.touch[g], old.touch[g], (size_t)np_f, cudaMemcpyDeviceToDevice));
+        for (int l = 0; l < 2; l++) {
+            mem_.release(old.L[l].nbr, (size_t)old.cap * 4);
+            mem_.release(old.L[l].own, (size_t)old.cap * 4);
+            mem_.release(old.L[l].bnbr, (size_t)old.cap * 4);
+            mem_.release(old.L[l].bpair, (size_t)old.cap * 4);
+            mem_.release(old.H[l], hist_bytes(old.cap));
+            mem_.release(old.touch[l], (size_t)old.cap);
+        }
+        mem_.release(old.xfcn, (size_t)old.cap * sizeof(R4<R>));
+        mem_.release(old.xcpt, (size_t)old.cap * sizeof(double4));
+        push_dev();
+    }
+
+    void push_dev() {
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(d_, &h_, sizeof(Dev), cudaMemcpyHostToDevice));
+    }
+    // the device swaps buffer pointers in k_commit: refresh the host copy
+    void refresh_dev() {
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaMemcpy(&h_, d_, sizeof(Dev), cudaMemcpyDeviceToHost));
+    }
+    int read_int(const int* p) {
+        CK(cudaStreamSynchronize(stream_));
+        int v = 0;
+        CK(cudaMemcpy(&v, p, sizeof(int), cudaMemcpyDeviceToHost));
+        return v;
+    }
+    int read_gstep() { return read_int(h_.gstep); }
+    SceneDyn read_dyn(int s) {
+        CK(cudaStreamSynchronize(stream_));
+        SceneDyn y;
+        CK(cudaMemcpy(&y, h_.dyn + s, sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        return y;
+    }
+    void pull_r4(const void* base, int off, int n, double* dst) {
+        if (!dst) return;
+        std::vector<R4<R>> tmp(n);
+        CK(cudaMemcpy(tmp.data(), (const R4<R>*)base + off, n * sizeof(R4<R>), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++) { dst[3 * i] = tmp[i].x; dst[3 * i + 1] = tmp[i].y; dst[3 * i + 2] = tmp[i].z; }
+    }
+    RowData pull_rows(int s) {
+        refresh_dev();
+        const ScenePar& P = hpar_[s];
+        int lc = read_int(h_.lcur);
+        const PairList& Lc = h_.L[lc & 1];
+        RowData rd;
+        rd.row.resize(P.nsub + 1);
+        rd.brow.resize(P.nsub + 1);
+        CK(cudaMemcpy(rd.row.data(), Lc.row + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(rd.brow.data(), Lc.brow + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        int nf = rd.row[P.nsub] - rd.row[0], nb = rd.brow[P.nsub] - rd.brow[0];
+        rd.nbr.resize(nf);
+        rd.bnbr.resize(nb);
+        rd.bpair.resize(nb);
+        CK(cudaMemcpy(rd.nbr.data(), Lc.nbr + rd.row[0], nf * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(rd.bnbr.data(), Lc.bnbr + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(rd.bpair.data(), Lc.bpair + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost));
+        return rd;
+    }
+
+    void check_errors() {
+        std::vector<SceneDyn> y(S_);
+        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < S_; s++)
+            if (y[s].err & ERR_NONFINITE) throw NonFinite("scene " + std::to_string(s) + ": non-finite force");
+    }
+
+    // ---- launches -------------------------------------------------------------
+    void launch_clump(int do_pre) {
+        int n = K_ + S_;
+        k_clump<R><<<cdiv(n, 128), 128, 0, stream_>>>(d_, do_pre);
+        CK(cudaGetLastError());
+        if (!capturing_ && timing_) launches_ += 1;
+    }
+    bool capturing_ = false;
+    void launch_contact(bool exp) {
+        if (exp) {
+            CK(cudaMemsetAsync(h_.xfcn, 0, (size_t)h_.cap * sizeof(R4<R>), stream_));
+            CK(cudaMemsetAsync(h_.xcpt, 0, (size_t)h_.cap * sizeof(double4), stream_));
+        }
+        dim3 g(h_.cblocks);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (capturing_) {
+            CK(cudaEventRecordWithFlags(gev_[0], stream_, cudaEventRecordExternal));
+            gev_node_[0] = last_captured_node();
+        } else if (timing_) {
+            auto pr = next_pair();
+            e0 = pr.first;
+            e1 = pr.second;
+            CK(cudaEventRecord(e0, stream_));
+        }
+#define NBC_CT(L)                                                                   \
+    if (exp) k_contact<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);             \
+    else k_contact<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
+        if (lanes_ == 8) { NBC_CT(8) }
+        else if (lanes_ == 32) { NBC_CT(32) }
+        else { NBC_CT(16) }
+#undef NBC_CT
+        CK(cudaGetLastError());
+        if (capturing_) {
+            CK(cudaEventRecordWithFlags(gev_[1], stream_, cudaEventRecordExternal));
+            gev_node_[1] = last_captured_node();
+        } else if (e1) {
+            CK(cudaEventRecord(e1, stream_));
+        }
+        k_count_contact<<<1, 1, 0, stream_>>>(h_.gstep, h_.hgen, h_.halt);
+        if (!capturing_ && timing_) launches_ += 2;
+    }
+    void scan(int* a, int n) {
+        int nb = cdiv(n, SC_TILE);
+        k_scan_tiles<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp);
+        k_scan_sums<<<1, SC_THREADS, 0, stream_>>>(h_.scan_tmp, nb);
+        k_scan_add<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp);
+    }
+    // the rebuild block of src/dem_simulation_clump.cu:124-176
+    void launch_rebuild(bool eager) {
+        const int B = 128;
+        k_hash<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        int *ki = h_.kA, *vi = h_.vA, *ko = h_.kB, *vo = h_.vB;
+        for (int p = 0; p < passes_; p++) {
+            k_rs_hist<<<rs_blocks_, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, rs_blocks_);
+            scan(h_.hist, 256 * rs_blocks_);
+            k_rs_scatter<<<rs_blocks_, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, rs_blocks_);
+            std::swap(ki, ko);
+            std::swap(vi, vo);
+        }
+        const int fb = std::min(cdiv(h_.cells, 256), 148 * 16);
+        k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_beg, h_.cells, -1);
+        k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_end, h_.cells, -1);
+        k_cellrange<<<cdiv(N_, B), B, 0, stream_>>>(d_, ki, vi);
+        k_reorder<R><<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        k_count<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        scan(h_.cnt_f, N_ + 1);
+        scan(h_.cnt_b, N_ + 1);
+        CK(cudaGetLastError());
+        if (eager) {
+            CK(cudaMemcpyAsync(hflag_, h_.cnt_f + N_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            CK(cudaMemcpyAsync(hflag_ + 1, h_.cnt_b + N_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            long long need = std::max(hflag_[0], hflag_[1]);
+            if (need > h_.cap) grow_pairs(need);
+        }
+        k_check_cap<<<1, 1, 0, stream_>>>(d_);
+        k_fill<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        k_carry<R><<<cdiv(std::max(h_.cap, 1), 256), 256, 0, stream_>>>(d_);
+        k_commit<<<cdiv(K_ + S_ + 1, B), B, 0, stream_>>>(d_);
+        CK(cudaGetLastError());
+    }
+
+    void run_step_eager(bool exp) {
+        launch_clump(1);
+        if (timing_) launches_ += 0;
+        CK(cudaMemcpyAsync(hflag_, h_.any_rebuild, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        if (hflag_[0]) launch_rebuild(true);
+        launch_contact(exp);
+        steps_done_ += 1;
+    }
+
+    // one step as a graph: k_clump, a conditional node holding the rebuild,
+    // k_contact
+    void capture() {
+        for (int k = 0; k < 2; k++) CK(cudaEventCreate(&gev_[k]));
+        capturing_ = true;
+        CK(cudaGraphCreate(&graph_, 0));
+        cudaGraphConditionalHandle hnd;
+        CK(cudaGraphConditionalHandleCreate(&hnd, graph_, 0, cudaGraphCondAssignDefault));
+        CK(cudaStreamBeginCaptureToGraph(stream_, graph_, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        launch_clump(1);
+        k_setcond<<<1, 1, 0, stream_>>>(hnd, h_.any_rebuild, h_.halt);
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, nullptr, &deps, &ndeps));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        CK(cudaGraphAddNode(&cnode, graph_, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamUpdateCaptureDependencies(stream_, &cnode, 1, cudaStreamSetCaptureDependencies));
+        launch_contact(false);
+        cudaGraph_t g2 = nullptr;
+        CK(cudaStreamEndCapture(stream_, &g2));
+        // the rebuild branch
+        CK(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        launch_rebuild(false);
+        cudaGraph_t b2 = nullptr;
+        CK(cudaStreamEndCapture(stream_, &b2));
+        capturing_ = false;
+        if (!gev_node_[0] || !gev_node_[1]) throw CudaError("event nodes missing from the step graph");
+        CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+    }
+    cudaGraphNode_t last_captured_node() {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, nullptr, &deps, &nd));
+        if (nd != 1) throw CudaError("unexpected capture dependencies");
+        return deps[0];
+    }
+    void launch_graph() {
+        if (timing_) {
+            auto pr = next_pair();
+            CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[0], pr.first));
+            CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[1], pr.second));
+            launches_ += 4;
+        }
+        CK(cudaGraphLaunch(gexec_, stream_));
+    }
+
+    // a graph launch stopped at a rebuild whose pairs did not fit: grow and
+    // finish that step's rebuild and contact pass on the host path
+    void recover_halt() {
+        refresh_dev();
+        long long need = std::max(read_int(h_.cnt_f + N_), read_int(h_.cnt_b + N_));
+        grow_pairs(need);
+        int zero = 0;
+        CK(cudaMemcpy(h_.halt, &zero, sizeof(int), cudaMemcpyHostToDevice));
+        std::vector<SceneDyn> y(S_);
+        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        for (auto& v : y) v.err &= ~ERR_LIST_OVERFLOW;
+        CK(cudaMemcpy(h_.dyn, y.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice));
+        launch_rebuild(true);
+        launch_contact(false);
+        CK(cudaStreamSynchronize(stream_));
+        steps_done_ += 1;
+    }
+};
+
+EngineBase* make_engine(const std::vector<const nbc_scene_desc*>& sc, const nbc_options& opt) {
+    if (opt.precision == NBC_PREC_F64) return new EngineT<double>(sc, opt);
+    return new EngineT<float>(sc, opt);
+}
+
+}  // namespace nbc

@@ -1,0 +1,43 @@
+// engine.h -- host interface of the B200 DEM engine (implementation in
+// engine.cu, C ABI in capi.cpp).
+#pragma once
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nbc.h"
+
+namespace nbc {
+
+struct NonFinite : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+// One batch of scenes resident on one GPU.
+class EngineBase {
+   public:
+    virtual ~EngineBase() {}
+    virtual void step(int n, bool export_last) = 0;
+    virtual void sync() = 0;
+    virtual int num_scenes() const = 0;
+    virtual void stats(int s, int* steps, int* rebuilds, int* npairs, int* err) = 0;
+    virtual void get_subspheres(int s, int* fix, int* cid, double* pos, double* rad) = 0;
+    virtual void get_body(int s, double* local, double* mass) = 0;
+    virtual void get_clump_prop(int s, double* prop) = 0;
+    virtual void get_clumps(int s, double* pos, double* vel, double* quat, double* w, double* f, double* t) = 0;
+    virtual void get_sub_forces(int s, double* f, double* t) = 0;
+    virtual void get_force_parts(int s, double* parts) = 0;
+    virtual void get_intruder_diag(int s, double* diag) = 0;
+    virtual void get_pairs(int s, int* np, int* lpa, int* lpb) = 0;
+    virtual void get_rows(int s, int bl, int* anei, int* ng, int* ni) = 0;
+    virtual void get_chain(int s, int bl, double* fcn, double* cpt) = 0;
+    virtual void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) = 0;
+    virtual void get_intruder_history(int s, int count, double* out) = 0;
+    virtual void info(double* bytes, double* ms) = 0;
+    virtual void timing_enable(bool on) = 0;
+    virtual void timing_read(double* contact_ms, int* contact_launches, long long* kernel_launches, int* rebuilds) = 0;
+};
+
+EngineBase* make_engine(const std::vector<const nbc_scene_desc*>& scenes, const nbc_options& opt);
+
+}  // namespace nbc

@@ -1,0 +1,1041 @@
+// kernels.cuh -- sm_100a kernels of the B200 DEM engine.
+//
+// Step structure (one CUDA graph per step, see engine.cu):
+//   k_clump      per clump: member force/torque sum and second half-kick of
+//                the previous step, first half-kick, drift, attitude and the
+//                pose of every member subsphere (+ rebuild test); one extra
+//                thread per scene advances the intruder.
+//   [rebuild]    only when some scene's subsphere moved more than Thresh
+//                since that scene's last rebuild: hash, radix sort, cell
+//                ranges, reorder, count/scan/fill of the half pair list in
+//                the reference's traversal order, back references, history
+//                carry, clump member lists.
+//   k_contact    one lane group per subsphere: every pair of its front and
+//                back lists, its wall faces and the intruder, summed in
+//                registers; the pair owner also writes the new spring history.
+#pragma once
+#include "nbc_dev.cuh"
+#include "nbc_math.cuh"
+
+namespace nbc {
+
+constexpr double FIX_F = 1099511627776.0;    // 2^40: fixed-point scale of intruder force sums
+constexpr double FIX_T = 17592186044416.0;   // 2^44: fixed-point scale of intruder torque sums
+constexpr int IDX_MASK = 0x7fffffff;
+constexpr int INTRA = (int)0x80000000u;
+
+// ===========================================================================
+// clump pass
+// ===========================================================================
+
+// Integrate_Before_clump_cuk / Attitude_clump_cuk / Integrate_After_clump_cuk
+// (src/dem_integrate_clumpsphere.cu:3-141), UpdatePos_cuk (src/dem_clump.cu:
+// 113-138), ComputeTorqueFromWorldPos_Kernel + reduce_by_key
+// (src/dem_clumpsphere.cu:86-151), IntegratePene_Before_cuk and
+// Integrate_After_cuk (src/dem_integrate_penetrator.cu:3-113).
+template <typename R>
+__global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int do_pre) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int post = *d.post_pending;
+    if (t < d.K) {
+        const int k = t;
+        const ScenePar& P = d.par[d.csid[k]];
+        double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cprop[k];
+        const double Dt = P.dt;
+        const int mb = d.mem_start[k], me = d.mem_start[k + 1];
+        const R4<R>* fs = (const R4<R>*)d.fsum;
+        const R4<R>* ts = fs + d.N;
+        V3<double> F, T;
+        if (post) {
+            F = v3(0.0, 0.0, 0.0);
+            T = F;
+            for (int m = mb; m < me; m++) {
+                int i = d.mem_idx[m];
+                double4 ps = d.posr[i];
+                V3<double> r = v3(ps.x - cp.x, ps.y - cp.y, ps.z - cp.z);
+                R4<R> f4 = fs[i], t4 = ts[i];
+                V3<double> f = v3((double)f4.x, (double)f4.y, (double)f4.z);
+                V3<double> tc = v3((double)t4.x + (r.y * f.z - r.z * f.y),
+                                   (double)t4.y + (r.z * f.x - r.x * f.z),
+                                   (double)t4.z + (r.x * f.y - r.y * f.x));
+                if (m == mb) { F = f; T = tc; }
+                else { F = F + f; T = T + tc; }
+            }
+            if (mb < me) {
+                d.cF[k] = make_double4(F.x, F.y, F.z, 0.0);
+                d.cT[k] = make_double4(T.x, T.y, T.z, 0.0);
+            } else {
+                F = xyzd(d.cF[k]);
+                T = xyzd(d.cT[k]);
+            }
+            V3<double> a = (1.0 / pr.w) * F;
+            a.z = a.z + P.gravity;
+            V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
+            cv.x += (0.5 * Dt) * a.x; cv.y += (0.5 * Dt) * a.y; cv.z += (0.5 * Dt) * a.z;
+            cw.x += (0.5 * Dt) * al.x; cw.y += (0.5 * Dt) * al.y; cw.z += (0.5 * Dt) * al.z;
+        } else {
+            F = xyzd(d.cF[k]);
+            T = xyzd(d.cT[k]);
+        }
+        if (do_pre) {
+            V3<double> a = (1.0 / pr.w) * F;
+            a.z = a.z + P.gravity;
+            V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
+            V3<double> v = xyzd(cv), w = xyzd(cw);
+            V3<double> dist = Dt * v + (0.5 * Dt * Dt) * a;
+            cp.x += dist.x; cp.y += dist.y; cp.z += dist.z;
+            v = v + (0.5 * Dt) * a;
+            w = w + (0.5 * Dt) * al;
+            // attitude with the half-kicked angular velocity
+            V3<double> Wb = rot_w2b(cq, w), Wdb = rot_w2b(cq, al);
+            double4 q = cq, qd, qdd;
+            qd.x = 0.50 * (Wb.x * q.w - Wb.y * q.z + Wb.z * q.y);
+            qd.y = 0.50 * (Wb.x * q.z + Wb.y * q.w - Wb.z * q.x);
+            qd.z = 0.50 * (-Wb.x * q.y + Wb.y * q.x + Wb.z * q.w);
+            qd.w = 0.50 * (-Wb.x * q.x - Wb.y * q.y - Wb.z * q.z);
+            qdd.x = (Wdb.x * q.w - Wdb.y * q.z + Wdb.z * q.y) * 0.50 + (Wb.x * qd.w - Wb.y * qd.z + Wb.z * qd.y) * 0.50;
+            qdd.y = (Wdb.x * q.z + Wdb.y * q.w - Wdb.z * q.x) * 0.50 + (Wb.x * qd.z + Wb.y * qd.w - Wb.z * qd.x) * 0.50;
+            qdd.z = (-Wdb.x * q.y + Wdb.y * q.x + Wdb.z * q.w) * 0.50 + (-Wb.x * qd.y + Wb.y * qd.x + Wb.z * qd.w) * 0.50;
+            qdd.w = (-Wdb.x * q.x - Wdb.y * q.y - Wdb.z * q.z) * 0.50 + (-Wb.x * qd.x - Wb.y * qd.y - Wb.z * qd.z) * 0.50;
+            const double h2 = 0.5 * Dt * Dt;
+            q.x = (q.x + Dt * qd.x) + h2 * qdd.x;
+            q.y = (q.y + Dt * qd.y) + h2 * qdd.y;
+            q.z = (q.z + Dt * qd.z) + h2 * qdd.z;
+            q.w = (q.w + Dt * qd.w) + h2 * qdd.w;
+            const double inv = 1.0 / sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+            q.x *= inv; q.y *= inv; q.z *= inv; q.w *= inv;
+            // pose of the members
+            R4<R>* kv = (R4<R>*)d.kin;
+            R4<R>* kw = kv + d.N;
+            R4<R>* ka = kw + d.N;
+            bool moved = false;
+            for (int m = mb; m < me; m++) {
+                int i = d.mem_idx[m];
+                double4 lo = d.lom[i];
+                V3<double> arm = rot_b2w(q, v3(lo.x, lo.y, lo.z));
+                V3<double> p = v3(cp.x + arm.x, cp.y + arm.y, cp.z + arm.z);
+                double4 old = d.posr[i];
+                double4 c = d.cum[i];
+                V3<double> cn = v3((c.x + p.x) - old.x, (c.y + p.y) - old.y, (c.z + p.z) - old.z);
+                if (len_floor(cn) > P.thresh) moved = true;
+                d.cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
+                d.posr[i] = make_double4(p.x, p.y, p.z, old.w);
+                kv[i] = pack<R>(cvt<R>(v), (R)lo.w);
+                kw[i] = pack<R>(cvt<R>(w), R(0));
+                ka[i] = pack<R>(cvt<R>(arm), R(0));
+            }
+            if (moved) {
+                d.dyn[d.csid[k]].rebuild = 1;
+                *d.any_rebuild = 1;
+            }
+            d.cpos[k] = cp;
+            d.cvel[k] = make_double4(v.x, v.y, v.z, 0.0);
+            d.cw[k] = make_double4(w.x, w.y, w.z, 0.0);
+            d.cq[k] = q;
+        } else if (post) {
+            d.cvel[k] = cv;
+            d.cw[k] = cw;
+        }
+    } else if (t < d.K + d.S) {
+        const int s = t - d.K;
+        const ScenePar& P = d.par[s];
+        SceneDyn& y = d.dyn[s];
+        const double Dt = P.dt;
+        if (post) {
+            long long* fx = (long long*)&y.ifix[0];
+            V3<double> tf = v3(fx[0] / FIX_F, fx[1] / FIX_F, fx[2] / FIX_F);
+            V3<double> tt = v3(fx[3] / FIX_T, fx[4] / FIX_T, fx[5] / FIX_T);
+            for (int c = 0; c < 6; c++) fx[c] = 0;
+            y.totF[0] = tf.x; y.totF[1] = tf.y; y.totF[2] = tf.z;
+            y.totT[0] = tt.x; y.totT[1] = tt.y; y.totT[2] = tt.z;
+            if (P.has_intr) {
+                if (P.intr_wait && y.intr_state == 1) y.intr_state = 2;
+                V3<double> reac = v3(-tf.x, -tf.y, -tf.z);
+                if (P.intr_motion == 1 && (!P.intr_wait || y.intr_state != 0)) {
+                    V3<double> a = (1.0 / P.intr_mass) * reac;
+                    a.z = a.z + P.gravity;
+                    for (int c = 0; c < 3; c++) y.intr_v[c] += (0.5 * Dt) * (&a.x)[c];
+                }
+                y.reaction[0] = reac.x; y.reaction[1] = reac.y; y.reaction[2] = reac.z;
+                y.reaction_t[0] = tt.x; y.reaction_t[1] = tt.y; y.reaction_t[2] = tt.z;
+                double* ring = d.ring + ((size_t)s * d.ring_len + (y.step % d.ring_len)) * 6;
+                ring[0] = reac.x; ring[1] = reac.y; ring[2] = reac.z;
+                ring[3] = tt.x; ring[4] = tt.y; ring[5] = tt.z;
+            }
+            y.step += 1;
+        }
+        if (do_pre && P.has_intr) {
+            if (P.intr_motion == 1 && (!P.intr_wait || y.intr_state != 0)) {
+                V3<double> a = (-1.0 / P.intr_mass) * v3(y.totF[0], y.totF[1], y.totF[2]);
+                a.z = a.z + P.gravity;
+                for (int c = 0; c < 3; c++) {
+                    y.intr_p[c] = (y.intr_p[c] + Dt * y.intr_v[c]) + (0.5 * Dt * Dt) * (&a.x)[c];
+                    y.intr_v[c] = y.intr_v[c] + (0.5 * Dt) * (&a.x)[c];
+                }
+            } else {
+                for (int c = 0; c < 3; c++) y.intr_p[c] = y.intr_p[c] + Dt * y.intr_v[c];
+            }
+        }
+    }
+}
+
+// ===========================================================================
+// broad phase
+// ===========================================================================
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// GetParticleCellIndex_cuk (src/dem_grid.cu:155-202); hierarchical variant
+// GetParticleCellIndex_hGrid_cuk (src/dem_hgrid.cu:205-242) with the
+// out-of-box bucket kept inside the scene's cell range.
+__global__ void k_hash(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const int s = d.sid[i];
+    const ScenePar& P = d.par[s];
+    d.vA[i] = i;
+    if (!d.dyn[s].rebuild) { d.kA[i] = d.key[i]; return; }
+    double4 p = d.posr[i];
+    int local;
+    if (P.levels <= 1) {
+        if (p.z >= P.box_hi[2] || p.y >= P.box_hi[1] || p.x >= P.box_hi[0] ||
+            p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
+            local = P.cellnum - 1;
+        } else {
+            int cx = (int)floor((p.x - P.origin[0]) / P.cell[0]);
+            int cy = (int)floor((p.y - P.origin[1]) / P.cell[1]);
+            int cz = (int)floor((p.z - P.origin[2]) / P.cell[2]);
+            cx = clampi(cx, 0, P.gdim[0] - 1);
+            cy = clampi(cy, 0, P.gdim[1] - 1);
+            cz = clampi(cz, 0, P.gdim[2] - 1);
+            local = cz * P.gdim[1] * P.gdim[0] + cy * P.gdim[0] + cx;
+            local = clampi(local, 0, P.cellnum - 1);
+        }
+    } else {
+        if (p.z > P.box_hi[2] || p.y > P.box_hi[1] || p.x > P.box_hi[0] ||
+            p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
+            local = P.cellnum - 1;
+        } else {
+            int t = d.level[i];
+            double c = P.lcell[t];
+            int cx = clampi((int)floor((p.x - P.origin[0]) / c), 0, P.ldim[t][0] - 1);
+            int cy = clampi((int)floor((p.y - P.origin[1]) / c), 0, P.ldim[t][1] - 1);
+            int cz = clampi((int)floor((p.z - P.origin[2]) / c), 0, P.ldim[t][2] - 1);
+            local = P.loff[t] + (cz * P.ldim[t][1] * P.ldim[t][0] + cy * P.ldim[t][0] + cx);
+        }
+    }
+    d.kA[i] = P.cell_off + local;
+}
+
+// --- LSD radix sort, 8-bit digits, stable (the reference sorts with CUB's
+// stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
+constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ keys, int n, int shift,
+                                                        int* __restrict__ hist, int nblk) {
+    __shared__ int h[256];
+    const int tid = threadIdx.x, blk = blockIdx.x;
+    h[tid] = 0;
+    __syncthreads();
+    for (int it = 0; it < RS_ITEMS; it++) {
+        int idx = blk * RS_TILE + it * RS_THREADS + tid;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255], 1);
+    }
+    __syncthreads();
+    hist[tid * nblk + blk] = h[tid];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
+                                                           int* __restrict__ kout, int* __restrict__ vout, int n,
+                                                           int shift, const int* __restrict__ hist, int nblk) {
+    __shared__ int base[256];
+    __shared__ int wcnt[RS_THREADS / 32][257];
+    const int tid = threadIdx.x, blk = blockIdx.x, lane = tid & 31, warp = tid >> 5;
+    base[tid] = hist[tid * nblk + blk];
+    for (int it = 0; it < RS_ITEMS; it++) {
+        for (int w = 0; w < RS_THREADS / 32; w++) wcnt[w][tid] = 0;
+        __syncthreads();
+        const int idx = blk * RS_TILE + it * RS_THREADS + tid;
+        const bool valid = idx < n;
+        const int k = valid ? kin[idx] : 0;
+        const int dig = valid ? ((k >> shift) & 255) : 256;
+        const unsigned peers = __match_any_sync(0xffffffffu, dig);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            int off = base[dig] + rank;
+            for (int w = 0; w < warp; w++) off += wcnt[w][dig];
+            kout[off] = k;
+            vout[off] = vin[idx];
+        }
+        __syncthreads();
+        int add = 0;
+        for (int w = 0; w < RS_THREADS / 32; w++) add += wcnt[w][tid];
+        base[tid] += add;
+        __syncthreads();
+    }
+}
+
+// --- exclusive scan of ints (three passes) --------------------------------
+constexpr int SC_THREADS = 256, SC_ITEMS = 4, SC_TILE = SC_THREADS * SC_ITEMS;
+
+__device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
+    // sh: SC_THREADS/32 ints
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < SC_THREADS / 32 ? sh[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SC_THREADS / 32) sh[lane] = w;
+    }
+    __syncthreads();
+    const int warp_base = warp > 0 ? sh[warp - 1] : 0;
+    total = sh[SC_THREADS / 32 - 1];
+    __syncthreads();
+    return warp_base + x - v;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, int n, int* __restrict__ sums) {
+    __shared__ int sh[SC_THREADS / 32];
+    const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
+    int v[SC_ITEMS], s = 0;
+    for (int j = 0; j < SC_ITEMS; j++) { v[j] = base + j < n ? a[base + j] : 0; s += v[j]; }
+    int total;
+    int ex = block_excl_scan(s, sh, total);
+    for (int j = 0; j < SC_ITEMS; j++) {
+        if (base + j < n) a[base + j] = ex;
+        ex += v[j];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums, int nb) {
+    __shared__ int sh[SC_THREADS / 32];
+    int carry = 0;
+    for (int off = 0; off < nb; off += SC_THREADS) {
+        int i = off + threadIdx.x;
+        int v = i < nb ? sums[i] : 0;
+        int total;
+        int ex = block_excl_scan(v, sh, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
+    }
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums) {
+    const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
+    const int add = sums[blockIdx.x];
+    for (int j = 0; j < SC_ITEMS; j++)
+        if (base + j < n) a[base + j] += add;
+}
+
+// --- cell ranges, reorder ------------------------------------------------
+__global__ void k_fill_i(int* __restrict__ a, int n, int v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
+
+// FindBegEndInCell_cuk (src/dem_grid.cu:105-153) over the global cell table,
+// plus the permutation, its inverse and the sorted keys (into key2).
+__global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    int k = skey[i];
+    if (i == 0 || skey[i - 1] != k) d.cell_beg[k] = i;
+    if (i == d.N - 1 || skey[i + 1] != k) d.cell_end[k] = i + 1;
+    d.inv[perm[i]] = i;
+    d.perm[i] = perm[i];
+    d.key2[i] = k;
+}
+
+// SortArray_*_cuk (src/dem_grid.cu:336-437) for every persistent per-subsphere
+// array at once, into the alternate buffers.  The displacement accumulator
+// restarts at zero in rebuilt scenes (src/dem_simulation_clump.cu:172).
+template <typename R>
+__global__ void k_reorder(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const int o = d.perm[i];
+    const size_t N = (size_t)d.N;
+    d.posr2[i] = d.posr[o];
+    d.lom2[i] = d.lom[o];
+    d.cum2[i] = d.dyn[d.sid[i]].rebuild ? make_double4(0, 0, 0, 0) : d.cum[o];
+    d.clump_id2[i] = d.clump_id[o];
+    d.part_fix2[i] = d.part_fix[o];
+    d.level2[i] = d.level[o];
+    d.bbits2[i] = d.bbits[o];
+    const R4<R>* k1 = (const R4<R>*)d.kin;
+    R4<R>* k2 = (R4<R>*)d.kin2;
+    for (int c = 0; c < 3; c++) k2[c * N + i] = k1[c * N + o];
+    const R4<R>* b1 = (const R4<R>*)d.bhist;
+    R4<R>* b2 = (R4<R>*)d.bhist2;
+    const uint16_t bits = d.bbits[o];
+    for (int sl = 0; sl < NB_SLOTS; sl++) {
+        if (!(bits & (1u << sl))) continue;  // only live histories are ever read
+        for (int c = 0; c < 3; c++) b2[((size_t)sl * 3 + c) * N + i] = b1[((size_t)sl * 3 + c) * N + o];
+    }
+}
+
+// --- neighbour search ----------------------------------------------------
+// The 27-cell scan of CreateAnei_cuk (src/dem_grid.cu:466-552): cells in
+// z, y, x order over -1..1, partners ascending within a cell, candidate if
+// |xi - xj|^2 < (1.5 (ri + rj))^2 in FP64; j > i goes to the front (owner)
+// row of i, j < i to its back row.  Runs on the new order (alternate buffers).
+template <bool FILL>
+__device__ __forceinline__ void search_single(const Dev& d, const ScenePar& P, int i, int* nf, int* nb,
+                                              int* out_f, int* out_b, int* own_f) {
+    const double4 pi = d.posr2[i];
+    const int ci = d.clump_id2[i];
+    const int cx0 = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
+    const int cy0 = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
+    const int cz0 = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
+    int f = 0, b = 0;
+    for (int cz = -1; cz <= 1; cz++)
+        for (int cy = -1; cy <= 1; cy++)
+            for (int cx = -1; cx <= 1; cx++) {
+                const int x = cx0 + cx, y = cy0 + cy, z = cz0 + cz;
+                if (x < 0 || x >= P.gdim[0] || y < 0 || y >= P.gdim[1] || z < 0 || z >= P.gdim[2]) continue;
+                const int cell = P.cell_off + (z * P.gdim[1] + y) * P.gdim[0] + x;
+                const int start = d.cell_beg[cell];
+                if (start == -1) continue;
+                const int end = d.cell_end[cell];
+                for (int j = start; j < end; j++) {
+                    if (j == i) continue;
+                    const double4 pj = d.posr2[j];
+                    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    const double lim = 1.50 * (pi.w + pj.w);
+                    if (d2 < lim * lim) {
+                        if (i < j) {
+                            if (FILL) {
+                                out_f[f] = j | (d.clump_id2[j] == ci ? INTRA : 0);
+                                own_f[f] = i;
+                            }
+                            f++;
+                        } else {
+                            if (FILL) out_b[b] = j | (d.clump_id2[j] == ci ? INTRA : 0);
+                            b++;
+                        }
+                    }
+                }
+            }
+    *nf = f;
+    *nb = b;
+}
+
+__global__ void k_count(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) { d.cnt_f[d.N] = 0; d.cnt_b[d.N] = 0; }
+    if (i >= d.N) return;
+    const int s = d.sid[i];
+    const ScenePar& P = d.par[s];
+    if (!d.dyn[s].rebuild) {
+        const PairList& O = d.L[*d.lcur & 1];
+        d.cnt_f[i] = O.row[i + 1] - O.row[i];
+        d.cnt_b[i] = O.brow[i + 1] - O.brow[i];
+        return;
+    }
+    int nf = 0, nb = 0;
+    if (d.key2[i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
+        search_single<false>(d, P, i, &nf, &nb, nullptr, nullptr, nullptr);
+    d.cnt_f[i] = nf;
+    d.cnt_b[i] = nb;
+    if (nf > P.bl / 2 || nb > P.bl / 2) atomicOr(&d.dyn[s].err, ERR_ROW_OVERFLOW);
+}
+
+// the pair totals are cnt_f[N] / cnt_b[N] after the scans
+__global__ void k_check_cap(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    if (d.cnt_f[d.N] > d.cap || d.cnt_b[d.N] > d.cap) {
+        *d.halt = 1;
+        for (int s = 0; s < d.S; s++) atomicOr(&d.dyn[s].err, ERR_LIST_OVERFLOW);
+    }
+}
+
+__global__ void k_fill(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const int s = d.sid[i];
+    const ScenePar& P = d.par[s];
+    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
+    const int rf = d.cnt_f[i], rb = d.cnt_b[i];
+    if (i == d.N - 1) { Nw.row[d.N] = d.cnt_f[d.N]; Nw.brow[d.N] = d.cnt_b[d.N]; }
+    Nw.row[i] = rf;
+    Nw.brow[i] = rb;
+    if (!d.dyn[s].rebuild) {
+        const PairList& O = d.L[*d.lcur & 1];
+        const int of = O.row[i], nf = O.row[i + 1] - of;
+        for (int g = 0; g < nf; g++) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
+        const int ob = O.brow[i], nb = O.brow[i + 1] - ob;
+        for (int g = 0; g < nb; g++) Nw.bnbr[rb + g] = O.bnbr[ob + g];
+        return;
+    }
+    if (d.key2[i] == P.cell_off + P.cellnum - 1) return;
+    int nf, nb;
+    search_single<true>(d, P, i, &nf, &nb, Nw.nbr + rf, Nw.bnbr + rb, Nw.own + rf);
+}
+
+// The reverse map of CreateContList_cuk (src/dem_grid.cu:561-601): for each
+// back entry of i (owner j), the index of the pair (j, i) in j's front row.
+__global__ void k_backref(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N) return;
+    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
+    for (int k = Nw.brow[i]; k < Nw.brow[i + 1]; k++) {
+        const int j = Nw.bnbr[k] & IDX_MASK;
+        int found = -1;
+        for (int q = Nw.row[j]; q < Nw.row[j + 1]; q++)
+            if ((Nw.nbr[q] & IDX_MASK) == i) { found = q; break; }
+        Nw.bpair[k] = found;
+    }
+}
+
+// InheritContHistory_cuk (src/dem_grid.cu:603-647): each new pair copies the
+// spring history of the same pair in the previous list, negated when the
+// owner changed.  Pairs absent from the previous list start from zero.
+template <typename R>
+__global__ void k_carry(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= d.cnt_f[d.N]) return;
+    const int lc = *d.lcur, hg = *d.hgen;
+    const PairList& O = d.L[lc & 1];
+    const PairList& Nw = d.L[(lc + 1) & 1];
+    const size_t cap = (size_t)d.cap;
+    const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
+    R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
+    const uint8_t* ti = d.touch[hg & 1];
+    uint8_t* to = d.touch[(hg + 1) & 1];
+    const int jr = Nw.nbr[p];
+    if (jr < 0) { to[p] = 0; return; }
+    const int i = Nw.own[p], j = jr;
+    const int s = d.sid[i];
+    const ScenePar& P = d.par[s];
+    int q = -1;
+    R sign = R(1);
+    if (!d.dyn[s].rebuild) {
+        q = p - Nw.row[P.sub_off] + O.row[P.sub_off];
+    } else {
+        const int io = d.perm[i], jo = d.perm[j];
+        int oo, ot;
+        if (P.levels > 1 && d.level2[i] != d.level2[j]) {
+            const bool i_coarse = d.level2[i] < d.level2[j];
+            oo = i_coarse ? io : jo;
+            ot = i_coarse ? jo : io;
+        } else {
+            oo = io < jo ? io : jo;
+            ot = io < jo ? jo : io;
+        }
+        sign = oo == io ? R(1) : R(-1);
+        for (int r = O.row[oo]; r < O.row[oo + 1]; r++)
+            if ((O.nbr[r] & IDX_MASK) == ot) { q = r; break; }
+    }
+    if (q >= 0 && ti[q]) {
+        for (int h = 0; h < 2; h++) {
+            R4<R> v = Hi[h * cap + q];
+            v.x *= sign; v.y *= sign; v.z *= sign; v.w *= sign;
+            Ho[h * cap + p] = v;
+        }
+        const R* h2i = (const R*)(Hi + 2 * cap);
+        R* h2o = (R*)(Ho + 2 * cap);
+        h2o[p] = sign * h2i[q];
+        to[p] = 1;
+    } else {
+        to[p] = 0;
+    }
+}
+
+// Finishes a rebuild: per-clump member lists in ascending subsphere order
+// (the order thrust::sort_by_key gives reduce_by_key, src/dem_clumpsphere.cu:
+// 123-147), scene bookkeeping, and the swap of list, history generation and
+// persistent per-subsphere buffers.
+__global__ void k_commit(Dev* __restrict__ dp) {
+    Dev& d = *dp;
+    if (*d.halt) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < d.K) {
+        const int mb = d.mem_start[t], me = d.mem_start[t + 1];
+        for (int m = mb; m < me; m++) d.mem_idx[m] = d.inv[d.mem_idx[m]];
+        for (int m = mb + 1; m < me; m++) {
+            int v = d.mem_idx[m], q = m - 1;
+            while (q >= mb && d.mem_idx[q] > v) { d.mem_idx[q + 1] = d.mem_idx[q]; q--; }
+            d.mem_idx[q + 1] = v;
+        }
+    } else if (t < d.K + d.S) {
+        const int s = t - d.K;
+        SceneDyn& y = d.dyn[s];
+        const int so = d.par[s].sub_off, ns = d.par[s].nsub;
+        y.pair_off = d.cnt_f[so];
+        y.npairs = d.cnt_f[so + ns] - d.cnt_f[so];
+        if (y.rebuild) { y.nrebuild++; y.rebuild = 0; }
+    } else if (t == d.K + d.S) {
+        *d.lcur += 1;
+        *d.hgen += 1;
+        *d.any_rebuild = 0;
+#define NBC_SWAP(a, b) { auto tmp_ = d.a; d.a = d.b; d.b = tmp_; }
+        NBC_SWAP(posr, posr2) NBC_SWAP(lom, lom2) NBC_SWAP(cum, cum2) NBC_SWAP(clump_id, clump_id2)
+        NBC_SWAP(part_fix, part_fix2) NBC_SWAP(level, level2) NBC_SWAP(key, key2) NBC_SWAP(kin, kin2)
+        NBC_SWAP(bhist, bhist2) NBC_SWAP(bbits, bbits2)
+#undef NBC_SWAP
+    }
+}
+
+// ===========================================================================
+// contact kernel
+// ===========================================================================
+
+template <typename R> struct Law {
+    R kn_fac, ks_fac, damping, beta, mu, dt;
+};
+
+template <typename R> struct LawOut {
+    V3<R> Fn, Ft, Mr, Mt;  // normal and tangential force on the body, rolling and twisting moments
+    V3<R> hs, ht, hr;      // new tangential, twisting and rolling histories
+    R FnL;
+};
+
+// The Hertz-Mindlin law with rolling and twisting springs shared by the
+// pair, wall and intruder kernels of the reference
+// (src/dem_force_clump.cu:66-161, src/dem_force_cube_wall_clump.cu:62-166,
+// src/dem_force_penetrator_clump.cu:76-173).  n points from the other body
+// toward this body's contact side, Vtot is this body's contact-point velocity
+// relative to the other's, Dth = dt (w_this - w_other) for walls and the
+// intruder, dt (w_other_side...) as the pair caller passes it.
+template <typename R>
+__device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vtot, V3<R> Dth, R Rij, R Mij,
+                                       R cs_mult, V3<R> H, V3<R> Mr, V3<R> Mt, LawOut<R>& o) {
+    const R sq = sqrt(Rij * Dn);
+    const R Kn = L.kn_fac * sq;
+    const R Cn = L.damping * sqrt(Kn * Mij);
+    const R Ks = L.ks_fac * sq;
+    const R Cs = cs_mult * L.damping * sqrt(Ks * Mij);
+    const R br = L.beta * Rij;
+    const R Kr = R(0.25) * Kn * br * br;
+    const R Cr = R(0.25) * Cn * br * br;
+    const R Kt = R(0.50) * Ks * br * br;
+    const R Ct = R(0.50) * Cs * br * br;
+    const R ERR = dot(n, Vtot);
+    const V3<R> Vnor = ERR * n;
+    const V3<R> Vtan = Vtot - Vnor;
+    o.Fn = (Kn * Dn) * n + Cn * Vnor;
+    o.FnL = len_floor(o.Fn);
+    V3<R> Ft = (-Ks) * (L.dt * Vtan) + Cs * Vtan + H;
+    const R FtL = len_floor(Ft);
+    if (FtL > o.FnL * L.mu) {
+        Ft = (L.mu * o.FnL * (R(1) / FtL)) * Ft;
+        o.hs = Ft;
+    } else {
+        o.hs = Ft - Cs * Vtan;
+    }
+    o.Ft = Ft;
+    const R DthL = dot(Dth, n);
+    const V3<R> DthT = DthL * n;
+    const V3<R> DthR = Dth - DthT;
+    V3<R> rm = Kr * DthR + Mr;
+    const R rmL = len_floor(rm);
+    const R rcap = R(0.525) * L.beta * Rij * o.FnL;
+    if (rmL > rcap) {
+        rm = (rcap * (R(1) / rmL)) * rm;
+        o.hr = rm;
+    } else {
+        o.hr = rm;
+        rm = rm - (Cr * (R(1) / L.dt)) * DthR;
+    }
+    V3<R> tm = Kt * DthT + Mt;
+    const R tmL = len_floor(tm);
+    const R tcap = R(0.65) * L.mu * L.beta * Rij * o.FnL;
+    if (tmL > tcap) {
+        tm = (tcap * (R(1) / tmL)) * tm;
+        o.ht = tm;
+    } else {
+        o.ht = tm;
+        tm = tm - (Ct * (R(1) / L.dt)) * DthT;
+    }
+    o.Mr = rm;
+    o.Mt = tm;
+}
+
+template <typename R> struct Body {
+    double4 p;         // position, radius
+    V3<R> v, w, arm;   // clump velocity, clump angular velocity, world arm
+    R m;
+};
+
+template <typename R>
+__device__ __forceinline__ Body<R> load_body(const Dev& d, int i) {
+    const R4<R>* kv = (const R4<R>*)d.kin;
+    Body<R> b;
+    b.p = d.posr[i];
+    R4<R> a = kv[i], w = kv[d.N + i], r = kv[2 * d.N + i];
+    b.v = xyz<R>(a);
+    b.m = a.w;
+    b.w = xyz<R>(w);
+    b.arm = xyz<R>(r);
+    return b;
+}
+
+// Pair contact seen from body a (the pair law of ContactForce_clump_cuk,
+// src/dem_force_clump.cu:3-163, with a in the role of particleI).  Returns
+// false when the pair does not overlap.
+template <typename R>
+__device__ __forceinline__ bool pair_contact(const Law<R>& L, R cohesion, const Body<R>& a, const Body<R>& b,
+                                             V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& fa, V3<R>& ta, LawOut<R>& o,
+                                             double& Ap_out, V3<double>& n_out) {
+    const double dx = b.p.x - a.p.x, dy = b.p.y - a.p.y, dz = b.p.z - a.p.z;
+    const double DistS = dx * dx + dy * dy + dz * dz;
+    const double DistL = sqrt(DistS);
+    const double Dn = a.p.w + b.p.w - DistL;
+    if (!(Dn > 0.0)) return false;
+    const double DistR = 1.0 / DistL;
+    const V3<double> nd = v3(DistR * dx, DistR * dy, DistR * dz);
+    const double Ap = 0.50 * (a.p.w * a.p.w - b.p.w * b.p.w + DistS) * DistR;
+    const double An = DistL - Ap;
+    const V3<R> n = cvt<R>(nd);
+    const R ra = (R)a.p.w, rb = (R)b.p.w;
+    const R Rij = ra * rb / (ra + rb);
+    const R Mij = a.m * b.m / (a.m + b.m);
+    const V3<R> ARMa = a.arm + (R)Ap * n;
+    const V3<R> ARMb = b.arm - (R)An * n;
+    const V3<R> Vtot = (b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
+    const V3<R> Dth = L.dt * (a.w - b.w);
+    hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
+    const R br = L.beta * Rij;
+    fa = (-o.Fn - o.Ft) + (cohesion * br * br) * n;
+    ta = ((-(R)Ap) * cross(n, o.Ft) - o.Mr) - o.Mt;
+    Ap_out = Ap;
+    n_out = nd;
+    return true;
+}
+
+// a wall or intruder contact: normal n (toward the subsphere), lever Ap,
+// overlap Dn, wall point RVo relative to the wall centre
+template <typename R>
+__device__ __forceinline__ void boundary_contact(const Law<R>& L, const Body<R>& a, V3<R> n, R Ap, R Dn,
+                                                 V3<R> RVo, V3<R> wv, V3<R> ww, R Rij, R Mij, R cs_mult,
+                                                 V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& f, V3<R>& t,
+                                                 LawOut<R>& o, V3<R>& arm_out) {
+    const V3<R> Arm = (-a.arm) + Ap * n;
+    const V3<R> Vwall = cross(ww, RVo);
+    const V3<R> Vtot = (a.v - wv) + (cross(Arm, a.w) - Vwall);
+    const V3<R> Dth = L.dt * (a.w - ww);
+    hm_law<R>(L, n, Dn, Vtot, Dth, Rij, Mij, cs_mult, H, Mr, Mt, o);
+    f = o.Fn + o.Ft;
+    t = ((-Ap) * cross(n, o.Ft) - o.Mr) - o.Mt;
+    arm_out = Arm;
+}
+
+// pair history layout: R4 (Dv.xyz, Dr.x) at [q], R4 (Dt.xyz, Dr.y) at
+// [cap + q], Dr.z as a scalar after the 2*cap R4s
+template <typename R>
+__device__ __forceinline__ void hist_read(const R4<R>* H, size_t cap, size_t q, V3<R>& hs, V3<R>& ht, V3<R>& hr) {
+    R4<R> a = H[q], b = H[cap + q];
+    const R c = ((const R*)(H + 2 * cap))[q];
+    hs = v3<R>(a.x, a.y, a.z);
+    ht = v3<R>(b.x, b.y, b.z);
+    hr = v3<R>(a.w, b.w, c);
+}
+template <typename R>
+__device__ __forceinline__ void hist_write(R4<R>* H, size_t cap, size_t q, V3<R> hs, V3<R> ht, V3<R> hr) {
+    H[q] = pack<R>(hs, hr.x);
+    H[cap + q] = pack<R>(ht, hr.y);
+    ((R*)(H + 2 * cap))[q] = hr.z;
+}
+
+template <int LANES>
+__device__ __forceinline__ unsigned group_mask() {
+    if (LANES == 32) return 0xffffffffu;
+    const int g = (threadIdx.x & 31) / LANES;
+    return ((1u << LANES) - 1u) << (g * LANES);
+}
+
+template <typename R, int LANES>
+__device__ __forceinline__ R group_sum(R v, unsigned mask) {
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+constexpr int CT_THREADS = 256;
+
+template <typename R, int LANES, bool EXPORT>
+__global__ void __launch_bounds__(CT_THREADS) k_contact(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    constexpr int SPB = CT_THREADS / LANES;
+    const int s = d.sblk_scene[blockIdx.x];
+    const ScenePar& P = d.par[s];
+    const int grp = threadIdx.x / LANES, lane = threadIdx.x % LANES;
+    const int i = P.sub_off + (blockIdx.x - P.cblk_off) * SPB + grp;
+    if (i >= P.sub_off + P.nsub) return;
+    const unsigned mask = group_mask<LANES>();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
+
+    Law<R> L;
+    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
+    const R coh = (R)P.cohesion;
+
+    const int lc = *d.lcur, hg = *d.hgen;
+    const PairList& Lst = d.L[lc & 1];
+    const size_t cap = (size_t)d.cap;
+    const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
+    R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
+    const uint8_t* ti = d.touch[hg & 1];
+    uint8_t* to = d.touch[(hg + 1) & 1];
+
+    const Body<R> me = load_body<R>(d, i);
+    V3<R> F = v3<R>(0, 0, 0), T = F;
+    V3<R> Fw = F, Tw = F, Fi = F, Ti = F;  // export parts
+
+    // front (owner) entries
+    const int rs = Lst.row[i], re = Lst.row[i + 1];
+    for (int k = rs + lane; k < re; k += LANES) {
+        const int jr = Lst.nbr[k];
+        if (jr < 0) continue;  // pair inside one clump (src/dem_force_clump.cu:18-19)
+        const Body<R> ot = load_body<R>(d, jr);
+        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+        const double dx = ot.p.x - me.p.x, dy = ot.p.y - me.p.y, dz = ot.p.z - me.p.z;
+        const double dl = sqrt(dx * dx + dy * dy + dz * dz);
+        if (!(me.p.w + ot.p.w - dl > 0.0)) { to[k] = 0; continue; }
+        if (ti[k]) hist_read<R>(Hi, cap, k, hs, ht, hr);
+        V3<R> fa, ta;
+        LawOut<R> o;
+        double Ap;
+        V3<double> nd;
+        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
+        F = F + fa;
+        T = T + ta;
+        hist_write<R>(Ho, cap, k, o.hs, o.ht, o.hr);
+        to[k] = 1;
+        if (EXPORT) {
+            R4<R>* xf = (R4<R>*)d.xfcn;
+            double4* xc = (double4*)d.xcpt;
+            xf[k] = pack<R>(-o.Fn, R(0));
+            xc[k] = make_double4(me.p.x + Ap * nd.x, me.p.y + Ap * nd.y, me.p.z + Ap * nd.z, 0.0);
+        }
+    }
+    // back entries: the owner's stored history, seen from this side
+    const int bs = Lst.brow[i], be = Lst.brow[i + 1];
+    for (int k = bs + lane; k < be; k += LANES) {
+        const int jr = Lst.bnbr[k];
+        if (jr < 0) continue;
+        const Body<R> ot = load_body<R>(d, jr);
+        const double dx = ot.p.x - me.p.x, dy = ot.p.y - me.p.y, dz = ot.p.z - me.p.z;
+        const double dl = sqrt(dx * dx + dy * dy + dz * dz);
+        if (!(me.p.w + ot.p.w - dl > 0.0)) continue;
+        const int q = Lst.bpair[k];
+        if (q < 0) continue;  // unreachable with a consistent list
+        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+        if (ti[q]) {
+            hist_read<R>(Hi, cap, q, hs, ht, hr);
+            hs = -hs; ht = -ht; hr = -hr;
+        }
+        V3<R> fa, ta;
+        LawOut<R> o;
+        double Ap;
+        V3<double> nd;
+        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
+        F = F + fa;
+        T = T + ta;
+    }
+    if (EXPORT) { Fw = F; Tw = T; }  // temporarily hold the pair part
+
+    // boundary slots: walls (cube faces or cylinder regions) and the intruder
+    const int nwall = P.wall == WALL_CUBE ? 6 : (P.wall == WALL_CYL ? 3 : 0);
+    const uint16_t bb_old = d.bbits[i];
+    uint16_t bb_new = 0;
+    R4<R>* BH = (R4<R>*)d.bhist;
+    const size_t N = (size_t)d.N;
+    V3<R> pF = v3<R>(0, 0, 0), pT = pF, iF = pF, iT = pF;
+    for (int slot = lane; slot < NB_SLOTS; slot += LANES) {
+        const bool is_wall = slot < nwall;
+        const bool is_intr = slot == SLOT_INTR && P.has_intr;
+        if (!is_wall && !is_intr) continue;
+        double Apd = 0, Dnd = 0;
+        V3<double> nd = v3(0.0, 0.0, 0.0), RVo = nd;
+        bool on = false;
+        R Rij = (R)me.p.w, Mij = me.m, csm = R(2);
+        V3<R> wv = v3<R>((R)P.w_v[0], (R)P.w_v[1], (R)P.w_v[2]);
+        V3<R> ww = v3<R>((R)P.w_w[0], (R)P.w_w[1], (R)P.w_w[2]);
+        const V3<double> RV = v3(me.p.x - P.w_c[0], me.p.y - P.w_c[1], me.p.z - P.w_c[2]);
+        const double r = me.p.w;
+        if (is_wall && P.wall == WALL_CUBE) {
+            // CubeWallInteraction_clump_cuk (src/dem_force_cube_wall_clump.cu:228-292)
+            const int ax = slot >> 1;
+            const bool up = (slot & 1) == 0;
+            const double e = (&RV.x)[ax], h = P.w_half[ax];
+            on = up ? (e > 0 && e + r - h > 0) : (e < 0 && e - r + h < 0);
+            if (on) {
+                RVo = RV;
+                (&RVo.x)[ax] = (h / fabs(e)) * e;
+                (&nd.x)[ax] = up ? -1.0 : 1.0;
+                const V3<double> RVn = RV - RVo;
+                Apd = dot(RVn, nd);
+                Dnd = r - Apd;
+                on = Dnd > 0.0;
+            }
+        } else if (is_wall && P.wall == WALL_CYL) {
+            // CylindWallInteraction_cuk (src/dem_force_cylind_wall.cu:152-237)
+            const V3<double> axv = v3(P.cyl_axis[0], P.cyl_axis[1], P.cyl_axis[2]);
+            const double ERR = dot(RV, axv);
+            const V3<double> RVb = RV - ERR * axv, RVt = ERR * axv;
+            const double nrm = len_floor(RVb);
+            const double d_cap = fabs(ERR) - P.cyl_H + r;
+            const double d_side = nrm - P.cyl_R + r;
+            if (slot == 0) on = d_cap >= 1e-14 && ERR < 0;
+            else if (slot == 1) on = d_cap >= 1e-14 && ERR > 0;
+            else on = d_side >= 1e-14;
+            if (on) {
+                RVo = slot < 2 ? (P.cyl_H / fabs(ERR)) * RVt + RVb : (P.cyl_R / nrm) * RVb + RVt;
+                const V3<double> RVn = RV - RVo;
+                Dnd = r - len_floor(RVn);
+                on = Dnd > 0.0;
+                if (on) {
+                    const double DistL = sqrt(RVn.x * RVn.x + RVn.y * RVn.y + RVn.z * RVn.z);
+                    nd = (1.0 / DistL) * RVn;
+                    Apd = DistL;
+                }
+            }
+        } else {
+            // PrePenetrator / GetSphereIntruderContact / ForcePene_clump_cuk
+            // (src/dem_contact_penetrator.cu:8-84, src/dem_sphere_intruder.cuh:20-51,
+            // src/dem_force_penetrator_clump.cu:4-182)
+            const SceneDyn& y = d.dyn[s];
+            const V3<double> RI = v3(me.p.x - y.intr_p[0], me.p.y - y.intr_p[1], me.p.z - y.intr_p[2]);
+            wv = v3<R>((R)y.intr_v[0], (R)y.intr_v[1], (R)y.intr_v[2]);
+            ww = v3<R>((R)P.intr_w[0], (R)P.intr_w[1], (R)P.intr_w[2]);
+            csm = R(1);
+            if (P.intr_motion == 1) Mij = (R)(me.m * P.intr_mass / (me.m + P.intr_mass));
+            if (P.intr_shape == 1) {
+                const double cd = len_floor(RI);
+                if (cd > 1.0e-15) nd = (1.0 / cd) * RI;
+                else {
+                    V3<double> fb = v3(P.intr_axis[0], P.intr_axis[1], P.intr_axis[2]);
+                    double t2 = sqrt(dot(fb, fb));
+                    nd = t2 > 1e-20 ? (1.0 / t2) * fb : v3(0.0, 0.0, 0.0);
+                    if (len_floor(nd) < 1.0e-15) nd = v3(0.0, 0.0, 1.0);
+                }
+                RVo = P.intr_R * nd;
+                const double gap = cd - P.intr_R;
+                Dnd = r - gap;
+                Apd = gap;
+                on = Dnd > 0.0;
+                Rij = (R)(r * P.intr_R / (r + P.intr_R));
+            } else {
+                const double LatDx = P.cell[0];
+                const V3<double> pv = v3(P.intr_axis[0], P.intr_axis[1], P.intr_axis[2]);
+                const double ERR = dot(RI, pv);
+                if (fabs(ERR) < (P.intr_H + 0.80 * LatDx)) {
+                    const V3<double> RVb = RI - ERR * pv;
+                    const double nrm = len_floor(RVb);
+                    if (nrm < (P.intr_R + 0.80 * LatDx)) {
+                        const V3<double> RVt = ERR * pv;
+                        if (fabs(ERR) < P.intr_H) RVo = ((1.0 / nrm) * P.intr_R) * RVb + RVt;
+                        else if (nrm < P.intr_R) RVo = ((1.0 / fabs(ERR)) * P.intr_H) * RVt + RVb;
+                        else RVo = ((1.0 / nrm) * P.intr_R) * RVb + ((1.0 / fabs(ERR)) * P.intr_H) * RVt;
+                        const V3<double> RVn = RI - RVo;
+                        const double DistL = sqrt(RVn.x * RVn.x + RVn.y * RVn.y + RVn.z * RVn.z);
+                        Dnd = r - DistL;
+                        on = Dnd > 0.0;
+                        if (on) { nd = (1.0 / DistL) * RVn; Apd = DistL; }
+                    }
+                }
+            }
+            if (on && P.intr_wait) atomicCAS(&d.dyn[s].intr_state, 0, 1);
+        }
+        if (!on) continue;
+        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+        const size_t hb = (size_t)slot * 3 * N;
+        if (bb_old & (1u << slot)) {
+            R4<R> a = BH[hb + i], b = BH[hb + N + i], c = BH[hb + 2 * N + i];
+            hs = xyz<R>(a); ht = xyz<R>(b); hr = xyz<R>(c);
+        }
+        V3<R> f, t, arm;
+        LawOut<R> o;
+        boundary_contact<R>(L, me, cvt<R>(nd), (R)Apd, (R)Dnd, cvt<R>(RVo), wv, ww, Rij, Mij, csm, hs, hr, ht,
+                            f, t, o, arm);
+        BH[hb + i] = pack<R>(o.hs, R(0));
+        BH[hb + N + i] = pack<R>(o.ht, R(0));
+        BH[hb + 2 * N + i] = pack<R>(o.hr, R(0));
+        bb_new |= (uint16_t)(1u << slot);
+        if (is_intr) {
+            iF = iF + f;
+            iT = iT + t;
+            // torque on the intruder about its centre (src/dem_force_penetrator_clump.cu:125,170)
+            const V3<R> pt = (-cross(cvt<R>(RVo), f) + o.Mr) + o.Mt;
+            long long* fx = (long long*)&d.dyn[s].ifix[0];
+            atomicAdd((unsigned long long*)&fx[0], (unsigned long long)llrint((double)f.x * FIX_F));
+            atomicAdd((unsigned long long*)&fx[1], (unsigned long long)llrint((double)f.y * FIX_F));
+            atomicAdd((unsigned long long*)&fx[2], (unsigned long long)llrint((double)f.z * FIX_F));
+            atomicAdd((unsigned long long*)&fx[3], (unsigned long long)llrint((double)pt.x * FIX_T));
+            atomicAdd((unsigned long long*)&fx[4], (unsigned long long)llrint((double)pt.y * FIX_T));
+            atomicAdd((unsigned long long*)&fx[5], (unsigned long long)llrint((double)pt.z * FIX_T));
+            if (EXPORT) {
+                R4<R>* xi = (R4<R>*)d.xintr;
+                xi[i] = pack<R>(o.Fn, R(0));
+                xi[N + i] = pack<R>(o.Ft, R(0));
+                xi[2 * N + i] = pack<R>(cross(o.Fn, arm), R(0));
+                xi[3 * N + i] = pack<R>((cross(o.Ft, arm) - o.Mr) - o.Mt, R(0));
+            }
+        } else {
+            pF = pF + f;
+            pT = pT + t;
+        }
+    }
+    F = (F + pF) + iF;
+    T = (T + pT) + iT;
+    // reduce over the lane group
+    F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
+    T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
+    unsigned bits = bb_new;
+    for (int o = LANES / 2; o > 0; o >>= 1) bits |= __shfl_xor_sync(mask, bits, o);
+    if (EXPORT) {
+        V3<R>* parts[6] = {&Fw, &Tw, &pF, &pT, &iF, &iT};
+        R4<R>* xp = (R4<R>*)d.xparts;
+        for (int c = 0; c < 6; c++) {
+            V3<R>& v = *parts[c];
+            v.x = group_sum<R, LANES>(v.x, mask); v.y = group_sum<R, LANES>(v.y, mask); v.z = group_sum<R, LANES>(v.z, mask);
+            if (lane == 0) xp[c * N + i] = pack<R>(v, R(0));
+        }
+        if (lane == 0 && !(bits & (1u << SLOT_INTR))) {
+            R4<R>* xi = (R4<R>*)d.xintr;
+            R4<R> z = pack<R>(v3<R>(0, 0, 0), R(0));
+            xi[i] = z; xi[N + i] = z; xi[2 * N + i] = z; xi[3 * N + i] = z;
+        }
+    }
+    if (lane == 0) {
+        R4<R>* fs = (R4<R>*)d.fsum;
+        fs[i] = pack<R>(F, R(0));
+        fs[N + i] = pack<R>(T, R(0));
+        d.bbits[i] = (uint16_t)bits;
+        if (!(isfinite((double)F.x) && isfinite((double)F.y) && isfinite((double)F.z) &&
+              isfinite((double)T.x) && isfinite((double)T.y) && isfinite((double)T.z)))
+            atomicOr(&d.dyn[s].err, ERR_NONFINITE);
+    }
+}
+
+}  // namespace nbc

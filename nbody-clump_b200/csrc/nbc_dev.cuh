@@ -1,0 +1,148 @@
+// nbc_dev.cuh -- device-side data layout of the B200 DEM engine.
+//
+// A *batch* holds S independent scenes concatenated: scene s owns the
+// subsphere range [sub_off, sub_off+nsub) and the clump range
+// [clump_off, clump_off+nclump).  Subspheres are stored in cell-sorted
+// order within their scene (the reference keeps its particle arrays in the
+// order of its last cell sort, src/dem_simulation_clump.cu:128-164); a
+// rebuild only permutes within a scene, so scenes stay contiguous.
+//
+// Every kernel receives one pointer to a device-resident `Dev` table that
+// holds all buffer pointers, so buffers can be re-allocated without
+// re-capturing the CUDA graph.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nbc {
+
+constexpr int MAX_LEVELS = 4;
+constexpr int WALL_NONE = 0, WALL_CUBE = 1, WALL_CYL = 2;
+// boundary slots of a subsphere: cube faces UpX, LowX, UpY, LowY, UpZ, LowZ
+// (src/dem_force_cube_wall_clump.cu:228-292), or cylinder regions bottom cap,
+// top cap, side (src/dem_force_cylind_wall.cu:178-233), then the intruder.
+constexpr int NB_WALL_MAX = 6;
+constexpr int SLOT_INTR = 6;
+constexpr int NB_SLOTS = 7;
+
+// error bits of SceneDyn::err
+constexpr int ERR_LIST_OVERFLOW = 1;   // pair capacity exceeded (host grows and retries)
+constexpr int ERR_NONFINITE = 2;       // non-finite wall input/output (src/dem_force_cube_wall_clump.cu:191-203)
+constexpr int ERR_BAD_CLUMP = 4;       // clump id out of range
+constexpr int ERR_ROW_OVERFLOW = 8;    // a row exceeded BranchLmtLen/2 (reference semantics, export only)
+
+struct ScenePar {
+    // integration and contact law (world.par, src/dem_parameters.h:49-66)
+    double dt, E, nu, mu, damping, gravity, beta, cohesion, thresh;
+    double kn_fac;  // 2E / (3 (1 - nu^2))                 src/dem_force_clump.cu:68
+    double ks_fac;  // 2E / (1 + nu) / (2 - nu)            src/dem_force_clump.cu:71
+    // grid (src/dem_subsphere_io.cu:195-230)
+    double origin[3], cell[3], icell[3], box_lo[3], box_hi[3];
+    int gdim[3];
+    int cellnum;    // cells of this scene incl. the out-of-box bucket
+    int cell_off;   // first global cell id of this scene
+    int levels;     // 1 = single level grid
+    double lcell[MAX_LEVELS];
+    int ldim[MAX_LEVELS][3];
+    int loff[MAX_LEVELS];
+    // ranges
+    int sub_off, nsub, clump_off, nclump;
+    int cblk_off, cblk_n;  // contact-kernel blocks of this scene
+    int bl;                // BranchLmtLen of the reference (row capacity of the export)
+    // walls
+    int wall;       // WALL_*
+    double w_half[3], w_c[3], w_v[3], w_w[3];   // cube: half sizes, centre, velocity, angular velocity
+    double cyl_R, cyl_H, cyl_axis[3];           // cylinder: radius, half height, axis (centre in w_c)
+    // intruder
+    int has_intr, intr_shape, intr_motion, intr_wait;  // shape 0 cylinder 1 sphere; motion 0 kinematic 1 gravity
+    double intr_R, intr_H, intr_axis[3], intr_mass, intr_w[3];
+};
+
+struct SceneDyn {
+    double intr_p[3], intr_v[3];
+    double totF[3], totT[3];       // sum over subspheres of the intruder force / torque (src/dem_force_penetrator.cu:237-248)
+    double reaction[3], reaction_t[3];
+    int intr_state;                // ContactState (src/dem_parameters.h:82-91)
+    int rebuild;                   // set by the pose pass when a subsphere moved > Thresh
+    int err;
+    int step;                      // completed steps
+    int nrebuild;
+    int npairs;                    // pairs in the current list
+    int pair_off;                  // first pair of this scene in the current list
+    long long ifix[6];             // fixed-point sums of intruder force (2^-40 N) and torque (2^-44 N m)
+};
+
+struct PairList {
+    int* row;     // [N+1] exclusive scan of front counts (owner rows)
+    int* brow;    // [N+1] exclusive scan of back counts
+    int* nbr;     // [cap] front partner, bit 31 set for pairs inside one clump
+    int* own;     // [cap] owner of each pair (the reference's Lpa)
+    int* bnbr;    // [cap] back partner (the owner), bit 31 set inside one clump
+    int* bpair;   // [cap] pair index of each back entry (the reference's Aref)
+};
+
+struct Dev {
+    int S, N, K;
+    int cap;          // pair capacity of each list buffer
+    int cells;        // total global cells (sum over scenes)
+    int sort_bits;    // key bits for the radix sort
+    int cblocks;      // total contact-kernel blocks
+    int nthreads_sub; // subsphere-parallel grid stride helpers
+    ScenePar* par;
+    SceneDyn* dyn;
+    int* sid;         // [N] scene of each subsphere
+    int* csid;        // [K] scene of each clump
+    // subspheres, sorted order.  Each persistent array has an alternate
+    // buffer (suffix 2): a rebuild gathers into the alternates and k_commit
+    // swaps the pointers in this table, so nothing changes if it stops early.
+    double4* posr;    double4* posr2;    // x y z r
+    double4* lom;     double4* lom2;     // local offset (body frame) xyz, mass
+    double4* cum;     double4* cum2;     // displacement since the last rebuild
+    int* clump_id;    int* clump_id2;
+    int* part_fix;    int* part_fix2;    // original index (ParticleID)
+    int* level;       int* level2;       // hgrid level (0 = coarsest)
+    int* key;         int* key2;         // global cell key at the last rebuild (sorted)
+    void* kin;        void* kin2;        // Real4 [3][N]: clump velocity + mass, clump angular velocity, world arm
+    void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][3][N] boundary histories (Dv, Dt, Dr)
+    uint16_t* bbits;  uint16_t* bbits2;  // [N] boundary slots in contact at the last step
+    void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder)
+    // clumps
+    double4* cpos;    // xyz
+    double4* cvel;
+    double4* cw;
+    double4* cq;      // x y z w
+    double4* cprop;   // Ixx Iyy Izz M
+    double4* cF;      // force on clump from the last force pass
+    double4* cT;
+    int* mem_start;   // [K+1]
+    int* mem_idx;     // [N] member subspheres of each clump, ascending
+    int* post_pending;// device flag: a force pass has run whose half-kick is pending
+    // broad phase scratch
+    int* kA; int* vA; int* kB; int* vB;   // radix sort ping-pong
+    int* hist;        // radix histograms
+    int* perm;        // [N] old index of new slot i (part_idx_pre)
+    int* inv;         // [N] new slot of old index
+    int* cell_beg; int* cell_end;         // [cells]
+    int* cnt_f; int* cnt_b;               // [N+1] counts, scanned in place
+    int* scan_tmp;                        // block sums
+    int* any_rebuild;                     // device flag: some scene rebuilds this step
+    int* halt;                            // device flag: pair capacity exceeded, kernels stand still
+    // pair lists and histories (ping-pong)
+    PairList L[2];
+    int* lcur;        // index of the current list
+    void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
+    uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
+    int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
+    int* gstep;       // contact passes completed (counts steps across graph launches)
+    // export (per pair), written by the export variant of the contact kernel
+    void* xfcn;       // Real4 [cap] normal force on the owner (CacheFcn)
+    void* xcpt;       // double4 [cap] contact point (CacheCpt)
+    void* xparts;     // Real4 [6][N]: pair F, T, wall F, T, intruder F, T
+    void* xintr;      // Real4 [4][N]: intruder Fcn, Fct, Tcn, Tct
+    // intruder force history ring (per scene), reaction force and torque
+    double* ring;     // [S][ring_len][6]
+    int ring_len;
+    int* sblk_scene;  // [cblocks] scene of each contact block
+};
+
+}  // namespace nbc

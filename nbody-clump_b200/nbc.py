@@ -1,0 +1,310 @@
+"""ctypes binding of libnbc.so (include/nbc.h) for Python callers.
+
+Mirrors the engine's C ABI one call per method; the engine itself is C++ and
+sm_100a CUDA.  There is no fallback: if libnbc.so is missing or no CUDA device
+is present, Engine() raises.
+
+    import nbc, scenegen
+    eng = nbc.Engine([scenegen.make_cfg0()], precision="f64")
+    eng.step(100); eng.sync()
+    state = eng.clumps(0)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnbc.so")
+
+NBC_OK = 0
+STATUS = {-1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_IO", -4: "ERR_NONFINITE", -5: "ERR_NO_DEVICE",
+          -6: "ERR_MEMORY", -7: "ERR_STATE"}
+PREC = {"f64": 0, "mixed": 1}
+WALL = {None: 0, "cube": 1, "cylinder": 2}
+MOTION = {"constant_velocity": 0, "gravity": 1, "gravity_after_contact": 2}
+
+D3 = C.c_double * 3
+D4 = C.c_double * 4
+P_D = C.POINTER(C.c_double)
+P_I = C.POINTER(C.c_int)
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("n_sub", C.c_int), ("n_clump", C.c_int), ("branch_len", C.c_int),
+        ("start_step", C.c_int), ("end_step", C.c_int), ("output_interval", C.c_int),
+        ("dt", C.c_double), ("ymod", C.c_double), ("prat", C.c_double), ("frcoe", C.c_double),
+        ("normres", C.c_double), ("beta", C.c_double), ("cohesion", C.c_double),
+        ("gravity", C.c_double), ("thresh", C.c_double),
+        ("world_origin", D3), ("world_size", D3), ("box_lo", D3), ("box_hi", D3),
+        ("is_wall_force", C.c_int),
+        ("clump_id", P_I), ("pos", P_D), ("local", P_D), ("mass", P_D), ("radius", P_D),
+        ("clump_pos", P_D), ("clump_vel", P_D), ("clump_quat", P_D), ("clump_angvel", P_D),
+        ("clump_prop", P_D),
+        ("wall", C.c_int),
+        ("cube_half", D3), ("cube_centre", D3), ("cube_vel", D3), ("cube_angvel", D3),
+        ("cyl_radius", C.c_double), ("cyl_half_height", C.c_double), ("cyl_axis", D3),
+        ("cyl_centre", D3), ("cyl_vel", D3), ("cyl_angvel", D3),
+        ("intruder", C.c_int), ("intr_motion", C.c_int),
+        ("intr_radius", C.c_double), ("intr_half_height", C.c_double), ("intr_axis", D3),
+        ("intr_prop", D4), ("intr_pos", D3), ("intr_vel", D3), ("intr_angvel", D3),
+        ("levels", C.c_int), ("level", P_I), ("level_cell", P_D),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int),
+                ("device", C.c_int), ("pair_slack", C.c_double)]
+
+
+EXPORTED = [
+    "nbc_last_error", "nbc_default_options", "nbc_open", "nbc_run", "nbc_create", "nbc_destroy",
+    "nbc_step", "nbc_step_export", "nbc_sync", "nbc_num_scenes", "nbc_scene_stats",
+    "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
+    "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
+    "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
+    "nbc_engine_info",
+]
+
+_lib = None
+
+
+class NbcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libnbc.so (building it first if this tree has not built it)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            import build as _b  # noqa: PLC0415  (the in-tree build script)
+            _b.build()
+        L = C.CDLL(LIB_PATH)
+        L.nbc_last_error.restype = C.c_char_p
+        L.nbc_default_options.argtypes = [C.POINTER(Options)]
+        L.nbc_default_options.restype = None
+        for f in EXPORTED:
+            if f not in ("nbc_last_error", "nbc_default_options"):
+                getattr(L, f).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != NBC_OK:
+        raise NbcError(rc, lib().nbc_last_error().decode(errors="replace"))
+
+
+def _p(a, t=P_D):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def _set(arr, vals):
+    for i, v in enumerate(vals):
+        arr[i] = float(v)
+
+
+def scene_desc(scene: dict):
+    """Build a SceneDesc (and the arrays it points to) from a scenegen scene."""
+    p, s, c = scene["params"], scene["sub"], scene["clump"]
+    keep = {
+        "cid": np.ascontiguousarray(s["clump_id"], dtype=np.int32),
+        "pos": np.ascontiguousarray(s["pos"], dtype=np.float64),
+        "local": np.ascontiguousarray(s["local"], dtype=np.float64),
+        "mass": np.ascontiguousarray(s["mass"], dtype=np.float64),
+        "radius": np.ascontiguousarray(s["radius"], dtype=np.float64),
+    }
+    for k in ("pos", "vel", "quat", "angvel", "prop"):
+        keep["c" + k] = np.ascontiguousarray(c[k], dtype=np.float64)
+    d = SceneDesc()
+    d.n_sub, d.n_clump = int(p["NumberBody"]), int(p["ClumpNum"])
+    d.branch_len = int(p["BranchLmtLen"])
+    d.start_step, d.end_step = int(p["StartStep"]), int(p["EndStep"])
+    d.output_interval = int(p["OutputInterval"])
+    d.dt, d.ymod, d.prat, d.frcoe = p["StepSize"], p["Ymod"], p["Prat"], p["Frcoe"]
+    d.normres, d.beta, d.cohesion = p["NormRes"], p["Beta"], p["Cohesion"]
+    d.gravity, d.thresh = p["Gravity"], p["Thresh"]
+    _set(d.world_origin, [p["WorldOrigin_" + a] for a in "xyz"])
+    _set(d.world_size, [p["WorldSize_" + a] for a in "xyz"])
+    _set(d.box_lo, [p["BoxLowLmt_" + a] for a in "xyz"])
+    _set(d.box_hi, [p["BoxUpLmt_" + a] for a in "xyz"])
+    d.is_wall_force = int(p["isWallForce"])
+    d.clump_id = _p(keep["cid"], P_I)
+    d.pos, d.local, d.mass, d.radius = _p(keep["pos"]), _p(keep["local"]), _p(keep["mass"]), _p(keep["radius"])
+    d.clump_pos, d.clump_vel, d.clump_quat = _p(keep["cpos"]), _p(keep["cvel"]), _p(keep["cquat"])
+    d.clump_angvel, d.clump_prop = _p(keep["cangvel"]), _p(keep["cprop"])
+    cube, cyl = scene.get("cube"), scene.get("cylinder")
+    if cube is not None:
+        d.wall = 1
+        _set(d.cube_half, cube["half"]); _set(d.cube_centre, cube["centre"])
+        _set(d.cube_vel, cube["vel"]); _set(d.cube_angvel, cube["angvel"])
+    elif cyl is not None:
+        d.wall = 2
+        d.cyl_radius, d.cyl_half_height = cyl["radius"], cyl["half_height"]
+        _set(d.cyl_axis, cyl["axis"]); _set(d.cyl_centre, cyl["centre"])
+        _set(d.cyl_vel, cyl["vel"]); _set(d.cyl_angvel, cyl["angvel"])
+    it = scene.get("intruder")
+    d.intruder = -1
+    if it is not None and int(p["isIntruder"]):
+        d.intruder = 1 if it["shape"] == "sphere" else 0
+        d.intr_motion = MOTION[it["motion"]]
+        d.intr_radius, d.intr_half_height = it["radius"], it["half_height"]
+        _set(d.intr_axis, it["axis"]); _set(d.intr_prop, it["prop"])
+        _set(d.intr_pos, it["pos"]); _set(d.intr_vel, it["vel"]); _set(d.intr_angvel, it["angvel"])
+    lv = scene.get("levels")
+    d.levels = 1
+    if lv is not None:
+        keep["level"] = np.ascontiguousarray(lv["level"], dtype=np.int32)
+        keep["level_cell"] = np.ascontiguousarray(lv["cell"], dtype=np.float64)
+        d.levels = len(keep["level_cell"])
+        d.level, d.level_cell = _p(keep["level"], P_I), _p(keep["level_cell"])
+    return d, keep
+
+
+class Engine:
+    """A batch of scenes resident on one GPU."""
+
+    def __init__(self, scenes, precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0):
+        L = lib()
+        self._descs = [scene_desc(s) for s in scenes]
+        self.N = [int(s["params"]["NumberBody"]) for s in scenes]
+        self.K = [int(s["params"]["ClumpNum"]) for s in scenes]
+        self.BL = [int(s["params"]["BranchLmtLen"]) for s in scenes]
+        arr = (C.POINTER(SceneDesc) * len(scenes))(*[C.pointer(d) for d, _ in self._descs])
+        o = Options()
+        L.nbc_default_options(C.byref(o))
+        o.precision, o.lanes, o.use_graph, o.device = PREC[precision], lanes, int(use_graph), device
+        o.pair_slack = pair_slack
+        h = C.c_void_p()
+        _check(L.nbc_create(arr, len(scenes), C.byref(o), C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def open(cls, workdir: str, precision="f64", use_graph=True):
+        """The drop-in path: read a reference working directory."""
+        self = cls.__new__(cls)
+        L = lib()
+        o = Options()
+        L.nbc_default_options(C.byref(o))
+        o.precision, o.use_graph = PREC[precision], int(use_graph)
+        h = C.c_void_p()
+        _check(L.nbc_open(workdir.encode(), C.byref(o), C.byref(h)))
+        self.h = h
+        self._descs = []
+        return self
+
+    def run(self):
+        _check(lib().nbc_run(self.h))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().nbc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        _check(lib().nbc_step(self.h, int(n)))
+
+    def step_export(self, n=1):
+        _check(lib().nbc_step_export(self.h, int(n)))
+
+    def sync(self):
+        _check(lib().nbc_sync(self.h))
+
+    def stats(self, s=0):
+        v = [C.c_int() for _ in range(4)]
+        _check(lib().nbc_scene_stats(self.h, s, *[C.byref(x) for x in v]))
+        return {"steps": v[0].value, "rebuilds": v[1].value, "npairs": v[2].value, "err": v[3].value}
+
+    def subspheres(self, s=0):
+        n = self.N[s]
+        fix, cid = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        pos, rad = np.zeros((n, 3)), np.zeros(n)
+        _check(lib().nbc_get_subspheres(self.h, s, _p(fix, P_I), _p(cid, P_I), _p(pos), _p(rad)))
+        return {"part_fix": fix, "clump_id": cid, "pos": pos, "radius": rad}
+
+    def clumps(self, s=0):
+        k = self.K[s]
+        o = {x: np.zeros((k, 3)) for x in ("pos", "vel", "angvel", "force", "torque")}
+        o["quat"] = np.zeros((k, 4))
+        _check(lib().nbc_get_clumps(self.h, s, _p(o["pos"]), _p(o["vel"]), _p(o["quat"]),
+                                    _p(o["angvel"]), _p(o["force"]), _p(o["torque"])))
+        return o
+
+    def sub_forces(self, s=0):
+        n = self.N[s]
+        f, t = np.zeros((n, 3)), np.zeros((n, 3))
+        _check(lib().nbc_get_sub_forces(self.h, s, _p(f), _p(t)))
+        return f, t
+
+    def force_parts(self, s=0):
+        n = self.N[s]
+        parts = np.zeros((6, n, 3))
+        _check(lib().nbc_get_force_parts(self.h, s, _p(parts)))
+        return {k: parts[i] for i, k in enumerate(("fc", "tc", "fw", "tw", "fi", "ti"))}
+
+    def pairs(self, s=0):
+        n = C.c_int(0)
+        _check(lib().nbc_get_pairs(self.h, s, C.byref(n), None, None))
+        a, b = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32)
+        _check(lib().nbc_get_pairs(self.h, s, C.byref(n), _p(a, P_I), _p(b, P_I)))
+        return a, b
+
+    def rows(self, s=0, bl=None):
+        bl = bl or self.BL[s]
+        n = self.N[s]
+        anei = np.zeros((n, bl), np.int32)
+        ng, ni = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        _check(lib().nbc_get_rows(self.h, s, bl, _p(anei, P_I), _p(ng, P_I), _p(ni, P_I)))
+        return anei, ng, ni
+
+    def chain(self, s=0, bl=None):
+        bl = bl or self.BL[s]
+        n = self.N[s]
+        f, c = np.zeros((n, bl, 3)), np.zeros((n, bl, 3))
+        _check(lib().nbc_get_chain(self.h, s, bl, _p(f), _p(c)))
+        return f, c
+
+    def intruder(self, s=0):
+        o = {k: np.zeros(3) for k in ("pos", "vel", "reaction", "torque")}
+        st = C.c_int()
+        _check(lib().nbc_get_intruder(self.h, s, _p(o["pos"]), _p(o["vel"]), _p(o["reaction"]),
+                                      _p(o["torque"]), C.byref(st)))
+        o["state"] = st.value
+        return o
+
+    def intruder_diag(self, s=0):
+        n = self.N[s]
+        d = np.zeros((4, n, 3))
+        _check(lib().nbc_get_intruder_diag(self.h, s, _p(d)))
+        return d
+
+    def intruder_history(self, s=0, count=1):
+        out = np.zeros((count, 6))
+        _check(lib().nbc_get_intruder_history(self.h, s, int(count), _p(out)))
+        return out
+
+    def timing_enable(self, on=True):
+        _check(lib().nbc_timing_enable(self.h, int(on)))
+
+    def timing_read(self):
+        ms, nc, nk, nr = C.c_double(), C.c_int(), C.c_longlong(), C.c_int()
+        _check(lib().nbc_timing_read(self.h, C.byref(ms), C.byref(nc), C.byref(nk), C.byref(nr)))
+        return {"contact_ms": ms.value, "contact_launches": nc.value, "kernel_launches": nk.value,
+                "rebuilds": nr.value}
+
+    def info(self):
+        b, ms = C.c_double(), C.c_double()
+        _check(lib().nbc_engine_info(self.h, C.byref(b), C.byref(ms)))
+        return {"device_bytes": b.value, "last_step_ms": ms.value}

@@ -274,22 +274,42 @@ def _tetra_members(scales, r, offset_ratio, rho):
     return locals_, radii, masses, np.array(props)
 
 
+def layered_packing(rng, diam, R, z0, jitter=0.02):
+    """Clump centres in horizontal square-lattice layers inside a circle of
+    radius R: clumps sorted by size (largest first), each layer spaced by its
+    largest member's diameter * 1.05, layer order shuffled within a layer."""
+    order = np.argsort(-diam, kind="stable")
+    pts = np.zeros((len(diam), 3))
+    z = z0
+    i = 0
+    while i < len(order):
+        d = 1.05 * diam[order[i]]
+        n = int(2 * (R - 0.5 * d) / d) + 1
+        g = (np.arange(n) - (n - 1) / 2.0) * d
+        gx, gy = np.meshgrid(g, g, indexing="ij")
+        inside = gx ** 2 + gy ** 2 <= (R - 0.5 * d) ** 2
+        xy = np.stack([gx[inside], gy[inside]], axis=1)
+        take = order[i:i + len(xy)]
+        sel = rng.permutation(len(xy))[:len(take)]
+        pts[take, 0:2] = xy[sel] + rng.uniform(-jitter * d, jitter * d, (len(take), 2))
+        pts[take, 2] = z + 0.5 * d
+        z += d
+        i += len(take)
+    return pts
+
+
 def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000) -> dict:
     """50,000 tetrahedral clumps (4 subspheres, r = 1 mm, centre offset 0.6 r,
-    log-normal(0, 0.2) size scale, random orientation) seeded on a lattice above
-    the floor of a closed cylinder wall (R = 60 mm, half-height 150 mm, axis z)."""
+    log-normal(0, 0.2) size scale, random orientation) seeded in layers inside
+    a closed cylinder wall (R = 60 mm, half-height 300 mm, axis z, floor at
+    z = 0) and settling under gravity."""
     rng = np.random.default_rng(seed)
     r, rho = 1e-3, MATERIAL["rho"]
     scales = rng.lognormal(0.0, 0.2, n_clumps)
     locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
-    rmax = max(rr.max() for rr in radii)
-    ext = 2.0 * (0.6 * rmax + rmax) * 1.05  # lattice spacing: clump diameter + 5 %
-    R, H = 0.06, 0.15
-    # square lattice inscribed in the cylinder cross-section
-    half = (R - ext) / math.sqrt(2.0)
-    nx = max(1, int(2 * half / ext))
-    pts = lattice_points(rng, n_clumps, ext, (-half + 0.5 * ext, -half + 0.5 * ext, -H + 0.6 * ext),
-                         nx, nx, 0.02 * ext)
+    diam = 2.0 * np.array([np.linalg.norm(l, axis=1).max() + rr.max() for l, rr in zip(locals_, radii)])
+    R, H = 0.06, 0.30
+    pts = layered_packing(rng, diam, R, 0.0)
     q = random_unit_quaternions(rng, n_clumps)
     rmin = min(rr.min() for rr in radii)
     dt = 0.2 * rayleigh_dt(rmin, rho, MATERIAL["Ymod"], MATERIAL["Prat"])
@@ -297,12 +317,11 @@ def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000) 
                             Ymod=MATERIAL["Ymod"], Prat=MATERIAL["Prat"],
                             Frcoe=MATERIAL["Frcoe"], NormRes=MATERIAL["NormRes"],
                             Thresh=0.2 * rmin, BranchLmtLen=96)
-    top = max(pts[:, 2].max() + ext, H)
-    set_world_box(params, (-R, -R, -H), (R, R, top))
+    set_world_box(params, (-R, -R, 0.0), (R, R, 2 * H))
     K = n_clumps
     return assemble(params, pts, q, np.zeros((K, 3)), np.zeros((K, 3)), props,
                     locals_, radii, masses,
-                    cylinder=make_cylinder(R, H, (0, 0, 0)))
+                    cylinder=make_cylinder(R, H, (0, 0, H)))
 
 
 # ----------------------------------------------------------------------------
