@@ -19,7 +19,8 @@ OUT = os.path.join(HERE, "libnbc.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "capi.cpp", "io.cpp"]
-HEADERS = ["kernels.cuh", "nbc_dev.cuh", "nbc_math.cuh", "engine.h", "io.h"]
+HEADERS = ["kernels.cuh", "nbc_dev.cuh", "nbc_math.cuh", "engine.h", "io.h", "dem_clump_main.h",
+           "dem_clump_main.cpp", "main.cpp"]
 
 
 def _stale() -> bool:
@@ -60,6 +61,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("link failed")
     for o in objs:
         os.remove(o)
+    # the drop-in executable: the reference's main() on DEMClumpMain
+    exe = os.path.join(HERE, "nbody_clump_b200")
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(HERE), "include"),
+           os.path.join(CSRC, "main.cpp"), os.path.join(CSRC, "dem_clump_main.cpp"), "-L", HERE, "-lnbc",
+           "-Wl,-rpath,$ORIGIN", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("drop-in executable failed to link")
     return OUT
 
 

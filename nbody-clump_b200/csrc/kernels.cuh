@@ -190,7 +190,7 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // GetParticleCellIndex_cuk (src/dem_grid.cu:155-202); hierarchical variant
 // GetParticleCellIndex_hGrid_cuk (src/dem_hgrid.cu:205-242) with the
 // out-of-box bucket kept inside the scene's cell range.
-__global__ void k_hash(const Dev* __restrict__ dp) {
+static __global__ void k_hash(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -235,7 +235,7 @@ __global__ void k_hash(const Dev* __restrict__ dp) {
 // stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
 constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ keys, int n, int shift,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ keys, int n, int shift,
                                                         int* __restrict__ hist, int nblk) {
     __shared__ int h[256];
     const int tid = threadIdx.x, blk = blockIdx.x;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ 
     hist[tid * nblk + blk] = h[tid];
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
                                                            int* __restrict__ kout, int* __restrict__ vout, int n,
                                                            int shift, const int* __restrict__ hist, int nblk) {
     __shared__ int base[256];
@@ -309,7 +309,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
     return warp_base + x - v;
 }
 
-__global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, int n, int* __restrict__ sums) {
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, int n, int* __restrict__ sums) {
     __shared__ int sh[SC_THREADS / 32];
     const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
     int v[SC_ITEMS], s = 0;
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, 
     if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums, int nb) {
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums, int nb) {
     __shared__ int sh[SC_THREADS / 32];
     int carry = 0;
     for (int off = 0; off < nb; off += SC_THREADS) {
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums
     }
 }
 
-__global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums) {
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums) {
     const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
     const int add = sums[blockIdx.x];
     for (int j = 0; j < SC_ITEMS; j++)
@@ -344,13 +344,13 @@ __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, in
 }
 
 // --- cell ranges, reorder ------------------------------------------------
-__global__ void k_fill_i(int* __restrict__ a, int n, int v) {
+static __global__ void k_fill_i(int* __restrict__ a, int n, int v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
 }
 
 // FindBegEndInCell_cuk (src/dem_grid.cu:105-153) over the global cell table,
 // plus the permutation, its inverse and the sorted keys (into key2).
-__global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
+static __global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -440,7 +440,7 @@ __device__ __forceinline__ void search_single(const Dev& d, const ScenePar& P, i
     *nb = b;
 }
 
-__global__ void k_count(const Dev* __restrict__ dp) {
+static __global__ void k_count(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,7 +463,7 @@ __global__ void k_count(const Dev* __restrict__ dp) {
 }
 
 // the pair totals are cnt_f[N] / cnt_b[N] after the scans
-__global__ void k_check_cap(const Dev* __restrict__ dp) {
+static __global__ void k_check_cap(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     if (d.cnt_f[d.N] > d.cap || d.cnt_b[d.N] > d.cap) {
@@ -472,7 +472,7 @@ __global__ void k_check_cap(const Dev* __restrict__ dp) {
     }
 }
 
-__global__ void k_fill(const Dev* __restrict__ dp) {
+static __global__ void k_fill(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -499,7 +499,7 @@ __global__ void k_fill(const Dev* __restrict__ dp) {
 
 // The reverse map of CreateContList_cuk (src/dem_grid.cu:561-601): for each
 // back entry of i (owner j), the index of the pair (j, i) in j's front row.
-__global__ void k_backref(const Dev* __restrict__ dp) {
+static __global__ void k_backref(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -574,7 +574,7 @@ __global__ void k_carry(const Dev* __restrict__ dp) {
 // (the order thrust::sort_by_key gives reduce_by_key, src/dem_clumpsphere.cu:
 // 123-147), scene bookkeeping, and the swap of list, history generation and
 // persistent per-subsphere buffers.
-__global__ void k_commit(Dev* __restrict__ dp) {
+static __global__ void k_commit(Dev* __restrict__ dp) {
     Dev& d = *dp;
     if (*d.halt) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
