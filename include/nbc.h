@@ -167,6 +167,35 @@ nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launc
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 
+/* --- allocation-free cell sort ------------------------------------------
+ * No counterpart in the reference (its sort allocates CUB scratch with
+ * cudaMalloc on first use, src/dem_grid.cu:278-305).  For callers that
+ * cannot call cudaMalloc -- device memory owned by another framework's pool,
+ * or a run whose memory budget is fixed at start-up: the cell hash of a
+ * list rebuild plus the engine's stable radix sort, with the caller's
+ * buffers and one scratch array compiled into the library (NBC_NOALLOC_MAX_N
+ * elements, about 2.2 MB per GPU that loads the library, kept until exit).
+ *   pos_dev   device array [n][3] of positions (caller-owned)
+ *   grid      the padded grid: origin, cell size, dims, the box whose
+ *             outside goes to the last cell (as the engine's hash)
+ *   perm_dev  device out [n]: index of the subsphere at each sorted slot
+ *   key_dev   device out [n]: its cell, ascending
+ *   stream    cudaStream_t to launch on (NULL: the default stream); the
+ *             call returns after launching, the caller synchronises.
+ * n above NBC_NOALLOC_MAX_N returns NBC_ERR_ARG.  The first call on a device
+ * looks up the scratch array's device address, so make that first call
+ * before any stream capture.  Calls share the scratch array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+#define NBC_NOALLOC_MAX_N 262144
+typedef struct {
+    double origin[3];
+    double cell;
+    int dims[3];
+    double box_lo[3], box_hi[3];
+} nbc_grid_desc;
+nbc_status nbc_cell_sort_noalloc(const double* pos_dev, int n, const nbc_grid_desc* grid, int* perm_dev,
+                                 int* key_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

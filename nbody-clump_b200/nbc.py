@@ -55,6 +55,19 @@ class SceneDesc(C.Structure):
     ]
 
 
+class GridDesc(C.Structure):
+    _fields_ = [("origin", D3), ("cell", C.c_double), ("dims", C.c_int * 3), ("box_lo", D3), ("box_hi", D3)]
+
+
+NOALLOC_MAX_N = 262144
+
+
+def cell_sort_noalloc(pos_ptr: int, n: int, grid: GridDesc, perm_ptr: int, key_ptr: int, stream: int = 0):
+    """nbc_cell_sort_noalloc on caller-owned device buffers (raw addresses)."""
+    _check(lib().nbc_cell_sort_noalloc(C.c_void_p(pos_ptr), int(n), C.byref(grid), C.c_void_p(perm_ptr),
+                                       C.c_void_p(key_ptr), C.c_void_p(stream)))
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int),
                 ("device", C.c_int), ("pair_slack", C.c_double)]
@@ -66,7 +79,7 @@ EXPORTED = [
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
-    "nbc_engine_info",
+    "nbc_engine_info", "nbc_cell_sort_noalloc",
 ]
 
 _lib = None
