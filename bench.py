@@ -152,6 +152,13 @@ def run_b200(args, world, rank, local):
     secs = reduce_max(local_s, world, backend)
     value = N * args.steps * world / secs
 
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": secs * 1e3 / args.steps,
+                              "contact_ms_avg": tm["contact_ms"] / max(1, tm["contact_launches"]),
+                              "npairs": st1["npairs"], "rebuilds": st1["rebuilds"] - st0["rebuilds"]}), flush=True)
+        return
+
     # ---- end to end through the C ABI with host buffers -----------------
     # create (H2D of the scene from host arrays), K steps, sync, D2H of the
     # clump state, all inside the timed region
@@ -297,6 +304,8 @@ def main():
     ap.add_argument("--clumps", type=int, default=50_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="short run for profilers: warm-up + timed steps only, no e2e / CPU legs")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)

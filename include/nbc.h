@@ -167,6 +167,12 @@ nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launc
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 
+/* Hierarchical-grid levels for a radius distribution (replaces the grid.bt
+ * level table the reference's sphere path reads, src/dem_io.cu:204-248):
+ * writes level[n] (0 = coarsest) and level_cell[<=max_levels], returns the
+ * number of levels (1 = the reference's single-level grid is best). */
+int nbc_choose_levels(const double* radius, int n, int max_levels, int* level, double* level_cell);
+
 /* --- allocation-free cell sort ------------------------------------------
  * No counterpart in the reference (its sort allocates CUB scratch with
  * cudaMalloc on first use, src/dem_grid.cu:278-305).  For callers that

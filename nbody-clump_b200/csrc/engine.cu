@@ -349,6 +349,7 @@ class EngineT final : public EngineBase {
     Dev h_{};            // host copy of the device table
     Dev* d_ = nullptr;   // device table
     int S_ = 0, N_ = 0, K_ = 0, lanes_ = 16, passes_ = 0, rs_blocks_ = 0;
+    bool hgrid_ = false;
     int ring_len_ = 1;
     std::vector<ScenePar> hpar_;
     std::vector<int> start_step_;
@@ -377,7 +378,7 @@ class EngineT final : public EngineBase {
         return n;
     }
     // kernels one rebuild launches (launch_rebuild)
-    int rebuild_launches() const { return 1 + passes_ * 5 + 2 + 1 + 1 + 1 + 6 + 1 + 4; }
+    int rebuild_launches() const { return 1 + passes_ * 5 + 2 + 1 + 1 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 5; }
     std::pair<cudaEvent_t, cudaEvent_t> next_pair() {
         if ((size_t)(2 * ev_used_ + 2) > ev_.size()) {
             for (int k = 0; k < 64; k++) {
@@ -444,8 +445,8 @@ class EngineT final : public EngineBase {
                 P.box_hi[a] = D.box_hi[a];
             }
             P.levels = D.levels > 1 ? D.levels : 1;
+            if (P.levels > 1) hgrid_ = true;
             if (P.levels > MAX_LEVELS) throw ArgError("too many grid levels");
-            if (P.levels > 1) throw ArgError("scene " + std::to_string(s) + ": hierarchical grid not built yet");
             if (P.levels == 1) {
                 P.cellnum = P.gdim[0] * P.gdim[1] * P.gdim[2];
             } else {
@@ -589,6 +590,8 @@ class EngineT final : public EngineBase {
         h_.cell_end = mem_.alloc<int>(cells);
         h_.cnt_f = mem_.alloc<int>(N + 1);
         h_.cnt_b = mem_.alloc<int>(N + 1);
+        h_.sfc = mem_.alloc<int>(N);
+        h_.xcnt = mem_.alloc<int>(N);
         h_.scan_tmp = mem_.alloc<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
         for (int l = 0; l < 2; l++) {
             h_.L[l].row = mem_.alloc<int>(N + 1);
@@ -801,7 +804,10 @@ class EngineT final : public EngineBase {
         k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_end, h_.cells, -1);
         k_cellrange<<<cdiv(N_, B), B, 0, stream_>>>(d_, ki, vi);
         k_reorder<R><<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        k_count<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        const int sb = cdiv(N_, SEARCH_WARPS);
+        k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, N_ + 1, 0);
+        k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, N_ + 1, 0);
+        k_count<<<sb, 32 * SEARCH_WARPS, 0, stream_>>>(d_);
         scan(h_.cnt_f, N_ + 1);
         scan(h_.cnt_b, N_ + 1);
         CK(cudaGetLastError());
@@ -813,7 +819,9 @@ class EngineT final : public EngineBase {
             if (need > h_.cap) grow_pairs(need);
         }
         k_check_cap<<<1, 1, 0, stream_>>>(d_);
-        k_fill<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        if (hgrid_) k_fill_i<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, N_, 0);
+        k_fill<<<sb, 32 * SEARCH_WARPS, 0, stream_>>>(d_);
+        if (hgrid_) k_xsort<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_carry<R><<<cdiv(std::max(h_.cap, 1), 256), 256, 0, stream_>>>(d_);
         k_commit<<<cdiv(K_ + S_ + 1, B), B, 0, stream_>>>(d_);

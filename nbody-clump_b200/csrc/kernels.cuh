@@ -394,72 +394,138 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
 }
 
 // --- neighbour search ----------------------------------------------------
-// The 27-cell scan of CreateAnei_cuk (src/dem_grid.cu:466-552): cells in
-// z, y, x order over -1..1, partners ascending within a cell, candidate if
-// |xi - xj|^2 < (1.5 (ri + rj))^2 in FP64; j > i goes to the front (owner)
-// row of i, j < i to its back row.  Runs on the new order (alternate buffers).
+// One warp per subsphere.  The candidate test and the order of CreateAnei_cuk
+// (src/dem_grid.cu:466-552): cells in z, y, x order over -1..1, partners
+// ascending within a cell, candidate if |xi - xj|^2 < (1.5 (ri + rj))^2 in
+// FP64; j > i goes to the front (owner) row of i, j < i to its back row.  The
+// three x-neighbour cells of one (z, y) stencil row hold one contiguous range
+// of the sorted order, so the warp walks 9 ranges per level with coalesced
+// loads and appends its hits in discovery order through ballot prefixes.
+//
+// Hierarchical grid (CreateAnei_hGrid_cuk, src/dem_hgrid_contlist.cu:57-161):
+// a subsphere searches its own level and every coarser one (level 0 is the
+// coarsest); a pair across levels is owned by the coarser subsphere: the
+// finer one records a back entry, the coarser one a front entry, placed after
+// its same-level front entries in ascending order of the finer partner.
+constexpr int SEARCH_WARPS = 4;  // subspheres per 128-thread block
+
 template <bool FILL>
-__device__ __forceinline__ void search_single(const Dev& d, const ScenePar& P, int i, int* nf, int* nb,
-                                              int* out_f, int* out_b, int* own_f) {
+__device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, const PairList& Nw, int i, int lane,
+                                            int& nf_out, int& nb_out, int& nx_out) {
     const double4 pi = d.posr2[i];
     const int ci = d.clump_id2[i];
-    const int cx0 = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
-    const int cy0 = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
-    const int cz0 = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
-    int f = 0, b = 0;
-    for (int cz = -1; cz <= 1; cz++)
-        for (int cy = -1; cy <= 1; cy++)
-            for (int cx = -1; cx <= 1; cx++) {
-                const int x = cx0 + cx, y = cy0 + cy, z = cz0 + cz;
-                if (x < 0 || x >= P.gdim[0] || y < 0 || y >= P.gdim[1] || z < 0 || z >= P.gdim[2]) continue;
-                const int cell = P.cell_off + (z * P.gdim[1] + y) * P.gdim[0] + x;
-                const int start = d.cell_beg[cell];
-                if (start == -1) continue;
-                const int end = d.cell_end[cell];
-                for (int j = start; j < end; j++) {
-                    if (j == i) continue;
-                    const double4 pj = d.posr2[j];
-                    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    const double d2 = dx * dx + dy * dy + dz * dz;
-                    const double lim = 1.50 * (pi.w + pj.w);
-                    if (d2 < lim * lim) {
-                        if (i < j) {
-                            if (FILL) {
-                                out_f[f] = j | (d.clump_id2[j] == ci ? INTRA : 0);
-                                own_f[f] = i;
-                            }
-                            f++;
-                        } else {
-                            if (FILL) out_b[b] = j | (d.clump_id2[j] == ci ? INTRA : 0);
-                            b++;
-                        }
+    const int my = P.levels > 1 ? d.level2[i] : 0;
+    const unsigned lt = (1u << lane) - 1u;
+    int nf = 0, nb = 0, nx = 0;  // same-level front, back (all levels), cross-level (this row's partners)
+    const int rf = FILL ? d.cnt_f[i] : 0, rb = FILL ? d.cnt_b[i] : 0;
+    for (int l = my; l >= 0; l--) {
+        int gx, gy, gz, base, cx0, cy0, cz0;
+        if (P.levels <= 1) {
+            gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
+            base = P.cell_off;
+            cx0 = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
+            cy0 = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
+            cz0 = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
+        } else {
+            gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
+            base = P.cell_off + P.loff[l];
+            const double c = P.lcell[l];
+            cx0 = (int)floor((pi.x - P.origin[0]) / c);
+            cy0 = (int)floor((pi.y - P.origin[1]) / c);
+            cz0 = (int)floor((pi.z - P.origin[2]) / c);
+        }
+        const bool same = l == my;
+        const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
+        if (xa > xb) continue;
+        for (int cz = -1; cz <= 1; cz++) {
+            const int z = cz0 + cz;
+            if (z < 0 || z >= gz) continue;
+            for (int cy = -1; cy <= 1; cy++) {
+                const int y = cy0 + cy;
+                if (y < 0 || y >= gy) continue;
+                const int c0 = base + (z * gy + y) * gx;
+                int s = -1, e = -1;
+                for (int x = xa; x <= xb; x++) {
+                    const int b = d.cell_beg[c0 + x];
+                    if (b != -1) {
+                        if (s == -1) s = b;
+                        e = d.cell_end[c0 + x];
                     }
                 }
+                if (s == -1) continue;
+                for (int k0 = s; k0 < e; k0 += 32) {
+                    const int j = k0 + lane;
+                    bool hit = false;
+                    if (j < e && j != i) {
+                        const double4 pj = d.posr2[j];
+                        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                        const double d2 = dx * dx + dy * dy + dz * dz;
+                        const double lim = 1.50 * (pi.w + pj.w);
+                        hit = d2 < lim * lim;
+                    }
+                    const bool front = hit && same && i < j;
+                    const bool back = hit && !front;
+                    const bool cross = hit && !same;
+                    const unsigned fm = __ballot_sync(0xffffffffu, front);
+                    const unsigned bm = __ballot_sync(0xffffffffu, back);
+                    if (FILL && hit) {
+                        const int flag = d.clump_id2[j] == ci ? INTRA : 0;
+                        if (front) {
+                            const int q = rf + nf + __popc(fm & lt);
+                            Nw.nbr[q] = j | flag;
+                            Nw.own[q] = i;
+                        } else {
+                            Nw.bnbr[rb + nb + __popc(bm & lt)] = j | flag;
+                            if (cross) {
+                                // the coarser partner owns the pair: claim a slot after
+                                // its same-level front entries (sorted afterwards)
+                                const int q = d.cnt_f[j] + d.sfc[j] + atomicAdd(&d.xcnt[j], 1);
+                                Nw.nbr[q] = i | flag;
+                                Nw.own[q] = j;
+                            }
+                        }
+                    }
+                    if (!FILL && cross) atomicAdd(&d.cnt_f[j], 1);
+                    nf += __popc(fm);
+                    nb += __popc(bm);
+                    nx += __popc(__ballot_sync(0xffffffffu, cross));
+                }
             }
-    *nf = f;
-    *nb = b;
+        }
+    }
+    nf_out = nf;
+    nb_out = nb;
+    nx_out = nx;
 }
 
-static __global__ void k_count(const Dev* __restrict__ dp) {
+// counts: cnt_f[i] = same-level front entries + cross-level entries claimed
+// by finer partners (added with integer atomics), cnt_b[i] = back entries
+static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_count(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) { d.cnt_f[d.N] = 0; d.cnt_b[d.N] = 0; }
+    const int i = blockIdx.x * SEARCH_WARPS + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
     if (i >= d.N) return;
     const int s = d.sid[i];
     const ScenePar& P = d.par[s];
     if (!d.dyn[s].rebuild) {
-        const PairList& O = d.L[*d.lcur & 1];
-        d.cnt_f[i] = O.row[i + 1] - O.row[i];
-        d.cnt_b[i] = O.brow[i + 1] - O.brow[i];
+        if (lane == 0) {
+            const PairList& O = d.L[*d.lcur & 1];
+            atomicAdd(&d.cnt_f[i], O.row[i + 1] - O.row[i]);
+            d.cnt_b[i] = O.brow[i + 1] - O.brow[i];
+            d.sfc[i] = 0;
+        }
         return;
     }
-    int nf = 0, nb = 0;
+    int nf = 0, nb = 0, nx = 0;
     if (d.key2[i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
-        search_single<false>(d, P, i, &nf, &nb, nullptr, nullptr, nullptr);
-    d.cnt_f[i] = nf;
-    d.cnt_b[i] = nb;
-    if (nf > P.bl / 2 || nb > P.bl / 2) atomicOr(&d.dyn[s].err, ERR_ROW_OVERFLOW);
+        warp_search<false>(d, P, d.L[0], i, lane, nf, nb, nx);
+    if (lane == 0) {
+        atomicAdd(&d.cnt_f[i], nf);
+        d.cnt_b[i] = nb;
+        d.sfc[i] = nf;
+        if (nf > P.bl / 2 || nb > P.bl / 2) atomicOr(&d.dyn[s].err, ERR_ROW_OVERFLOW);
+    }
 }
 
 // the pair totals are cnt_f[N] / cnt_b[N] after the scans
@@ -472,29 +538,49 @@ static __global__ void k_check_cap(const Dev* __restrict__ dp) {
     }
 }
 
-static __global__ void k_fill(const Dev* __restrict__ dp) {
+static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_fill(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * SEARCH_WARPS + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
     if (i >= d.N) return;
     const int s = d.sid[i];
     const ScenePar& P = d.par[s];
     const PairList& Nw = d.L[(*d.lcur + 1) & 1];
     const int rf = d.cnt_f[i], rb = d.cnt_b[i];
-    if (i == d.N - 1) { Nw.row[d.N] = d.cnt_f[d.N]; Nw.brow[d.N] = d.cnt_b[d.N]; }
-    Nw.row[i] = rf;
-    Nw.brow[i] = rb;
+    if (lane == 0) {
+        if (i == d.N - 1) { Nw.row[d.N] = d.cnt_f[d.N]; Nw.brow[d.N] = d.cnt_b[d.N]; }
+        Nw.row[i] = rf;
+        Nw.brow[i] = rb;
+    }
     if (!d.dyn[s].rebuild) {
         const PairList& O = d.L[*d.lcur & 1];
         const int of = O.row[i], nf = O.row[i + 1] - of;
-        for (int g = 0; g < nf; g++) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
+        for (int g = lane; g < nf; g += 32) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
         const int ob = O.brow[i], nb = O.brow[i + 1] - ob;
-        for (int g = 0; g < nb; g++) Nw.bnbr[rb + g] = O.bnbr[ob + g];
+        for (int g = lane; g < nb; g += 32) Nw.bnbr[rb + g] = O.bnbr[ob + g];
         return;
     }
     if (d.key2[i] == P.cell_off + P.cellnum - 1) return;
-    int nf, nb;
-    search_single<true>(d, P, i, &nf, &nb, Nw.nbr + rf, Nw.bnbr + rb, Nw.own + rf);
+    int nf, nb, nx;
+    warp_search<true>(d, P, Nw, i, lane, nf, nb, nx);
+}
+
+// hierarchical grid: the cross-level entries of each owner row in ascending
+// order of the finer partner (their slots were claimed with atomics)
+static __global__ void k_xsort(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.N || !d.dyn[d.sid[i]].rebuild) return;
+    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
+    const int b = Nw.row[i] + d.sfc[i], e = Nw.row[i + 1];
+    for (int m = b + 1; m < e; m++) {
+        const int v = Nw.nbr[m];
+        int q = m - 1;
+        while (q >= b && (Nw.nbr[q] & IDX_MASK) > (v & IDX_MASK)) { Nw.nbr[q + 1] = Nw.nbr[q]; q--; }
+        Nw.nbr[q + 1] = v;
+    }
 }
 
 // The reverse map of CreateContList_cuk (src/dem_grid.cu:561-601): for each

@@ -124,6 +124,8 @@ struct Dev {
     int* inv;         // [N] new slot of old index
     int* cell_beg; int* cell_end;         // [cells]
     int* cnt_f; int* cnt_b;               // [N+1] counts, scanned in place
+    int* sfc;                             // [N] same-level front count (hierarchical grid)
+    int* xcnt;                            // [N] cross-level entries placed so far (hierarchical grid)
     int* scan_tmp;                        // block sums
     int* any_rebuild;                     // device flag: some scene rebuilds this step
     int* halt;                            // device flag: pair capacity exceeded, kernels stand still

@@ -68,6 +68,24 @@ def cell_sort_noalloc(pos_ptr: int, n: int, grid: GridDesc, perm_ptr: int, key_p
                                        C.c_void_p(key_ptr), C.c_void_p(stream)))
 
 
+def choose_levels(radius, max_levels=4):
+    """Hierarchical-grid levels for these radii: (level[n], level_cell[L])."""
+    r = np.ascontiguousarray(radius, dtype=np.float64)
+    lv = np.zeros(len(r), np.int32)
+    cell = np.zeros(4)
+    L = lib().nbc_choose_levels(_p(r), len(r), int(max_levels), _p(lv, P_I), _p(cell))
+    return lv, cell[:L].copy()
+
+
+def with_levels(scene: dict, max_levels=4) -> dict:
+    """The scene with a hierarchical grid chosen by nbc_choose_levels (or
+    unchanged when one level is best)."""
+    lv, cell = choose_levels(scene["sub"]["radius"], max_levels)
+    out = dict(scene)
+    out["levels"] = {"level": lv, "cell": cell} if len(cell) > 1 else None
+    return out
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int),
                 ("device", C.c_int), ("pair_slack", C.c_double)]
@@ -79,7 +97,7 @@ EXPORTED = [
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
-    "nbc_engine_info", "nbc_cell_sort_noalloc",
+    "nbc_engine_info", "nbc_cell_sort_noalloc", "nbc_choose_levels",
 ]
 
 _lib = None

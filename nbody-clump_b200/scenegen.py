@@ -621,3 +621,53 @@ def scene_from_npz(path: str) -> dict:
                     v = str(v)
             scene[grp][k] = v
     return scene
+
+
+def make_test_poly(n_clumps=150, seed=3, rmin=0.5e-3, rmax=2.5e-3, max_members=3, vel=0.5, angvel=200.0,
+                   intruder="sphere", motion="constant_velocity", thresh_ratio=0.0003, dt=1e-7, steps=24,
+                   wall="cube", bl=256):
+    """Polydisperse clumps (1..max_members subspheres, radii log-uniform in
+    [rmin, rmax]) on a lattice sized by the median clump, so large clumps
+    overlap their neighbours: a contact-rich scene for hierarchical grids."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    locals_, radii, masses, props = [], [], [], []
+    for k in range(n_clumps):
+        m = int(rng.integers(1, max_members + 1))
+        rr = np.exp(rng.uniform(np.log(rmin), np.log(rmax), m))
+        if m == 1:
+            cen = np.zeros((1, 3))
+        else:
+            d = rng.normal(size=(m, 3))
+            d /= np.linalg.norm(d, axis=1)[:, None]
+            cen = d * (0.6 * rr.min())
+        cen = cen - cen.mean(0)
+        M = float(np.sum(rho * 4.0 / 3.0 * np.pi * rr ** 3)) * 0.8
+        I = 0.4 * M * float(np.max(rr)) ** 2
+        locals_.append(cen)
+        radii.append(rr)
+        masses.append(np.full(m, M / m))
+        props.append([I, I, I, M])
+    props = np.array(props)
+    ext = 2.0 * np.median([np.linalg.norm(c, axis=1).max() + r.max() for c, r in zip(locals_, radii)])
+    nx = int(round(n_clumps ** (1 / 3))) + 1
+    pts = lattice_points(rng, n_clumps, ext, np.full(3, 0.5 * ext), nx, nx, 0.03 * ext)
+    hi = pts.max(0) + 0.5 * ext
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=1, Thresh=thresh_ratio * rmin,
+                            BranchLmtLen=bl)
+    set_world_box(params, -rmax * np.ones(3), hi + np.array([rmax, rmax, 6 * rmax]))
+    cube = make_cube(0.5 * hi, 0.5 * hi) if wall == "cube" else None
+    cyl = make_cylinder(0.5 * max(hi[0], hi[1]), 0.5 * hi[2], 0.5 * hi) if wall == "cylinder" else None
+    K = n_clumps
+    quats = random_unit_quaternions(rng, K)
+    intr = None
+    if intruder is not None:
+        cid = np.repeat(np.arange(K), [len(m) for m in locals_])
+        R = quat_to_body2world(quats)
+        sub_pos = pts[cid] + np.einsum("nij,nj->ni", R[cid], np.concatenate(locals_))
+        xy = (0.5 * hi[0], 0.5 * hi[1])
+        z = _place_intruder_on_bed(sub_pos, np.concatenate(radii), xy, intruder, 3 * rmax, 2 * rmax, 0.2 * rmin)
+        intr = make_intruder(intruder, 3 * rmax, (xy[0], xy[1], z), (0, 0, -0.5), half_height=2 * rmax,
+                             prop=(1, 1, 1, 0.05), motion=motion)
+    return assemble(params, pts, quats, rng.uniform(-vel, vel, (K, 3)), rng.uniform(-angvel, angvel, (K, 3)),
+                    props, locals_, radii, masses, cube=cube, cylinder=cyl, intruder=intr)
