@@ -131,11 +131,12 @@ def run_b200(args, world, rank, local):
         from datetime import timedelta
         dist.init_process_group(backend, timeout=timedelta(seconds=120))
     seed = 20260828 + rank
-    scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
+    scene = workload(args, seed)
     N, K = scene["params"]["NumberBody"], scene["params"]["ClumpNum"]
+    levels = 1 if scene.get("levels") is None else len(scene["levels"]["cell"])
 
     # ---- device-resident throughput -----------------------------------
-    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True, device=local)
+    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local)
     eng.step(args.warmup)
     eng.sync()
     st0 = eng.stats()
@@ -166,7 +167,7 @@ def run_b200(args, world, rank, local):
         sum(np.asarray(v).nbytes for v in scene["clump"].values())
     barrier(world)
     te0 = time.perf_counter()
-    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True, device=local)
+    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local)
     e2.step(args.warmup + args.steps)
     e2.sync()
     out = e2.clumps()
@@ -202,7 +203,7 @@ def run_b200(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy bed, no dataset)",
             "config": {"workload": WORKLOAD, "subspheres": N, "clumps": K, "precision": args.precision,
-                       "lanes": args.lanes, "graph": True, "pairs_listed": npairs,
+                       "lanes": args.lanes, "graph": bool(args.graph), "grid_levels": levels, "pairs_listed": npairs,
                        "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
                        "l2": "working set 60+ MB per step; not flushed between steps (state is resident by design)",
                        "parallelism": f"replicas x{world} (independent scenes)"},
@@ -221,6 +222,13 @@ def run_b200(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def workload(args, seed):
+    """The cfg1 scene with the hierarchical-grid levels nbc_choose_levels picks."""
+    import nbc
+    scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
+    return nbc.with_levels(scene) if args.levels else scene
 
 
 def algorithmic_contact_bytes(N, K, npairs, precision):
@@ -242,7 +250,7 @@ def cpu_baseline(args):
     """The FP64 CPU oracle on a bounded sample of the same workload."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    scene = sg.make_cfg1(n_clumps=args.clumps, seed=20260828, steps=10)
+    scene = workload(args, 20260828)
     threads = 1
     o = oracle.OracleScene(scene, threads=threads)
     o.step(1)  # first step includes the initial list build, like the GPU warm-up
@@ -268,7 +276,7 @@ def run_reference(args, world, rank, local):
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
-    scene = sg.make_cfg1(n_clumps=args.clumps, seed=20260828, steps=args.warmup + args.steps)
+    scene = workload(args, 20260828)
     N = scene["params"]["NumberBody"]
     o = oracle.OracleScene(scene, threads=threads)
     t = time.perf_counter()
@@ -300,10 +308,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
-    ap.add_argument("--lanes", type=int, default=16)
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per subsphere in the contact kernel (0 = engine default)")
     ap.add_argument("--clumps", type=int, default=50_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graph", type=int, default=1, help="1: CUDA graph per step; 0: eager launches (for ncu)")
+    ap.add_argument("--levels", type=int, default=1, help="1: hierarchical grid chosen by nbc_choose_levels")
     ap.add_argument("--profile", action="store_true",
                     help="short run for profilers: warm-up + timed steps only, no e2e / CPU legs")
     args = ap.parse_args()

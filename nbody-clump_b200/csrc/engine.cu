@@ -41,18 +41,6 @@ struct ArgError : std::runtime_error {
                             __FILE__ + ":" + std::to_string(__LINE__));                      \
     } while (0)
 
-__global__ void k_setcond(cudaGraphConditionalHandle h, const int* flag, const int* halt) {
-    cudaGraphSetConditional(h, (*flag && !*halt) ? 1u : 0u);
-}
-
-// after every contact pass: count it, and advance the spring-history
-// generation so the next pass reads what this one wrote
-__global__ void k_count_contact(int* gstep, int* hgen, const int* halt) {
-    if (!*halt) {
-        *gstep += 1;
-        *hgen += 1;
-    }
-}
 
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
@@ -119,10 +107,17 @@ class EngineT final : public EngineBase {
             int before = read_gstep();
             for (int i = 0; i < chunk; i++) launch_graph();
             CK(cudaStreamSynchronize(stream_));
-            int done = read_gstep() - before;
-            steps_done_ += done;
-            left -= done;
-            if (done < chunk) recover_halt();
+            int started = read_gstep() - before;
+            if (read_int(h_.halt)) {
+                // the last step started stopped at its rebuild: finish it on the host path
+                steps_done_ += started - 1;
+                left -= started - 1;
+                recover_halt();
+                left -= 1;
+            } else {
+                steps_done_ += started;
+                left -= started;
+            }
         }
         CK(cudaStreamSynchronize(stream_));
         check_errors();
@@ -350,6 +345,8 @@ class EngineT final : public EngineBase {
     Dev* d_ = nullptr;   // device table
     int S_ = 0, N_ = 0, K_ = 0, lanes_ = 16, passes_ = 0, rs_blocks_ = 0;
     bool hgrid_ = false;
+    bool first_list_ = true;
+    int search_lanes_ = 8;
     int ring_len_ = 1;
     std::vector<ScenePar> hpar_;
     std::vector<int> start_step_;
@@ -410,7 +407,8 @@ class EngineT final : public EngineBase {
         CK(cudaSetDevice(opt_.device));
         CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CK(cudaMallocHost(&hflag_, 4 * sizeof(int)));
-        lanes_ = opt_.lanes == 8 || opt_.lanes == 16 || opt_.lanes == 32 ? opt_.lanes : 16;
+        lanes_ = opt_.lanes == 1 || opt_.lanes == 2 || opt_.lanes == 4 || opt_.lanes == 8 || opt_.lanes == 16 ||
+                         opt_.lanes == 32 ? opt_.lanes : 4;
         const int spb = CT_THREADS / lanes_;
         S_ = (int)sc.size();
         hpar_.resize(S_);
@@ -570,6 +568,7 @@ class EngineT final : public EngineBase {
         h_.bhist = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N); h_.bhist2 = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N);
         h_.bbits = mem_.alloc<uint16_t>(N); h_.bbits2 = mem_.alloc<uint16_t>(N);
         h_.fsum = mem_.alloc<R4<R>>(2 * N);
+        h_.fbnd = mem_.alloc<R4<R>>(2 * N);
         h_.cpos = mem_.alloc<double4>(K_); h_.cvel = mem_.alloc<double4>(K_); h_.cw = mem_.alloc<double4>(K_);
         h_.cq = mem_.alloc<double4>(K_); h_.cprop = mem_.alloc<double4>(K_);
         h_.cF = mem_.alloc<double4>(K_); h_.cT = mem_.alloc<double4>(K_);
@@ -582,6 +581,7 @@ class EngineT final : public EngineBase {
         h_.lcur = flags + 3;
         h_.hgen = flags + 4;
         h_.gstep = flags + 5;
+        h_.kc_done = flags + 6;
         h_.kA = mem_.alloc<int>(N); h_.vA = mem_.alloc<int>(N); h_.kB = mem_.alloc<int>(N); h_.vB = mem_.alloc<int>(N);
         h_.hist = mem_.alloc<int>((size_t)256 * rs_blocks_);
         h_.perm = mem_.alloc<int>(N);
@@ -646,11 +646,14 @@ class EngineT final : public EngineBase {
     }
     static size_t hist_bytes(long long cap) { return (size_t)cap * (2 * sizeof(R4<R>) + sizeof(R)); }
 
+    double slack() const { return opt_.pair_slack >= 1.0 ? opt_.pair_slack : 1.6; }
     // grow the pair buffers, keeping the current list and history generation
     void grow_pairs(long long need) {
         refresh_dev();
-        const double slack = opt_.pair_slack > 1.0 ? opt_.pair_slack : 1.6;
-        long long cap = std::max<long long>((long long)(need * slack), (long long)h_.cap + 1024);
+        resize_pairs(std::max<long long>((long long)(need * slack()), (long long)h_.cap + 1024));
+    }
+    void resize_pairs(long long cap) {
+        refresh_dev();
         Dev old = h_;
         int lc = read_int(h_.lcur), hg = read_int(h_.hgen);
         const PairList& Lo = old.L[lc & 1];
@@ -741,9 +744,9 @@ class EngineT final : public EngineBase {
     }
 
     // ---- launches -------------------------------------------------------------
-    void launch_clump(int do_pre) {
+    void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
         int n = K_ + S_;
-        k_clump<R><<<cdiv(n, 128), 128, 0, stream_>>>(d_, do_pre);
+        k_clump<R><<<cdiv(n, 128), 128, 0, stream_>>>(d_, do_pre, cond, use_cond);
         CK(cudaGetLastError());
         if (!capturing_ && timing_) launches_ += 1;
     }
@@ -753,6 +756,9 @@ class EngineT final : public EngineBase {
             CK(cudaMemsetAsync(h_.xfcn, 0, (size_t)h_.cap * sizeof(R4<R>), stream_));
             CK(cudaMemsetAsync(h_.xcpt, 0, (size_t)h_.cap * sizeof(double4), stream_));
         }
+        if (exp) k_boundary<R, true><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream_>>>(d_);
+        else k_boundary<R, false><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream_>>>(d_);
+        if (!capturing_ && timing_) launches_ += 1;
         dim3 g(h_.cblocks);
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (capturing_) {
@@ -767,9 +773,12 @@ class EngineT final : public EngineBase {
 #define NBC_CT(L)                                                                   \
     if (exp) k_contact<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);             \
     else k_contact<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
-        if (lanes_ == 8) { NBC_CT(8) }
+        if (lanes_ == 1) { NBC_CT(1) }
+        else if (lanes_ == 2) { NBC_CT(2) }
+        else if (lanes_ == 4) { NBC_CT(4) }
+        else if (lanes_ == 16) { NBC_CT(16) }
         else if (lanes_ == 32) { NBC_CT(32) }
-        else { NBC_CT(16) }
+        else { NBC_CT(8) }
 #undef NBC_CT
         CK(cudaGetLastError());
         if (capturing_) {
@@ -778,8 +787,7 @@ class EngineT final : public EngineBase {
         } else if (e1) {
             CK(cudaEventRecord(e1, stream_));
         }
-        k_count_contact<<<1, 1, 0, stream_>>>(h_.gstep, h_.hgen, h_.halt);
-        if (!capturing_ && timing_) launches_ += 2;
+        if (!capturing_ && timing_) launches_ += 1;
     }
     void scan(int* a, int n) {
         int nb = cdiv(n, SC_TILE);
@@ -804,10 +812,14 @@ class EngineT final : public EngineBase {
         k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_end, h_.cells, -1);
         k_cellrange<<<cdiv(N_, B), B, 0, stream_>>>(d_, ki, vi);
         k_reorder<R><<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        const int sb = cdiv(N_, SEARCH_WARPS);
+        const int sl = search_lanes_;
+        const int sb = cdiv(N_, SEARCH_THREADS / sl);
         k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, N_ + 1, 0);
         k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, N_ + 1, 0);
-        k_count<<<sb, 32 * SEARCH_WARPS, 0, stream_>>>(d_);
+        if (sl == 4) k_count<4><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 16) k_count<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_count<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_count<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
         scan(h_.cnt_f, N_ + 1);
         scan(h_.cnt_b, N_ + 1);
         CK(cudaGetLastError());
@@ -816,11 +828,20 @@ class EngineT final : public EngineBase {
             CK(cudaMemcpyAsync(hflag_ + 1, h_.cnt_b + N_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
             CK(cudaStreamSynchronize(stream_));
             long long need = std::max(hflag_[0], hflag_[1]);
-            if (need > h_.cap) grow_pairs(need);
+            if (first_list_) {
+                // size the pair buffers to the first list: capacity = slack x pairs
+                resize_pairs(std::max<long long>(1024, (long long)(need * slack())));
+                first_list_ = false;
+            } else if (need > h_.cap) {
+                grow_pairs(need);
+            }
         }
         k_check_cap<<<1, 1, 0, stream_>>>(d_);
         if (hgrid_) k_fill_i<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, N_, 0);
-        k_fill<<<sb, 32 * SEARCH_WARPS, 0, stream_>>>(d_);
+        if (sl == 4) k_fill<4><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 16) k_fill<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_fill<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_fill<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
         if (hgrid_) k_xsort<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_carry<R><<<cdiv(std::max(h_.cap, 1), 256), 256, 0, stream_>>>(d_);
@@ -847,8 +868,7 @@ class EngineT final : public EngineBase {
         cudaGraphConditionalHandle hnd;
         CK(cudaGraphConditionalHandleCreate(&hnd, graph_, 0, cudaGraphCondAssignDefault));
         CK(cudaStreamBeginCaptureToGraph(stream_, graph_, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        launch_clump(1);
-        k_setcond<<<1, 1, 0, stream_>>>(hnd, h_.any_rebuild, h_.halt);
+        launch_clump(1, hnd, 1);
         cudaStreamCaptureStatus st;
         const cudaGraphNode_t* deps = nullptr;
         size_t ndeps = 0;
@@ -886,7 +906,7 @@ class EngineT final : public EngineBase {
             auto pr = next_pair();
             CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[0], pr.first));
             CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[1], pr.second));
-            launches_ += 4;
+            launches_ += 3;
         }
         CK(cudaGraphLaunch(gexec_, stream_));
     }

@@ -33,12 +33,21 @@ constexpr int INTRA = (int)0x80000000u;
 // 113-138), ComputeTorqueFromWorldPos_Kernel + reduce_by_key
 // (src/dem_clumpsphere.cu:86-151), IntegratePene_Before_cuk and
 // Integrate_After_cuk (src/dem_integrate_penetrator.cu:3-113).
+//
+// A step (do_pre) also advances the spring-history generation so the next
+// contact pass reads what the previous one wrote, and counts itself; the last
+// block to finish sets the graph's rebuild condition (when given a handle).
 template <typename R>
-__global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int do_pre) {
+__global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int do_pre,
+                                               cudaGraphConditionalHandle cond, int use_cond) {
     const Dev& d = *dp;
     if (*d.halt) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int post = *d.post_pending;
+    if (do_pre && t == 0) {
+        *d.hgen += 1;
+        *d.gstep += 1;
+    }
     if (t < d.K) {
         const int k = t;
         const ScenePar& P = d.par[d.csid[k]];
@@ -127,8 +136,8 @@ __global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int d
                 ka[i] = pack<R>(cvt<R>(arm), R(0));
             }
             if (moved) {
-                d.dyn[d.csid[k]].rebuild = 1;
-                *d.any_rebuild = 1;
+                atomicExch(&d.dyn[d.csid[k]].rebuild, 1);
+                atomicExch(d.any_rebuild, 1);
             }
             d.cpos[k] = cp;
             d.cvel[k] = make_double4(v.x, v.y, v.z, 0.0);
@@ -176,6 +185,16 @@ __global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int d
                 }
             } else {
                 for (int c = 0; c < 3; c++) y.intr_p[c] = y.intr_p[c] + Dt * y.intr_v[c];
+            }
+        }
+    }
+    if (use_cond) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(d.kc_done, 1) == (int)gridDim.x - 1) {
+                *d.kc_done = 0;
+                cudaGraphSetConditional(cond, atomicAdd(d.any_rebuild, 0) ? 1u : 0u);
             }
         }
     }
@@ -407,11 +426,15 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
 // coarsest); a pair across levels is owned by the coarser subsphere: the
 // finer one records a back entry, the coarser one a front entry, placed after
 // its same-level front entries in ascending order of the finer partner.
-constexpr int SEARCH_WARPS = 4;  // subspheres per 128-thread block
+constexpr int SEARCH_THREADS = 128;
 
-template <bool FILL>
+// SL lanes (4, 8, 16 or 32) search for one subsphere; lane masks and ballots
+// are restricted to the lane group so groups of one warp proceed independently
+template <bool FILL, int SL>
 __device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, const PairList& Nw, int i, int lane,
                                             int& nf_out, int& nb_out, int& nx_out) {
+    const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
+    const int gshift = (threadIdx.x & 31) & ~(SL - 1);
     const double4 pi = d.posr2[i];
     const int ci = d.clump_id2[i];
     const int my = P.levels > 1 ? d.level2[i] : 0;
@@ -453,7 +476,7 @@ __device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, con
                     }
                 }
                 if (s == -1) continue;
-                for (int k0 = s; k0 < e; k0 += 32) {
+                for (int k0 = s; k0 < e; k0 += SL) {
                     const int j = k0 + lane;
                     bool hit = false;
                     if (j < e && j != i) {
@@ -466,8 +489,8 @@ __device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, con
                     const bool front = hit && same && i < j;
                     const bool back = hit && !front;
                     const bool cross = hit && !same;
-                    const unsigned fm = __ballot_sync(0xffffffffu, front);
-                    const unsigned bm = __ballot_sync(0xffffffffu, back);
+                    const unsigned fm = __ballot_sync(gm, front) >> gshift;
+                    const unsigned bm = __ballot_sync(gm, back) >> gshift;
                     if (FILL && hit) {
                         const int flag = d.clump_id2[j] == ci ? INTRA : 0;
                         if (front) {
@@ -488,7 +511,7 @@ __device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, con
                     if (!FILL && cross) atomicAdd(&d.cnt_f[j], 1);
                     nf += __popc(fm);
                     nb += __popc(bm);
-                    nx += __popc(__ballot_sync(0xffffffffu, cross));
+                    nx += __popc(__ballot_sync(gm, cross));
                 }
             }
         }
@@ -500,11 +523,12 @@ __device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, con
 
 // counts: cnt_f[i] = same-level front entries + cross-level entries claimed
 // by finer partners (added with integer atomics), cnt_b[i] = back entries
-static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_count(const Dev* __restrict__ dp) {
+template <int SL>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_count(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * SEARCH_WARPS + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int lane = threadIdx.x % SL;
     if (i >= d.N) return;
     const int s = d.sid[i];
     const ScenePar& P = d.par[s];
@@ -519,7 +543,7 @@ static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_count(const Dev* _
     }
     int nf = 0, nb = 0, nx = 0;
     if (d.key2[i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
-        warp_search<false>(d, P, d.L[0], i, lane, nf, nb, nx);
+        warp_search<false, SL>(d, P, d.L[0], i, lane, nf, nb, nx);
     if (lane == 0) {
         atomicAdd(&d.cnt_f[i], nf);
         d.cnt_b[i] = nb;
@@ -538,11 +562,12 @@ static __global__ void k_check_cap(const Dev* __restrict__ dp) {
     }
 }
 
-static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_fill(const Dev* __restrict__ dp) {
+template <int SL>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_fill(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * SEARCH_WARPS + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int lane = threadIdx.x % SL;
     if (i >= d.N) return;
     const int s = d.sid[i];
     const ScenePar& P = d.par[s];
@@ -556,14 +581,14 @@ static __global__ void __launch_bounds__(32 * SEARCH_WARPS) k_fill(const Dev* __
     if (!d.dyn[s].rebuild) {
         const PairList& O = d.L[*d.lcur & 1];
         const int of = O.row[i], nf = O.row[i + 1] - of;
-        for (int g = lane; g < nf; g += 32) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
+        for (int g = lane; g < nf; g += SL) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
         const int ob = O.brow[i], nb = O.brow[i + 1] - ob;
-        for (int g = lane; g < nb; g += 32) Nw.bnbr[rb + g] = O.bnbr[ob + g];
+        for (int g = lane; g < nb; g += SL) Nw.bnbr[rb + g] = O.bnbr[ob + g];
         return;
     }
     if (d.key2[i] == P.cell_off + P.cellnum - 1) return;
     int nf, nb, nx;
-    warp_search<true>(d, P, Nw, i, lane, nf, nb, nx);
+    warp_search<true, SL>(d, P, Nw, i, lane, nf, nb, nx);
 }
 
 // hierarchical grid: the cross-level entries of each owner row in ascending
@@ -773,6 +798,16 @@ template <typename R> struct Body {
 };
 
 template <typename R>
+__device__ __forceinline__ void load_kin(const Dev& d, int i, Body<R>& b) {
+    const R4<R>* kv = (const R4<R>*)d.kin;
+    R4<R> a = kv[i], w = kv[d.N + i], r = kv[2 * d.N + i];
+    b.v = xyz<R>(a);
+    b.m = a.w;
+    b.w = xyz<R>(w);
+    b.arm = xyz<R>(r);
+}
+
+template <typename R>
 __device__ __forceinline__ Body<R> load_body(const Dev& d, int i) {
     const R4<R>* kv = (const R4<R>*)d.kin;
     Body<R> b;
@@ -866,137 +901,81 @@ __device__ __forceinline__ R group_sum(R v, unsigned mask) {
 }
 
 constexpr int CT_THREADS = 256;
+constexpr int BD_THREADS = 128;
 
-template <typename R, int LANES, bool EXPORT>
-__global__ void __launch_bounds__(CT_THREADS) k_contact(const Dev* __restrict__ dp) {
+// Walls and intruder, one thread per subsphere: the face tests of
+// CubeWallInteraction_clump_cuk (src/dem_force_cube_wall_clump.cu:185-298),
+// the region tests of CylindWallInteraction_cuk (src/dem_force_cylind_wall.cu:
+// 152-237) with clump kinematics, PrePenetrator / GetSphereIntruderContact /
+// ForcePene_clump_cuk (src/dem_contact_penetrator.cu:8-84,
+// src/dem_sphere_intruder.cuh:20-51, src/dem_force_penetrator_clump.cu:4-182).
+// Writes the summed boundary force/torque where some slot is in contact and
+// the slot mask; the intruder totals go to fixed-point accumulators.
+template <typename R, bool EXPORT>
+__global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    constexpr int SPB = CT_THREADS / LANES;
-    const int s = d.sblk_scene[blockIdx.x];
+    const int i = blockIdx.x * BD_THREADS + threadIdx.x;
+    if (i >= d.N) return;
+    const int s = d.sid[i];
     const ScenePar& P = d.par[s];
-    const int grp = threadIdx.x / LANES, lane = threadIdx.x % LANES;
-    const int i = P.sub_off + (blockIdx.x - P.cblk_off) * SPB + grp;
-    if (i >= P.sub_off + P.nsub) return;
-    const unsigned mask = group_mask<LANES>();
-    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-
-    Law<R> L;
-    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
-    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
-    const R coh = (R)P.cohesion;
-
-    const int lc = *d.lcur, hg = *d.hgen;
-    const PairList& Lst = d.L[lc & 1];
-    const size_t cap = (size_t)d.cap;
-    const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
-    R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
-    const uint8_t* ti = d.touch[hg & 1];
-    uint8_t* to = d.touch[(hg + 1) & 1];
-
-    const Body<R> me = load_body<R>(d, i);
-    V3<R> F = v3<R>(0, 0, 0), T = F;
-    V3<R> Fw = F, Tw = F, Fi = F, Ti = F;  // export parts
-
-    // front (owner) entries
-    const int rs = Lst.row[i], re = Lst.row[i + 1];
-    for (int k = rs + lane; k < re; k += LANES) {
-        const int jr = Lst.nbr[k];
-        if (jr < 0) continue;  // pair inside one clump (src/dem_force_clump.cu:18-19)
-        const Body<R> ot = load_body<R>(d, jr);
-        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
-        const double dx = ot.p.x - me.p.x, dy = ot.p.y - me.p.y, dz = ot.p.z - me.p.z;
-        const double dl = sqrt(dx * dx + dy * dy + dz * dz);
-        if (!(me.p.w + ot.p.w - dl > 0.0)) { to[k] = 0; continue; }
-        if (ti[k]) hist_read<R>(Hi, cap, k, hs, ht, hr);
-        V3<R> fa, ta;
-        LawOut<R> o;
-        double Ap;
-        V3<double> nd;
-        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
-        F = F + fa;
-        T = T + ta;
-        hist_write<R>(Ho, cap, k, o.hs, o.ht, o.hr);
-        to[k] = 1;
-        if (EXPORT) {
-            R4<R>* xf = (R4<R>*)d.xfcn;
-            double4* xc = (double4*)d.xcpt;
-            xf[k] = pack<R>(-o.Fn, R(0));
-            xc[k] = make_double4(me.p.x + Ap * nd.x, me.p.y + Ap * nd.y, me.p.z + Ap * nd.z, 0.0);
-        }
-    }
-    // back entries: the owner's stored history, seen from this side
-    const int bs = Lst.brow[i], be = Lst.brow[i + 1];
-    for (int k = bs + lane; k < be; k += LANES) {
-        const int jr = Lst.bnbr[k];
-        if (jr < 0) continue;
-        const Body<R> ot = load_body<R>(d, jr);
-        const double dx = ot.p.x - me.p.x, dy = ot.p.y - me.p.y, dz = ot.p.z - me.p.z;
-        const double dl = sqrt(dx * dx + dy * dy + dz * dz);
-        if (!(me.p.w + ot.p.w - dl > 0.0)) continue;
-        const int q = Lst.bpair[k];
-        if (q < 0) continue;  // unreachable with a consistent list
-        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
-        if (ti[q]) {
-            hist_read<R>(Hi, cap, q, hs, ht, hr);
-            hs = -hs; ht = -ht; hr = -hr;
-        }
-        V3<R> fa, ta;
-        LawOut<R> o;
-        double Ap;
-        V3<double> nd;
-        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
-        F = F + fa;
-        T = T + ta;
-    }
-    if (EXPORT) { Fw = F; Tw = T; }  // temporarily hold the pair part
-
-    // boundary slots: walls (cube faces or cylinder regions) and the intruder
+    const size_t N = (size_t)d.N;
+    const double4 pp = d.posr[i];
+    const double r = pp.w;
     const int nwall = P.wall == WALL_CUBE ? 6 : (P.wall == WALL_CYL ? 3 : 0);
     const uint16_t bb_old = d.bbits[i];
     uint16_t bb_new = 0;
     R4<R>* BH = (R4<R>*)d.bhist;
-    const size_t N = (size_t)d.N;
-    V3<R> pF = v3<R>(0, 0, 0), pT = pF, iF = pF, iT = pF;
-    for (int slot = lane; slot < NB_SLOTS; slot += LANES) {
+    V3<R> wF = v3<R>(0, 0, 0), wT = wF, iF = wF, iT = wF;
+    Body<R> me;
+    bool have_kin = false;
+    Law<R> L;
+    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
+    const V3<double> RV = v3(pp.x - P.w_c[0], pp.y - P.w_c[1], pp.z - P.w_c[2]);
+    // cylinder geometry shared by its three regions
+    double ERRc = 0, nrmc = 0;
+    V3<double> RVbc = v3(0.0, 0.0, 0.0), RVtc = RVbc, axv = RVbc;
+    if (P.wall == WALL_CYL) {
+        axv = v3(P.cyl_axis[0], P.cyl_axis[1], P.cyl_axis[2]);
+        ERRc = dot(RV, axv);
+        RVbc = RV - ERRc * axv;
+        RVtc = ERRc * axv;
+        nrmc = len_floor(RVbc);
+    }
+    for (int slot = 0; slot < NB_SLOTS; slot++) {
         const bool is_wall = slot < nwall;
         const bool is_intr = slot == SLOT_INTR && P.has_intr;
         if (!is_wall && !is_intr) continue;
         double Apd = 0, Dnd = 0;
         V3<double> nd = v3(0.0, 0.0, 0.0), RVo = nd;
         bool on = false;
-        R Rij = (R)me.p.w, Mij = me.m, csm = R(2);
+        R Rij = (R)r, Mij = R(0), csm = R(2);
         V3<R> wv = v3<R>((R)P.w_v[0], (R)P.w_v[1], (R)P.w_v[2]);
         V3<R> ww = v3<R>((R)P.w_w[0], (R)P.w_w[1], (R)P.w_w[2]);
-        const V3<double> RV = v3(me.p.x - P.w_c[0], me.p.y - P.w_c[1], me.p.z - P.w_c[2]);
-        const double r = me.p.w;
         if (is_wall && P.wall == WALL_CUBE) {
-            // CubeWallInteraction_clump_cuk (src/dem_force_cube_wall_clump.cu:228-292)
             const int ax = slot >> 1;
             const bool up = (slot & 1) == 0;
-            const double e = (&RV.x)[ax], h = P.w_half[ax];
+            const double e = (ax == 0 ? RV.x : (ax == 1 ? RV.y : RV.z)), h = P.w_half[ax];
             on = up ? (e > 0 && e + r - h > 0) : (e < 0 && e - r + h < 0);
             if (on) {
+                const double o = (h / fabs(e)) * e;
                 RVo = RV;
-                (&RVo.x)[ax] = (h / fabs(e)) * e;
-                (&nd.x)[ax] = up ? -1.0 : 1.0;
-                const V3<double> RVn = RV - RVo;
-                Apd = dot(RVn, nd);
+                if (ax == 0) RVo.x = o; else if (ax == 1) RVo.y = o; else RVo.z = o;
+                const double sgn = up ? -1.0 : 1.0;
+                if (ax == 0) nd.x = sgn; else if (ax == 1) nd.y = sgn; else nd.z = sgn;
+                Apd = dot(RV - RVo, nd);
                 Dnd = r - Apd;
                 on = Dnd > 0.0;
             }
-        } else if (is_wall && P.wall == WALL_CYL) {
-            // CylindWallInteraction_cuk (src/dem_force_cylind_wall.cu:152-237)
-            const V3<double> axv = v3(P.cyl_axis[0], P.cyl_axis[1], P.cyl_axis[2]);
-            const double ERR = dot(RV, axv);
-            const V3<double> RVb = RV - ERR * axv, RVt = ERR * axv;
-            const double nrm = len_floor(RVb);
-            const double d_cap = fabs(ERR) - P.cyl_H + r;
-            const double d_side = nrm - P.cyl_R + r;
-            if (slot == 0) on = d_cap >= 1e-14 && ERR < 0;
-            else if (slot == 1) on = d_cap >= 1e-14 && ERR > 0;
+        } else if (is_wall) {
+            const double d_cap = fabs(ERRc) - P.cyl_H + r;
+            const double d_side = nrmc - P.cyl_R + r;
+            if (slot == 0) on = d_cap >= 1e-14 && ERRc < 0;
+            else if (slot == 1) on = d_cap >= 1e-14 && ERRc > 0;
             else on = d_side >= 1e-14;
             if (on) {
-                RVo = slot < 2 ? (P.cyl_H / fabs(ERR)) * RVt + RVb : (P.cyl_R / nrm) * RVb + RVt;
+                RVo = slot < 2 ? (P.cyl_H / fabs(ERRc)) * RVtc + RVbc : (P.cyl_R / nrmc) * RVbc + RVtc;
                 const V3<double> RVn = RV - RVo;
                 Dnd = r - len_floor(RVn);
                 on = Dnd > 0.0;
@@ -1007,15 +986,11 @@ __global__ void __launch_bounds__(CT_THREADS) k_contact(const Dev* __restrict__ 
                 }
             }
         } else {
-            // PrePenetrator / GetSphereIntruderContact / ForcePene_clump_cuk
-            // (src/dem_contact_penetrator.cu:8-84, src/dem_sphere_intruder.cuh:20-51,
-            // src/dem_force_penetrator_clump.cu:4-182)
             const SceneDyn& y = d.dyn[s];
-            const V3<double> RI = v3(me.p.x - y.intr_p[0], me.p.y - y.intr_p[1], me.p.z - y.intr_p[2]);
+            const V3<double> RI = v3(pp.x - y.intr_p[0], pp.y - y.intr_p[1], pp.z - y.intr_p[2]);
             wv = v3<R>((R)y.intr_v[0], (R)y.intr_v[1], (R)y.intr_v[2]);
             ww = v3<R>((R)P.intr_w[0], (R)P.intr_w[1], (R)P.intr_w[2]);
             csm = R(1);
-            if (P.intr_motion == 1) Mij = (R)(me.m * P.intr_mass / (me.m + P.intr_mass));
             if (P.intr_shape == 1) {
                 const double cd = len_floor(RI);
                 if (cd > 1.0e-15) nd = (1.0 / cd) * RI;
@@ -1054,6 +1029,13 @@ __global__ void __launch_bounds__(CT_THREADS) k_contact(const Dev* __restrict__ 
             if (on && P.intr_wait) atomicCAS(&d.dyn[s].intr_state, 0, 1);
         }
         if (!on) continue;
+        if (!have_kin) {
+            me.p = pp;
+            load_kin<R>(d, i, me);
+            have_kin = true;
+        }
+        if (is_intr) Mij = P.intr_motion == 1 ? (R)((double)me.m * P.intr_mass / ((double)me.m + P.intr_mass)) : me.m;
+        else Mij = me.m;
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         const size_t hb = (size_t)slot * 3 * N;
         if (bb_old & (1u << slot)) {
@@ -1088,36 +1070,148 @@ __global__ void __launch_bounds__(CT_THREADS) k_contact(const Dev* __restrict__ 
                 xi[3 * N + i] = pack<R>((cross(o.Ft, arm) - o.Mr) - o.Mt, R(0));
             }
         } else {
-            pF = pF + f;
-            pT = pT + t;
+            wF = wF + f;
+            wT = wT + t;
         }
     }
-    F = (F + pF) + iF;
-    T = (T + pT) + iT;
-    // reduce over the lane group
-    F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
-    T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
-    unsigned bits = bb_new;
-    for (int o = LANES / 2; o > 0; o >>= 1) bits |= __shfl_xor_sync(mask, bits, o);
+    d.bbits[i] = bb_new;
+    if (bb_new) {
+        R4<R>* fb = (R4<R>*)d.fbnd;
+        fb[i] = pack<R>(wF + iF, R(0));
+        fb[N + i] = pack<R>(wT + iT, R(0));
+    }
     if (EXPORT) {
-        V3<R>* parts[6] = {&Fw, &Tw, &pF, &pT, &iF, &iT};
         R4<R>* xp = (R4<R>*)d.xparts;
-        for (int c = 0; c < 6; c++) {
-            V3<R>& v = *parts[c];
-            v.x = group_sum<R, LANES>(v.x, mask); v.y = group_sum<R, LANES>(v.y, mask); v.z = group_sum<R, LANES>(v.z, mask);
-            if (lane == 0) xp[c * N + i] = pack<R>(v, R(0));
-        }
-        if (lane == 0 && !(bits & (1u << SLOT_INTR))) {
+        xp[2 * N + i] = pack<R>(wF, R(0));
+        xp[3 * N + i] = pack<R>(wT, R(0));
+        xp[4 * N + i] = pack<R>(iF, R(0));
+        xp[5 * N + i] = pack<R>(iT, R(0));
+        if (!(bb_new & (1u << SLOT_INTR))) {
             R4<R>* xi = (R4<R>*)d.xintr;
-            R4<R> z = pack<R>(v3<R>(0, 0, 0), R(0));
+            const R4<R> z = pack<R>(v3<R>(0, 0, 0), R(0));
             xi[i] = z; xi[N + i] = z; xi[2 * N + i] = z; xi[3 * N + i] = z;
         }
     }
+}
+
+// Overlap of a listed pair: the reference's test ri + rj - |d| > 0 in FP64
+// (src/dem_force_clump.cu:46-50), with the square root taken only when |d|^2
+// is within 1e-12 of (ri + rj)^2, so the decision is the reference's exactly.
+__device__ __forceinline__ bool overlaps(double4 a, double4 b) {
+    const double dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    const double s = a.w + b.w, s2 = s * s;
+    if (d2 > s2 * (1.0 + 1e-12)) return false;
+    if (d2 < s2 * (1.0 - 1e-12)) return true;
+    return a.w + b.w - sqrt(d2) > 0.0;
+}
+
+// Pairs, one lane group per subsphere: every pair of its front (owner) and
+// back lists, the owner's spring history read from the previous generation
+// and, for owner entries, the new history written; the boundary force from
+// k_boundary added in; the sum written once per subsphere.
+template <typename R, int LANES, bool EXPORT>
+__global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    constexpr int SPB = CT_THREADS / LANES;
+    const int s = d.sblk_scene[blockIdx.x];
+    const ScenePar& P = d.par[s];
+    const int grp = threadIdx.x / LANES, lane = threadIdx.x % LANES;
+    const int i = P.sub_off + (blockIdx.x - P.cblk_off) * SPB + grp;
+    if (i >= P.sub_off + P.nsub) return;
+    const unsigned mask = group_mask<LANES>();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
+
+    Law<R> L;
+    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
+    const R coh = (R)P.cohesion;
+
+    const int lc = *d.lcur, hg = *d.hgen;
+    const PairList& Lst = d.L[lc & 1];
+    const size_t cap = (size_t)d.cap;
+    const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
+    R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
+    const uint8_t* ti = d.touch[hg & 1];
+    uint8_t* to = d.touch[(hg + 1) & 1];
+
+    Body<R> me;
+    me.p = d.posr[i];
+    bool have_kin = false;
+    V3<R> F = v3<R>(0, 0, 0), T = F;
+
+    // front (owner) entries
+    const int rs = Lst.row[i], re = Lst.row[i + 1];
+    for (int k = rs + lane; k < re; k += LANES) {
+        const int jr = Lst.nbr[k];
+        if (jr < 0) continue;  // pair inside one clump (src/dem_force_clump.cu:18-19)
+        Body<R> ot;
+        ot.p = d.posr[jr];
+        if (!overlaps(me.p, ot.p)) { to[k] = 0; continue; }
+        if (!have_kin) { load_kin<R>(d, i, me); have_kin = true; }
+        load_kin<R>(d, jr, ot);
+        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+        if (ti[k]) hist_read<R>(Hi, cap, k, hs, ht, hr);
+        V3<R> fa, ta;
+        LawOut<R> o;
+        double Ap;
+        V3<double> nd;
+        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
+        F = F + fa;
+        T = T + ta;
+        hist_write<R>(Ho, cap, k, o.hs, o.ht, o.hr);
+        to[k] = 1;
+        if (EXPORT) {
+            R4<R>* xf = (R4<R>*)d.xfcn;
+            double4* xc = (double4*)d.xcpt;
+            xf[k] = pack<R>(-o.Fn, R(0));
+            xc[k] = make_double4(me.p.x + Ap * nd.x, me.p.y + Ap * nd.y, me.p.z + Ap * nd.z, 0.0);
+        }
+    }
+    // back entries: the owner's stored history, seen from this side
+    const int bs = Lst.brow[i], be = Lst.brow[i + 1];
+    for (int k = bs + lane; k < be; k += LANES) {
+        const int jr = Lst.bnbr[k];
+        if (jr < 0) continue;
+        Body<R> ot;
+        ot.p = d.posr[jr];
+        if (!overlaps(me.p, ot.p)) continue;
+        const int q = Lst.bpair[k];
+        if (q < 0) continue;  // unreachable with a consistent list
+        if (!have_kin) { load_kin<R>(d, i, me); have_kin = true; }
+        load_kin<R>(d, jr, ot);
+        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+        if (ti[q]) {
+            hist_read<R>(Hi, cap, q, hs, ht, hr);
+            hs = -hs; ht = -ht; hr = -hr;
+        }
+        V3<R> fa, ta;
+        LawOut<R> o;
+        double Ap;
+        V3<double> nd;
+        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
+        F = F + fa;
+        T = T + ta;
+    }
+    F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
+    T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
     if (lane == 0) {
+        const size_t N = (size_t)d.N;
+        if (EXPORT) {
+            R4<R>* xp = (R4<R>*)d.xparts;
+            xp[i] = pack<R>(F, R(0));
+            xp[N + i] = pack<R>(T, R(0));
+        }
+        if (d.bbits[i]) {
+            const R4<R>* fb = (const R4<R>*)d.fbnd;
+            const R4<R> bf = fb[i], bt = fb[N + i];
+            F = F + xyz<R>(bf);
+            T = T + xyz<R>(bt);
+        }
         R4<R>* fs = (R4<R>*)d.fsum;
         fs[i] = pack<R>(F, R(0));
         fs[N + i] = pack<R>(T, R(0));
-        d.bbits[i] = (uint16_t)bits;
         if (!(isfinite((double)F.x) && isfinite((double)F.y) && isfinite((double)F.z) &&
               isfinite((double)T.x) && isfinite((double)T.y) && isfinite((double)T.z)))
             atomicOr(&d.dyn[s].err, ERR_NONFINITE);

@@ -106,6 +106,7 @@ struct Dev {
     void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][3][N] boundary histories (Dv, Dt, Dr)
     uint16_t* bbits;  uint16_t* bbits2;  // [N] boundary slots in contact at the last step
     void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder)
+    void* fbnd;       // Real4 [2][N]: wall + intruder force and torque, valid where bbits != 0
     // clumps
     double4* cpos;    // xyz
     double4* cvel;
@@ -135,7 +136,8 @@ struct Dev {
     void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
-    int* gstep;       // contact passes completed (counts steps across graph launches)
+    int* gstep;       // steps started by k_clump (counts steps across graph launches)
+    int* kc_done;     // blocks of k_clump finished (last-block detection)
     // export (per pair), written by the export variant of the contact kernel
     void* xfcn;       // Real4 [cap] normal force on the owner (CacheFcn)
     void* xcpt;       // double4 [cap] contact point (CacheCpt)

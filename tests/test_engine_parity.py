@@ -274,3 +274,24 @@ def test_batch_results_equal_alone(golden_dir):
         assert both.stats(s)["rebuilds"] == e.stats(0)["rebuilds"]
         ib, ia = both.intruder(s), e.intruder(0)
         assert np.array_equal(ib["reaction"], ia["reaction"])
+
+
+def test_pair_capacity_overflow_recovers_identically(golden_dir):
+    """Pair buffers sized exactly to the first list (slack 1.0): a later,
+    longer list overflows inside a graph launch, the kernels stand still, the
+    host grows the buffers and replays that step's rebuild.  The result equals
+    a run that never overflowed."""
+    sc = _scene(golden_dir, "tetra_gravity")      # its list grows from 2963 to 2966 pairs
+    tight = nbc.Engine([sc], precision="mixed", use_graph=True, pair_slack=1.0)
+    roomy = nbc.Engine([sc], precision="mixed", use_graph=True, pair_slack=3.0)
+    tight.step(1)
+    bytes_first = tight.info()["device_bytes"]
+    tight.step(23)
+    assert tight.info()["device_bytes"] > bytes_first, "the capacity overflow path was not taken"
+    roomy.step(24)
+    tight.sync()
+    roomy.sync()
+    for k in ("pos", "vel", "angvel", "quat"):
+        assert np.array_equal(tight.clumps()[k], roomy.clumps()[k]), k
+    st = tight.stats()
+    assert st["err"] == 0 and st["steps"] == 24
