@@ -924,6 +924,39 @@ __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__
     const double r = pp.w;
     const int nwall = P.wall == WALL_CUBE ? 6 : (P.wall == WALL_CYL ? 3 : 0);
     const uint16_t bb_old = d.bbits[i];
+    {
+        // conservative early-out: clearly inside every wall and outside the
+        // intruder's bounding sphere (margins of 1e-9 relative cover rounding)
+        const double ex = pp.x - P.w_c[0], ey = pp.y - P.w_c[1], ez = pp.z - P.w_c[2];
+        bool near = false;
+        if (P.wall == WALL_CUBE) {
+            near = fabs(ex) + r >= P.w_half[0] * (1 - 1e-9) || fabs(ey) + r >= P.w_half[1] * (1 - 1e-9) ||
+                   fabs(ez) + r >= P.w_half[2] * (1 - 1e-9);
+        } else if (P.wall == WALL_CYL) {
+            const double ax = ex * P.cyl_axis[0] + ey * P.cyl_axis[1] + ez * P.cyl_axis[2];
+            const double rr = ex * ex + ey * ey + ez * ez - ax * ax;
+            const double in = P.cyl_R - r;
+            near = fabs(ax) + r >= P.cyl_H * (1 - 1e-9) || in <= 0 || rr >= in * in * (1 - 1e-9);
+        }
+        if (!near && P.has_intr) {
+            const SceneDyn& y = d.dyn[s];
+            const double qx = pp.x - y.intr_p[0], qy = pp.y - y.intr_p[1], qz = pp.z - y.intr_p[2];
+            const double reach = (P.intr_shape == 1 ? P.intr_R : sqrt(P.intr_R * P.intr_R + P.intr_H * P.intr_H) +
+                                  0.80 * P.cell[0] * 1.7320508075688772) + r;
+            near = qx * qx + qy * qy + qz * qz <= reach * reach * (1 + 1e-9);
+        }
+        if (!near) {
+            if (bb_old) d.bbits[i] = 0;
+            if (EXPORT) {
+                R4<R>* xp = (R4<R>*)d.xparts;
+                R4<R>* xi = (R4<R>*)d.xintr;
+                const R4<R> z = pack<R>(v3<R>(0, 0, 0), R(0));
+                for (int c = 2; c < 6; c++) xp[(size_t)c * N + i] = z;
+                for (int c = 0; c < 4; c++) xi[(size_t)c * N + i] = z;
+            }
+            return;
+        }
+    }
     uint16_t bb_new = 0;
     R4<R>* BH = (R4<R>*)d.bhist;
     V3<R> wF = v3<R>(0, 0, 0), wT = wF, iF = wF, iT = wF;
