@@ -136,11 +136,12 @@ def run_b200(args, world, rank, local):
     levels = 1 if scene.get("levels") is None else len(scene["levels"]["cell"])
 
     # ---- device-resident throughput -----------------------------------
-    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local)
+    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local,
+                     pair_slack=args.pair_slack, search_lanes=args.search_lanes)
     eng.step(args.warmup)
     eng.sync()
     st0 = eng.stats()
-    eng.timing_enable(True)
+    eng.timing_enable(2 if args.profile else 1)
     barrier(world)
     pair_samples = []
     with ClockSampler(local) as clk:
@@ -163,7 +164,8 @@ def run_b200(args, world, rank, local):
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": secs * 1e3 / args.steps,
                               "contact_ms_avg": tm["contact_ms"] / max(1, tm["contact_launches"]),
-                              "npairs": st1["npairs"], "rebuilds": st1["rebuilds"] - st0["rebuilds"]}), flush=True)
+                              "npairs": st1["npairs"], "rebuilds": st1["rebuilds"] - st0["rebuilds"],
+                              "phases_ms": eng.timing_phases()}), flush=True)
         return
 
     # ---- end to end through the C ABI with host buffers -----------------
@@ -173,7 +175,8 @@ def run_b200(args, world, rank, local):
         sum(np.asarray(v).nbytes for v in scene["clump"].values())
     barrier(world)
     te0 = time.perf_counter()
-    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local)
+    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local,
+                    pair_slack=args.pair_slack, search_lanes=args.search_lanes)
     e2.step(args.warmup + args.steps)
     e2.sync()
     out = e2.clumps()
@@ -238,10 +241,27 @@ def eng_lanes(args):
 
 
 def workload(args, seed):
-    """The cfg1 scene with the hierarchical-grid levels nbc_choose_levels picks."""
+    """The cfg1 scene with the hierarchical-grid levels nbc_choose_levels picks
+    (or, with --scene, a scene saved by --save-state)."""
     import nbc
-    scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
+    if args.scene:
+        scene = sg.scene_from_npz(args.scene)
+    else:
+        scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
     return nbc.with_levels(scene) if args.levels else scene
+
+
+def save_state(args):
+    """Advance the workload --advance steps and save the state it reached as a
+    scene file (a late-settle starting point for short profiler runs)."""
+    import nbc
+    scene = workload(args, 20260828)
+    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True)
+    eng.step(args.advance)
+    out = eng.restart_scene(scene)
+    out.pop("levels", None)
+    sg.scene_to_npz(out, args.save_state)
+    print(json.dumps({"saved": args.save_state, "steps": args.advance, "npairs": eng.stats()["npairs"]}), flush=True)
 
 
 def algorithmic_contact_bytes(N, K, npairs, precision):
@@ -329,10 +349,18 @@ def main():
     ap.add_argument("--levels", type=int, default=1, help="1: hierarchical grid chosen by nbc_choose_levels")
     ap.add_argument("--profile", action="store_true",
                     help="short run for profilers: warm-up + timed steps only, no e2e / CPU legs")
+    ap.add_argument("--pair-slack", type=float, default=0.0,
+                    help="pair buffer capacity over the first list (0 = engine default)")
+    ap.add_argument("--search-lanes", type=int, default=0, help="lanes per subsphere in the neighbour search")
+    ap.add_argument("--scene", default=None, help="run this scene file instead of generating cfg1")
+    ap.add_argument("--save-state", default=None, help="advance --advance steps, save the state to this file, exit")
+    ap.add_argument("--advance", type=int, default=18000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)
-    if args.impl == "reference":
+    if args.save_state:
+        save_state(args)
+    elif args.impl == "reference":
         run_reference(args, world, rank, local)
     else:
         run_b200(args, world, rank, local)

@@ -88,10 +88,12 @@ typedef struct {
 
 typedef struct {
     int precision;      /* NBC_PREC_* */
-    int lanes;          /* lanes per subsphere in the contact kernel: 0 = autotuned, 8, 16 or 32 */
+    int lanes;          /* lanes per subsphere in the contact kernel: 1, 2, 4, 8, 16 or 32 (0 = 4) */
     int use_graph;      /* 1: one CUDA graph per step with a conditional rebuild node */
     int device;         /* CUDA device ordinal */
-    double pair_slack;  /* pair capacity = slack * pairs of the first list (0 = 1.6) */
+    double pair_slack;  /* pair capacity = slack * pairs of the first list; 0 = 1.6 and at least
+                           the reference's own n_sub * BranchLmtLen/2 as far as 30% of free memory allows */
+    int search_lanes;   /* lanes per subsphere in the neighbour search: 8, 16 or 32 (0 = 8) */
 } nbc_options;
 
 typedef struct nbc_engine nbc_engine;
@@ -157,13 +159,21 @@ nbc_status nbc_get_intruder_diag(nbc_engine* e, int scene, double* diag);
 /* reaction force/torque recorded at each of the last `count` completed
  * steps (CacheFc/CacheTc of src/dem_integrate_penetrator.cu:108-109), [count][6] */
 nbc_status nbc_get_intruder_history(nbc_engine* e, int scene, int count, double* out);
-/* CUDA-event timing of the contact kernel on the engine's stream (also
- * inside graph launches): enable resets the totals; read returns the summed
- * kernel time in ms, the number of timed contact launches, the number of
- * engine kernels launched and the number of rebuilds since enabling */
+/* CUDA-event timing on the engine's streams (also inside graph launches, as
+ * event nodes): enable = 1 times the contact kernel, 2 also every phase of
+ * the step (nbc_timing_phases), 0 switches timing off; enabling resets the
+ * totals.  read returns the summed contact-kernel time in ms, the number of
+ * timed steps, the number of engine kernels launched and the number of
+ * rebuilds since enabling */
 nbc_status nbc_timing_enable(nbc_engine* e, int enable);
 nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launches, long long* kernel_launches,
                            int* rebuilds);
+/* (timing level 2) mean CUDA-event time per timed step, in ms, of its
+ * phases: [0] k_clump, [1] the rebuild node (its condition evaluated, the
+ * rebuild when taken), [2] k_boundary, [3] k_contact, [4] the whole step from
+ * its first kernel to its last (k_boundary runs beside k_contact); no
+ * reference counterpart */
+nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 

@@ -72,7 +72,8 @@ void nbc_default_options(nbc_options* o) {
     o->lanes = 0;
     o->use_graph = 1;
     o->device = 0;
-    o->pair_slack = 1.6;
+    o->pair_slack = 0.0;
+    o->search_lanes = 0;
 }
 
 nbc_status nbc_create(const nbc_scene_desc* const* scenes, int n, const nbc_options* opt, nbc_engine** out) {
@@ -181,12 +182,17 @@ nbc_status nbc_get_intruder_history(nbc_engine* e, int s, int count, double* out
 
 nbc_status nbc_timing_enable(nbc_engine* e, int on) {
     if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
-    return guard([&] { e->eng->timing_enable(on != 0); });
+    return guard([&] { e->eng->timing_enable(on); });
 }
 
 nbc_status nbc_timing_read(nbc_engine* e, double* ms, int* nc, long long* nk, int* nr) {
     if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
     return guard([&] { e->eng->timing_read(ms, nc, nk, nr); });
+}
+
+nbc_status nbc_timing_phases(nbc_engine* e, double* ms) {
+    if (!e || !e->eng || !ms) return fail(NBC_ERR_ARG, "null engine or output");
+    return guard([&] { e->eng->timing_phases(ms); });
 }
 
 nbc_status nbc_engine_info(nbc_engine* e, double* bytes, double* ms) {

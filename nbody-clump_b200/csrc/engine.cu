@@ -76,8 +76,16 @@ class EngineT final : public EngineBase {
    public:
     EngineT(const std::vector<const nbc_scene_desc*>& sc, const nbc_options& opt) : opt_(opt) { setup(sc); }
     ~EngineT() override {
-        if (gexec_) cudaGraphExecDestroy(gexec_);
-        if (graph_) cudaGraphDestroy(graph_);
+        for (int t = 0; t < 3; t++) {
+            if (gexec_[t]) cudaGraphExecDestroy(gexec_[t]);
+            if (graph_[t]) cudaGraphDestroy(graph_[t]);
+        }
+        for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+        for (auto& row : gev_)
+            for (cudaEvent_t e : row) if (e) cudaEventDestroy(e);
+        if (ev_fork_) cudaEventDestroy(ev_fork_);
+        if (ev_join_) cudaEventDestroy(ev_join_);
+        if (stream2_) cudaStreamDestroy(stream2_);
         if (stream_) cudaStreamDestroy(stream_);
         if (hflag_) cudaFreeHost(hflag_);
     }
@@ -102,7 +110,7 @@ class EngineT final : public EngineBase {
                 left -= 1;
                 continue;
             }
-            if (!gexec_) capture();
+            if (!gexec_[timing_]) capture(timing_);
             int chunk = exp ? left - 1 : left;
             int before = read_gstep();
             for (int i = 0; i < chunk; i++) launch_graph();
@@ -206,11 +214,28 @@ class EngineT final : public EngineBase {
             }
         }
     }
+    // pair sum (k_contact) plus, where a boundary was touched, the wall and
+    // intruder force (k_boundary), added in Real as k_clump adds them
     void get_sub_forces(int s, double* f, double* t) override {
         refresh_dev();
         const ScenePar& P = hpar_[s];
-        pull_r4(h_.fsum, P.sub_off, P.nsub, f);
-        pull_r4((char*)h_.fsum + (size_t)N_ * sizeof(R4<R>), P.sub_off, P.nsub, t);
+        const int n = P.nsub, o = P.sub_off;
+        std::vector<uint16_t> bb(n);
+        CK(cudaMemcpy(bb.data(), h_.bbits + o, n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 2; c++) {
+            double* dst = c == 0 ? f : t;
+            if (!dst) continue;
+            std::vector<R4<R>> a(n), b(n);
+            CK(cudaMemcpy(a.data(), (const R4<R>*)h_.fsum + (size_t)c * N_ + o, n * sizeof(R4<R>),
+                          cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(b.data(), (const R4<R>*)h_.fbnd + (size_t)c * N_ + o, n * sizeof(R4<R>),
+                          cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) {
+                R x = a[i].x, y = a[i].y, z = a[i].z;
+                if (bb[i]) { x = x + b[i].x; y = y + b[i].y; z = z + b[i].z; }
+                dst[3 * i] = x; dst[3 * i + 1] = y; dst[3 * i + 2] = z;
+            }
+        }
     }
     void get_force_parts(int s, double* parts) override {
         refresh_dev();
@@ -315,10 +340,10 @@ class EngineT final : public EngineBase {
             for (int q = 0; q < 6; q++) out[c * 6 + q] = ring[(size_t)slot * 6 + q];
         }
     }
-    void timing_enable(bool on) override {
+    void timing_enable(int level) override {
         CK(cudaStreamSynchronize(stream_));
-        timing_ = on;
-        t_contact_ms_ = 0;
+        timing_ = level <= 0 ? 0 : (level == 1 ? 1 : 2);
+        for (double& v : t_phase_ms_) v = 0;
         t_contact_n_ = 0;
         launches_ = 0;
         rebuilds_at_enable_ = total_rebuilds();
@@ -327,10 +352,15 @@ class EngineT final : public EngineBase {
     void timing_read(double* ms, int* nc, long long* nk, int* nr) override {
         CK(cudaStreamSynchronize(stream_));
         harvest_events();
-        if (ms) *ms = t_contact_ms_;
+        if (ms) *ms = t_phase_ms_[PH_CONTACT];
         if (nc) *nc = t_contact_n_;
         if (nk) *nk = launches_ + (long long)(total_rebuilds() - rebuilds_at_enable_) * rebuild_launches();
         if (nr) *nr = total_rebuilds() - rebuilds_at_enable_;
+    }
+    void timing_phases(double* ms) override {
+        CK(cudaStreamSynchronize(stream_));
+        harvest_events();
+        for (int k = 0; k < NPH; k++) ms[k] = t_contact_n_ ? t_phase_ms_[k] / t_contact_n_ : 0.0;
     }
     void info(double* bytes, double* ms) override {
         if (bytes) *bytes = mem_.bytes;
@@ -341,6 +371,8 @@ class EngineT final : public EngineBase {
     nbc_options opt_;
     DevMem mem_;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t stream2_ = nullptr;   // second branch of a step: k_boundary beside k_contact
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Dev h_{};            // host copy of the device table
     Dev* d_ = nullptr;   // device table
     int S_ = 0, N_ = 0, K_ = 0, lanes_ = 16, passes_ = 0, rs_blocks_ = 0;
@@ -354,18 +386,27 @@ class EngineT final : public EngineBase {
     int steps_done_ = 0;
     bool post_done_ = false;
     double last_ms_ = 0;
-    cudaGraph_t graph_ = nullptr;
-    cudaGraphExec_t gexec_ = nullptr;
-    // kernel timing: event pairs around the contact kernel
-    bool timing_ = false;
-    double t_contact_ms_ = 0;
+    // step graphs by timing level: [0] plain, [1] event nodes around
+    // k_contact, [2] event nodes at every mark
+    cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};
+    cudaGraphExec_t gexec_[3] = {nullptr, nullptr, nullptr};
+    // kernel timing: one record of NMARK events per step, at the marks
+    //   0 step start  1 after k_clump  2 after the rebuild node
+    //   3/4 around k_boundary and 5 start of k_contact (second branch)
+    //   6 end of k_contact  7 step end
+    static constexpr int NMARK = 8;
+    static constexpr int PH_CLUMP = 0, PH_REBUILD = 1, PH_BOUNDARY = 2, PH_CONTACT = 3, PH_STEP = 4, NPH = 5;
+    int timing_ = 0;
+    double t_phase_ms_[NPH] = {0, 0, 0, 0, 0};
     int t_contact_n_ = 0;
     long long launches_ = 0;
     int rebuilds_at_enable_ = 0;
-    std::vector<cudaEvent_t> ev_;   // pairs
-    int ev_used_ = 0;               // pairs recorded and not yet harvested
-    cudaEvent_t gev_[2] = {nullptr, nullptr};
-    cudaGraphNode_t gev_node_[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> ev_;   // records of NMARK events
+    int ev_used_ = 0;               // records made and not yet harvested
+    cudaEvent_t* rec_ = nullptr;    // the record being made by an eager step (null: none)
+    int capture_timed_ = 0;
+    cudaEvent_t gev_[3][NMARK] = {};
+    cudaGraphNode_t gev_node_[3][NMARK] = {};
 
     int total_rebuilds() {
         std::vector<SceneDyn> y(S_);
@@ -375,27 +416,45 @@ class EngineT final : public EngineBase {
         return n;
     }
     // kernels one rebuild launches (launch_rebuild)
-    int rebuild_launches() const { return 1 + passes_ * 5 + 2 + 1 + 1 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 5; }
-    std::pair<cudaEvent_t, cudaEvent_t> next_pair() {
-        if ((size_t)(2 * ev_used_ + 2) > ev_.size()) {
-            for (int k = 0; k < 64; k++) {
+    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4; }
+    cudaEvent_t* next_record() {
+        if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
+            for (int k = 0; k < 64 * NMARK; k++) {
                 cudaEvent_t e;
                 CK(cudaEventCreate(&e));
                 ev_.push_back(e);
             }
         }
-        auto p = std::make_pair(ev_[2 * ev_used_], ev_[2 * ev_used_ + 1]);
-        ev_used_++;
-        return p;
+        return &ev_[(size_t)NMARK * ev_used_++];
     }
+    // marks recorded at timing level 1: only those around k_contact
+    static bool mark_on(int level, int k) { return level >= 2 || (level == 1 && (k == 5 || k == 6)); }
     void harvest_events() {
         for (int k = 0; k < ev_used_; k++) {
-            float ms = 0;
-            CK(cudaEventElapsedTime(&ms, ev_[2 * k], ev_[2 * k + 1]));
-            t_contact_ms_ += ms;
+            const cudaEvent_t* e = &ev_[(size_t)NMARK * k];
+            float ms[NPH] = {0, 0, 0, 0, 0};
+            CK(cudaEventElapsedTime(&ms[PH_CONTACT], e[5], e[6]));
+            if (timing_ >= 2) {
+                CK(cudaEventElapsedTime(&ms[PH_CLUMP], e[0], e[1]));
+                CK(cudaEventElapsedTime(&ms[PH_REBUILD], e[1], e[2]));
+                CK(cudaEventElapsedTime(&ms[PH_BOUNDARY], e[3], e[4]));
+                CK(cudaEventElapsedTime(&ms[PH_STEP], e[0], e[7]));
+            }
+            for (int p = 0; p < NPH; p++) t_phase_ms_[p] += ms[p];
             t_contact_n_++;
         }
         ev_used_ = 0;
+    }
+    // a timing mark on stream st: an event node while capturing a timed
+    // graph, an event of the current record on an eager step
+    void mark(int k, cudaStream_t st) {
+        if (capturing_) {
+            if (!mark_on(capture_timed_, k)) return;
+            CK(cudaEventRecordWithFlags(gev_[capture_timed_][k], st, cudaEventRecordExternal));
+            gev_node_[capture_timed_][k] = last_captured_node(st);
+        } else if (rec_ && mark_on(timing_, k)) {
+            CK(cudaEventRecord(rec_[k], st));
+        }
     }
 
     struct RowData { std::vector<int> row, brow, nbr, bnbr, bpair; };
@@ -406,9 +465,13 @@ class EngineT final : public EngineBase {
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device");
         CK(cudaSetDevice(opt_.device));
         CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
         CK(cudaMallocHost(&hflag_, 4 * sizeof(int)));
         lanes_ = opt_.lanes == 1 || opt_.lanes == 2 || opt_.lanes == 4 || opt_.lanes == 8 || opt_.lanes == 16 ||
                          opt_.lanes == 32 ? opt_.lanes : 4;
+        search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
         const int spb = CT_THREADS / lanes_;
         S_ = (int)sc.size();
         hpar_.resize(S_);
@@ -505,6 +568,8 @@ class EngineT final : public EngineBase {
             ring_len_ = std::max(ring_len_, std::max(1, D.output_interval));
         }
         ring_len_ = std::max(ring_len_, 1024);
+        // list entries keep two flag bits above the subsphere index
+        if ((long long)N_ >= (1LL << 30)) throw ArgError("more than 2^30 subspheres in one engine");
         h_.S = S_; h_.N = N_; h_.K = K_;
         h_.cells = cells;
         h_.cblocks = cblk;
@@ -586,8 +651,8 @@ class EngineT final : public EngineBase {
         h_.hist = mem_.alloc<int>((size_t)256 * rs_blocks_);
         h_.perm = mem_.alloc<int>(N);
         h_.inv = mem_.alloc<int>(N);
-        h_.cell_beg = mem_.alloc<int>(cells);
-        h_.cell_end = mem_.alloc<int>(cells);
+        h_.cstart = mem_.alloc<int>(cells + 1);
+        h_.scr = mem_.alloc<int>((size_t)N * 2 * SCR_CAP);
         h_.cnt_f = mem_.alloc<int>(N + 1);
         h_.cnt_b = mem_.alloc<int>(N + 1);
         h_.sfc = mem_.alloc<int>(N);
@@ -647,6 +712,21 @@ class EngineT final : public EngineBase {
     static size_t hist_bytes(long long cap) { return (size_t)cap * (2 * sizeof(R4<R>) + sizeof(R)); }
 
     double slack() const { return opt_.pair_slack >= 1.0 ? opt_.pair_slack : 1.6; }
+    // capacity of the pair buffers at the first list: slack x its pairs; with
+    // the default slack at least the reference's own list capacity, the sum
+    // over scenes of n_sub x BranchLmtLen/2, as far as 30% of the free device
+    // memory allows (growing later costs a host round trip and re-allocation)
+    long long first_capacity(long long need) {
+        long long cap = std::max<long long>(1024, (long long)(need * slack()));
+        if (opt_.pair_slack >= 1.0) return cap;
+        long long ref = 0;
+        for (const ScenePar& P : hpar_) ref += (long long)P.nsub * (P.bl / 2);
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + sizeof(R4<R>) + sizeof(double4);
+        const long long budget = (long long)(0.3 * (double)fr / per_pair);
+        return std::min<long long>(std::max(cap, std::min(ref, budget)), 2000000000LL);
+    }
     // grow the pair buffers, keeping the current list and history generation
     void grow_pairs(long long need) {
         refresh_dev();
@@ -745,31 +825,29 @@ class EngineT final : public EngineBase {
 
     // ---- launches -------------------------------------------------------------
     void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
-        int n = K_ + S_;
-        k_clump<R><<<cdiv(n, 128), 128, 0, stream_>>>(d_, do_pre, cond, use_cond);
+        k_clump<R><<<cdiv(K_ + S_, CL_THREADS), CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond);
         CK(cudaGetLastError());
         if (!capturing_ && timing_) launches_ += 1;
     }
     bool capturing_ = false;
+    // k_boundary on the second stream beside k_contact (fork and join by
+    // events, which become graph edges when captured)
     void launch_contact(bool exp) {
         if (exp) {
             CK(cudaMemsetAsync(h_.xfcn, 0, (size_t)h_.cap * sizeof(R4<R>), stream_));
             CK(cudaMemsetAsync(h_.xcpt, 0, (size_t)h_.cap * sizeof(double4), stream_));
         }
-        if (exp) k_boundary<R, true><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream_>>>(d_);
-        else k_boundary<R, false><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream_>>>(d_);
-        if (!capturing_ && timing_) launches_ += 1;
+        CK(cudaEventRecord(ev_fork_, stream_));
+        CK(cudaStreamWaitEvent(stream2_, ev_fork_, 0));
+        // the start of k_contact is marked on the side branch (same
+        // dependencies), so only its end mark sits on the critical path
+        mark(5, stream2_);
+        mark(3, stream2_);
+        if (exp) k_boundary<R, true><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream2_>>>(d_);
+        else k_boundary<R, false><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream2_>>>(d_);
+        mark(4, stream2_);
+        CK(cudaEventRecord(ev_join_, stream2_));
         dim3 g(h_.cblocks);
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        if (capturing_) {
-            CK(cudaEventRecordWithFlags(gev_[0], stream_, cudaEventRecordExternal));
-            gev_node_[0] = last_captured_node();
-        } else if (timing_) {
-            auto pr = next_pair();
-            e0 = pr.first;
-            e1 = pr.second;
-            CK(cudaEventRecord(e0, stream_));
-        }
 #define NBC_CT(L)                                                                   \
     if (exp) k_contact<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);             \
     else k_contact<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
@@ -781,13 +859,9 @@ class EngineT final : public EngineBase {
         else { NBC_CT(8) }
 #undef NBC_CT
         CK(cudaGetLastError());
-        if (capturing_) {
-            CK(cudaEventRecordWithFlags(gev_[1], stream_, cudaEventRecordExternal));
-            gev_node_[1] = last_captured_node();
-        } else if (e1) {
-            CK(cudaEventRecord(e1, stream_));
-        }
-        if (!capturing_ && timing_) launches_ += 1;
+        mark(6, stream_);
+        CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
+        if (!capturing_ && timing_) launches_ += 2;
     }
     void scan(int* a, int n) {
         int nb = cdiv(n, SC_TILE);
@@ -807,19 +881,16 @@ class EngineT final : public EngineBase {
             std::swap(ki, ko);
             std::swap(vi, vo);
         }
-        const int fb = std::min(cdiv(h_.cells, 256), 148 * 16);
-        k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_beg, h_.cells, -1);
-        k_fill_i<<<fb, 256, 0, stream_>>>(h_.cell_end, h_.cells, -1);
         k_cellrange<<<cdiv(N_, B), B, 0, stream_>>>(d_, ki, vi);
+        k_cellstart<<<std::min(cdiv(h_.cells + 1, 256), 148 * 16), 256, 0, stream_>>>(d_);
         k_reorder<R><<<cdiv(N_, B), B, 0, stream_>>>(d_);
         const int sl = search_lanes_;
         const int sb = cdiv(N_, SEARCH_THREADS / sl);
         k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, N_ + 1, 0);
         k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, N_ + 1, 0);
-        if (sl == 4) k_count<4><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 16) k_count<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 32) k_count<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else k_count<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        if (sl == 16) k_search<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_search<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_search<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
         scan(h_.cnt_f, N_ + 1);
         scan(h_.cnt_b, N_ + 1);
         CK(cudaGetLastError());
@@ -830,7 +901,7 @@ class EngineT final : public EngineBase {
             long long need = std::max(hflag_[0], hflag_[1]);
             if (first_list_) {
                 // size the pair buffers to the first list: capacity = slack x pairs
-                resize_pairs(std::max<long long>(1024, (long long)(need * slack())));
+                resize_pairs(first_capacity(need));
                 first_list_ = false;
             } else if (need > h_.cap) {
                 grow_pairs(need);
@@ -838,37 +909,47 @@ class EngineT final : public EngineBase {
         }
         k_check_cap<<<1, 1, 0, stream_>>>(d_);
         if (hgrid_) k_fill_i<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, N_, 0);
-        if (sl == 4) k_fill<4><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 16) k_fill<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 32) k_fill<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else k_fill<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        if (sl == 16) k_compact<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_compact<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_compact<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
         if (hgrid_) k_xsort<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        k_carry<R><<<cdiv(std::max(h_.cap, 1), 256), 256, 0, stream_>>>(d_);
+        k_carry<R><<<148 * 8, 256, 0, stream_>>>(d_);
         k_commit<<<cdiv(K_ + S_ + 1, B), B, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
 
     void run_step_eager(bool exp) {
+        rec_ = timing_ ? next_record() : nullptr;
+        mark(0, stream_);
         launch_clump(1);
-        if (timing_) launches_ += 0;
+        mark(1, stream_);
         CK(cudaMemcpyAsync(hflag_, h_.any_rebuild, sizeof(int), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
         if (hflag_[0]) launch_rebuild(true);
+        mark(2, stream_);
         launch_contact(exp);
+        mark(7, stream_);
+        rec_ = nullptr;
         steps_done_ += 1;
     }
 
     // one step as a graph: k_clump, a conditional node holding the rebuild,
-    // k_contact
-    void capture() {
-        for (int k = 0; k < 2; k++) CK(cudaEventCreate(&gev_[k]));
+    // then k_boundary and k_contact on two branches; the timed variants have
+    // event nodes at the timing marks
+    void capture(int timed) {
+        if (timed && !gev_[timed][0])
+            for (int k = 0; k < NMARK; k++) CK(cudaEventCreate(&gev_[timed][k]));
         capturing_ = true;
-        CK(cudaGraphCreate(&graph_, 0));
+        capture_timed_ = timed;
+        cudaGraph_t& graph = graph_[timed];
+        CK(cudaGraphCreate(&graph, 0));
         cudaGraphConditionalHandle hnd;
-        CK(cudaGraphConditionalHandleCreate(&hnd, graph_, 0, cudaGraphCondAssignDefault));
-        CK(cudaStreamBeginCaptureToGraph(stream_, graph_, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        CK(cudaGraphConditionalHandleCreate(&hnd, graph, 0, cudaGraphCondAssignDefault));
+        CK(cudaStreamBeginCaptureToGraph(stream_, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        mark(0, stream_);
         launch_clump(1, hnd, 1);
+        mark(1, stream_);
         cudaStreamCaptureStatus st;
         const cudaGraphNode_t* deps = nullptr;
         size_t ndeps = 0;
@@ -878,37 +959,42 @@ class EngineT final : public EngineBase {
         cp.conditional.type = cudaGraphCondTypeIf;
         cp.conditional.size = 1;
         cudaGraphNode_t cnode;
-        CK(cudaGraphAddNode(&cnode, graph_, deps, ndeps, &cp));
+        CK(cudaGraphAddNode(&cnode, graph, deps, ndeps, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         CK(cudaStreamUpdateCaptureDependencies(stream_, &cnode, 1, cudaStreamSetCaptureDependencies));
+        mark(2, stream_);
         launch_contact(false);
+        mark(7, stream_);
         cudaGraph_t g2 = nullptr;
         CK(cudaStreamEndCapture(stream_, &g2));
         // the rebuild branch
+        capture_timed_ = 0;
         CK(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         launch_rebuild(false);
         cudaGraph_t b2 = nullptr;
         CK(cudaStreamEndCapture(stream_, &b2));
         capturing_ = false;
-        if (!gev_node_[0] || !gev_node_[1]) throw CudaError("event nodes missing from the step graph");
-        CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+        for (int k = 0; k < NMARK; k++)
+            if (mark_on(timed, k) && !gev_node_[timed][k]) throw CudaError("event nodes missing from the step graph");
+        CK(cudaGraphInstantiate(&gexec_[timed], graph, 0));
     }
-    cudaGraphNode_t last_captured_node() {
-        cudaStreamCaptureStatus st;
+    cudaGraphNode_t last_captured_node(cudaStream_t st) {
+        cudaStreamCaptureStatus cs;
         const cudaGraphNode_t* deps = nullptr;
         size_t nd = 0;
-        CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, nullptr, &deps, &nd));
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd));
         if (nd != 1) throw CudaError("unexpected capture dependencies");
         return deps[0];
     }
     void launch_graph() {
         if (timing_) {
-            auto pr = next_pair();
-            CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[0], pr.first));
-            CK(cudaGraphExecEventRecordNodeSetEvent(gexec_, gev_node_[1], pr.second));
+            cudaEvent_t* r = next_record();
+            for (int k = 0; k < NMARK; k++)
+                if (mark_on(timing_, k))
+                    CK(cudaGraphExecEventRecordNodeSetEvent(gexec_[timing_], gev_node_[timing_][k], r[k]));
             launches_ += 3;
         }
-        CK(cudaGraphLaunch(gexec_, stream_));
+        CK(cudaGraphLaunch(gexec_[timing_], stream_));
     }
 
     // a graph launch stopped at a rebuild whose pairs did not fit: grow and

@@ -10,9 +10,10 @@
 //                ranges, reorder, count/scan/fill of the half pair list in
 //                the reference's traversal order, back references, history
 //                carry, clump member lists.
+//   k_boundary   per subsphere: walls and intruder (beside k_contact)
 //   k_contact    one lane group per subsphere: every pair of its front and
-//                back lists, its wall faces and the intruder, summed in
-//                registers; the pair owner also writes the new spring history.
+//                back lists summed in registers; the pair owner also writes
+//                the new spring history.
 #pragma once
 #include "nbc_dev.cuh"
 #include "nbc_math.cuh"
@@ -34,68 +35,159 @@ constexpr int INTRA = (int)0x80000000u;
 // (src/dem_clumpsphere.cu:86-151), IntegratePene_Before_cuk and
 // Integrate_After_cuk (src/dem_integrate_penetrator.cu:3-113).
 //
+// One clump per lane, 32 clumps per warp.  The member work is spread over
+// the warp instead: the members of the warp's clumps are one contiguous range
+// of the member list, the lanes load all member indices of a chunk and then
+// all member records (every load of the chunk in flight at once), each
+// member's force and lever-arm torque go to shared memory, and each lane then
+// sums its own clump's members in ascending order (the reduce_by_key order)
+// and integrates its clump once.  The new poses are shared the same way and
+// the lanes pose the members 32 at a time.  The lanes after the last clump
+// hold one thread per scene for the intruder.
+//
 // A step (do_pre) also advances the spring-history generation so the next
 // contact pass reads what the previous one wrote, and counts itself; the last
 // block to finish sets the graph's rebuild condition (when given a handle).
+constexpr int CL_THREADS = 128;
+constexpr int CL_WARPS = CL_THREADS / 32;
+constexpr int CL_CHUNK = 128;   // members staged in shared memory per warp at a time
+
 template <typename R>
-__global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int do_pre,
-                                               cudaGraphConditionalHandle cond, int use_cond) {
+__global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp, int do_pre,
+                                                      cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ double s_mf[CL_WARPS][6][CL_CHUNK];   // member force xyz, torque xyz
+    __shared__ double s_cl[CL_WARPS][13][32];        // clump position, velocity, angular velocity, quaternion
+    __shared__ int s_ms[CL_WARPS][33];               // member-list offsets of the warp's clumps
+    __shared__ int s_sc[CL_WARPS][32];               // scene of each of the warp's clumps
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k0 = (blockIdx.x * CL_WARPS + warp) * 32;
+    const int t = k0 + lane;
     const int post = *d.post_pending;
-    if (do_pre && t == 0) {
+    if (do_pre && blockIdx.x == 0 && threadIdx.x == 0) {
         *d.hgen += 1;
         *d.gstep += 1;
     }
-    if (t < d.K) {
-        const int k = t;
-        const ScenePar& P = d.par[d.csid[k]];
+    if (k0 < d.K) {   // warp-uniform: this warp holds clumps
+        const int* __restrict__ mem_start = d.mem_start;
+        const int* __restrict__ mem_idx = d.mem_idx;
+        const double4* __restrict__ posr = d.posr;
+        const int nk = min(32, d.K - k0);
+        const bool isc = lane < nk;
+        const int k = isc ? t : k0 + nk - 1;
+        s_ms[warp][lane] = mem_start[k0 + min(lane, nk)];
+        if (lane == 0) s_ms[warp][32] = mem_start[k0 + nk];
+        const int sc = d.csid[k];
         double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cprop[k];
+        s_sc[warp][lane] = sc;
+        s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
+        __syncwarp();
+        const int M0 = s_ms[warp][0], M1 = s_ms[warp][nk];
+        const int mb = s_ms[warp][isc ? lane : nk - 1], me = s_ms[warp][isc ? lane + 1 : nk];
+        // the warp-local clump holding member slot m (members are grouped by clump)
+        auto owner = [&](int m) {
+            int lo = 0, hi = nk - 1;
+            while (lo < hi) {
+                const int h = (lo + hi + 1) >> 1;
+                if (s_ms[warp][h] <= m) lo = h; else hi = h - 1;
+            }
+            return lo;
+        };
+        const ScenePar& P = d.par[sc];
         const double Dt = P.dt;
-        const int mb = d.mem_start[k], me = d.mem_start[k + 1];
-        const R4<R>* fs = (const R4<R>*)d.fsum;
-        const R4<R>* ts = fs + d.N;
         V3<double> F, T;
         if (post) {
+            // ---- member sums, CL_CHUNK members of the warp's range at a time
+            const R4<R>* __restrict__ fs = (const R4<R>*)d.fsum;
+            const R4<R>* __restrict__ fb = (const R4<R>*)d.fbnd;
+            const uint16_t* __restrict__ bbits = d.bbits;
+            const size_t N = (size_t)d.N;
+            constexpr int J = CL_CHUNK / 32;
             F = v3(0.0, 0.0, 0.0);
             T = F;
-            for (int m = mb; m < me; m++) {
-                int i = d.mem_idx[m];
-                double4 ps = d.posr[i];
-                V3<double> r = v3(ps.x - cp.x, ps.y - cp.y, ps.z - cp.z);
-                R4<R> f4 = fs[i], t4 = ts[i];
-                V3<double> f = v3((double)f4.x, (double)f4.y, (double)f4.z);
-                V3<double> tc = v3((double)t4.x + (r.y * f.z - r.z * f.y),
-                                   (double)t4.y + (r.z * f.x - r.x * f.z),
-                                   (double)t4.z + (r.x * f.y - r.y * f.x));
-                if (m == mb) { F = f; T = tc; }
-                else { F = F + f; T = T + tc; }
+            for (int c0 = M0; c0 < M1; c0 += CL_CHUNK) {
+                int idx[J];
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    const int m = c0 + 32 * j + lane;
+                    idx[j] = m < M1 ? mem_idx[m] : -1;
+                }
+                double4 ps[J];
+                R4<R> f4[J], t4[J];
+                uint16_t bb[J];
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    const int i = idx[j] < 0 ? 0 : idx[j];
+                    ps[j] = posr[i];
+                    f4[j] = fs[i];
+                    t4[j] = fs[N + i];
+                    bb[j] = bbits[i];
+                }
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    if (idx[j] < 0) continue;
+                    const int kk = owner(c0 + 32 * j + lane);
+                    R4<R> a = f4[j], b = t4[j];
+                    if (bb[j]) {
+                        // walls and intruder (k_boundary) after the pairs, in Real
+                        const R4<R> bf = fb[idx[j]], bt = fb[N + idx[j]];
+                        a.x = a.x + bf.x; a.y = a.y + bf.y; a.z = a.z + bf.z;
+                        b.x = b.x + bt.x; b.y = b.y + bt.y; b.z = b.z + bt.z;
+                    }
+                    const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
+                                            ps[j].z - s_cl[warp][2][kk]);
+                    const V3<double> f = v3((double)a.x, (double)a.y, (double)a.z);
+                    const int q = 32 * j + lane;
+                    s_mf[warp][0][q] = f.x;
+                    s_mf[warp][1][q] = f.y;
+                    s_mf[warp][2][q] = f.z;
+                    s_mf[warp][3][q] = (double)b.x + (r.y * f.z - r.z * f.y);
+                    s_mf[warp][4][q] = (double)b.y + (r.z * f.x - r.x * f.z);
+                    s_mf[warp][5][q] = (double)b.z + (r.x * f.y - r.y * f.x);
+                }
+                __syncwarp();
+                if (isc) {
+                    const int lo = max(mb, c0), hi = min(me, c0 + CL_CHUNK);
+                    for (int m = lo; m < hi; m++) {
+                        const int q = m - c0;
+                        const V3<double> f = v3(s_mf[warp][0][q], s_mf[warp][1][q], s_mf[warp][2][q]);
+                        const V3<double> tc = v3(s_mf[warp][3][q], s_mf[warp][4][q], s_mf[warp][5][q]);
+                        if (m == mb) { F = f; T = tc; }
+                        else { F = F + f; T = T + tc; }
+                    }
+                }
+                __syncwarp();
             }
-            if (mb < me) {
-                d.cF[k] = make_double4(F.x, F.y, F.z, 0.0);
-                d.cT[k] = make_double4(T.x, T.y, T.z, 0.0);
-            } else {
-                F = xyzd(d.cF[k]);
-                T = xyzd(d.cT[k]);
+            if (isc) {
+                if (mb < me) {
+                    if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z) && isfinite(T.x) && isfinite(T.y) &&
+                          isfinite(T.z)))
+                        atomicOr(&d.dyn[sc].err, ERR_NONFINITE);
+                    d.cF[k] = make_double4(F.x, F.y, F.z, 0.0);
+                    d.cT[k] = make_double4(T.x, T.y, T.z, 0.0);
+                } else {
+                    F = xyzd(d.cF[k]);
+                    T = xyzd(d.cT[k]);
+                }
             }
-            V3<double> a = (1.0 / pr.w) * F;
-            a.z = a.z + P.gravity;
+            V3<double> ac = (1.0 / pr.w) * F;
+            ac.z = ac.z + P.gravity;
             V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
-            cv.x += (0.5 * Dt) * a.x; cv.y += (0.5 * Dt) * a.y; cv.z += (0.5 * Dt) * a.z;
+            cv.x += (0.5 * Dt) * ac.x; cv.y += (0.5 * Dt) * ac.y; cv.z += (0.5 * Dt) * ac.z;
             cw.x += (0.5 * Dt) * al.x; cw.y += (0.5 * Dt) * al.y; cw.z += (0.5 * Dt) * al.z;
         } else {
             F = xyzd(d.cF[k]);
             T = xyzd(d.cT[k]);
         }
         if (do_pre) {
-            V3<double> a = (1.0 / pr.w) * F;
-            a.z = a.z + P.gravity;
+            V3<double> ac = (1.0 / pr.w) * F;
+            ac.z = ac.z + P.gravity;
             V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
             V3<double> v = xyzd(cv), w = xyzd(cw);
-            V3<double> dist = Dt * v + (0.5 * Dt * Dt) * a;
+            V3<double> dist = Dt * v + (0.5 * Dt * Dt) * ac;
             cp.x += dist.x; cp.y += dist.y; cp.z += dist.z;
-            v = v + (0.5 * Dt) * a;
+            v = v + (0.5 * Dt) * ac;
             w = w + (0.5 * Dt) * al;
             // attitude with the half-kicked angular velocity
             V3<double> Wb = rot_w2b(cq, w), Wdb = rot_w2b(cq, al);
@@ -115,39 +207,55 @@ __global__ void __launch_bounds__(128) k_clump(const Dev* __restrict__ dp, int d
             q.w = (q.w + Dt * qd.w) + h2 * qdd.w;
             const double inv = 1.0 / sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
             q.x *= inv; q.y *= inv; q.z *= inv; q.w *= inv;
-            // pose of the members
-            R4<R>* kv = (R4<R>*)d.kin;
-            R4<R>* kw = kv + d.N;
-            R4<R>* ka = kw + d.N;
-            bool moved = false;
-            for (int m = mb; m < me; m++) {
-                int i = d.mem_idx[m];
-                double4 lo = d.lom[i];
-                V3<double> arm = rot_b2w(q, v3(lo.x, lo.y, lo.z));
-                V3<double> p = v3(cp.x + arm.x, cp.y + arm.y, cp.z + arm.z);
-                double4 old = d.posr[i];
-                double4 c = d.cum[i];
-                V3<double> cn = v3((c.x + p.x) - old.x, (c.y + p.y) - old.y, (c.z + p.z) - old.z);
-                if (len_floor(cn) > P.thresh) moved = true;
-                d.cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
-                d.posr[i] = make_double4(p.x, p.y, p.z, old.w);
-                kv[i] = pack<R>(cvt<R>(v), (R)lo.w);
-                kw[i] = pack<R>(cvt<R>(w), R(0));
+            if (isc) {
+                d.cpos[k] = cp;
+                d.cvel[k] = make_double4(v.x, v.y, v.z, 0.0);
+                d.cw[k] = make_double4(w.x, w.y, w.z, 0.0);
+                d.cq[k] = q;
+            }
+            __syncwarp();   // the old positions in s_cl are no longer read
+            s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
+            s_cl[warp][3][lane] = v.x; s_cl[warp][4][lane] = v.y; s_cl[warp][5][lane] = v.z;
+            s_cl[warp][6][lane] = w.x; s_cl[warp][7][lane] = w.y; s_cl[warp][8][lane] = w.z;
+            s_cl[warp][9][lane] = q.x; s_cl[warp][10][lane] = q.y; s_cl[warp][11][lane] = q.z;
+            s_cl[warp][12][lane] = q.w;
+            __syncwarp();
+            // ---- poses of the members, 32 at a time
+            R4<R>* __restrict__ kv = (R4<R>*)d.kin;
+            R4<R>* __restrict__ kw = kv + d.N;
+            R4<R>* __restrict__ ka = kw + d.N;
+            const double4* __restrict__ lom = d.lom;
+            double4* __restrict__ cum = d.cum;
+            double4* __restrict__ posw = d.posr;
+            for (int m = M0 + lane; m < M1; m += 32) {
+                const int i = mem_idx[m];
+                const int kk = owner(m);
+                const double4 lo = lom[i], old = posw[i], c = cum[i];
+                const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
+                                                s_cl[warp][12][kk]);
+                const V3<double> arm = rot_b2w(qk, v3(lo.x, lo.y, lo.z));
+                const V3<double> p = v3(s_cl[warp][0][kk] + arm.x, s_cl[warp][1][kk] + arm.y, s_cl[warp][2][kk] + arm.z);
+                const V3<double> cn = v3((c.x + p.x) - old.x, (c.y + p.y) - old.y, (c.z + p.z) - old.z);
+                const V3<double> vk = v3(s_cl[warp][3][kk], s_cl[warp][4][kk], s_cl[warp][5][kk]);
+                const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
+                cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
+                posw[i] = make_double4(p.x, p.y, p.z, old.w);
+                kv[i] = pack<R>(cvt<R>(vk), (R)lo.w);
+                kw[i] = pack<R>(cvt<R>(wk), R(0));
                 ka[i] = pack<R>(cvt<R>(arm), R(0));
+                const int sk = s_sc[warp][kk];
+                if (len_floor(cn) > d.par[sk].thresh) {
+                    SceneDyn& y = d.dyn[sk];
+                    if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
+                    if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
+                }
             }
-            if (moved) {
-                atomicExch(&d.dyn[d.csid[k]].rebuild, 1);
-                atomicExch(d.any_rebuild, 1);
-            }
-            d.cpos[k] = cp;
-            d.cvel[k] = make_double4(v.x, v.y, v.z, 0.0);
-            d.cw[k] = make_double4(w.x, w.y, w.z, 0.0);
-            d.cq[k] = q;
-        } else if (post) {
+        } else if (post && isc) {
             d.cvel[k] = cv;
             d.cw[k] = cw;
         }
-    } else if (t < d.K + d.S) {
+    }
+    if (t >= d.K && t < d.K + d.S) {
         const int s = t - d.K;
         const ScenePar& P = d.par[s];
         SceneDyn& y = d.dyn[s];
@@ -367,16 +475,16 @@ static __global__ void k_fill_i(int* __restrict__ a, int n, int v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
 }
 
-// FindBegEndInCell_cuk (src/dem_grid.cu:105-153) over the global cell table,
-// plus the permutation, its inverse and the sorted keys (into key2).
+// The permutation of the sort, its inverse and the sorted keys (into key2).
+// The cell table is built from key2 by k_cellstart (FindBegEndInCell_cuk,
+// src/dem_grid.cu:105-153, as one start offset per cell: cell c holds the
+// sorted slots [cstart[c], cstart[c + 1])).
 static __global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
     const Dev& d = *dp;
     if (*d.halt) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.N) return;
     int k = skey[i];
-    if (i == 0 || skey[i - 1] != k) d.cell_beg[k] = i;
-    if (i == d.N - 1 || skey[i + 1] != k) d.cell_end[k] = i + 1;
     d.inv[perm[i]] = i;
     d.perm[i] = perm[i];
     d.key2[i] = k;
@@ -413,121 +521,211 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
 }
 
 // --- neighbour search ----------------------------------------------------
-// One warp per subsphere.  The candidate test and the order of CreateAnei_cuk
-// (src/dem_grid.cu:466-552): cells in z, y, x order over -1..1, partners
-// ascending within a cell, candidate if |xi - xj|^2 < (1.5 (ri + rj))^2 in
-// FP64; j > i goes to the front (owner) row of i, j < i to its back row.  The
-// three x-neighbour cells of one (z, y) stencil row hold one contiguous range
-// of the sorted order, so the warp walks 9 ranges per level with coalesced
-// loads and appends its hits in discovery order through ballot prefixes.
+// The candidate test and the order of CreateAnei_cuk (src/dem_grid.cu:466-552):
+// cells in z, y, x order over -1..1, partners ascending within a cell,
+// candidate if |xi - xj|^2 < (1.5 (ri + rj))^2 in FP64; j > i goes to the
+// front (owner) row of i, j < i to its back row.
 //
 // Hierarchical grid (CreateAnei_hGrid_cuk, src/dem_hgrid_contlist.cu:57-161):
 // a subsphere searches its own level and every coarser one (level 0 is the
 // coarsest); a pair across levels is owned by the coarser subsphere: the
 // finer one records a back entry, the coarser one a front entry, placed after
 // its same-level front entries in ascending order of the finer partner.
+//
+// A group of SL lanes searches for one subsphere.  The three x-neighbour
+// cells of one (z, y) stencil row hold one contiguous range of the sorted
+// order, [cstart[first cell], cstart[last cell + 1]), so a subsphere on level
+// t visits 9 (t + 1) ranges.  The lanes first resolve all ranges at once
+// (each lane a contiguous chunk of rows), prefix-sum their lengths, and then
+// walk the concatenation of the ranges SL candidates at a time: the
+// concatenation is the discovery order, and hits are appended in it through
+// ballot prefixes.  One pass both counts and stores the hits: into a
+// fixed-size scratch row per subsphere (the fused search), or, for rows too
+// long for the scratch, straight into the final list once its offsets are
+// known (the fallback of k_compact).
 constexpr int SEARCH_THREADS = 128;
+constexpr int SCR_CAP = 32;                   // scratch entries per front row and per back row
+constexpr int CROSS_TAG = 0x40000000;         // scratch only: back entry whose partner is coarser
+constexpr int MAX_ROWS = 9 * MAX_LEVELS;
 
-// SL lanes (4, 8, 16 or 32) search for one subsphere; lane masks and ballots
-// are restricted to the lane group so groups of one warp proceed independently
+template <int SL>
+struct SearchShared {
+    int rs[SEARCH_THREADS / SL][MAX_ROWS];        // first sorted index of each stencil row
+    int pre[SEARCH_THREADS / SL][MAX_ROWS + 1];   // exclusive prefix of the row lengths
+};
+
+// FILL = false: count the hits and store them in subsphere i's scratch rows,
+// count cross-level entries into the coarser partner's cnt_f.  FILL = true:
+// write the hits into the list rows at the scanned offsets and claim the
+// cross-level slots of the coarser partners.
 template <bool FILL, int SL>
-__device__ __forceinline__ void warp_search(const Dev& d, const ScenePar& P, const PairList& Nw, int i, int lane,
-                                            int& nf_out, int& nb_out, int& nx_out) {
+__device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, const PairList& Nw, int i, int lane,
+                                             int* __restrict__ rs, int* __restrict__ pre, int& nf_out, int& nb_out) {
+    // buffer pointers in registers: the stores below could otherwise alias
+    // the pointer table and force it to be re-read on every candidate
+    const double4* __restrict__ posr = d.posr2;
+    const int* __restrict__ cid = d.clump_id2;
+    const int* __restrict__ cstart = d.cstart;
+    int* __restrict__ cnt_f = d.cnt_f;
+    int* __restrict__ xcnt = d.xcnt;
+    const int* __restrict__ sfc = d.sfc;
+    int* __restrict__ nbr = Nw.nbr;
+    int* __restrict__ own = Nw.own;
+    int* __restrict__ bnbr = Nw.bnbr;
     const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
     const int gshift = (threadIdx.x & 31) & ~(SL - 1);
-    const double4 pi = d.posr2[i];
-    const int ci = d.clump_id2[i];
+    const double4 pi = posr[i];
+    const int ci = cid[i];
     const int my = P.levels > 1 ? d.level2[i] : 0;
-    const unsigned lt = (1u << lane) - 1u;
-    int nf = 0, nb = 0, nx = 0;  // same-level front, back (all levels), cross-level (this row's partners)
-    const int rf = FILL ? d.cnt_f[i] : 0, rb = FILL ? d.cnt_b[i] : 0;
-    for (int l = my; l >= 0; l--) {
-        int gx, gy, gz, base, cx0, cy0, cz0;
-        if (P.levels <= 1) {
-            gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
-            base = P.cell_off;
-            cx0 = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
-            cy0 = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
-            cz0 = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
-        } else {
-            gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
-            base = P.cell_off + P.loff[l];
-            const double c = P.lcell[l];
-            cx0 = (int)floor((pi.x - P.origin[0]) / c);
-            cy0 = (int)floor((pi.y - P.origin[1]) / c);
-            cz0 = (int)floor((pi.z - P.origin[2]) / c);
-        }
-        const bool same = l == my;
-        const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
-        if (xa > xb) continue;
-        for (int cz = -1; cz <= 1; cz++) {
-            const int z = cz0 + cz;
-            if (z < 0 || z >= gz) continue;
-            for (int cy = -1; cy <= 1; cy++) {
-                const int y = cy0 + cy;
-                if (y < 0 || y >= gy) continue;
+    const int nrows = 9 * (my + 1);
+    // ---- ranges of the stencil rows: lane k resolves rows [k C, k C + C)
+    {
+        const int C = (nrows + SL - 1) / SL;
+        const int r0 = min(lane * C, nrows), r1 = min(r0 + C, nrows);
+        int acc = 0, lc = -1, gx = 0, gy = 0, gz = 0, base = 0, cx0 = 0, cy0 = 0, cz0 = 0;
+        for (int r = r0; r < r1; r++) {
+            const int l = my - r / 9, rr = r % 9;
+            if (l != lc) {
+                lc = l;
+                if (P.levels <= 1) {
+                    gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
+                    base = P.cell_off;
+                    cx0 = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
+                    cy0 = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
+                    cz0 = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
+                } else {
+                    gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
+                    base = P.cell_off + P.loff[l];
+                    const double c = P.lcell[l];
+                    cx0 = (int)floor((pi.x - P.origin[0]) / c);
+                    cy0 = (int)floor((pi.y - P.origin[1]) / c);
+                    cz0 = (int)floor((pi.z - P.origin[2]) / c);
+                }
+            }
+            const int z = cz0 + rr / 3 - 1, y = cy0 + rr % 3 - 1;
+            const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
+            int s = 0, n = 0;
+            if (xa <= xb && z >= 0 && z < gz && y >= 0 && y < gy) {
                 const int c0 = base + (z * gy + y) * gx;
-                int s = -1, e = -1;
-                for (int x = xa; x <= xb; x++) {
-                    const int b = d.cell_beg[c0 + x];
-                    if (b != -1) {
-                        if (s == -1) s = b;
-                        e = d.cell_end[c0 + x];
+                s = cstart[c0 + xa];
+                n = cstart[c0 + xb + 1] - s;
+            }
+            rs[r] = s;
+            pre[r] = acc;
+            acc += n;
+        }
+        int inc = acc;
+#pragma unroll
+        for (int o = 1; o < SL; o <<= 1) {
+            const int v = __shfl_up_sync(gm, inc, o, SL);
+            if (lane >= o) inc += v;
+        }
+        const int ex = inc - acc;
+        for (int r = r0; r < r1; r++) pre[r] += ex;
+        const int total = __shfl_sync(gm, inc, SL - 1, SL);
+        if (lane == 0) pre[nrows] = total;
+        __syncwarp(gm);
+    }
+    const int total = pre[nrows];
+    // ---- candidates in discovery order, SL at a time; the next batch's
+    // positions are loaded before the current batch is tested
+    const unsigned lt = (1u << lane) - 1u;
+    int nf = 0, nb = 0;
+    const int rf = FILL ? cnt_f[i] : 0, rb = FILL ? d.cnt_b[i] : 0;
+    int* __restrict__ scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
+    int* __restrict__ scr_b = scr_f + SCR_CAP;
+    int r = 0;
+    int jn = -1, rn = 0;
+    double4 pn = make_double4(0, 0, 0, 0);
+    if (lane < total) {
+        while (pre[r + 1] <= lane) r++;
+        jn = rs[r] + (lane - pre[r]);
+        rn = r;
+        pn = posr[jn];
+    }
+    for (int b0 = 0; b0 < total; b0 += SL) {
+        const int j = jn, rj = rn;
+        const double4 pj = pn;
+        const int f = b0 + SL + lane;
+        jn = -1;
+        if (f < total) {
+            while (pre[r + 1] <= f) r++;
+            jn = rs[r] + (f - pre[r]);
+            rn = r;
+            pn = posr[jn];
+        }
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double lim = 1.50 * (pi.w + pj.w);
+        const bool hit = j >= 0 && j != i && d2 < lim * lim;
+        const bool same = rj < 9;
+        const bool front = hit && same && i < j;
+        const bool back = hit && !front;
+        const bool cross = hit && !same;
+        const unsigned fm = __ballot_sync(gm, front) >> gshift;
+        const unsigned bm = __ballot_sync(gm, back) >> gshift;
+        if (hit) {
+            const int flag = cid[j] == ci ? INTRA : 0;
+            if (FILL) {
+                if (front) {
+                    const int q = rf + nf + __popc(fm & lt);
+                    nbr[q] = j | flag;
+                    own[q] = i;
+                } else {
+                    bnbr[rb + nb + __popc(bm & lt)] = j | flag;
+                    if (cross) {
+                        // the coarser partner owns the pair: claim a slot after
+                        // its same-level front entries (sorted afterwards)
+                        const int q = cnt_f[j] + sfc[j] + atomicAdd(&xcnt[j], 1);
+                        nbr[q] = i | flag;
+                        own[q] = j;
                     }
                 }
-                if (s == -1) continue;
-                for (int k0 = s; k0 < e; k0 += SL) {
-                    const int j = k0 + lane;
-                    bool hit = false;
-                    if (j < e && j != i) {
-                        const double4 pj = d.posr2[j];
-                        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                        const double d2 = dx * dx + dy * dy + dz * dz;
-                        const double lim = 1.50 * (pi.w + pj.w);
-                        hit = d2 < lim * lim;
-                    }
-                    const bool front = hit && same && i < j;
-                    const bool back = hit && !front;
-                    const bool cross = hit && !same;
-                    const unsigned fm = __ballot_sync(gm, front) >> gshift;
-                    const unsigned bm = __ballot_sync(gm, back) >> gshift;
-                    if (FILL && hit) {
-                        const int flag = d.clump_id2[j] == ci ? INTRA : 0;
-                        if (front) {
-                            const int q = rf + nf + __popc(fm & lt);
-                            Nw.nbr[q] = j | flag;
-                            Nw.own[q] = i;
-                        } else {
-                            Nw.bnbr[rb + nb + __popc(bm & lt)] = j | flag;
-                            if (cross) {
-                                // the coarser partner owns the pair: claim a slot after
-                                // its same-level front entries (sorted afterwards)
-                                const int q = d.cnt_f[j] + d.sfc[j] + atomicAdd(&d.xcnt[j], 1);
-                                Nw.nbr[q] = i | flag;
-                                Nw.own[q] = j;
-                            }
-                        }
-                    }
-                    if (!FILL && cross) atomicAdd(&d.cnt_f[j], 1);
-                    nf += __popc(fm);
-                    nb += __popc(bm);
-                    nx += __popc(__ballot_sync(gm, cross));
+            } else {
+                if (front) {
+                    const int q = nf + __popc(fm & lt);
+                    if (q < SCR_CAP) scr_f[q] = j | flag;
+                } else {
+                    const int q = nb + __popc(bm & lt);
+                    if (q < SCR_CAP) scr_b[q] = j | flag | (cross ? CROSS_TAG : 0);
+                    if (cross) atomicAdd(&cnt_f[j], 1);
                 }
             }
         }
+        nf += __popc(fm);
+        nb += __popc(bm);
     }
     nf_out = nf;
     nb_out = nb;
-    nx_out = nx;
 }
 
-// counts: cnt_f[i] = same-level front entries + cross-level entries claimed
-// by finer partners (added with integer atomics), cnt_b[i] = back entries
-template <int SL>
-__global__ void __launch_bounds__(SEARCH_THREADS) k_count(const Dev* __restrict__ dp) {
+// cstart[c] = first sorted slot whose cell key is >= c, for c in [0, cells]
+static __global__ void k_cellstart(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int n = d.N;
+    const int* __restrict__ key = d.key2;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= d.cells; c += gridDim.x * blockDim.x) {
+        int lo = 0, len = n;
+        while (len > 0) {
+            const int h = len >> 1;
+            if (key[lo + h] < c) { lo += h + 1; len -= h + 1; }
+            else len = h;
+        }
+        d.cstart[c] = lo;
+    }
+}
+
+// The fused search: counts (cnt_f[i] = same-level front entries + cross-level
+// entries found by finer partners, cnt_b[i] = back entries) and the hits in
+// scratch rows.  Scenes that are not rebuilt keep their rows.
+template <int SL>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_search(const Dev* __restrict__ dp) {
+    __shared__ SearchShared<SL> sh;
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int g = threadIdx.x / SL;
+    const int i = blockIdx.x * (SEARCH_THREADS / SL) + g;
     const int lane = threadIdx.x % SL;
     if (i >= d.N) return;
     const int s = d.sid[i];
@@ -541,9 +739,9 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_count(const Dev* __restrict_
         }
         return;
     }
-    int nf = 0, nb = 0, nx = 0;
+    int nf = 0, nb = 0;
     if (d.key2[i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
-        warp_search<false, SL>(d, P, d.L[0], i, lane, nf, nb, nx);
+        group_search<false, SL>(d, P, d.L[0], i, lane, sh.rs[g], sh.pre[g], nf, nb);
     if (lane == 0) {
         atomicAdd(&d.cnt_f[i], nf);
         d.cnt_b[i] = nb;
@@ -562,11 +760,17 @@ static __global__ void k_check_cap(const Dev* __restrict__ dp) {
     }
 }
 
+// The list rows at their scanned offsets: copied from the scratch rows (and
+// the cross-level slots of coarser partners claimed), searched again for rows
+// longer than the scratch, or copied from the previous list for scenes that
+// were not rebuilt.
 template <int SL>
-__global__ void __launch_bounds__(SEARCH_THREADS) k_fill(const Dev* __restrict__ dp) {
+__global__ void __launch_bounds__(SEARCH_THREADS) k_compact(const Dev* __restrict__ dp) {
+    __shared__ SearchShared<SL> sh;
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int g = threadIdx.x / SL;
+    const int i = blockIdx.x * (SEARCH_THREADS / SL) + g;
     const int lane = threadIdx.x % SL;
     if (i >= d.N) return;
     const int s = d.sid[i];
@@ -581,14 +785,31 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_fill(const Dev* __restrict__
     if (!d.dyn[s].rebuild) {
         const PairList& O = d.L[*d.lcur & 1];
         const int of = O.row[i], nf = O.row[i + 1] - of;
-        for (int g = lane; g < nf; g += SL) { Nw.nbr[rf + g] = O.nbr[of + g]; Nw.own[rf + g] = i; }
+        for (int k = lane; k < nf; k += SL) { Nw.nbr[rf + k] = O.nbr[of + k]; Nw.own[rf + k] = i; }
         const int ob = O.brow[i], nb = O.brow[i + 1] - ob;
-        for (int g = lane; g < nb; g += SL) Nw.bnbr[rb + g] = O.bnbr[ob + g];
+        for (int k = lane; k < nb; k += SL) Nw.bnbr[rb + k] = O.bnbr[ob + k];
         return;
     }
     if (d.key2[i] == P.cell_off + P.cellnum - 1) return;
-    int nf, nb, nx;
-    warp_search<true, SL>(d, P, Nw, i, lane, nf, nb, nx);
+    const int nf = d.sfc[i], nb = d.cnt_b[i + 1] - rb;
+    if (nf <= SCR_CAP && nb <= SCR_CAP) {
+        const int* scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
+        const int* scr_b = scr_f + SCR_CAP;
+        for (int k = lane; k < nf; k += SL) { Nw.nbr[rf + k] = scr_f[k]; Nw.own[rf + k] = i; }
+        for (int k = lane; k < nb; k += SL) {
+            const int v = scr_b[k];
+            Nw.bnbr[rb + k] = v & ~CROSS_TAG;
+            if (v & CROSS_TAG) {
+                const int j = v & (IDX_MASK & ~CROSS_TAG);
+                const int q = d.cnt_f[j] + d.sfc[j] + atomicAdd(&d.xcnt[j], 1);
+                Nw.nbr[q] = i | (v & INTRA);
+                Nw.own[q] = j;
+            }
+        }
+    } else {
+        int f2, b2;
+        group_search<true, SL>(d, P, Nw, i, lane, sh.rs[g], sh.pre[g], f2, b2);
+    }
 }
 
 // hierarchical grid: the cross-level entries of each owner row in ascending
@@ -629,11 +850,7 @@ static __global__ void k_backref(const Dev* __restrict__ dp) {
 // spring history of the same pair in the previous list, negated when the
 // owner changed.  Pairs absent from the previous list start from zero.
 template <typename R>
-__global__ void k_carry(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= d.cnt_f[d.N]) return;
+__device__ __forceinline__ void carry_one(const Dev& d, int p) {
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& O = d.L[lc & 1];
     const PairList& Nw = d.L[(lc + 1) & 1];
@@ -679,6 +896,16 @@ __global__ void k_carry(const Dev* __restrict__ dp) {
     } else {
         to[p] = 0;
     }
+}
+
+template <typename R>
+__global__ void k_carry(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    // grid-stride: the launch is captured once and the list may have grown since
+    const int np = d.cnt_f[d.N];
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
+        carry_one<R>(d, p);
 }
 
 // Finishes a rebuild: per-clump member lists in ascending subsphere order
@@ -801,6 +1028,15 @@ template <typename R>
 __device__ __forceinline__ void load_kin(const Dev& d, int i, Body<R>& b) {
     const R4<R>* kv = (const R4<R>*)d.kin;
     R4<R> a = kv[i], w = kv[d.N + i], r = kv[2 * d.N + i];
+    b.v = xyz<R>(a);
+    b.m = a.w;
+    b.w = xyz<R>(w);
+    b.arm = xyz<R>(r);
+}
+
+template <typename R>
+__device__ __forceinline__ void load_kin(const R4<R>* __restrict__ kv, size_t N, int i, Body<R>& b) {
+    const R4<R> a = kv[i], w = kv[N + i], r = kv[2 * N + i];
     b.v = xyz<R>(a);
     b.m = a.w;
     b.w = xyz<R>(w);
@@ -1141,8 +1377,9 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
 
 // Pairs, one lane group per subsphere: every pair of its front (owner) and
 // back lists, the owner's spring history read from the previous generation
-// and, for owner entries, the new history written; the boundary force from
-// k_boundary added in; the sum written once per subsphere.
+// and, for owner entries, the new history written; the pair sum written once
+// per subsphere (k_boundary runs beside it on a second graph branch; k_clump
+// adds its wall and intruder force after the pair sum).
 template <typename R, int LANES, bool EXPORT>
 __global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -1161,29 +1398,37 @@ __global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict
     L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
     const R coh = (R)P.cohesion;
 
+    // buffer pointers in registers: the history and flag stores could
+    // otherwise alias the pointer table and force re-reads per pair
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& Lst = d.L[lc & 1];
+    const int* __restrict__ nbr = Lst.nbr;
+    const int* __restrict__ bnbr = Lst.bnbr;
+    const int* __restrict__ bpair = Lst.bpair;
+    const double4* __restrict__ posr = d.posr;
+    const R4<R>* __restrict__ kin = (const R4<R>*)d.kin;
+    const size_t N = (size_t)d.N;
     const size_t cap = (size_t)d.cap;
-    const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
-    R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
-    const uint8_t* ti = d.touch[hg & 1];
-    uint8_t* to = d.touch[(hg + 1) & 1];
+    const R4<R>* __restrict__ Hi = (const R4<R>*)d.H[hg & 1];
+    R4<R>* __restrict__ Ho = (R4<R>*)d.H[(hg + 1) & 1];
+    const uint8_t* __restrict__ ti = d.touch[hg & 1];
+    uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
 
     Body<R> me;
-    me.p = d.posr[i];
+    me.p = posr[i];
     bool have_kin = false;
     V3<R> F = v3<R>(0, 0, 0), T = F;
 
     // front (owner) entries
     const int rs = Lst.row[i], re = Lst.row[i + 1];
     for (int k = rs + lane; k < re; k += LANES) {
-        const int jr = Lst.nbr[k];
+        const int jr = nbr[k];
         if (jr < 0) continue;  // pair inside one clump (src/dem_force_clump.cu:18-19)
         Body<R> ot;
-        ot.p = d.posr[jr];
+        ot.p = posr[jr];
         if (!overlaps(me.p, ot.p)) { to[k] = 0; continue; }
-        if (!have_kin) { load_kin<R>(d, i, me); have_kin = true; }
-        load_kin<R>(d, jr, ot);
+        if (!have_kin) { load_kin<R>(kin, N, i, me); have_kin = true; }
+        load_kin<R>(kin, N, jr, ot);
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         if (ti[k]) hist_read<R>(Hi, cap, k, hs, ht, hr);
         V3<R> fa, ta;
@@ -1205,15 +1450,15 @@ __global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict
     // back entries: the owner's stored history, seen from this side
     const int bs = Lst.brow[i], be = Lst.brow[i + 1];
     for (int k = bs + lane; k < be; k += LANES) {
-        const int jr = Lst.bnbr[k];
+        const int jr = bnbr[k];
         if (jr < 0) continue;
         Body<R> ot;
-        ot.p = d.posr[jr];
+        ot.p = posr[jr];
         if (!overlaps(me.p, ot.p)) continue;
-        const int q = Lst.bpair[k];
+        const int q = bpair[k];
         if (q < 0) continue;  // unreachable with a consistent list
-        if (!have_kin) { load_kin<R>(d, i, me); have_kin = true; }
-        load_kin<R>(d, jr, ot);
+        if (!have_kin) { load_kin<R>(kin, N, i, me); have_kin = true; }
+        load_kin<R>(kin, N, jr, ot);
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         if (ti[q]) {
             hist_read<R>(Hi, cap, q, hs, ht, hr);
@@ -1230,17 +1475,10 @@ __global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict
     F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
     T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
     if (lane == 0) {
-        const size_t N = (size_t)d.N;
         if (EXPORT) {
             R4<R>* xp = (R4<R>*)d.xparts;
             xp[i] = pack<R>(F, R(0));
             xp[N + i] = pack<R>(T, R(0));
-        }
-        if (d.bbits[i]) {
-            const R4<R>* fb = (const R4<R>*)d.fbnd;
-            const R4<R> bf = fb[i], bt = fb[N + i];
-            F = F + xyz<R>(bf);
-            T = T + xyz<R>(bt);
         }
         R4<R>* fs = (R4<R>*)d.fsum;
         fs[i] = pack<R>(F, R(0));

@@ -123,7 +123,8 @@ struct Dev {
     int* hist;        // radix histograms
     int* perm;        // [N] old index of new slot i (part_idx_pre)
     int* inv;         // [N] new slot of old index
-    int* cell_beg; int* cell_end;         // [cells]
+    int* cstart;                          // [cells+1] first sorted slot of each cell
+    int* scr;                             // [N][2][SCR_CAP] front / back scratch rows of the fused search
     int* cnt_f; int* cnt_b;               // [N+1] counts, scanned in place
     int* sfc;                             // [N] same-level front count (hierarchical grid)
     int* xcnt;                            // [N] cross-level entries placed so far (hierarchical grid)

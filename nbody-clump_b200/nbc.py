@@ -88,7 +88,7 @@ def with_levels(scene: dict, max_levels=4) -> dict:
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int),
-                ("device", C.c_int), ("pair_slack", C.c_double)]
+                ("device", C.c_int), ("pair_slack", C.c_double), ("search_lanes", C.c_int)]
 
 
 EXPORTED = [
@@ -97,6 +97,7 @@ EXPORTED = [
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
+    "nbc_timing_phases",
     "nbc_engine_info", "nbc_cell_sort_noalloc", "nbc_choose_levels",
 ]
 
@@ -201,7 +202,8 @@ def scene_desc(scene: dict):
 class Engine:
     """A batch of scenes resident on one GPU."""
 
-    def __init__(self, scenes, precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0):
+    def __init__(self, scenes, precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0,
+                 search_lanes=0):
         L = lib()
         self._descs = [scene_desc(s) for s in scenes]
         self.N = [int(s["params"]["NumberBody"]) for s in scenes]
@@ -212,6 +214,7 @@ class Engine:
         L.nbc_default_options(C.byref(o))
         o.precision, o.lanes, o.use_graph, o.device = PREC[precision], lanes, int(use_graph), device
         o.pair_slack = pair_slack
+        o.search_lanes = search_lanes
         h = C.c_void_p()
         _check(L.nbc_create(arr, len(scenes), C.byref(o), C.byref(h)))
         self.h = h
@@ -272,6 +275,26 @@ class Engine:
         _check(lib().nbc_get_clumps(self.h, s, _p(o["pos"]), _p(o["vel"]), _p(o["quat"]),
                                     _p(o["angvel"]), _p(o["force"]), _p(o["torque"])))
         return o
+
+    def restart_scene(self, base, s=0):
+        """A scene that starts from scene s's current state: subsphere
+        positions, clump poses and velocities, intruder position and velocity
+        (spring histories start from zero, as in a reference run restarted
+        from its OutPart/OutClump snapshot)."""
+        self.sync()
+        sub, cl = self.subspheres(s), self.clumps(s)
+        out = dict(base)
+        out["sub"] = dict(base["sub"])
+        out["clump"] = dict(base["clump"])
+        pos = np.empty_like(sub["pos"])
+        pos[sub["part_fix"]] = sub["pos"]
+        out["sub"]["pos"] = pos
+        for k in ("pos", "vel", "quat", "angvel"):
+            out["clump"][k] = cl[k].copy()
+        if base.get("intruder") is not None:
+            it = self.intruder(s)
+            out["intruder"] = dict(base["intruder"], pos=it["pos"].copy(), vel=it["vel"].copy())
+        return out
 
     def sub_forces(self, s=0):
         n = self.N[s]
@@ -334,6 +357,12 @@ class Engine:
         _check(lib().nbc_timing_read(self.h, C.byref(ms), C.byref(nc), C.byref(nk), C.byref(nr)))
         return {"contact_ms": ms.value, "contact_launches": nc.value, "kernel_launches": nk.value,
                 "rebuilds": nr.value}
+
+    def timing_phases(self):
+        """Mean ms per timed step (timing level 2): clump, rebuild node, boundary, contact, step."""
+        a = np.zeros(5)
+        _check(lib().nbc_timing_phases(self.h, _p(a, P_D)))
+        return dict(zip(("clump", "rebuild", "boundary", "contact", "step"), a.tolist()))
 
     def info(self):
         b, ms = C.c_double(), C.c_double()

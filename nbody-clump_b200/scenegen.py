@@ -623,6 +623,34 @@ def scene_from_npz(path: str) -> dict:
     return scene
 
 
+def make_test_converging(n_side=8, seed=5, r=1e-3, loose=1.6, shrink=0.45, steps=1500, sigma=0.15):
+    """Tetrahedral clumps on a loose lattice (spacing `loose` x their extent, so
+    the first list holds little more than the pairs inside clumps), moving
+    towards the centre with a uniform compression rate that would shrink the
+    lattice by `shrink` over `steps` steps: the list grows several-fold
+    after the first step.  No walls, no gravity."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    K = n_side ** 3
+    scales = rng.lognormal(0.0, sigma, K)
+    locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
+    rmed = r * float(np.median(scales))
+    sp = 2 * 1.6 * rmed * loose
+    lo = np.array([0.5 * sp] * 3)
+    pts = lattice_points(rng, K, sp, lo, n_side, n_side, 0.03 * sp)
+    hi = pts.max(0) + 0.5 * sp
+    dt = 0.2 * rayleigh_dt(r * float(scales.min()), rho, MATERIAL["Ymod"], MATERIAL["Prat"])
+    rate = shrink / (steps * dt)
+    centre = 0.5 * (pts.min(0) + pts.max(0))
+    vel = -rate * (pts - centre)
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=steps, Thresh=0.2 * r,
+                            BranchLmtLen=96, Gravity=0.0,
+                            **{k: v for k, v in MATERIAL.items() if k != "rho"})
+    set_world_box(params, -4 * sp * np.ones(3), hi + 4 * sp)
+    return assemble(params, pts, random_unit_quaternions(rng, K), vel,
+                    rng.uniform(-50.0, 50.0, (K, 3)), props, locals_, radii, masses)
+
+
 def make_test_poly(n_clumps=150, seed=3, rmin=0.5e-3, rmax=2.5e-3, max_members=3, vel=0.5, angvel=200.0,
                    intruder="sphere", motion="constant_velocity", thresh_ratio=0.0003, dt=1e-7, steps=24,
                    wall="cube", bl=256):

@@ -295,3 +295,59 @@ def test_pair_capacity_overflow_recovers_identically(golden_dir):
         assert np.array_equal(tight.clumps()[k], roomy.clumps()[k]), k
     st = tight.stats()
     assert st["err"] == 0 and st["steps"] == 24
+
+
+def test_list_growth_inside_graph_keeps_history():
+    """Clumps converging from a loose lattice: the list grows from 3,099 to
+    ~17,000 pairs after the step graph was captured with buffers sized for
+    the first list (slack 1.0), so the pair buffers grow several times while
+    graph launches run.  Every kernel of the captured rebuild must cover the
+    grown list: the graph run equals the eager run bitwise and matches the
+    FP64 oracle's pair list and states."""
+    sc = sg.make_test_converging(steps=1500)
+    graph = nbc.Engine([sc], precision="f64", use_graph=True, pair_slack=1.0)
+    eager = nbc.Engine([sc], precision="f64", use_graph=False, pair_slack=1.0)
+    graph.step(1)
+    bytes_first = graph.info()["device_bytes"]
+    graph.step(1499)
+    eager.step(1500)
+    assert graph.info()["device_bytes"] > bytes_first, "the pair buffers never grew"
+    st = graph.stats()
+    assert st["err"] == 0 and st["npairs"] > 4 * 3099, st
+    graph.sync()
+    eager.sync()
+    for k in ("pos", "vel", "angvel", "quat"):
+        assert np.array_equal(graph.clumps()[k], eager.clumps()[k]), k
+    o = oracle.OracleScene(sc, threads=4)
+    o.step(1500)
+    lp_e, lpb_e = graph.pairs()
+    lp_o, lpb_o = o.pairs()
+    assert np.array_equal(lp_e, lp_o) and np.array_equal(lpb_e, lpb_o), "pair list differs from the oracle"
+    ce, co = graph.clumps(), o.clumps()
+    for k in ("pos", "quat"):
+        assert _rel(ce[k], co[k]) < 1e-9, (k, _rel(ce[k], co[k]))
+    for k in ("vel", "angvel"):
+        assert _rel(ce[k], co[k]) < 1e-6, (k, _rel(ce[k], co[k]))
+
+
+def test_restart_scene_carries_the_state(golden_dir):
+    """Engine.restart_scene: a new engine created from another engine's
+    state starts with that state (subsphere positions, clump poses and
+    velocities, intruder) and steps from it."""
+    sc = _scene(golden_dir, "tetra_gravity")
+    a = nbc.Engine([sc], precision="f64", use_graph=True)
+    a.step(12)
+    sc2 = a.restart_scene(sc)
+    b = nbc.Engine([sc2], precision="f64", use_graph=True)
+    ca, cb = a.clumps(), b.clumps()
+    for k in ("pos", "vel", "angvel", "quat"):
+        assert np.array_equal(ca[k], cb[k]), k
+    sa, sb = a.subspheres(), b.subspheres()
+    pa = np.empty_like(sa["pos"]); pa[sa["part_fix"]] = sa["pos"]
+    pb = np.empty_like(sb["pos"]); pb[sb["part_fix"]] = sb["pos"]
+    assert np.array_equal(pa, pb)
+    if sc.get("intruder") is not None:
+        assert np.array_equal(a.intruder()["pos"], b.intruder()["pos"])
+    b.step(5)
+    b.sync()
+    assert b.stats()["err"] == 0 and b.stats()["steps"] == 5
