@@ -214,28 +214,11 @@ class EngineT final : public EngineBase {
             }
         }
     }
-    // pair sum (k_contact) plus, where a boundary was touched, the wall and
-    // intruder force (k_boundary), added in Real as k_clump adds them
     void get_sub_forces(int s, double* f, double* t) override {
         refresh_dev();
         const ScenePar& P = hpar_[s];
-        const int n = P.nsub, o = P.sub_off;
-        std::vector<uint16_t> bb(n);
-        CK(cudaMemcpy(bb.data(), h_.bbits + o, n * sizeof(uint16_t), cudaMemcpyDeviceToHost));
-        for (int c = 0; c < 2; c++) {
-            double* dst = c == 0 ? f : t;
-            if (!dst) continue;
-            std::vector<R4<R>> a(n), b(n);
-            CK(cudaMemcpy(a.data(), (const R4<R>*)h_.fsum + (size_t)c * N_ + o, n * sizeof(R4<R>),
-                          cudaMemcpyDeviceToHost));
-            CK(cudaMemcpy(b.data(), (const R4<R>*)h_.fbnd + (size_t)c * N_ + o, n * sizeof(R4<R>),
-                          cudaMemcpyDeviceToHost));
-            for (int i = 0; i < n; i++) {
-                R x = a[i].x, y = a[i].y, z = a[i].z;
-                if (bb[i]) { x = x + b[i].x; y = y + b[i].y; z = z + b[i].z; }
-                dst[3 * i] = x; dst[3 * i + 1] = y; dst[3 * i + 2] = z;
-            }
-        }
+        pull_r4(h_.fsum, P.sub_off, P.nsub, f);
+        pull_r4((char*)h_.fsum + (size_t)N_ * sizeof(R4<R>), P.sub_off, P.nsub, t);
     }
     void get_force_parts(int s, double* parts) override {
         refresh_dev();
@@ -371,7 +354,7 @@ class EngineT final : public EngineBase {
     nbc_options opt_;
     DevMem mem_;
     cudaStream_t stream_ = nullptr;
-    cudaStream_t stream2_ = nullptr;   // second branch of a step: k_boundary beside k_contact
+    cudaStream_t stream2_ = nullptr;   // second branch of a step: k_boundary beside k_pairs
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Dev h_{};            // host copy of the device table
     Dev* d_ = nullptr;   // device table
@@ -386,14 +369,14 @@ class EngineT final : public EngineBase {
     int steps_done_ = 0;
     bool post_done_ = false;
     double last_ms_ = 0;
-    // step graphs by timing level: [0] plain, [1] event nodes around
-    // k_contact, [2] event nodes at every mark
+    // step graphs by timing level: [0] plain, [1] event nodes around the
+    // contact pass (k_pairs + k_sum), [2] event nodes at every mark
     cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t gexec_[3] = {nullptr, nullptr, nullptr};
     // kernel timing: one record of NMARK events per step, at the marks
     //   0 step start  1 after k_clump  2 after the rebuild node
-    //   3/4 around k_boundary and 5 start of k_contact (second branch)
-    //   6 end of k_contact  7 step end
+    //   3/4 around k_boundary and 5 start of the contact pass (second branch)
+    //   6 end of the contact pass (after k_sum)  7 step end
     static constexpr int NMARK = 8;
     static constexpr int PH_CLUMP = 0, PH_REBUILD = 1, PH_BOUNDARY = 2, PH_CONTACT = 3, PH_STEP = 4, NPH = 5;
     int timing_ = 0;
@@ -427,7 +410,7 @@ class EngineT final : public EngineBase {
         }
         return &ev_[(size_t)NMARK * ev_used_++];
     }
-    // marks recorded at timing level 1: only those around k_contact
+    // marks recorded at timing level 1: only those around the contact pass
     static bool mark_on(int level, int k) { return level >= 2 || (level == 1 && (k == 5 || k == 6)); }
     void harvest_events() {
         for (int k = 0; k < ev_used_; k++) {
@@ -706,6 +689,7 @@ class EngineT final : public EngineBase {
             h_.H[l] = mem_.alloc<char>(hist_bytes(cap));
             h_.touch[l] = mem_.alloc<uint8_t>(cap);
         }
+        h_.ctb = mem_.alloc<R4<R>>(4 * cap);
         h_.xfcn = mem_.alloc<R4<R>>(cap);
         h_.xcpt = mem_.alloc<double4>(cap);
     }
@@ -723,7 +707,7 @@ class EngineT final : public EngineBase {
         for (const ScenePar& P : hpar_) ref += (long long)P.nsub * (P.bl / 2);
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + sizeof(R4<R>) + sizeof(double4);
+        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4);
         const long long budget = (long long)(0.3 * (double)fr / per_pair);
         return std::min<long long>(std::max(cap, std::min(ref, budget)), 2000000000LL);
     }
@@ -763,6 +747,7 @@ class EngineT final : public EngineBase {
             mem_.release(old.H[l], hist_bytes(old.cap));
             mem_.release(old.touch[l], (size_t)old.cap);
         }
+        mem_.release(old.ctb, (size_t)old.cap * 4 * sizeof(R4<R>));
         mem_.release(old.xfcn, (size_t)old.cap * sizeof(R4<R>));
         mem_.release(old.xcpt, (size_t)old.cap * sizeof(double4));
         push_dev();
@@ -830,8 +815,9 @@ class EngineT final : public EngineBase {
         if (!capturing_ && timing_) launches_ += 1;
     }
     bool capturing_ = false;
-    // k_boundary on the second stream beside k_contact (fork and join by
-    // events, which become graph edges when captured)
+    // the contact pass: k_pairs, with k_boundary beside it on the second
+    // stream (fork and join by events, which become graph edges when
+    // captured), then k_sum
     void launch_contact(bool exp) {
         if (exp) {
             CK(cudaMemsetAsync(h_.xfcn, 0, (size_t)h_.cap * sizeof(R4<R>), stream_));
@@ -839,7 +825,7 @@ class EngineT final : public EngineBase {
         }
         CK(cudaEventRecord(ev_fork_, stream_));
         CK(cudaStreamWaitEvent(stream2_, ev_fork_, 0));
-        // the start of k_contact is marked on the side branch (same
+        // the start of the contact pass is marked on the side branch (same
         // dependencies), so only its end mark sits on the critical path
         mark(5, stream2_);
         mark(3, stream2_);
@@ -847,10 +833,14 @@ class EngineT final : public EngineBase {
         else k_boundary<R, false><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream2_>>>(d_);
         mark(4, stream2_);
         CK(cudaEventRecord(ev_join_, stream2_));
-        dim3 g(h_.cblocks);
+        // grid-stride over the pairs: a fixed grid stays valid as the list grows
+        if (exp) k_pairs<R, true><<<148 * 12, PR_THREADS, 0, stream_>>>(d_);
+        else k_pairs<R, false><<<148 * 12, PR_THREADS, 0, stream_>>>(d_);
+        CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
+        const dim3 g(cdiv(N_ * lanes_, CT_THREADS));
 #define NBC_CT(L)                                                                   \
-    if (exp) k_contact<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);             \
-    else k_contact<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
+    if (exp) k_sum<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);                 \
+    else k_sum<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
         if (lanes_ == 1) { NBC_CT(1) }
         else if (lanes_ == 2) { NBC_CT(2) }
         else if (lanes_ == 4) { NBC_CT(4) }
@@ -860,8 +850,7 @@ class EngineT final : public EngineBase {
 #undef NBC_CT
         CK(cudaGetLastError());
         mark(6, stream_);
-        CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
-        if (!capturing_ && timing_) launches_ += 2;
+        if (!capturing_ && timing_) launches_ += 3;
     }
     void scan(int* a, int n) {
         int nb = cdiv(n, SC_TILE);
@@ -992,7 +981,7 @@ class EngineT final : public EngineBase {
             for (int k = 0; k < NMARK; k++)
                 if (mark_on(timing_, k))
                     CK(cudaGraphExecEventRecordNodeSetEvent(gexec_[timing_], gev_node_[timing_][k], r[k]));
-            launches_ += 3;
+            launches_ += 4;
         }
         CK(cudaGraphLaunch(gexec_[timing_], stream_));
     }

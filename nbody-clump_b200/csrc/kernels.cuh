@@ -10,10 +10,10 @@
 //                ranges, reorder, count/scan/fill of the half pair list in
 //                the reference's traversal order, back references, history
 //                carry, clump member lists.
-//   k_boundary   per subsphere: walls and intruder (beside k_contact)
-//   k_contact    one lane group per subsphere: every pair of its front and
-//                back lists summed in registers; the pair owner also writes
-//                the new spring history.
+//   k_pairs      per listed pair: overlap test, the law once for both
+//                subspheres of a touching pair, the new spring history
+//   k_boundary   per subsphere: walls and intruder (beside k_pairs)
+//   k_sum        per subsphere: its pair slots, then walls and intruder
 #pragma once
 #include "nbc_dev.cuh"
 #include "nbc_math.cuh"
@@ -100,8 +100,6 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
         if (post) {
             // ---- member sums, CL_CHUNK members of the warp's range at a time
             const R4<R>* __restrict__ fs = (const R4<R>*)d.fsum;
-            const R4<R>* __restrict__ fb = (const R4<R>*)d.fbnd;
-            const uint16_t* __restrict__ bbits = d.bbits;
             const size_t N = (size_t)d.N;
             constexpr int J = CL_CHUNK / 32;
             F = v3(0.0, 0.0, 0.0);
@@ -115,26 +113,18 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
                 }
                 double4 ps[J];
                 R4<R> f4[J], t4[J];
-                uint16_t bb[J];
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     const int i = idx[j] < 0 ? 0 : idx[j];
                     ps[j] = posr[i];
                     f4[j] = fs[i];
                     t4[j] = fs[N + i];
-                    bb[j] = bbits[i];
                 }
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     if (idx[j] < 0) continue;
                     const int kk = owner(c0 + 32 * j + lane);
-                    R4<R> a = f4[j], b = t4[j];
-                    if (bb[j]) {
-                        // walls and intruder (k_boundary) after the pairs, in Real
-                        const R4<R> bf = fb[idx[j]], bt = fb[N + idx[j]];
-                        a.x = a.x + bf.x; a.y = a.y + bf.y; a.z = a.z + bf.z;
-                        b.x = b.x + bt.x; b.y = b.y + bt.y; b.z = b.z + bt.z;
-                    }
+                    const R4<R> a = f4[j], b = t4[j];
                     const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
                                             ps[j].z - s_cl[warp][2][kk]);
                     const V3<double> f = v3((double)a.x, (double)a.y, (double)a.z);
@@ -1089,6 +1079,44 @@ __device__ __forceinline__ bool pair_contact(const Law<R>& L, R cohesion, const 
     return true;
 }
 
+// The pair law evaluated once for both bodies of a touching pair: the force
+// and torque on a (as pair_contact) and on b.  Seen from b every input of the
+// law is exactly negated (normal, relative velocity, rotation increment,
+// negated history), so the law's outputs are negated too: the force on b is
+// -fa and its torque uses b's own lever Ab = (rb^2 - ra^2 + d^2) / 2d.
+template <typename R>
+__device__ __forceinline__ bool pair_contact2(const Law<R>& L, R cohesion, const Body<R>& a, const Body<R>& b,
+                                              V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& fa, V3<R>& ta, V3<R>& tb,
+                                              LawOut<R>& o, double& Ap_out, V3<double>& n_out) {
+    const double dx = b.p.x - a.p.x, dy = b.p.y - a.p.y, dz = b.p.z - a.p.z;
+    const double DistS = dx * dx + dy * dy + dz * dz;
+    const double DistL = sqrt(DistS);
+    const double Dn = a.p.w + b.p.w - DistL;
+    if (!(Dn > 0.0)) return false;
+    const double DistR = 1.0 / DistL;
+    const V3<double> nd = v3(DistR * dx, DistR * dy, DistR * dz);
+    const double Ap = 0.50 * (a.p.w * a.p.w - b.p.w * b.p.w + DistS) * DistR;
+    const double An = DistL - Ap;
+    const double Ab = 0.50 * (b.p.w * b.p.w - a.p.w * a.p.w + DistS) * DistR;
+    const V3<R> n = cvt<R>(nd);
+    const R ra = (R)a.p.w, rb = (R)b.p.w;
+    const R Rij = ra * rb / (ra + rb);
+    const R Mij = a.m * b.m / (a.m + b.m);
+    const V3<R> ARMa = a.arm + (R)Ap * n;
+    const V3<R> ARMb = b.arm - (R)An * n;
+    const V3<R> Vtot = (b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
+    const V3<R> Dth = L.dt * (a.w - b.w);
+    hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
+    const R br = L.beta * Rij;
+    fa = (-o.Fn - o.Ft) + (cohesion * br * br) * n;
+    const V3<R> nxF = cross(n, o.Ft);
+    ta = ((-(R)Ap) * nxF - o.Mr) - o.Mt;
+    tb = ((-(R)Ab) * nxF + o.Mr) + o.Mt;
+    Ap_out = Ap;
+    n_out = nd;
+    return true;
+}
+
 // a wall or intruder contact: normal n (toward the subsphere), lever Ap,
 // overlap Dn, wall point RVo relative to the wall centre
 template <typename R>
@@ -1375,102 +1403,103 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
     return a.w + b.w - sqrt(d2) > 0.0;
 }
 
-// Pairs, one lane group per subsphere: every pair of its front (owner) and
-// back lists, the owner's spring history read from the previous generation
-// and, for owner entries, the new history written; the pair sum written once
-// per subsphere (k_boundary runs beside it on a second graph branch; k_clump
-// adds its wall and intruder force after the pair sum).
-template <typename R, int LANES, bool EXPORT>
-__global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict__ dp) {
+// Pairs, one thread per listed owner pair (grid-stride, so a captured launch
+// covers a list that has grown since): the overlap test, and for touching
+// pairs the law once (ContactForce_clump_cuk, src/dem_force_clump.cu:3-163,
+// for both particles of the pair), the owner's new spring history, and the
+// force and torque on each of the two subspheres into per-pair slots.
+// k_sum adds the slots per subsphere in a fixed order.
+constexpr int PR_THREADS = 256;
+
+template <typename R, bool EXPORT>
+__global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    constexpr int SPB = CT_THREADS / LANES;
-    const int s = d.sblk_scene[blockIdx.x];
-    const ScenePar& P = d.par[s];
-    const int grp = threadIdx.x / LANES, lane = threadIdx.x % LANES;
-    const int i = P.sub_off + (blockIdx.x - P.cblk_off) * SPB + grp;
-    if (i >= P.sub_off + P.nsub) return;
-    const unsigned mask = group_mask<LANES>();
-    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-
-    Law<R> L;
-    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
-    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
-    const R coh = (R)P.cohesion;
-
-    // buffer pointers in registers: the history and flag stores could
-    // otherwise alias the pointer table and force re-reads per pair
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& Lst = d.L[lc & 1];
+    const int np = Lst.row[d.N];
     const int* __restrict__ nbr = Lst.nbr;
-    const int* __restrict__ bnbr = Lst.bnbr;
-    const int* __restrict__ bpair = Lst.bpair;
+    const int* __restrict__ own = Lst.own;
     const double4* __restrict__ posr = d.posr;
     const R4<R>* __restrict__ kin = (const R4<R>*)d.kin;
+    const int* __restrict__ sid = d.sid;
     const size_t N = (size_t)d.N;
     const size_t cap = (size_t)d.cap;
     const R4<R>* __restrict__ Hi = (const R4<R>*)d.H[hg & 1];
     R4<R>* __restrict__ Ho = (R4<R>*)d.H[(hg + 1) & 1];
     const uint8_t* __restrict__ ti = d.touch[hg & 1];
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
-
-    Body<R> me;
-    me.p = posr[i];
-    bool have_kin = false;
-    V3<R> F = v3<R>(0, 0, 0), T = F;
-
-    // front (owner) entries
-    const int rs = Lst.row[i], re = Lst.row[i + 1];
-    for (int k = rs + lane; k < re; k += LANES) {
-        const int jr = nbr[k];
-        if (jr < 0) continue;  // pair inside one clump (src/dem_force_clump.cu:18-19)
-        Body<R> ot;
-        ot.p = posr[jr];
-        if (!overlaps(me.p, ot.p)) { to[k] = 0; continue; }
-        if (!have_kin) { load_kin<R>(kin, N, i, me); have_kin = true; }
-        load_kin<R>(kin, N, jr, ot);
+    R4<R>* __restrict__ ct = (R4<R>*)d.ctb;
+    const bool one_scene = d.S == 1;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+        const int jr = nbr[p];
+        if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
+        const int i = own[p];
+        Body<R> a, b;
+        a.p = posr[i];
+        b.p = posr[jr];
+        if (!overlaps(a.p, b.p)) { to[p] = 0; continue; }
+        load_kin<R>(kin, N, i, a);
+        load_kin<R>(kin, N, jr, b);
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
-        if (ti[k]) hist_read<R>(Hi, cap, k, hs, ht, hr);
-        V3<R> fa, ta;
+        if (ti[p]) hist_read<R>(Hi, cap, p, hs, ht, hr);
+        const ScenePar& P = d.par[one_scene ? 0 : sid[i]];
+        Law<R> L;
+        L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+        L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
+        V3<R> fa, ta, tb;
         LawOut<R> o;
         double Ap;
         V3<double> nd;
-        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
-        F = F + fa;
-        T = T + ta;
-        hist_write<R>(Ho, cap, k, o.hs, o.ht, o.hr);
-        to[k] = 1;
+        pair_contact2<R>(L, (R)P.cohesion, a, b, hs, hr, ht, fa, ta, tb, o, Ap, nd);
+        hist_write<R>(Ho, cap, p, o.hs, o.ht, o.hr);
+        to[p] = 1;
+        ct[p] = pack<R>(fa, R(0));
+        ct[cap + p] = pack<R>(ta, R(0));
+        ct[2 * cap + p] = pack<R>(-fa, R(0));
+        ct[3 * cap + p] = pack<R>(tb, R(0));
         if (EXPORT) {
             R4<R>* xf = (R4<R>*)d.xfcn;
             double4* xc = (double4*)d.xcpt;
-            xf[k] = pack<R>(-o.Fn, R(0));
-            xc[k] = make_double4(me.p.x + Ap * nd.x, me.p.y + Ap * nd.y, me.p.z + Ap * nd.z, 0.0);
+            xf[p] = pack<R>(-o.Fn, R(0));
+            xc[p] = make_double4(a.p.x + Ap * nd.x, a.p.y + Ap * nd.y, a.p.z + Ap * nd.z, 0.0);
         }
     }
-    // back entries: the owner's stored history, seen from this side
+}
+
+// Per subsphere, one lane group: the pair slots of its front entries, then
+// those of its back entries (through the back-to-pair index), summed in
+// registers, then the wall and intruder force of k_boundary where a boundary
+// is touched; the sum written once (the force and torque k_clump reduces).
+template <typename R, int LANES, bool EXPORT>
+__global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int grp = (blockIdx.x * CT_THREADS + threadIdx.x) / LANES, lane = threadIdx.x % LANES;
+    const int i = grp;
+    if (i >= d.N) return;
+    const unsigned mask = group_mask<LANES>();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
+    const int lc = *d.lcur, hg = *d.hgen;
+    const PairList& Lst = d.L[lc & 1];
+    const size_t N = (size_t)d.N;
+    const size_t cap = (size_t)d.cap;
+    const uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
+    const R4<R>* __restrict__ ct = (const R4<R>*)d.ctb;
+    const int* __restrict__ bpair = Lst.bpair;
+    V3<R> F = v3<R>(0, 0, 0), T = F;
+    const int rs = Lst.row[i], re = Lst.row[i + 1];
+    for (int k = rs + lane; k < re; k += LANES) {
+        if (!to[k]) continue;
+        F = F + xyz<R>(ct[k]);
+        T = T + xyz<R>(ct[cap + k]);
+    }
     const int bs = Lst.brow[i], be = Lst.brow[i + 1];
     for (int k = bs + lane; k < be; k += LANES) {
-        const int jr = bnbr[k];
-        if (jr < 0) continue;
-        Body<R> ot;
-        ot.p = posr[jr];
-        if (!overlaps(me.p, ot.p)) continue;
         const int q = bpair[k];
-        if (q < 0) continue;  // unreachable with a consistent list
-        if (!have_kin) { load_kin<R>(kin, N, i, me); have_kin = true; }
-        load_kin<R>(kin, N, jr, ot);
-        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
-        if (ti[q]) {
-            hist_read<R>(Hi, cap, q, hs, ht, hr);
-            hs = -hs; ht = -ht; hr = -hr;
-        }
-        V3<R> fa, ta;
-        LawOut<R> o;
-        double Ap;
-        V3<double> nd;
-        pair_contact<R>(L, coh, me, ot, hs, hr, ht, fa, ta, o, Ap, nd);
-        F = F + fa;
-        T = T + ta;
+        if (q < 0 || !to[q]) continue;
+        F = F + xyz<R>(ct[2 * cap + q]);
+        T = T + xyz<R>(ct[3 * cap + q]);
     }
     F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
     T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
@@ -1480,12 +1509,17 @@ __global__ void __launch_bounds__(CT_THREADS, 3) k_contact(const Dev* __restrict
             xp[i] = pack<R>(F, R(0));
             xp[N + i] = pack<R>(T, R(0));
         }
+        if (d.bbits[i]) {
+            const R4<R>* fb = (const R4<R>*)d.fbnd;
+            F = F + xyz<R>(fb[i]);
+            T = T + xyz<R>(fb[N + i]);
+        }
         R4<R>* fs = (R4<R>*)d.fsum;
         fs[i] = pack<R>(F, R(0));
         fs[N + i] = pack<R>(T, R(0));
         if (!(isfinite((double)F.x) && isfinite((double)F.y) && isfinite((double)F.z) &&
               isfinite((double)T.x) && isfinite((double)T.y) && isfinite((double)T.z)))
-            atomicOr(&d.dyn[s].err, ERR_NONFINITE);
+            atomicOr(&d.dyn[d.sid[i]].err, ERR_NONFINITE);
     }
 }
 
