@@ -399,7 +399,7 @@ class EngineT final : public EngineBase {
         return n;
     }
     // kernels one rebuild launches (launch_rebuild)
-    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4; }
+    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4 + 8; }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -637,6 +637,8 @@ class EngineT final : public EngineBase {
         h_.cstart = mem_.alloc<int>(cells + 1);
         h_.scr = mem_.alloc<int>((size_t)N * 2 * SCR_CAP);
         h_.cnt_f = mem_.alloc<int>(N + 1);
+        h_.nrow = mem_.alloc<int>(N + 1);
+        h_.nbrow = mem_.alloc<int>(N + 1);
         h_.cnt_b = mem_.alloc<int>(N + 1);
         h_.sfc = mem_.alloc<int>(N);
         h_.xcnt = mem_.alloc<int>(N);
@@ -690,6 +692,8 @@ class EngineT final : public EngineBase {
             h_.touch[l] = mem_.alloc<uint8_t>(cap);
         }
         h_.ctb = mem_.alloc<R4<R>>(4 * cap);
+        h_.nfp = mem_.alloc<int>(cap);
+        h_.nbq = mem_.alloc<int>(cap);
         h_.xfcn = mem_.alloc<R4<R>>(cap);
         h_.xcpt = mem_.alloc<double4>(cap);
     }
@@ -707,7 +711,7 @@ class EngineT final : public EngineBase {
         for (const ScenePar& P : hpar_) ref += (long long)P.nsub * (P.bl / 2);
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4);
+        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) + 2 * sizeof(int);
         const long long budget = (long long)(0.3 * (double)fr / per_pair);
         return std::min<long long>(std::max(cap, std::min(ref, budget)), 2000000000LL);
     }
@@ -748,6 +752,8 @@ class EngineT final : public EngineBase {
             mem_.release(old.touch[l], (size_t)old.cap);
         }
         mem_.release(old.ctb, (size_t)old.cap * 4 * sizeof(R4<R>));
+        mem_.release(old.nfp, (size_t)old.cap * sizeof(int));
+        mem_.release(old.nbq, (size_t)old.cap * sizeof(int));
         mem_.release(old.xfcn, (size_t)old.cap * sizeof(R4<R>));
         mem_.release(old.xcpt, (size_t)old.cap * sizeof(double4));
         push_dev();
@@ -904,6 +910,11 @@ class EngineT final : public EngineBase {
         if (hgrid_) k_xsort<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
         k_carry<R><<<148 * 8, 256, 0, stream_>>>(d_);
+        // near rows of the new list
+        k_near<false, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
+        scan(h_.nrow, N_ + 1);
+        scan(h_.nbrow, N_ + 1);
+        k_near<true, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
         k_commit<<<cdiv(K_ + S_ + 1, B), B, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }

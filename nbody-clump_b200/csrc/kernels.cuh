@@ -898,6 +898,79 @@ __global__ void k_carry(const Dev* __restrict__ dp) {
         carry_one<R>(d, p);
 }
 
+// Near lists.  Between two rebuilds of a scene every subsphere stays within
+// Thresh of where it was at the rebuild (a larger displacement triggers the
+// next one), so a pair can only touch in that interval if its distance now is
+// below ri + rj + (Thresh + |c_i|) + (Thresh + |c_j|), where c is the
+// displacement since the scene's last rebuild (zero for the scenes rebuilt
+// now).  The near rows hold those entries of the new list: front entries as
+// pair indices, back entries as the index of their pair; the contact pass
+// visits only them.  Pairs left out cannot touch before the next rebuild, so
+// both of their touch flags are cleared here, as every contact pass in the
+// interval would have cleared them: results are the same as visiting the
+// whole list.
+template <bool FILL, int SL>
+__global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int lane = threadIdx.x % SL;
+    if (i >= d.N) return;
+    const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
+    const int gshift = (threadIdx.x & 31) & ~(SL - 1);
+    const unsigned lt = (1u << lane) - 1u;
+    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
+    const double4* __restrict__ posr = d.posr2;
+    const double4* __restrict__ cum = d.cum2;
+    uint8_t* __restrict__ t0 = d.touch[0];
+    uint8_t* __restrict__ t1 = d.touch[1];
+    const double th = d.par[d.sid[i]].thresh;
+    const double4 pi = posr[i];
+    const double4 c4 = cum[i];
+    const double ci = sqrt(c4.x * c4.x + c4.y * c4.y + c4.z * c4.z);
+    auto is_near = [&](int jr) {
+        const double4 pj = posr[jr];
+        const double4 cj4 = cum[jr];
+        const double cj = sqrt(cj4.x * cj4.x + cj4.y * cj4.y + cj4.z * cj4.z);
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        // a relative margin of 1e-6 covers the rounding of the displacement sums
+        const double lim = (pi.w + pj.w) + ((2.0 * th + ci + cj) * (1.0 + 1e-6) + 1e-12);
+        return dx * dx + dy * dy + dz * dz < lim * lim;
+    };
+    int nf = 0, nb = 0;
+    const int rf = FILL ? d.nrow[i] : 0, rb = FILL ? d.nbrow[i] : 0;
+    const int rs = Nw.row[i], re = Nw.row[i + 1];
+    for (int k0 = rs; k0 < re; k0 += SL) {
+        const int k = k0 + lane;
+        bool nr = false;
+        if (k < re) {
+            const int jr = Nw.nbr[k];
+            nr = jr >= 0 && is_near(jr);
+            if (!FILL && !nr) { t0[k] = 0; t1[k] = 0; }
+        }
+        const unsigned m = __ballot_sync(gm, nr) >> gshift;
+        if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
+        nf += __popc(m);
+    }
+    const int bs = Nw.brow[i], be = Nw.brow[i + 1];
+    for (int k0 = bs; k0 < be; k0 += SL) {
+        const int k = k0 + lane;
+        bool nr = false;
+        if (k < be) {
+            const int jr = Nw.bnbr[k];
+            nr = jr >= 0 && Nw.bpair[k] >= 0 && is_near(jr);
+        }
+        const unsigned m = __ballot_sync(gm, nr) >> gshift;
+        if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = Nw.bpair[k];
+        nb += __popc(m);
+    }
+    if (!FILL && lane == 0) {
+        d.nrow[i] = nf;
+        d.nbrow[i] = nb;
+        if (i == d.N - 1) { d.nrow[d.N] = 0; d.nbrow[d.N] = 0; }
+    }
+}
+
 // Finishes a rebuild: per-clump member lists in ascending subsphere order
 // (the order thrust::sort_by_key gives reduce_by_key, src/dem_clumpsphere.cu:
 // 123-147), scene bookkeeping, and the swap of list, history generation and
@@ -1403,7 +1476,7 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
     return a.w + b.w - sqrt(d2) > 0.0;
 }
 
-// Pairs, one thread per listed owner pair (grid-stride, so a captured launch
+// Pairs, one thread per near owner pair (grid-stride, so a captured launch
 // covers a list that has grown since): the overlap test, and for touching
 // pairs the law once (ContactForce_clump_cuk, src/dem_force_clump.cu:3-163,
 // for both particles of the pair), the owner's new spring history, and the
@@ -1417,7 +1490,8 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     if (*d.halt) return;
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& Lst = d.L[lc & 1];
-    const int np = Lst.row[d.N];
+    const int np = d.nrow[d.N];
+    const int* __restrict__ nfp = d.nfp;
     const int* __restrict__ nbr = Lst.nbr;
     const int* __restrict__ own = Lst.own;
     const double4* __restrict__ posr = d.posr;
@@ -1431,7 +1505,8 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
     R4<R>* __restrict__ ct = (R4<R>*)d.ctb;
     const bool one_scene = d.S == 1;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
+        const int p = nfp[w];
         const int jr = nbr[p];
         if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
         const int i = own[p];
@@ -1467,8 +1542,8 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     }
 }
 
-// Per subsphere, one lane group: the pair slots of its front entries, then
-// those of its back entries (through the back-to-pair index), summed in
+// Per subsphere, one lane group: the pair slots of its near front entries,
+// then those of its near back entries (by their pair index), summed in
 // registers, then the wall and intruder force of k_boundary where a boundary
 // is touched; the sum written once (the force and torque k_clump reduces).
 template <typename R, int LANES, bool EXPORT>
@@ -1480,24 +1555,25 @@ __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) 
     if (i >= d.N) return;
     const unsigned mask = group_mask<LANES>();
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-    const int lc = *d.lcur, hg = *d.hgen;
-    const PairList& Lst = d.L[lc & 1];
+    const int hg = *d.hgen;
     const size_t N = (size_t)d.N;
     const size_t cap = (size_t)d.cap;
     const uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
     const R4<R>* __restrict__ ct = (const R4<R>*)d.ctb;
-    const int* __restrict__ bpair = Lst.bpair;
+    const int* __restrict__ nfp = d.nfp;
+    const int* __restrict__ nbq = d.nbq;
     V3<R> F = v3<R>(0, 0, 0), T = F;
-    const int rs = Lst.row[i], re = Lst.row[i + 1];
-    for (int k = rs + lane; k < re; k += LANES) {
+    const int rs = d.nrow[i], re = d.nrow[i + 1];
+    for (int e = rs + lane; e < re; e += LANES) {
+        const int k = nfp[e];
         if (!to[k]) continue;
         F = F + xyz<R>(ct[k]);
         T = T + xyz<R>(ct[cap + k]);
     }
-    const int bs = Lst.brow[i], be = Lst.brow[i + 1];
-    for (int k = bs + lane; k < be; k += LANES) {
-        const int q = bpair[k];
-        if (q < 0 || !to[q]) continue;
+    const int bs = d.nbrow[i], be = d.nbrow[i + 1];
+    for (int e = bs + lane; e < be; e += LANES) {
+        const int q = nbq[e];
+        if (!to[q]) continue;
         F = F + xyz<R>(ct[2 * cap + q]);
         T = T + xyz<R>(ct[3 * cap + q]);
     }

@@ -137,6 +137,11 @@ struct Dev {
     void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
     void* ctb;        // Real4 [4][cap]: per pair force and torque on the owner, then on the partner
+    // near rows (the entries that can touch before the next rebuild)
+    int* nrow;        // [N+1] near front offsets
+    int* nbrow;       // [N+1] near back offsets
+    int* nfp;         // [cap] near front entries: pair index
+    int* nbq;         // [cap] near back entries: pair index
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
     int* gstep;       // steps started by k_clump (counts steps across graph launches)
     int* kc_done;     // blocks of k_clump finished (last-block detection)
