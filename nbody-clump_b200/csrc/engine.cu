@@ -694,6 +694,7 @@ class EngineT final : public EngineBase {
         h_.ctb = mem_.alloc<R4<R>>(4 * cap);
         h_.nfp = mem_.alloc<int>(cap);
         h_.nbq = mem_.alloc<int>(cap);
+        h_.nearf = mem_.alloc<uint8_t>(cap);
         h_.xfcn = mem_.alloc<R4<R>>(cap);
         h_.xcpt = mem_.alloc<double4>(cap);
     }
@@ -711,7 +712,7 @@ class EngineT final : public EngineBase {
         for (const ScenePar& P : hpar_) ref += (long long)P.nsub * (P.bl / 2);
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) + 2 * sizeof(int);
+        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) + 2 * sizeof(int) + 1;
         const long long budget = (long long)(0.3 * (double)fr / per_pair);
         return std::min<long long>(std::max(cap, std::min(ref, budget)), 2000000000LL);
     }
@@ -754,6 +755,7 @@ class EngineT final : public EngineBase {
         mem_.release(old.ctb, (size_t)old.cap * 4 * sizeof(R4<R>));
         mem_.release(old.nfp, (size_t)old.cap * sizeof(int));
         mem_.release(old.nbq, (size_t)old.cap * sizeof(int));
+        mem_.release(old.nearf, (size_t)old.cap);
         mem_.release(old.xfcn, (size_t)old.cap * sizeof(R4<R>));
         mem_.release(old.xcpt, (size_t)old.cap * sizeof(double4));
         push_dev();

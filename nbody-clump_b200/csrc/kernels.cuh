@@ -850,10 +850,27 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p) {
     const uint8_t* ti = d.touch[hg & 1];
     uint8_t* to = d.touch[(hg + 1) & 1];
     const int jr = Nw.nbr[p];
-    if (jr < 0) { to[p] = 0; return; }
+    if (jr < 0) { to[p] = 0; d.nearf[p] = 0; return; }  // pair inside one clump
     const int i = Nw.own[p], j = jr;
     const int s = d.sid[i];
     const ScenePar& P = d.par[s];
+    // near flag of the new pair (see k_near): distance below ri + rj + m, with
+    // m = 2 Thresh in a scene rebuilt now and 4 Thresh in one that is not (its
+    // subspheres are up to Thresh from their last rebuild already)
+    {
+        const double4 pi = d.posr2[i], pj = d.posr2[j];
+        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const double m = (d.dyn[s].rebuild ? 2.0 : 4.0) * P.thresh * (1.0 + 1e-6) + 1e-12;
+        const double lim = (pi.w + pj.w) + m;
+        const bool nr = dx * dx + dy * dy + dz * dz < lim * lim;
+        d.nearf[p] = nr;
+        if (!nr) {
+            // cannot touch before the next rebuild: no live history (the
+            // other touch buffer is still read here and is cleared by k_near)
+            to[p] = 0;
+            return;
+        }
+    }
     int q = -1;
     R sign = R(1);
     if (!d.dyn[s].rebuild) {
@@ -898,17 +915,18 @@ __global__ void k_carry(const Dev* __restrict__ dp) {
         carry_one<R>(d, p);
 }
 
-// Near lists.  Between two rebuilds of a scene every subsphere stays within
+// Near rows.  Between two rebuilds of a scene every subsphere stays within
 // Thresh of where it was at the rebuild (a larger displacement triggers the
-// next one), so a pair can only touch in that interval if its distance now is
-// below ri + rj + (Thresh + |c_i|) + (Thresh + |c_j|), where c is the
-// displacement since the scene's last rebuild (zero for the scenes rebuilt
-// now).  The near rows hold those entries of the new list: front entries as
-// pair indices, back entries as the index of their pair; the contact pass
-// visits only them.  Pairs left out cannot touch before the next rebuild, so
-// both of their touch flags are cleared here, as every contact pass in the
-// interval would have cleared them: results are the same as visiting the
-// whole list.
+// next one), so a pair whose distance at a rebuild is at least ri + rj +
+// 2 Thresh cannot touch before the next one (4 Thresh for a scene of the
+// batch that is not rebuilt now: its subspheres are up to Thresh from their
+// last rebuild already).  k_carry flags the near pairs of the new list and
+// clears the touch flag it writes for the others, k_near the other flag (the
+// one k_carry reads), as every contact pass in the interval would have
+// cleared them; the near rows list the near entries
+// (front: pair index in row order, back: the pair index of each near back
+// entry) and the contact pass visits only them, with the same results as
+// visiting the whole list.
 template <bool FILL, int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -920,34 +938,16 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     const int gshift = (threadIdx.x & 31) & ~(SL - 1);
     const unsigned lt = (1u << lane) - 1u;
     const PairList& Nw = d.L[(*d.lcur + 1) & 1];
-    const double4* __restrict__ posr = d.posr2;
-    const double4* __restrict__ cum = d.cum2;
-    uint8_t* __restrict__ t0 = d.touch[0];
-    uint8_t* __restrict__ t1 = d.touch[1];
-    const double th = d.par[d.sid[i]].thresh;
-    const double4 pi = posr[i];
-    const double4 c4 = cum[i];
-    const double ci = sqrt(c4.x * c4.x + c4.y * c4.y + c4.z * c4.z);
-    auto is_near = [&](int jr) {
-        const double4 pj = posr[jr];
-        const double4 cj4 = cum[jr];
-        const double cj = sqrt(cj4.x * cj4.x + cj4.y * cj4.y + cj4.z * cj4.z);
-        const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        // a relative margin of 1e-6 covers the rounding of the displacement sums
-        const double lim = (pi.w + pj.w) + ((2.0 * th + ci + cj) * (1.0 + 1e-6) + 1e-12);
-        return dx * dx + dy * dy + dz * dz < lim * lim;
-    };
+    const uint8_t* __restrict__ nearf = d.nearf;
+    const int* __restrict__ bpair = Nw.bpair;
+    uint8_t* __restrict__ tprev = d.touch[*d.hgen & 1];   // read by k_carry, free now
     int nf = 0, nb = 0;
     const int rf = FILL ? d.nrow[i] : 0, rb = FILL ? d.nbrow[i] : 0;
     const int rs = Nw.row[i], re = Nw.row[i + 1];
     for (int k0 = rs; k0 < re; k0 += SL) {
         const int k = k0 + lane;
-        bool nr = false;
-        if (k < re) {
-            const int jr = Nw.nbr[k];
-            nr = jr >= 0 && is_near(jr);
-            if (!FILL && !nr) { t0[k] = 0; t1[k] = 0; }
-        }
+        const bool nr = k < re && nearf[k];
+        if (!FILL && k < re && !nr) tprev[k] = 0;
         const unsigned m = __ballot_sync(gm, nr) >> gshift;
         if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
         nf += __popc(m);
@@ -955,13 +955,11 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     const int bs = Nw.brow[i], be = Nw.brow[i + 1];
     for (int k0 = bs; k0 < be; k0 += SL) {
         const int k = k0 + lane;
-        bool nr = false;
-        if (k < be) {
-            const int jr = Nw.bnbr[k];
-            nr = jr >= 0 && Nw.bpair[k] >= 0 && is_near(jr);
-        }
+        int q = -1;
+        if (k < be) q = bpair[k];
+        const bool nr = q >= 0 && nearf[q];
         const unsigned m = __ballot_sync(gm, nr) >> gshift;
-        if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = Nw.bpair[k];
+        if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = q;
         nb += __popc(m);
     }
     if (!FILL && lane == 0) {

@@ -142,6 +142,7 @@ struct Dev {
     int* nbrow;       // [N+1] near back offsets
     int* nfp;         // [cap] near front entries: pair index
     int* nbq;         // [cap] near back entries: pair index
+    uint8_t* nearf;   // [cap] pair can touch before the next rebuild
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
     int* gstep;       // steps started by k_clump (counts steps across graph launches)
     int* kc_done;     // blocks of k_clump finished (last-block detection)
