@@ -181,6 +181,7 @@ nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_ste
  * level table the reference's sphere path reads, src/dem_io.cu:204-248):
  * writes level[n] (0 = coarsest) and level_cell[<=max_levels], returns the
  * number of levels (1 = the reference's single-level grid is best). */
+#define NBC_MAX_LEVELS 6
 int nbc_choose_levels(const double* radius, int n, int max_levels, int* level, double* level_cell);
 
 /* --- allocation-free cell sort ------------------------------------------

@@ -16,7 +16,7 @@
 
 namespace nbc {
 
-constexpr int MAX_LEVELS = 4;
+constexpr int MAX_LEVELS = 6;   // NBC_MAX_LEVELS of the C ABI
 constexpr int WALL_NONE = 0, WALL_CUBE = 1, WALL_CYL = 2;
 // boundary slots of a subsphere: cube faces UpX, LowX, UpY, LowY, UpZ, LowZ
 // (src/dem_force_cube_wall_clump.cu:228-292), or cylinder regions bottom cap,

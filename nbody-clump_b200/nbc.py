@@ -68,16 +68,16 @@ def cell_sort_noalloc(pos_ptr: int, n: int, grid: GridDesc, perm_ptr: int, key_p
                                        C.c_void_p(key_ptr), C.c_void_p(stream)))
 
 
-def choose_levels(radius, max_levels=4):
+def choose_levels(radius, max_levels=6):
     """Hierarchical-grid levels for these radii: (level[n], level_cell[L])."""
     r = np.ascontiguousarray(radius, dtype=np.float64)
     lv = np.zeros(len(r), np.int32)
-    cell = np.zeros(4)
+    cell = np.zeros(max(8, int(max_levels)))
     L = lib().nbc_choose_levels(_p(r), len(r), int(max_levels), _p(lv, P_I), _p(cell))
     return lv, cell[:L].copy()
 
 
-def with_levels(scene: dict, max_levels=4) -> dict:
+def with_levels(scene: dict, max_levels=6) -> dict:
     """The scene with a hierarchical grid chosen by nbc_choose_levels (or
     unchanged when one level is best)."""
     lv, cell = choose_levels(scene["sub"]["radius"], max_levels)
