@@ -217,27 +217,49 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
-            for (int m = M0 + lane; m < M1; m += 32) {
-                const int i = mem_idx[m];
-                const int kk = owner(m);
-                const double4 lo = lom[i], old = posw[i], c = cum[i];
-                const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
-                                                s_cl[warp][12][kk]);
-                const V3<double> arm = rot_b2w(qk, v3(lo.x, lo.y, lo.z));
-                const V3<double> p = v3(s_cl[warp][0][kk] + arm.x, s_cl[warp][1][kk] + arm.y, s_cl[warp][2][kk] + arm.z);
-                const V3<double> cn = v3((c.x + p.x) - old.x, (c.y + p.y) - old.y, (c.z + p.z) - old.z);
-                const V3<double> vk = v3(s_cl[warp][3][kk], s_cl[warp][4][kk], s_cl[warp][5][kk]);
-                const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
-                cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
-                posw[i] = make_double4(p.x, p.y, p.z, old.w);
-                kv[i] = pack<R>(cvt<R>(vk), (R)lo.w);
-                kw[i] = pack<R>(cvt<R>(wk), R(0));
-                ka[i] = pack<R>(cvt<R>(arm), R(0));
-                const int sk = s_sc[warp][kk];
-                if (len_floor(cn) > d.par[sk].thresh) {
-                    SceneDyn& y = d.dyn[sk];
-                    if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
-                    if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
+            // J members per lane at a time: all indices, then all member
+            // records, in flight together
+            constexpr int JP = CL_CHUNK / 32;
+            for (int c0 = M0; c0 < M1; c0 += 32 * JP) {
+                int idx[JP];
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    const int m = c0 + 32 * j + lane;
+                    idx[j] = m < M1 ? mem_idx[m] : -1;
+                }
+                double4 lo[JP], old[JP], cu[JP];
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    const int i = idx[j] < 0 ? 0 : idx[j];
+                    lo[j] = lom[i];
+                    old[j] = posw[i];
+                    cu[j] = cum[i];
+                }
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    if (idx[j] < 0) continue;
+                    const int i = idx[j];
+                    const int kk = owner(c0 + 32 * j + lane);
+                    const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
+                                                    s_cl[warp][12][kk]);
+                    const V3<double> arm = rot_b2w(qk, v3(lo[j].x, lo[j].y, lo[j].z));
+                    const V3<double> p = v3(s_cl[warp][0][kk] + arm.x, s_cl[warp][1][kk] + arm.y,
+                                            s_cl[warp][2][kk] + arm.z);
+                    const double4 c = cu[j], o = old[j];
+                    const V3<double> cn = v3((c.x + p.x) - o.x, (c.y + p.y) - o.y, (c.z + p.z) - o.z);
+                    const V3<double> vk = v3(s_cl[warp][3][kk], s_cl[warp][4][kk], s_cl[warp][5][kk]);
+                    const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
+                    cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
+                    posw[i] = make_double4(p.x, p.y, p.z, o.w);
+                    kv[i] = pack<R>(cvt<R>(vk), (R)lo[j].w);
+                    kw[i] = pack<R>(cvt<R>(wk), R(0));
+                    ka[i] = pack<R>(cvt<R>(arm), R(0));
+                    const int sk = s_sc[warp][kk];
+                    if (len_floor(cn) > d.par[sk].thresh) {
+                        SceneDyn& y = d.dyn[sk];
+                        if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
+                        if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
+                    }
                 }
             }
         } else if (post && isc) {
