@@ -150,7 +150,7 @@ def run_b200(args, world, rank, local):
         while left > 0:           # each call returns after the device finished (stream synchronised)
             c = min(left, 1000)
             eng.step(c)
-            pair_samples.append((c, eng.stats()["npairs"]))
+            pair_samples.append((c, eng.stats()["npairs"]) + eng.contact_counts())
             left -= c
         t1 = time.perf_counter()
     tm = eng.timing_read()
@@ -165,7 +165,10 @@ def run_b200(args, world, rank, local):
             print(json.dumps({"profile_run": True, "ms_per_step": secs * 1e3 / args.steps,
                               "contact_ms_avg": tm["contact_ms"] / max(1, tm["contact_launches"]),
                               "npairs": st1["npairs"], "rebuilds": st1["rebuilds"] - st0["rebuilds"],
-                              "phases_ms": eng.timing_phases()}), flush=True)
+                              "phases_ms": eng.timing_phases(),
+                              "near_touching": eng.contact_counts(),
+                              "alg_bytes": algorithmic_contact_bytes(N, *eng.contact_counts(), args.precision)}),
+                  flush=True)
         return
 
     # ---- end to end through the C ABI with host buffers -----------------
@@ -189,15 +192,17 @@ def run_b200(args, world, rank, local):
 
     # ---- roofline of the contact kernel -----------------------------------
     pk, pk_kind = peaks()
-    npairs = sum(c * p for c, p in pair_samples) / max(1, sum(c for c, _ in pair_samples))
-    alg = algorithmic_contact_bytes(N, K, npairs, args.precision)
+    wsum = max(1, sum(s[0] for s in pair_samples))
+    npairs, nnear, ntouch = (sum(s[0] * s[q] for s in pair_samples) / wsum for q in (1, 2, 3))
+    alg = algorithmic_contact_bytes(N, nnear, ntouch, args.precision)
     avg_ms = tm["contact_ms"] / max(1, tm["contact_launches"])
     achieved = alg / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
     traffic, traffic_note = None, None
     tp = os.path.join(REPO, "profiles", "contact_traffic.json")
     if os.path.exists(tp):
         tj = json.load(open(tp))
-        if tj.get("lanes") == eng_lanes(args) and tj.get("precision") == args.precision:
+        if (tj.get("kernels") == ["k_pairs", "k_sum"] and tj.get("lanes") == eng_lanes(args)
+                and tj.get("precision") == args.precision):
             # captured on a smaller list state; scaled to this run's mean
             # listed pairs by the ratio of algorithmic bytes
             traffic = tj["dram_bytes_per_launch"] * alg / tj["algorithmic_bytes_at_capture"]
@@ -224,8 +229,9 @@ def run_b200(args, world, rank, local):
             "gpu_launches": tm["kernel_launches"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
                          "frac": achieved / pk if pk else None, "traffic": traffic,
-                         "kernel": "k_contact", "avg_launch_ms": avg_ms,
-                         "alg_bytes_per_launch": alg, "mean_pairs_listed": npairs, "peak_kind": pk_kind,
+                         "kernel": "contact pass (k_pairs + k_sum)", "avg_launch_ms": avg_ms,
+                         "alg_bytes_per_launch": alg, "mean_pairs_listed": npairs,
+                         "mean_pairs_near": nnear, "mean_pairs_touching": ntouch, "peak_kind": pk_kind,
                          "traffic_note": traffic_note},
             "cpu_baseline": cpu,
             "clocks": clocks,
@@ -237,7 +243,7 @@ def run_b200(args, world, rank, local):
 
 
 def eng_lanes(args):
-    return args.lanes if args.lanes in (1, 2, 4, 8, 16, 32) else 4
+    return args.lanes if args.lanes in (1, 2, 4, 8, 16, 32) else 2
 
 
 def workload(args, seed):
@@ -264,19 +270,23 @@ def save_state(args):
     print(json.dumps({"saved": args.save_state, "steps": args.advance, "npairs": eng.stats()["npairs"]}), flush=True)
 
 
-def algorithmic_contact_bytes(N, K, npairs, precision):
-    """Unique bytes the contact kernel must move per launch.
+def algorithmic_contact_bytes(N, nnear, ntouch, precision):
+    """Unique bytes the contact pass (k_pairs + k_sum) must move per step.
 
-    Per listed pair (front + back entry): partner indices 4 + 8 B and the
-    contact flag written 1 B.  Per subsphere: FP64 position and radius 32 B,
-    contact kinematics 3 x Real4, list offsets 4 x 4 B, boundary bits 2 B,
-    force and torque out 2 x Real4.  History traffic (36 B per touching pair
-    each way in FP32) is excluded here because the touching fraction is not
-    known host-side; ncu's DRAM bytes are reported beside this figure."""
-    r4 = 16 if precision == "mixed" else 32
-    per_pair = 4 + 8 + 1
+    Per near pair (the pairs that can touch before the next rebuild): its
+    index in the near front and back rows 4 + 4 B, partner and owner 4 + 4 B,
+    the touch flag written 1 B and read twice by the sum 2 B.  Per touching
+    pair: the previous touch flag 1 B, the spring history read and written
+    (2 Real4 + 1 Real each way) and the four per-pair force slots written and
+    read (4 Real4 each way).  Per subsphere: FP64 position and radius 32 B,
+    contact kinematics 3 Real4, near-row offsets 16 B, boundary bits 2 B,
+    force and torque out 2 Real4."""
+    r = 4 if precision == "mixed" else 8
+    r4 = 4 * r
+    per_near = 4 + 4 + 4 + 4 + 1 + 2
+    per_touch = 1 + 2 * (2 * r4 + r) + 2 * 4 * r4
     per_sub = 32 + 3 * r4 + 16 + 2 + 2 * r4
-    return per_pair * npairs + per_sub * N
+    return per_near * nnear + per_touch * ntouch + per_sub * N
 
 
 def cpu_baseline(args):

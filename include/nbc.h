@@ -88,7 +88,7 @@ typedef struct {
 
 typedef struct {
     int precision;      /* NBC_PREC_* */
-    int lanes;          /* lanes per subsphere in the contact kernel: 1, 2, 4, 8, 16 or 32 (0 = 4) */
+    int lanes;          /* lanes per subsphere in the contact sum: 1, 2, 4, 8, 16 or 32 (0 = 2) */
     int use_graph;      /* 1: one CUDA graph per step with a conditional rebuild node */
     int device;         /* CUDA device ordinal */
     double pair_slack;  /* pair capacity = slack * pairs of the first list; 0 = 1.6 and at least
@@ -127,6 +127,10 @@ nbc_status nbc_sync(nbc_engine* e);
 nbc_status nbc_num_scenes(const nbc_engine* e, int* n);
 /* steps, rebuilds, pairs in the current list, error bits */
 nbc_status nbc_scene_stats(nbc_engine* e, int scene, int* steps, int* rebuilds, int* npairs, int* err);
+/* over all scenes: the near pairs of the current list (those that can touch
+ * before the next rebuild; the contact pass visits only them) and how many
+ * of them touched at the last contact pass; no reference counterpart */
+nbc_status nbc_contact_counts(nbc_engine* e, long long* near_pairs, long long* touching_pairs);
 /* subspheres in the engine's current (cell-sorted) order; part_fix is the
  * original ph row (ParticleID of src/dem_clump.cu:170-171) */
 nbc_status nbc_get_subspheres(nbc_engine* e, int scene, int* part_fix, int* clump_id, double* pos,

@@ -119,6 +119,11 @@ nbc_status nbc_num_scenes(const nbc_engine* e, int* n) {
     return NBC_OK;
 }
 
+nbc_status nbc_contact_counts(nbc_engine* e, long long* nnear, long long* ntouch) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
+    return guard([&] { e->eng->contact_counts(nnear, ntouch); });
+}
+
 nbc_status nbc_scene_stats(nbc_engine* e, int s, int* steps, int* rebuilds, int* npairs, int* err) {
     if (bad_scene(e, s)) return fail(NBC_ERR_ARG, "bad scene");
     return guard([&] { e->eng->stats(s, steps, rebuilds, npairs, err); });

@@ -154,6 +154,21 @@ class EngineT final : public EngineBase {
         if (npairs) *npairs = y.npairs;
         if (err) *err = y.err;
     }
+    // near pairs of the current list (the pairs the contact pass visits) and
+    // those of them that touched at the last contact pass, over all scenes
+    void contact_counts(long long* nnear, long long* ntouch) override {
+        refresh_dev();
+        const int nn = read_int(h_.nrow + N_);
+        const int hg = read_int(h_.hgen);
+        std::vector<int> idx(nn);
+        std::vector<uint8_t> t(h_.cap);
+        if (nn) CK(cudaMemcpy(idx.data(), h_.nfp, (size_t)nn * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(t.data(), h_.touch[(hg + 1) & 1], (size_t)h_.cap, cudaMemcpyDeviceToHost));
+        long long c = 0;
+        for (int p : idx) c += t[p] != 0;
+        if (nnear) *nnear = nn;
+        if (ntouch) *ntouch = c;
+    }
     void get_subspheres(int s, int* fix, int* cid, double* pos, double* rad) override {
         refresh_dev();
         const ScenePar& P = hpar_[s];
@@ -453,7 +468,7 @@ class EngineT final : public EngineBase {
         CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
         CK(cudaMallocHost(&hflag_, 4 * sizeof(int)));
         lanes_ = opt_.lanes == 1 || opt_.lanes == 2 || opt_.lanes == 4 || opt_.lanes == 8 || opt_.lanes == 16 ||
-                         opt_.lanes == 32 ? opt_.lanes : 4;
+                         opt_.lanes == 32 ? opt_.lanes : 2;
         search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
         const int spb = CT_THREADS / lanes_;
         S_ = (int)sc.size();

@@ -21,6 +21,7 @@ class EngineBase {
     virtual void sync() = 0;
     virtual int num_scenes() const = 0;
     virtual void stats(int s, int* steps, int* rebuilds, int* npairs, int* err) = 0;
+    virtual void contact_counts(long long* nnear, long long* ntouch) = 0;
     virtual void get_subspheres(int s, int* fix, int* cid, double* pos, double* rad) = 0;
     virtual void get_body(int s, double* local, double* mass) = 0;
     virtual void get_clump_prop(int s, double* prop) = 0;

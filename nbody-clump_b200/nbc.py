@@ -93,7 +93,7 @@ class Options(C.Structure):
 
 EXPORTED = [
     "nbc_last_error", "nbc_default_options", "nbc_open", "nbc_run", "nbc_create", "nbc_destroy",
-    "nbc_step", "nbc_step_export", "nbc_sync", "nbc_num_scenes", "nbc_scene_stats",
+    "nbc_step", "nbc_step_export", "nbc_sync", "nbc_num_scenes", "nbc_scene_stats", "nbc_contact_counts",
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
@@ -275,6 +275,12 @@ class Engine:
         _check(lib().nbc_get_clumps(self.h, s, _p(o["pos"]), _p(o["vel"]), _p(o["quat"]),
                                     _p(o["angvel"]), _p(o["force"]), _p(o["torque"])))
         return o
+
+    def contact_counts(self):
+        """(near pairs of the current list, those that touched at the last step)."""
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(lib().nbc_contact_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def restart_scene(self, base, s=0):
         """A scene that starts from scene s's current state: subsphere
