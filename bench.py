@@ -31,6 +31,9 @@ import time
 import numpy as np
 
 REPO = os.path.dirname(os.path.abspath(__file__))
+# concurrent scene streams (batch and serving modes) need more than the default
+# 8 hardware work queues; read by CUDA when the process first uses it
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 sys.path.insert(0, os.path.join(REPO, "nbody-clump_b200"))
 import scenegen as sg  # noqa: E402
 
@@ -310,6 +313,128 @@ def cpu_baseline(args):
             "sample": f"{n} steps of the same 200,000-subsphere scene after its first step, single thread"}
 
 
+def run_batch(args):
+    """cfg3: n independent cfg1-style scenes (clump counts log-uniform in
+    [500, 50,000], friction U[0.2, 0.8], own seeds), advanced together
+    (nbc_batch: one engine, stream and graph per scene, launches interleaved)
+    against the same scenes one at a time on the plain engine.  Both timings
+    include engine creation (upload) and the first list build."""
+    import nbc
+    scenes = [nbc.with_levels(s) for s in sg.make_cfg3(args.scenes, steps=args.steps)]
+    n_sub = sum(int(s["params"]["NumberBody"]) for s in scenes)
+    opts = dict(precision=args.precision, pair_slack=1.6)
+    t0 = time.perf_counter()
+    b = nbc.Batch(scenes, **opts)
+    t1 = time.perf_counter()
+    b.step(args.steps)
+    for e in b.engines:
+        e.sync()
+    t2 = time.perf_counter()
+    b.close()
+    bc, bs = t1 - t0, t2 - t1
+    pc = ps = 0.0
+    for sc in scenes:
+        t0 = time.perf_counter()
+        e = nbc.Engine([sc], **opts)
+        t1 = time.perf_counter()
+        e.step(args.steps)
+        e.sync()
+        ps += time.perf_counter() - t1
+        pc += t1 - t0
+        e.close()
+    work = n_sub * args.steps
+    arm = lambda c, st: {"create_s": c, "step_s": st, "scenes_per_s": args.scenes / (c + st),
+                         "subsphere_steps_per_s": work / st}
+    line = {"metric": "scenes/s and subsphere-steps/s, batched vs plain (cfg3)",
+            "workload": f"cfg3: {args.scenes} settling scenes, clumps log-uniform in [500, 50000], {args.steps} steps each",
+            "subspheres_total": n_sub, "batched": arm(bc, bs), "plain": arm(pc, ps),
+            "speedup_steps": ps / bs, "speedup_scenes_per_s": (pc + ps) / (bc + bs),
+            "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded numpy beds)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """cfg4: a Poisson stream (rate --rate) of --requests penetration
+    requests.  Beds come from a bank of pre-settled polydisperse beds (clumps
+    of 1..8 subspheres, radii log-uniform in [0.5, 5] mm) at log-spaced sizes
+    between 1k and 200k subspheres; a request takes the bank bed nearest its
+    size (log-uniform in [1k, 200k]), a sphere intruder of radius U[5, 20] mm
+    driven down at U[0.05, 0.5] m/s, friction U[0.2, 0.8], and ends when the
+    intruder has travelled --depth-ratio x its radius.  Served: nbc_server
+    (admission by HBM budget, continuous batching); plain: the same requests
+    solved one at a time, their time-to-result from the same arrival times."""
+    import nbc
+    rng = np.random.default_rng(20260828)
+    sizes = np.unique(np.round(np.exp(np.linspace(np.log(1000), np.log(200_000), args.bank))).astype(int))
+    bank = []
+    for i, n in enumerate(sizes):
+        half = 0.5 * (n * 3.0e-7) ** (1 / 3) + 0.01
+        bed = nbc.with_levels(sg.make_poly_bed(int(n), 20260828 + i, half))
+        e = nbc.Engine([bed], precision=args.precision)
+        e.step(args.settle)
+        bank.append(e.restart_scene(bed))
+        e.close()
+    reqs = []
+    t_arr = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    for k in range(args.requests):
+        n = np.exp(rng.uniform(np.log(1000), np.log(200_000)))
+        bed = bank[int(np.argmin(np.abs(np.log(sizes) - np.log(n))))]
+        r_i, v, mu = rng.uniform(5e-3, 20e-3), rng.uniform(0.05, 0.5), rng.uniform(0.2, 0.8)
+        sc = sg.with_sphere_intruder(bed, r_i, v, mu=mu)
+        nsteps = int(math.ceil(args.depth_ratio * r_i / (v * sc["params"]["StepSize"])))
+        reqs.append((t_arr[k], sc, nsteps))
+    work = sum(int(sc["params"]["NumberBody"]) * n for _, sc, n in reqs)
+    # served: arrivals replayed in real time
+    srv = nbc.Server(budget_bytes=args.budget_gb * 1e9, max_active=args.slots, precision=args.precision)
+    t0 = time.perf_counter()
+    nxt, ids, done_at = 0, {}, {}
+    while len(done_at) < len(reqs):
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and reqs[nxt][0] <= now:
+            ids[srv.submit(reqs[nxt][1], reqs[nxt][2], 100)] = nxt
+            nxt += 1
+        st = srv.advance(chunk=args.chunk)
+        if st["running"] == 0 and st["queued"] == 0 and nxt < len(reqs):
+            time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
+        now = time.perf_counter() - t0
+        for rid in [r for r in ids if srv.state(r)[0] >= 2]:
+            done_at[ids.pop(rid)] = now
+            srv.release(rid)
+    makespan = time.perf_counter() - t0
+    srv.close()
+    ttr_srv = [done_at[k] - reqs[k][0] for k in range(len(reqs))]
+    # plain: the same requests one at a time; time-to-result from the same arrivals
+    svc = []
+    for _, sc, n in reqs:
+        t = time.perf_counter()
+        e = nbc.Engine([sc], precision=args.precision, pair_slack=1.6)
+        e.step(n)
+        e.sync()
+        e.intruder_history(count=min(n, 1024))
+        e.close()
+        svc.append(time.perf_counter() - t)
+    fin, ttr_plain = 0.0, []
+    for (arr, _, _), sv in zip(reqs, svc):
+        fin = max(arr, fin) + sv
+        ttr_plain.append(fin - arr)
+    q = lambda v, p: float(np.percentile(v, p))
+    line = {"metric": "time-to-result p50/p99 and throughput, served vs plain (cfg4)",
+            "workload": f"cfg4: {len(reqs)} penetration requests, Poisson rate {args.rate}/s, "
+                        f"subspheres log-uniform in [1k, 200k] (bank of {len(sizes)} pre-settled beds), "
+                        f"depth {args.depth_ratio} x intruder radius",
+            "subsphere_steps_total": work,
+            "served": {"p50_s": q(ttr_srv, 50), "p99_s": q(ttr_srv, 99), "makespan_s": makespan,
+                       "requests_per_s": len(reqs) / makespan, "subsphere_steps_per_s": work / makespan},
+            "plain": {"p50_s": q(ttr_plain, 50), "p99_s": q(ttr_plain, 99), "makespan_s": fin,
+                      "requests_per_s": len(reqs) / sum(svc), "subsphere_steps_per_s": work / sum(svc)},
+            "throughput_ratio": (work / makespan) / (work / sum(svc)),
+            "slots": args.slots, "budget_gb": args.budget_gb,
+            "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded numpy beds settled by the engine)"}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank, local):
     """The reference arm: the project's FP64 CPU restatement of the
     reference's clump step (the reference itself has no CPU implementation),
@@ -365,10 +490,24 @@ def main():
     ap.add_argument("--scene", default=None, help="run this scene file instead of generating cfg1")
     ap.add_argument("--save-state", default=None, help="advance --advance steps, save the state to this file, exit")
     ap.add_argument("--advance", type=int, default=18000)
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg3", "cfg4"])
+    ap.add_argument("--scenes", type=int, default=256, help="cfg3: number of scenes")
+    ap.add_argument("--requests", type=int, default=200, help="cfg4: number of requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="cfg4: mean arrivals per second")
+    ap.add_argument("--bank", type=int, default=8, help="cfg4: pre-settled beds in the bank")
+    ap.add_argument("--settle", type=int, default=3000, help="cfg4: settling steps of each bank bed")
+    ap.add_argument("--depth-ratio", type=float, default=0.5, help="cfg4: intruder travel / radius")
+    ap.add_argument("--slots", type=int, default=64, help="cfg4: requests running at once at most")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="cfg4: device memory for requests")
+    ap.add_argument("--chunk", type=int, default=256, help="cfg4: steps per server round")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)
-    if args.save_state:
+    if args.workload == "cfg3":
+        run_batch(args)
+    elif args.workload == "cfg4":
+        run_serve(args)
+    elif args.save_state:
         save_state(args)
     elif args.impl == "reference":
         run_reference(args, world, rank, local)

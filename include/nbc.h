@@ -181,6 +181,45 @@ nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 
+/* --- batches of independent scenes ---------------------------------------
+ * No reference counterpart (the reference runs one scene per process).  Each
+ * scene gets its own engine, stream and step graph; nbc_batch_step enqueues a
+ * chunk of steps on every scene's stream before it waits for any, so the
+ * scenes' kernels overlap on the GPU.  Each scene rebuilds its list on its
+ * own schedule: its results are bitwise those of the scene run alone.  For
+ * the streams to run concurrently set CUDA_DEVICE_MAX_CONNECTIONS (e.g. 32)
+ * in the environment before the process first uses CUDA. */
+typedef struct nbc_batch nbc_batch;
+nbc_status nbc_batch_create(const nbc_scene_desc* const* scenes, int n_scenes, const nbc_options* opt,
+                            nbc_batch** out);
+nbc_status nbc_batch_step(nbc_batch* b, int nsteps);
+/* the engine of scene i, for the getters above; owned by the batch (do not
+ * pass it to nbc_destroy), valid until nbc_batch_destroy */
+nbc_status nbc_batch_engine(nbc_batch* b, int i, nbc_engine** e);
+nbc_status nbc_batch_destroy(nbc_batch* b);
+
+/* --- request server (continuous batching) ---------------------------------
+ * No reference counterpart.  A request is a scene (copied at submission) and
+ * a step count.  nbc_server_advance admits queued requests in arrival order
+ * while the head fits the device-memory budget (estimated before creation,
+ * actual after) and fewer than max_active run, advances every running request
+ * by up to `chunk` steps (at most 1024) with their kernels overlapping, and
+ * retires the finished ones, freeing their memory.  A request's result is
+ * the intruder reaction force and torque every sample_every steps and at its
+ * last step ([n_samples][6], the reference's fc record,
+ * src/dem_integrate_penetrator.cu:108-109) and the intruder's final position;
+ * it equals the result of the same scene run alone.  state: 0 queued,
+ * 1 running, 2 done, 3 failed (the error is returned). */
+typedef struct nbc_server nbc_server;
+nbc_status nbc_server_create(const nbc_options* opt, double budget_bytes, int max_active, nbc_server** out);
+nbc_status nbc_server_submit(nbc_server* s, const nbc_scene_desc* scene, int nsteps, int sample_every, int* id);
+nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_running, int* n_queued, int* n_finished);
+nbc_status nbc_server_result(nbc_server* s, int id, int* state, int* steps_done, int* n_samples, double* curve,
+                             double* intr_pos);
+nbc_status nbc_server_release(nbc_server* s, int id);
+nbc_status nbc_server_memory(nbc_server* s, double* used_bytes, double* budget_bytes);
+nbc_status nbc_server_destroy(nbc_server* s);
+
 /* Hierarchical-grid levels for a radius distribution (replaces the grid.bt
  * level table the reference's sphere path reads, src/dem_io.cu:204-248):
  * writes level[n] (0 = coarsest) and level_cell[<=max_levels], returns the

@@ -92,44 +92,69 @@ class EngineT final : public EngineBase {
 
     void step(int n, bool exp) override {
         auto t0 = std::chrono::steady_clock::now();
+        int left = n;
+        while (left > 0) {
+            if (exp && left == 1) {
+                clear_post_done();
+                run_step_eager(true);
+                left -= 1;
+                continue;
+            }
+            enqueue(exp ? left - 1 : left);
+            left -= wait_steps();
+        }
+        CK(cudaStreamSynchronize(stream_));
+        check_errors();
+        last_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    // Asynchronous stepping: enqueue puts up to n steps on the engine's
+    // stream and returns without waiting for them (an engine's first step,
+    // and every step without a graph, runs eagerly before it returns);
+    // wait_steps waits, finishes a step that a pair-capacity overflow stopped
+    // and returns the number of steps done.  A step after an overflow is not
+    // done: the caller enqueues the rest again.
+    int enqueue(int n) override {
+        clear_post_done();
+        pend_ = 0;
+        pend_eager_ = 0;
+        while (n > 0 && (!opt_.use_graph || steps_done_ < 1)) {
+            run_step_eager(false);
+            pend_eager_++;
+            n--;
+        }
+        if (n <= 0) return pend_eager_;
+        if (!gexec_[timing_]) capture(timing_);
+        pend_before_ = read_gstep();
+        for (int i = 0; i < n; i++) launch_graph();
+        pend_ = n;
+        return pend_eager_ + n;
+    }
+    int wait_steps() override {
+        int done = pend_eager_;
+        if (pend_ > 0) {
+            CK(cudaStreamSynchronize(stream_));
+            const int started = read_gstep() - pend_before_;
+            if (read_int(h_.halt)) {
+                // the last step started stopped at its rebuild: finish it on the host path
+                steps_done_ += started - 1;
+                recover_halt();
+            } else {
+                steps_done_ += started;
+            }
+            done += started;
+        }
+        pend_ = pend_eager_ = 0;
+        CK(cudaStreamSynchronize(stream_));
+        check_errors();
+        return done;
+    }
+    void clear_post_done() {
         if (post_done_) {
             // a sync applied the pending half-kick: the next pass must not repeat it
             CK(cudaMemsetAsync(h_.post_pending, 0, sizeof(int), stream_));
             post_done_ = false;
         }
-        int left = n;
-        while (left > 0) {
-            bool last = left == 1;
-            if (exp && last) {
-                run_step_eager(true);
-                left -= 1;
-                continue;
-            }
-            if (!opt_.use_graph || steps_done_ < 1) {
-                run_step_eager(false);
-                left -= 1;
-                continue;
-            }
-            if (!gexec_[timing_]) capture(timing_);
-            int chunk = exp ? left - 1 : left;
-            int before = read_gstep();
-            for (int i = 0; i < chunk; i++) launch_graph();
-            CK(cudaStreamSynchronize(stream_));
-            int started = read_gstep() - before;
-            if (read_int(h_.halt)) {
-                // the last step started stopped at its rebuild: finish it on the host path
-                steps_done_ += started - 1;
-                left -= started - 1;
-                recover_halt();
-                left -= 1;
-            } else {
-                steps_done_ += started;
-                left -= started;
-            }
-        }
-        CK(cudaStreamSynchronize(stream_));
-        check_errors();
-        last_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
 
     void sync() override {
@@ -382,6 +407,7 @@ class EngineT final : public EngineBase {
     std::vector<int> start_step_;
     int* hflag_ = nullptr;  // pinned
     int steps_done_ = 0;
+    int pend_ = 0, pend_eager_ = 0, pend_before_ = 0;  // steps enqueued and not yet waited for
     bool post_done_ = false;
     double last_ms_ = 0;
     // step graphs by timing level: [0] plain, [1] event nodes around the

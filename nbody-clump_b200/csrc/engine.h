@@ -18,6 +18,8 @@ class EngineBase {
    public:
     virtual ~EngineBase() {}
     virtual void step(int n, bool export_last) = 0;
+    virtual int enqueue(int n) = 0;   // launch up to n steps without waiting
+    virtual int wait_steps() = 0;     // wait for them; the number done
     virtual void sync() = 0;
     virtual int num_scenes() const = 0;
     virtual void stats(int s, int* steps, int* rebuilds, int* npairs, int* err) = 0;

@@ -99,6 +99,9 @@ EXPORTED = [
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
     "nbc_timing_phases",
     "nbc_engine_info", "nbc_cell_sort_noalloc", "nbc_choose_levels",
+    "nbc_batch_create", "nbc_batch_step", "nbc_batch_engine", "nbc_batch_destroy",
+    "nbc_server_create", "nbc_server_submit", "nbc_server_advance", "nbc_server_result",
+    "nbc_server_release", "nbc_server_memory", "nbc_server_destroy",
 ]
 
 _lib = None
@@ -236,10 +239,22 @@ class Engine:
     def run(self):
         _check(lib().nbc_run(self.h))
 
+    @classmethod
+    def borrowed(cls, handle, scene):
+        """A view of an engine owned by a Batch (not destroyed by close)."""
+        self = cls.__new__(cls)
+        self._descs = []
+        self.N = [int(scene["params"]["NumberBody"])]
+        self.K = [int(scene["params"]["ClumpNum"])]
+        self.BL = [int(scene["params"]["BranchLmtLen"])]
+        self.h = handle
+        self._owner = False
+        return self
+
     def close(self):
-        if getattr(self, "h", None) is not None and self.h.value:
+        if getattr(self, "h", None) is not None and self.h.value and getattr(self, "_owner", True):
             lib().nbc_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -374,3 +389,102 @@ class Engine:
         b, ms = C.c_double(), C.c_double()
         _check(lib().nbc_engine_info(self.h, C.byref(b), C.byref(ms)))
         return {"device_bytes": b.value, "last_step_ms": ms.value}
+
+
+def _options(precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0, search_lanes=0):
+    o = Options()
+    lib().nbc_default_options(C.byref(o))
+    o.precision, o.lanes, o.use_graph, o.device = PREC[precision], lanes, int(use_graph), device
+    o.pair_slack = pair_slack
+    o.search_lanes = search_lanes
+    return o
+
+
+class Batch:
+    """Independent scenes advanced together (nbc_batch_*): one engine, stream
+    and step graph per scene, their launches interleaved; each scene's
+    results equal those of the scene run alone."""
+
+    def __init__(self, scenes, **opts):
+        self._descs = [scene_desc(s) for s in scenes]
+        arr = (C.POINTER(SceneDesc) * len(scenes))(*[C.pointer(d) for d, _ in self._descs])
+        o = _options(**opts)
+        h = C.c_void_p()
+        _check(lib().nbc_batch_create(arr, len(scenes), C.byref(o), C.byref(h)))
+        self.h = h
+        self.engines = []
+        for i, sc in enumerate(scenes):
+            e = C.c_void_p()
+            _check(lib().nbc_batch_engine(self.h, i, C.byref(e)))
+            self.engines.append(Engine.borrowed(e, sc))
+
+    def step(self, n=1):
+        _check(lib().nbc_batch_step(self.h, int(n)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            for e in self.engines:
+                e.h = None
+            lib().nbc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous batching of requests (nbc_server_*): a request is a scene
+    and a step count; its result is the intruder reaction sampled every
+    sample_every steps and the intruder's final position."""
+
+    def __init__(self, budget_bytes, max_active=64, **opts):
+        o = _options(**opts)
+        h = C.c_void_p()
+        _check(lib().nbc_server_create(C.byref(o), C.c_double(budget_bytes), int(max_active), C.byref(h)))
+        self.h = h
+
+    def submit(self, scene, nsteps, sample_every=100):
+        d, keep = scene_desc(scene)
+        rid = C.c_int()
+        _check(lib().nbc_server_submit(self.h, C.byref(d), int(nsteps), int(sample_every), C.byref(rid)))
+        return rid.value
+
+    def advance(self, chunk=200):
+        a, q, f = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().nbc_server_advance(self.h, int(chunk), C.byref(a), C.byref(q), C.byref(f)))
+        return {"running": a.value, "queued": q.value, "finished": f.value}
+
+    def state(self, rid):
+        st, done, ns = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().nbc_server_result(self.h, int(rid), C.byref(st), C.byref(done), C.byref(ns), None, None))
+        return st.value, done.value, ns.value
+
+    def result(self, rid):
+        st, done, ns = self.state(rid)
+        if st != 2:
+            return None
+        curve, pos = np.zeros((ns, 6)), np.zeros(3)
+        _check(lib().nbc_server_result(self.h, int(rid), None, None, None, _p(curve), _p(pos)))
+        return {"curve": curve, "intr_pos": pos, "steps": done}
+
+    def release(self, rid):
+        _check(lib().nbc_server_release(self.h, int(rid)))
+
+    def memory(self):
+        u, b = C.c_double(), C.c_double()
+        _check(lib().nbc_server_memory(self.h, C.byref(u), C.byref(b)))
+        return u.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().nbc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -298,11 +298,14 @@ def layered_packing(rng, diam, R, z0, jitter=0.02):
     return pts
 
 
-def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000) -> dict:
+def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000, mu: float = None,
+              fit_box: bool = False) -> dict:
     """50,000 tetrahedral clumps (4 subspheres, r = 1 mm, centre offset 0.6 r,
     log-normal(0, 0.2) size scale, random orientation) seeded in layers inside
     a closed cylinder wall (R = 60 mm, half-height 300 mm, axis z, floor at
-    z = 0) and settling under gravity."""
+    z = 0) and settling under gravity.  mu overrides the friction; fit_box
+    ends the hashing box a few clump sizes above the seeded bed (the bed only
+    falls) instead of at the cylinder top, so small beds get small grids."""
     rng = np.random.default_rng(seed)
     r, rho = 1e-3, MATERIAL["rho"]
     scales = rng.lognormal(0.0, 0.2, n_clumps)
@@ -315,13 +318,123 @@ def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000) 
     dt = 0.2 * rayleigh_dt(rmin, rho, MATERIAL["Ymod"], MATERIAL["Prat"])
     params = default_params(StepSize=dt, EndStep=steps, OutputInterval=steps,
                             Ymod=MATERIAL["Ymod"], Prat=MATERIAL["Prat"],
-                            Frcoe=MATERIAL["Frcoe"], NormRes=MATERIAL["NormRes"],
+                            Frcoe=MATERIAL["Frcoe"] if mu is None else float(mu), NormRes=MATERIAL["NormRes"],
                             Thresh=0.2 * rmin, BranchLmtLen=96)
-    set_world_box(params, (-R, -R, 0.0), (R, R, 2 * H))
+    top = min(2 * H, float(pts[:, 2].max() + 5 * diam.max())) if fit_box else 2 * H
+    set_world_box(params, (-R, -R, 0.0), (R, R, top))
     K = n_clumps
     return assemble(params, pts, q, np.zeros((K, 3)), np.zeros((K, 3)), props,
                     locals_, radii, masses,
                     cylinder=make_cylinder(R, H, (0, 0, H)))
+
+
+def make_cfg3(n_scenes: int = 256, seed: int = 20260828, steps: int = 20000, kmin: int = 500,
+              kmax: int = 50_000) -> list:
+    """The batched workload: n_scenes independent cfg1-style settling scenes,
+    clump counts log-uniform in [kmin, kmax], friction uniform in [0.2, 0.8],
+    scene s seeded with seed + s."""
+    rng = np.random.default_rng(seed)
+    ks = np.exp(rng.uniform(np.log(kmin), np.log(kmax), n_scenes)).astype(int)
+    mus = rng.uniform(0.2, 0.8, n_scenes)
+    return [make_cfg1(int(k), seed + s, steps, mu=float(m), fit_box=True) for s, (k, m) in enumerate(zip(ks, mus))]
+
+
+def _poly_members(rng, n_clumps, rmin, rmax, max_members, rho):
+    """Clumps of 1..max_members subspheres (uniform): a clump size r_c
+    log-uniform in [rmin, rmax], member radii r_c x U(0.8, 1), centres at
+    0.6 r_c in random directions; mass 0.8 x the spheres' and inertia
+    0.4 M r_c^2 (a filled-clump approximation)."""
+    m = rng.integers(1, max_members + 1, n_clumps)
+    rc = np.exp(rng.uniform(np.log(rmin), np.log(rmax), n_clumps))
+    locals_, radii, masses, props, ext = [], [], [], [], np.zeros(n_clumps)
+    for k in range(n_clumps):
+        rr = rc[k] * rng.uniform(0.8, 1.0, m[k])
+        if m[k] == 1:
+            cen = np.zeros((1, 3))
+        else:
+            d = rng.normal(size=(m[k], 3))
+            d /= np.linalg.norm(d, axis=1)[:, None]
+            cen = d * (0.6 * rc[k])
+            cen = cen - cen.mean(0)
+        M = 0.8 * float(np.sum(rho * 4.0 / 3.0 * np.pi * rr ** 3))
+        I = 0.4 * M * rc[k] ** 2
+        locals_.append(cen)
+        radii.append(rr)
+        masses.append(np.full(m[k], M / m[k]))
+        props.append([I, I, I, M])
+        ext[k] = 2.0 * (np.linalg.norm(cen, axis=1).max() + rr.max())
+    return locals_, radii, masses, np.array(props), ext
+
+
+def layered_packing_box(rng, diam, hx, hy, z0, jitter=0.02):
+    """Clump centres in square-lattice layers inside [-hx, hx] x [-hy, hy],
+    largest clumps first, each layer spaced by its largest diameter * 1.05."""
+    order = np.argsort(-diam, kind="stable")
+    pts = np.zeros((len(diam), 3))
+    z, i = z0, 0
+    while i < len(order):
+        d = 1.05 * diam[order[i]]
+        nx, ny = max(1, int(2 * hx / d)), max(1, int(2 * hy / d))
+        gx = (np.arange(nx) - (nx - 1) / 2.0) * d
+        gy = (np.arange(ny) - (ny - 1) / 2.0) * d
+        X, Y = np.meshgrid(gx, gy, indexing="ij")
+        xy = np.stack([X.ravel(), Y.ravel()], axis=1)
+        take = order[i:i + len(xy)]
+        sel = rng.permutation(len(xy))[:len(take)]
+        pts[take, 0:2] = xy[sel] + rng.uniform(-jitter * d, jitter * d, (len(take), 2))
+        pts[take, 2] = z + 0.5 * d
+        z += d
+        i += len(take)
+    return pts
+
+
+def make_poly_bed(n_sub, seed, half_xy, rmin=0.5e-3, rmax=5e-3, max_members=8, mu=0.5, steps=1000):
+    """A polydisperse bed of about n_sub subspheres (clumps of 1..8, radii
+    log-uniform in [rmin, rmax]) seeded in layers in a cube wall of half
+    width half_xy, floor at z = 0, the wall and hashing box 1.5 x the seeded
+    height tall; settling under gravity from rest."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    k = max(1, int(round(n_sub / (0.5 * (1 + max_members)))))
+    locals_, radii, masses, props, ext = _poly_members(rng, k, rmin, rmax, max_members, rho)
+    pts = layered_packing_box(rng, ext, half_xy, half_xy, 0.0)
+    top = float(pts[:, 2].max() + ext.max())
+    H = 0.75 * top
+    rs = np.concatenate(radii)
+    dt = 0.2 * rayleigh_dt(float(rs.min()), rho, MATERIAL["Ymod"], MATERIAL["Prat"])
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=steps,
+                            Ymod=MATERIAL["Ymod"], Prat=MATERIAL["Prat"], Frcoe=float(mu),
+                            NormRes=MATERIAL["NormRes"], Thresh=0.2 * float(rs.min()), BranchLmtLen=96)
+    set_world_box(params, (-half_xy, -half_xy, 0.0), (half_xy, half_xy, 2 * H))
+    K = len(locals_)
+    return assemble(params, pts, random_unit_quaternions(rng, K), np.zeros((K, 3)), np.zeros((K, 3)),
+                    props, locals_, radii, masses, cube=make_cube((half_xy, half_xy, H), (0, 0, H)))
+
+
+def with_sphere_intruder(scene, radius, speed, mu=None, xy=(0.0, 0.0), gap=0.0, mass=1.0):
+    """The scene with a sphere intruder of this radius above xy, its lowest
+    point `gap` above the highest subsphere under it, driven down at a
+    constant speed (the reference's constant_velocity motion)."""
+    out = dict(scene)
+    out["params"] = dict(scene["params"])
+    if mu is not None:
+        out["params"]["Frcoe"] = float(mu)
+    pos, rad = scene["sub"]["pos"], scene["sub"]["radius"]
+    z = _place_intruder_on_bed(pos, rad, xy, "sphere", radius, radius, -gap)
+    I = 0.4 * mass * radius ** 2
+    out["intruder"] = make_intruder("sphere", radius, (xy[0], xy[1], z), (0, 0, -float(speed)),
+                                    prop=(I, I, I, mass), motion="constant_velocity")
+    out["params"]["isIntruder"] = 1
+    return out
+
+
+def make_cfg2(n_sub: int = 1_000_000, seed: int = 20260828, steps: int = 56000, half_xy: float = 0.2) -> dict:
+    """Polydisperse penetration bed: 1,000,000 subspheres in clumps of 1..8,
+    radii log-uniform in [0.5, 5] mm, in a 0.4 x 0.4 m cube wall made tall
+    enough for the seeded bed (the 0.3 m box of the configuration cannot hold
+    these spheres); settle it, then add the 20 mm intruder with
+    with_sphere_intruder(bed, 0.02, 0.1)."""
+    return make_poly_bed(n_sub, seed, half_xy, steps=steps)
 
 
 # ----------------------------------------------------------------------------
