@@ -354,16 +354,9 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
-    """cfg4: a Poisson stream (rate --rate) of --requests penetration
-    requests.  Beds come from a bank of pre-settled polydisperse beds (clumps
-    of 1..8 subspheres, radii log-uniform in [0.5, 5] mm) at log-spaced sizes
-    between 1k and 200k subspheres; a request takes the bank bed nearest its
-    size (log-uniform in [1k, 200k]), a sphere intruder of radius U[5, 20] mm
-    driven down at U[0.05, 0.5] m/s, friction U[0.2, 0.8], and ends when the
-    intruder has travelled --depth-ratio x its radius.  Served: nbc_server
-    (admission by HBM budget, continuous batching); plain: the same requests
-    solved one at a time, their time-to-result from the same arrival times."""
+def serve_requests(args):
+    """The cfg4 requests: (arrival time, scene, steps) in arrival order, and
+    the bank bed sizes."""
     import nbc
     rng = np.random.default_rng(20260828)
     sizes = np.unique(np.round(np.exp(np.linspace(np.log(1000), np.log(200_000), args.bank))).astype(int))
@@ -384,11 +377,26 @@ def run_serve(args):
         sc = sg.with_sphere_intruder(bed, r_i, v, mu=mu)
         nsteps = int(math.ceil(args.depth_ratio * r_i / (v * sc["params"]["StepSize"])))
         reqs.append((t_arr[k], sc, nsteps))
+    return sizes, reqs
+
+
+def run_serve(args):
+    """cfg4: a Poisson stream (rate --rate) of --requests penetration
+    requests.  Beds come from a bank of pre-settled polydisperse beds (clumps
+    of 1..8 subspheres, radii log-uniform in [0.5, 5] mm) at log-spaced sizes
+    between 1k and 200k subspheres; a request takes the bank bed nearest its
+    size (log-uniform in [1k, 200k]), a sphere intruder of radius U[5, 20] mm
+    driven down at U[0.05, 0.5] m/s, friction U[0.2, 0.8], and ends when the
+    intruder has travelled --depth-ratio x its radius.  Served: nbc_server
+    (admission by HBM budget, continuous batching); plain: the same requests
+    solved one at a time, their time-to-result from the same arrival times."""
+    import nbc
+    sizes, reqs = serve_requests(args)
     work = sum(int(sc["params"]["NumberBody"]) * n for _, sc, n in reqs)
     # served: arrivals replayed in real time
     srv = nbc.Server(budget_bytes=args.budget_gb * 1e9, max_active=args.slots, precision=args.precision)
     t0 = time.perf_counter()
-    nxt, ids, done_at = 0, {}, {}
+    nxt, ids, done_at, failed = 0, {}, {}, []
     while len(done_at) < len(reqs):
         now = time.perf_counter() - t0
         while nxt < len(reqs) and reqs[nxt][0] <= now:
@@ -399,19 +407,30 @@ def run_serve(args):
             time.sleep(max(0.0, reqs[nxt][0] - (time.perf_counter() - t0)))
         now = time.perf_counter() - t0
         for rid in [r for r in ids if srv.state(r)[0] >= 2]:
-            done_at[ids.pop(rid)] = now
+            k = ids.pop(rid)
+            done_at[k] = now
+            try:
+                srv.result(rid)
+            except nbc.NbcError as err:
+                failed.append({"request": k, "subspheres": int(reqs[k][1]["params"]["NumberBody"]),
+                               "intruder_radius": reqs[k][1]["intruder"]["radius"],
+                               "speed": -float(reqs[k][1]["intruder"]["vel"][2]),
+                               "friction": reqs[k][1]["params"]["Frcoe"], "error": str(err)})
             srv.release(rid)
     makespan = time.perf_counter() - t0
     srv.close()
     ttr_srv = [done_at[k] - reqs[k][0] for k in range(len(reqs))]
     # plain: the same requests one at a time; time-to-result from the same arrivals
-    svc = []
-    for _, sc, n in reqs:
+    svc, failed_plain = [], []
+    for k, (_, sc, n) in enumerate(reqs):
         t = time.perf_counter()
         e = nbc.Engine([sc], precision=args.precision, pair_slack=1.6)
-        e.step(n)
-        e.sync()
-        e.intruder_history(count=min(n, 1024))
+        try:
+            e.step(n)
+            e.sync()
+            e.intruder_history(count=min(n, 1024))
+        except nbc.NbcError:
+            failed_plain.append(k)
         e.close()
         svc.append(time.perf_counter() - t)
     fin, ttr_plain = 0.0, []
@@ -429,6 +448,7 @@ def run_serve(args):
             "plain": {"p50_s": q(ttr_plain, 50), "p99_s": q(ttr_plain, 99), "makespan_s": fin,
                       "requests_per_s": len(reqs) / sum(svc), "subsphere_steps_per_s": work / sum(svc)},
             "throughput_ratio": (work / makespan) / (work / sum(svc)),
+            "failed": failed, "failed_plain": failed_plain,
             "slots": args.slots, "budget_gb": args.budget_gb,
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy beds settled by the engine)"}

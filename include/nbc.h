@@ -209,7 +209,8 @@ nbc_status nbc_batch_destroy(nbc_batch* b);
  * last step ([n_samples][6], the reference's fc record,
  * src/dem_integrate_penetrator.cu:108-109) and the intruder's final position;
  * it equals the result of the same scene run alone.  state: 0 queued,
- * 1 running, 2 done, 3 failed (the error is returned). */
+ * 1 running, 2 done, 3 failed (a request whose engine fails is retired with
+ * its error and the others go on; asking for its curve returns the error). */
 typedef struct nbc_server nbc_server;
 nbc_status nbc_server_create(const nbc_options* opt, double budget_bytes, int max_active, nbc_server** out);
 nbc_status nbc_server_submit(nbc_server* s, const nbc_scene_desc* scene, int nsteps, int sample_every, int* id);

@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -47,29 +49,82 @@ static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b)
 // ---------------------------------------------------------------------------
 // device memory helper
 // ---------------------------------------------------------------------------
+// Stream-ordered allocations from the device's default memory pool, kept in
+// the pool when freed: creating and destroying engines while others run (a
+// request server) neither synchronises the device (as cudaMalloc / cudaFree
+// do) nor returns memory to the driver between requests.
 struct DevMem {
     std::vector<void*> ptrs;
     double bytes = 0;
+    cudaStream_t stream = nullptr;
     template <typename T>
     T* alloc(size_t n) {
         void* p = nullptr;
         size_t b = std::max<size_t>(n, 1) * sizeof(T);
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = cudaMallocAsync(&p, b, stream);
         if (e != cudaSuccess) throw CudaError(std::string("cudaMalloc ") + std::to_string(b) + ": " + cudaGetErrorString(e));
-        CK(cudaMemset(p, 0, b));
+        CK(cudaMemsetAsync(p, 0, b, stream));
+        CK(cudaStreamSynchronize(stream));  // usable from any stream from here on
         ptrs.push_back(p);
         bytes += (double)b;
         return (T*)p;
     }
     void release(void* p, size_t b) {
         for (auto& q : ptrs)
-            if (q == p) { cudaFree(p); q = nullptr; bytes -= (double)b; }
+            if (q == p) { cudaFreeAsync(p, stream); q = nullptr; bytes -= (double)b; }
     }
-    ~DevMem() {
+    void free_all() {
         for (void* p : ptrs)
-            if (p) cudaFree(p);
+            if (p) cudaFreeAsync(p, stream);
+        ptrs.clear();
+        if (stream) cudaStreamSynchronize(stream);
+    }
+    static void keep_pool(int device) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
     }
 };
+
+// Lays buffers out back to back (256-byte aligned) in one slab.  A layout
+// function runs twice: with base 0 to size the slab, then with the slab's base.
+struct Carver {
+    uintptr_t base = 0;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t n) {
+        off = (off + 255) & ~(size_t)255;
+        T* p = (T*)(base + off);
+        off += std::max<size_t>(n, 1) * sizeof(T);
+        return p;
+    }
+};
+
+// Pinned host words for the engines' asynchronous flag reads, carved from
+// pinned blocks shared by all engines of the process (pinned allocation is
+// slow): a 16-word slot per engine, returned to a free list.
+struct PinnedSlots {
+    std::mutex mu;
+    std::vector<int*> free_slots;
+    int* get() {
+        std::lock_guard<std::mutex> lk(mu);
+        if (free_slots.empty()) {
+            int* blk = nullptr;
+            CK(cudaMallocHost(&blk, 4096 * sizeof(int)));
+            for (int k = 0; k < 4096; k += 16) free_slots.push_back(blk + k);
+        }
+        int* p = free_slots.back();
+        free_slots.pop_back();
+        return p;
+    }
+    void put(int* p) {
+        std::lock_guard<std::mutex> lk(mu);
+        free_slots.push_back(p);
+    }
+};
+static PinnedSlots g_pinned;
 
 template <typename R>
 class EngineT final : public EngineBase {
@@ -85,9 +140,10 @@ class EngineT final : public EngineBase {
             for (cudaEvent_t e : row) if (e) cudaEventDestroy(e);
         if (ev_fork_) cudaEventDestroy(ev_fork_);
         if (ev_join_) cudaEventDestroy(ev_join_);
+        mem_.free_all();
         if (stream2_) cudaStreamDestroy(stream2_);
         if (stream_) cudaStreamDestroy(stream_);
-        if (hflag_) cudaFreeHost(hflag_);
+        if (hflag_) g_pinned.put(hflag_);
     }
 
     void step(int n, bool exp) override {
@@ -161,7 +217,7 @@ class EngineT final : public EngineBase {
         // apply the pending second half-kick so the state is that of the last step
         int pending = 0;
         CK(cudaStreamSynchronize(stream_));
-        CK(cudaMemcpy(&pending, h_.post_pending, sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(&pending, h_.post_pending, sizeof(int), cudaMemcpyDeviceToHost);
         if (pending && !post_done_) {
             launch_clump(0);
             post_done_ = true;
@@ -187,8 +243,8 @@ class EngineT final : public EngineBase {
         const int hg = read_int(h_.hgen);
         std::vector<int> idx(nn);
         std::vector<uint8_t> t(h_.cap);
-        if (nn) CK(cudaMemcpy(idx.data(), h_.nfp, (size_t)nn * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(t.data(), h_.touch[(hg + 1) & 1], (size_t)h_.cap, cudaMemcpyDeviceToHost));
+        if (nn) copy_(idx.data(), h_.nfp, (size_t)nn * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(t.data(), h_.touch[(hg + 1) & 1], (size_t)h_.cap, cudaMemcpyDeviceToHost);
         long long c = 0;
         for (int p : idx) c += t[p] != 0;
         if (nnear) *nnear = nn;
@@ -199,15 +255,15 @@ class EngineT final : public EngineBase {
         const ScenePar& P = hpar_[s];
         int n = P.nsub, o = P.sub_off;
         if (fix) {
-            CK(cudaMemcpy(fix, h_.part_fix + o, n * sizeof(int), cudaMemcpyDeviceToHost));
+            copy_(fix, h_.part_fix + o, n * sizeof(int), cudaMemcpyDeviceToHost);
         }
         if (cid) {
-            CK(cudaMemcpy(cid, h_.clump_id + o, n * sizeof(int), cudaMemcpyDeviceToHost));
+            copy_(cid, h_.clump_id + o, n * sizeof(int), cudaMemcpyDeviceToHost);
             for (int i = 0; i < n; i++) cid[i] -= P.clump_off;
         }
         if (pos || rad) {
             std::vector<double4> tmp(n);
-            CK(cudaMemcpy(tmp.data(), h_.posr + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            copy_(tmp.data(), h_.posr + o, n * sizeof(double4), cudaMemcpyDeviceToHost);
             for (int i = 0; i < n; i++) {
                 if (pos) { pos[3 * i] = tmp[i].x; pos[3 * i + 1] = tmp[i].y; pos[3 * i + 2] = tmp[i].z; }
                 if (rad) rad[i] = tmp[i].w;
@@ -218,7 +274,7 @@ class EngineT final : public EngineBase {
         refresh_dev();
         const ScenePar& P = hpar_[s];
         std::vector<double4> tmp(P.nsub);
-        CK(cudaMemcpy(tmp.data(), h_.lom + P.sub_off, P.nsub * sizeof(double4), cudaMemcpyDeviceToHost));
+        copy_(tmp.data(), h_.lom + P.sub_off, P.nsub * sizeof(double4), cudaMemcpyDeviceToHost);
         for (int i = 0; i < P.nsub; i++) {
             if (local) { local[3 * i] = tmp[i].x; local[3 * i + 1] = tmp[i].y; local[3 * i + 2] = tmp[i].z; }
             if (mass) mass[i] = tmp[i].w;
@@ -227,7 +283,7 @@ class EngineT final : public EngineBase {
     void get_clump_prop(int s, double* prop) override {
         const ScenePar& P = hpar_[s];
         std::vector<double4> tmp(P.nclump);
-        CK(cudaMemcpy(tmp.data(), h_.cprop + P.clump_off, P.nclump * sizeof(double4), cudaMemcpyDeviceToHost));
+        copy_(tmp.data(), h_.cprop + P.clump_off, P.nclump * sizeof(double4), cudaMemcpyDeviceToHost);
         for (int i = 0; i < P.nclump; i++) {
             prop[4 * i] = tmp[i].x; prop[4 * i + 1] = tmp[i].y; prop[4 * i + 2] = tmp[i].z; prop[4 * i + 3] = tmp[i].w;
         }
@@ -239,7 +295,7 @@ class EngineT final : public EngineBase {
         std::vector<double4> tmp(n);
         auto pull3 = [&](double4* src, double* dst) {
             if (!dst) return;
-            CK(cudaMemcpy(tmp.data(), src + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            copy_(tmp.data(), src + o, n * sizeof(double4), cudaMemcpyDeviceToHost);
             for (int i = 0; i < n; i++) { dst[3 * i] = tmp[i].x; dst[3 * i + 1] = tmp[i].y; dst[3 * i + 2] = tmp[i].z; }
         };
         pull3(h_.cpos, pos);
@@ -248,7 +304,7 @@ class EngineT final : public EngineBase {
         pull3(h_.cF, f);
         pull3(h_.cT, t);
         if (quat) {
-            CK(cudaMemcpy(tmp.data(), h_.cq + o, n * sizeof(double4), cudaMemcpyDeviceToHost));
+            copy_(tmp.data(), h_.cq + o, n * sizeof(double4), cudaMemcpyDeviceToHost);
             for (int i = 0; i < n; i++) {
                 quat[4 * i] = tmp[i].x; quat[4 * i + 1] = tmp[i].y; quat[4 * i + 2] = tmp[i].z; quat[4 * i + 3] = tmp[i].w;
             }
@@ -283,8 +339,8 @@ class EngineT final : public EngineBase {
         int lc = read_int(h_.lcur);
         const PairList& Lc = h_.L[lc & 1];
         std::vector<int> own(y.npairs), nbr(y.npairs);
-        CK(cudaMemcpy(own.data(), Lc.own + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(nbr.data(), Lc.nbr + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(own.data(), Lc.own + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(nbr.data(), Lc.nbr + y.pair_off, y.npairs * sizeof(int), cudaMemcpyDeviceToHost);
         for (int p = 0; p < y.npairs; p++) {
             if (lpa) lpa[p] = own[p] - P.sub_off;
             if (lpb) lpb[p] = (nbr[p] & IDX_MASK) - P.sub_off;
@@ -315,8 +371,8 @@ class EngineT final : public EngineBase {
         SceneDyn y = read_dyn(s);
         std::vector<R4<R>> xf(y.npairs);
         std::vector<double4> xc(y.npairs);
-        CK(cudaMemcpy(xf.data(), (R4<R>*)h_.xfcn + y.pair_off, y.npairs * sizeof(R4<R>), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(xc.data(), (double4*)h_.xcpt + y.pair_off, y.npairs * sizeof(double4), cudaMemcpyDeviceToHost));
+        copy_(xf.data(), (R4<R>*)h_.xfcn + y.pair_off, y.npairs * sizeof(R4<R>), cudaMemcpyDeviceToHost);
+        copy_(xc.data(), (double4*)h_.xcpt + y.pair_off, y.npairs * sizeof(double4), cudaMemcpyDeviceToHost);
         std::fill(fcn, fcn + (size_t)n * bl * 3, 0.0);
         std::fill(cpt, cpt + (size_t)n * bl * 3, 0.0);
         const int p0 = rd.row[0];
@@ -354,8 +410,8 @@ class EngineT final : public EngineBase {
         SceneDyn y = read_dyn(s);
         if (count > ring_len_) throw ArgError("history longer than the ring");
         std::vector<double> ring((size_t)ring_len_ * 6);
-        CK(cudaMemcpy(ring.data(), h_.ring + (size_t)s * ring_len_ * 6, ring.size() * sizeof(double),
-                      cudaMemcpyDeviceToHost));
+        copy_(ring.data(), h_.ring + (size_t)s * ring_len_ * 6, ring.size() * sizeof(double),
+                      cudaMemcpyDeviceToHost);
         for (int c = 0; c < count; c++) {
             int st = y.step - count + c;
             if (st < 0) { for (int q = 0; q < 6; q++) out[c * 6 + q] = 0; continue; }
@@ -393,6 +449,8 @@ class EngineT final : public EngineBase {
    private:
     nbc_options opt_;
     DevMem mem_;
+    char* pslab_ = nullptr;  // the pair buffers' slab
+    size_t pslab_bytes_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaStream_t stream2_ = nullptr;   // second branch of a step: k_boundary beside k_pairs
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
@@ -434,7 +492,7 @@ class EngineT final : public EngineBase {
 
     int total_rebuilds() {
         std::vector<SceneDyn> y(S_);
-        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
         int n = 0;
         for (auto& v : y) n = std::max(n, v.nrebuild);
         return n;
@@ -492,7 +550,9 @@ class EngineT final : public EngineBase {
         CK(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
-        CK(cudaMallocHost(&hflag_, 4 * sizeof(int)));
+        hflag_ = g_pinned.get();
+        mem_.stream = stream_;
+        DevMem::keep_pool(opt_.device);
         lanes_ = opt_.lanes == 1 || opt_.lanes == 2 || opt_.lanes == 4 || opt_.lanes == 8 || opt_.lanes == 16 ||
                          opt_.lanes == 32 ? opt_.lanes : 2;
         search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
@@ -640,104 +700,119 @@ class EngineT final : public EngineBase {
             for (int i = 0; i < N_; i++) midx[cur[cid[i]]++] = i;
         }
 
-        // device allocation
+        // device allocation: the per-subsphere and per-clump buffers in one
+        // slab, the pair buffers (which grow) in another
         const size_t N = N_;
-        h_.par = mem_.alloc<ScenePar>(S_);
-        h_.dyn = mem_.alloc<SceneDyn>(S_);
-        h_.sid = mem_.alloc<int>(N);
-        h_.csid = mem_.alloc<int>(K_);
-        h_.posr = mem_.alloc<double4>(N); h_.posr2 = mem_.alloc<double4>(N);
-        h_.lom = mem_.alloc<double4>(N); h_.lom2 = mem_.alloc<double4>(N);
-        h_.cum = mem_.alloc<double4>(N); h_.cum2 = mem_.alloc<double4>(N);
-        h_.clump_id = mem_.alloc<int>(N); h_.clump_id2 = mem_.alloc<int>(N);
-        h_.part_fix = mem_.alloc<int>(N); h_.part_fix2 = mem_.alloc<int>(N);
-        h_.level = mem_.alloc<int>(N); h_.level2 = mem_.alloc<int>(N);
-        h_.key = mem_.alloc<int>(N); h_.key2 = mem_.alloc<int>(N);
-        h_.kin = mem_.alloc<R4<R>>(3 * N); h_.kin2 = mem_.alloc<R4<R>>(3 * N);
-        h_.bhist = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N); h_.bhist2 = mem_.alloc<R4<R>>((size_t)NB_SLOTS * 3 * N);
-        h_.bbits = mem_.alloc<uint16_t>(N); h_.bbits2 = mem_.alloc<uint16_t>(N);
-        h_.fsum = mem_.alloc<R4<R>>(2 * N);
-        h_.fbnd = mem_.alloc<R4<R>>(2 * N);
-        h_.cpos = mem_.alloc<double4>(K_); h_.cvel = mem_.alloc<double4>(K_); h_.cw = mem_.alloc<double4>(K_);
-        h_.cq = mem_.alloc<double4>(K_); h_.cprop = mem_.alloc<double4>(K_);
-        h_.cF = mem_.alloc<double4>(K_); h_.cT = mem_.alloc<double4>(K_);
-        h_.mem_start = mem_.alloc<int>(K_ + 1);
-        h_.mem_idx = mem_.alloc<int>(N);
-        int* flags = mem_.alloc<int>(16);
-        h_.post_pending = flags + 0;
-        h_.any_rebuild = flags + 1;
-        h_.halt = flags + 2;
-        h_.lcur = flags + 3;
-        h_.hgen = flags + 4;
-        h_.gstep = flags + 5;
-        h_.kc_done = flags + 6;
-        h_.kA = mem_.alloc<int>(N); h_.vA = mem_.alloc<int>(N); h_.kB = mem_.alloc<int>(N); h_.vB = mem_.alloc<int>(N);
-        h_.hist = mem_.alloc<int>((size_t)256 * rs_blocks_);
-        h_.perm = mem_.alloc<int>(N);
-        h_.inv = mem_.alloc<int>(N);
-        h_.cstart = mem_.alloc<int>(cells + 1);
-        h_.scr = mem_.alloc<int>((size_t)N * 2 * SCR_CAP);
-        h_.cnt_f = mem_.alloc<int>(N + 1);
-        h_.nrow = mem_.alloc<int>(N + 1);
-        h_.nbrow = mem_.alloc<int>(N + 1);
-        h_.cnt_b = mem_.alloc<int>(N + 1);
-        h_.sfc = mem_.alloc<int>(N);
-        h_.xcnt = mem_.alloc<int>(N);
-        h_.scan_tmp = mem_.alloc<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
-        for (int l = 0; l < 2; l++) {
-            h_.L[l].row = mem_.alloc<int>(N + 1);
-            h_.L[l].brow = mem_.alloc<int>(N + 1);
-        }
+        auto layout = [&](Carver& m) {
+            h_.par = m.take<ScenePar>(S_);
+            h_.dyn = m.take<SceneDyn>(S_);
+            h_.sid = m.take<int>(N);
+            h_.csid = m.take<int>(K_);
+            h_.posr = m.take<double4>(N); h_.posr2 = m.take<double4>(N);
+            h_.lom = m.take<double4>(N); h_.lom2 = m.take<double4>(N);
+            h_.cum = m.take<double4>(N); h_.cum2 = m.take<double4>(N);
+            h_.clump_id = m.take<int>(N); h_.clump_id2 = m.take<int>(N);
+            h_.part_fix = m.take<int>(N); h_.part_fix2 = m.take<int>(N);
+            h_.level = m.take<int>(N); h_.level2 = m.take<int>(N);
+            h_.key = m.take<int>(N); h_.key2 = m.take<int>(N);
+            h_.kin = m.take<R4<R>>(3 * N); h_.kin2 = m.take<R4<R>>(3 * N);
+            h_.bhist = m.take<R4<R>>((size_t)NB_SLOTS * 3 * N); h_.bhist2 = m.take<R4<R>>((size_t)NB_SLOTS * 3 * N);
+            h_.bbits = m.take<uint16_t>(N); h_.bbits2 = m.take<uint16_t>(N);
+            h_.fsum = m.take<R4<R>>(2 * N);
+            h_.fbnd = m.take<R4<R>>(2 * N);
+            h_.cpos = m.take<double4>(K_); h_.cvel = m.take<double4>(K_); h_.cw = m.take<double4>(K_);
+            h_.cq = m.take<double4>(K_); h_.cprop = m.take<double4>(K_);
+            h_.cF = m.take<double4>(K_); h_.cT = m.take<double4>(K_);
+            h_.mem_start = m.take<int>(K_ + 1);
+            h_.mem_idx = m.take<int>(N);
+            int* flags = m.take<int>(16);
+            h_.post_pending = flags + 0;
+            h_.any_rebuild = flags + 1;
+            h_.halt = flags + 2;
+            h_.lcur = flags + 3;
+            h_.hgen = flags + 4;
+            h_.gstep = flags + 5;
+            h_.kc_done = flags + 6;
+            h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
+            h_.hist = m.take<int>((size_t)256 * rs_blocks_);
+            h_.perm = m.take<int>(N);
+            h_.inv = m.take<int>(N);
+            h_.cstart = m.take<int>(cells + 1);
+            h_.scr = m.take<int>((size_t)N * 2 * SCR_CAP);
+            h_.cnt_f = m.take<int>(N + 1);
+            h_.nrow = m.take<int>(N + 1);
+            h_.nbrow = m.take<int>(N + 1);
+            h_.cnt_b = m.take<int>(N + 1);
+            h_.sfc = m.take<int>(N);
+            h_.xcnt = m.take<int>(N);
+            h_.scan_tmp = m.take<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
+            for (int l = 0; l < 2; l++) {
+                h_.L[l].row = m.take<int>(N + 1);
+                h_.L[l].brow = m.take<int>(N + 1);
+            }
+            h_.xparts = m.take<R4<R>>(6 * N);
+            h_.xintr = m.take<R4<R>>(4 * N);
+            h_.ring_len = ring_len_;
+            h_.ring = m.take<double>((size_t)S_ * ring_len_ * 6);
+            h_.sblk_scene = m.take<int>(cblk);
+            d_ = m.take<Dev>(1);
+        };
+        Carver sz;
+        layout(sz);
+        Carver m{(uintptr_t)mem_.alloc<char>(sz.off)};
+        layout(m);
         alloc_pairs(std::max<long long>(1024, 24LL * N_));
-        h_.xparts = mem_.alloc<R4<R>>(6 * N);
-        h_.xintr = mem_.alloc<R4<R>>(4 * N);
-        h_.ring_len = ring_len_;
-        h_.ring = mem_.alloc<double>((size_t)S_ * ring_len_ * 6);
-        h_.sblk_scene = mem_.alloc<int>(cblk);
-        d_ = mem_.alloc<Dev>(1);
 
-        CK(cudaMemcpy(h_.par, hpar_.data(), S_ * sizeof(ScenePar), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.dyn, hdyn.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.sid, sid.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.csid, csid.data(), K_ * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.posr, posr.data(), N * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.lom, lom.data(), N * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.clump_id, cid.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.part_fix, fix.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.level, lev.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.cpos, cpos.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.cvel, cvel.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.cw, cw.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.cq, cq.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h_.sblk_scene, sblk.data(), cblk * sizeof(int), cudaMemcpyHostToDevice));
+        copy_(h_.par, hpar_.data(), S_ * sizeof(ScenePar), cudaMemcpyHostToDevice);
+        copy_(h_.dyn, hdyn.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice);
+        copy_(h_.sid, sid.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.csid, csid.data(), K_ * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.posr, posr.data(), N * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.lom, lom.data(), N * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.clump_id, cid.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.part_fix, fix.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.level, lev.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.cpos, cpos.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.cvel, cvel.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.cw, cw.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.cq, cq.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        copy_(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        copy_(h_.sblk_scene, sblk.data(), cblk * sizeof(int), cudaMemcpyHostToDevice);
         // the first list is empty: rows of zeros
-        CK(cudaMemset(h_.L[0].row, 0, (N + 1) * sizeof(int)));
-        CK(cudaMemset(h_.L[0].brow, 0, (N + 1) * sizeof(int)));
+        CK(cudaMemsetAsync(h_.L[0].row, 0, (N + 1) * sizeof(int), stream_));
+        CK(cudaMemsetAsync(h_.L[0].brow, 0, (N + 1) * sizeof(int), stream_));
         int one = 1;
-        CK(cudaMemcpy(h_.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+        copy_(h_.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice);
         push_dev();
     }
 
     void alloc_pairs(long long cap) {
         if (cap > 2000000000LL) throw CudaError("pair capacity above 2^31");
         h_.cap = (int)cap;
-        for (int l = 0; l < 2; l++) {
-            h_.L[l].nbr = mem_.alloc<int>(cap);
-            h_.L[l].own = mem_.alloc<int>(cap);
-            h_.L[l].bnbr = mem_.alloc<int>(cap);
-            h_.L[l].bpair = mem_.alloc<int>(cap);
-            h_.H[l] = mem_.alloc<char>(hist_bytes(cap));
-            h_.touch[l] = mem_.alloc<uint8_t>(cap);
-        }
-        h_.ctb = mem_.alloc<R4<R>>(4 * cap);
-        h_.nfp = mem_.alloc<int>(cap);
-        h_.nbq = mem_.alloc<int>(cap);
-        h_.nearf = mem_.alloc<uint8_t>(cap);
-        h_.xfcn = mem_.alloc<R4<R>>(cap);
-        h_.xcpt = mem_.alloc<double4>(cap);
+        auto layout = [&](Carver& m) {
+            for (int l = 0; l < 2; l++) {
+                h_.L[l].nbr = m.take<int>(cap);
+                h_.L[l].own = m.take<int>(cap);
+                h_.L[l].bnbr = m.take<int>(cap);
+                h_.L[l].bpair = m.take<int>(cap);
+                h_.H[l] = m.take<char>(hist_bytes(cap));
+                h_.touch[l] = m.take<uint8_t>(cap);
+            }
+            h_.ctb = m.take<R4<R>>(4 * cap);
+            h_.nfp = m.take<int>(cap);
+            h_.nbq = m.take<int>(cap);
+            h_.nearf = m.take<uint8_t>(cap);
+            h_.xfcn = m.take<R4<R>>(cap);
+            h_.xcpt = m.take<double4>(cap);
+        };
+        Carver sz;
+        layout(sz);
+        pslab_bytes_ = sz.off;
+        pslab_ = mem_.alloc<char>(pslab_bytes_);
+        Carver m{(uintptr_t)pslab_};
+        layout(m);
     }
     static size_t hist_bytes(long long cap) { return (size_t)cap * (2 * sizeof(R4<R>) + sizeof(R)); }
 
@@ -768,66 +843,66 @@ class EngineT final : public EngineBase {
         int lc = read_int(h_.lcur), hg = read_int(h_.hgen);
         const PairList& Lo = old.L[lc & 1];
         int np_f = 0, np_b = 0;
-        CK(cudaMemcpy(&np_f, Lo.row + N_, sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(&np_b, Lo.brow + N_, sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(&np_f, Lo.row + N_, sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(&np_b, Lo.brow + N_, sizeof(int), cudaMemcpyDeviceToHost);
+        char* old_slab = pslab_;
+        const size_t old_bytes = pslab_bytes_;
         alloc_pairs(cap);
         PairList& Ln = h_.L[lc & 1];
-        CK(cudaMemcpy(Ln.nbr, Lo.nbr, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(Ln.own, Lo.own, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(Ln.bnbr, Lo.bnbr, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(Ln.bpair, Lo.bpair, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice));
+        copy_(Ln.nbr, Lo.nbr, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice);
+        copy_(Ln.own, Lo.own, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice);
+        copy_(Ln.bnbr, Lo.bnbr, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice);
+        copy_(Ln.bpair, Lo.bpair, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice);
         const int g = hg & 1;
         char* ho = (char*)old.H[g];
         char* hn = (char*)h_.H[g];
-        CK(cudaMemcpy(hn, ho, (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(hn + (size_t)h_.cap * sizeof(R4<R>), ho + (size_t)old.cap * sizeof(R4<R>),
-                      (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(hn + (size_t)h_.cap * 2 * sizeof(R4<R>), ho + (size_t)old.cap * 2 * sizeof(R4<R>),
-                      (size_t)np_f * sizeof(R), cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy(h_.touch[g], old.touch[g], (size_t)np_f, cudaMemcpyDeviceToDevice));
-        for (int l = 0; l < 2; l++) {
-            mem_.release(old.L[l].nbr, (size_t)old.cap * 4);
-            mem_.release(old.L[l].own, (size_t)old.cap * 4);
-            mem_.release(old.L[l].bnbr, (size_t)old.cap * 4);
-            mem_.release(old.L[l].bpair, (size_t)old.cap * 4);
-            mem_.release(old.H[l], hist_bytes(old.cap));
-            mem_.release(old.touch[l], (size_t)old.cap);
-        }
-        mem_.release(old.ctb, (size_t)old.cap * 4 * sizeof(R4<R>));
-        mem_.release(old.nfp, (size_t)old.cap * sizeof(int));
-        mem_.release(old.nbq, (size_t)old.cap * sizeof(int));
-        mem_.release(old.nearf, (size_t)old.cap);
-        mem_.release(old.xfcn, (size_t)old.cap * sizeof(R4<R>));
-        mem_.release(old.xcpt, (size_t)old.cap * sizeof(double4));
+        copy_(hn, ho, (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice);
+        copy_(hn + (size_t)h_.cap * sizeof(R4<R>), ho + (size_t)old.cap * sizeof(R4<R>),
+              (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice);
+        copy_(hn + (size_t)h_.cap * 2 * sizeof(R4<R>), ho + (size_t)old.cap * 2 * sizeof(R4<R>),
+              (size_t)np_f * sizeof(R), cudaMemcpyDeviceToDevice);
+        copy_(h_.touch[g], old.touch[g], (size_t)np_f, cudaMemcpyDeviceToDevice);
+        mem_.release(old_slab, old_bytes);
         push_dev();
     }
 
+    // Every copy goes through the engine's own stream.  cudaMemcpy would run
+    // on the legacy default stream, which is not ordered with the engine's
+    // non-blocking streams: a device-to-device copy (and the DMA of a pageable
+    // host-to-device copy) may still be in flight when cudaMemcpy returns, so
+    // a later kernel, or a stream-ordered free of the source, would race it.
+    // Copies that touch host memory wait for the stream before returning.
+    void copy_(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+        if (!bytes) return;
+        CK(cudaMemcpyAsync(dst, src, bytes, kind, stream_));
+        if (kind != cudaMemcpyDeviceToDevice) CK(cudaStreamSynchronize(stream_));
+    }
     void push_dev() {
         CK(cudaStreamSynchronize(stream_));
-        CK(cudaMemcpy(d_, &h_, sizeof(Dev), cudaMemcpyHostToDevice));
+        copy_(d_, &h_, sizeof(Dev), cudaMemcpyHostToDevice);
     }
     // the device swaps buffer pointers in k_commit: refresh the host copy
     void refresh_dev() {
         CK(cudaStreamSynchronize(stream_));
-        CK(cudaMemcpy(&h_, d_, sizeof(Dev), cudaMemcpyDeviceToHost));
+        copy_(&h_, d_, sizeof(Dev), cudaMemcpyDeviceToHost);
     }
     int read_int(const int* p) {
         CK(cudaStreamSynchronize(stream_));
         int v = 0;
-        CK(cudaMemcpy(&v, p, sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(&v, p, sizeof(int), cudaMemcpyDeviceToHost);
         return v;
     }
     int read_gstep() { return read_int(h_.gstep); }
     SceneDyn read_dyn(int s) {
         CK(cudaStreamSynchronize(stream_));
         SceneDyn y;
-        CK(cudaMemcpy(&y, h_.dyn + s, sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        copy_(&y, h_.dyn + s, sizeof(SceneDyn), cudaMemcpyDeviceToHost);
         return y;
     }
     void pull_r4(const void* base, int off, int n, double* dst) {
         if (!dst) return;
         std::vector<R4<R>> tmp(n);
-        CK(cudaMemcpy(tmp.data(), (const R4<R>*)base + off, n * sizeof(R4<R>), cudaMemcpyDeviceToHost));
+        copy_(tmp.data(), (const R4<R>*)base + off, n * sizeof(R4<R>), cudaMemcpyDeviceToHost);
         for (int i = 0; i < n; i++) { dst[3 * i] = tmp[i].x; dst[3 * i + 1] = tmp[i].y; dst[3 * i + 2] = tmp[i].z; }
     }
     RowData pull_rows(int s) {
@@ -838,21 +913,21 @@ class EngineT final : public EngineBase {
         RowData rd;
         rd.row.resize(P.nsub + 1);
         rd.brow.resize(P.nsub + 1);
-        CK(cudaMemcpy(rd.row.data(), Lc.row + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(rd.brow.data(), Lc.brow + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(rd.row.data(), Lc.row + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(rd.brow.data(), Lc.brow + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
         int nf = rd.row[P.nsub] - rd.row[0], nb = rd.brow[P.nsub] - rd.brow[0];
         rd.nbr.resize(nf);
         rd.bnbr.resize(nb);
         rd.bpair.resize(nb);
-        CK(cudaMemcpy(rd.nbr.data(), Lc.nbr + rd.row[0], nf * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(rd.bnbr.data(), Lc.bnbr + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(rd.bpair.data(), Lc.bpair + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost));
+        copy_(rd.nbr.data(), Lc.nbr + rd.row[0], nf * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(rd.bnbr.data(), Lc.bnbr + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(rd.bpair.data(), Lc.bpair + rd.brow[0], nb * sizeof(int), cudaMemcpyDeviceToHost);
         return rd;
     }
 
     void check_errors() {
         std::vector<SceneDyn> y(S_);
-        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
         for (int s = 0; s < S_; s++)
             if (y[s].err & ERR_NONFINITE) throw NonFinite("scene " + std::to_string(s) + ": non-finite force");
     }
@@ -1047,11 +1122,11 @@ class EngineT final : public EngineBase {
         long long need = std::max(read_int(h_.cnt_f + N_), read_int(h_.cnt_b + N_));
         grow_pairs(need);
         int zero = 0;
-        CK(cudaMemcpy(h_.halt, &zero, sizeof(int), cudaMemcpyHostToDevice));
+        copy_(h_.halt, &zero, sizeof(int), cudaMemcpyHostToDevice);
         std::vector<SceneDyn> y(S_);
-        CK(cudaMemcpy(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost));
+        copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
         for (auto& v : y) v.err &= ~ERR_LIST_OVERFLOW;
-        CK(cudaMemcpy(h_.dyn, y.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice));
+        copy_(h_.dyn, y.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice);
         launch_rebuild(true);
         launch_contact(false);
         CK(cudaStreamSynchronize(stream_));

@@ -214,7 +214,29 @@ nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_active, int* n_qu
     if (!s || chunk < 1) return fail(NBC_ERR_ARG, "nbc_server_advance: bad arguments");
     chunk = std::min(chunk, 1024);  // the engine's intruder ring keeps the last 1024 steps at least
     nbc_status st = guard([&] {
-        // admission
+        // one chunk of every running request is put on its stream first, so
+        // the GPU works while new requests are admitted and created
+        const std::vector<int> running = s->active;
+        std::vector<int> launched(running.size(), 0), want(running.size(), 0), did(running.size(), 0);
+        // a request whose engine fails (non-finite force, device memory) is
+        // retired with its error; the others go on
+        auto retire_failed = [&](Request& r, const std::exception& e) {
+            r.state = 3;
+            r.error = e.what();
+            s->used -= r.bytes;
+            r.eng.reset();
+            r.scene.reset();
+        };
+        for (size_t k = 0; k < running.size(); k++) {
+            Request& r = *s->req[running[k]];
+            want[k] = std::min(chunk, r.nsteps - r.done);
+            try {
+                launched[k] = r.eng->eng->enqueue(want[k]);
+            } catch (const std::exception& e) {
+                retire_failed(r, e);
+            }
+        }
+        // admission: arrival order, while the head fits and a slot is free
         while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
             Request& r = *s->req[s->queue.front()];
             if (!s->active.empty() && s->used + r.est_bytes > s->budget) break;
@@ -238,19 +260,25 @@ nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_active, int* n_qu
             r.state = 1;
             s->active.push_back(r.id);
         }
-        // one chunk of every active request, enqueued before any is waited for
-        std::vector<nbc_engine*> e;
-        std::vector<int> want;
-        for (int id : s->active) {
-            Request& r = *s->req[id];
-            e.push_back(r.eng.get());
-            want.push_back(std::min(chunk, r.nsteps - r.done));
+        // the rest of each running request's chunk (a capacity overflow can
+        // stop a chunk early), waited for in turn
+        for (size_t k = 0; k < running.size(); k++) {
+            Request& r = *s->req[running[k]];
+            if (r.state != 1) continue;
+            try {
+                if (launched[k] > 0) did[k] = r.eng->eng->wait_steps();
+                while (did[k] < want[k]) {
+                    r.eng->eng->enqueue(want[k] - did[k]);
+                    did[k] += r.eng->eng->wait_steps();
+                }
+            } catch (const std::exception& e) {
+                retire_failed(r, e);
+            }
         }
-        std::vector<int> did;
-        advance_all(e, want, chunk, &did);
         std::vector<int> still;
-        for (size_t k = 0; k < s->active.size(); k++) {
-            Request& r = *s->req[s->active[k]];
+        for (size_t k = 0; k < running.size(); k++) {
+            Request& r = *s->req[running[k]];
+            if (r.state != 1) continue;
             // samples at the steps of this chunk that are multiples of sample_every
             const int first = r.done + 1, last = r.done + did[k];
             if (did[k] > 0) {
@@ -275,6 +303,8 @@ nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_active, int* n_qu
                 still.push_back(r.id);
             }
         }
+        // the requests admitted in this round run from the next one
+        for (size_t k = running.size(); k < s->active.size(); k++) still.push_back(s->active[k]);
         s->active = still;
     });
     if (n_active) *n_active = (int)s->active.size();
@@ -298,7 +328,8 @@ nbc_status nbc_server_result(nbc_server* s, int id, int* state, int* steps_done,
     if (n_samples) *n_samples = (int)(r.curve.size() / 6);
     if (curve && r.state == 2) std::copy(r.curve.begin(), r.curve.end(), curve);
     if (intr_pos && r.state == 2) std::copy(r.intr_pos, r.intr_pos + 3, intr_pos);
-    if (r.state == 3) return fail(NBC_ERR_MEMORY, "request " + std::to_string(id) + ": " + r.error);
+    // a failed request reports its state; asking for its result returns its error
+    if (r.state == 3 && (curve || intr_pos)) return fail(NBC_ERR_STATE, "request " + std::to_string(id) + ": " + r.error);
     return NBC_OK;
 }
 

@@ -464,7 +464,7 @@ class Server:
 
     def result(self, rid):
         st, done, ns = self.state(rid)
-        if st != 2:
+        if st not in (2, 3):
             return None
         curve, pos = np.zeros((ns, 6)), np.zeros(3)
         _check(lib().nbc_server_result(self.h, int(rid), None, None, None, _p(curve), _p(pos)))
