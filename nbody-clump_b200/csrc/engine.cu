@@ -450,6 +450,7 @@ class EngineT final : public EngineBase {
     nbc_options opt_;
     DevMem mem_;
     char* pslab_ = nullptr;  // the pair buffers' slab
+    int4* relmap_ = nullptr; // [S] region moves of a re-layout
     size_t pslab_bytes_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaStream_t stream2_ = nullptr;   // second branch of a step: k_boundary beside k_pairs
@@ -747,9 +748,17 @@ class EngineT final : public EngineBase {
             h_.xcnt = m.take<int>(N);
             h_.scan_tmp = m.take<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
             for (int l = 0; l < 2; l++) {
-                h_.L[l].row = m.take<int>(N + 1);
-                h_.L[l].brow = m.take<int>(N + 1);
+                h_.L[l].row = m.take<int>(N + S_);
+                h_.L[l].brow = m.take<int>(N + S_);
             }
+            h_.plan = m.take<int>(PL_SIZE);
+            h_.pscene = m.take<int>(S_);
+            h_.psub = m.take<int>(S_ + 1);
+            h_.pcell = m.take<int>(S_ + 1);
+            h_.pclump = m.take<int>(S_ + 1);
+            h_.ppair = m.take<int>(S_ + 1);
+            h_.need = m.take<int>(S_);
+            relmap_ = m.take<int4>(S_);
             h_.xparts = m.take<R4<R>>(6 * N);
             h_.xintr = m.take<R4<R>>(4 * N);
             h_.ring_len = ring_len_;
@@ -761,7 +770,8 @@ class EngineT final : public EngineBase {
         layout(sz);
         Carver m{(uintptr_t)mem_.alloc<char>(sz.off)};
         layout(m);
-        alloc_pairs(std::max<long long>(1024, 24LL * N_));
+        // the pair regions are sized at the first list (nothing is stored in them before)
+        alloc_pairs(1);
 
         copy_(h_.par, hpar_.data(), S_ * sizeof(ScenePar), cudaMemcpyHostToDevice);
         copy_(h_.dyn, hdyn.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice);
@@ -780,9 +790,7 @@ class EngineT final : public EngineBase {
         copy_(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice);
         copy_(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice);
         copy_(h_.sblk_scene, sblk.data(), cblk * sizeof(int), cudaMemcpyHostToDevice);
-        // the first list is empty: rows of zeros
-        CK(cudaMemsetAsync(h_.L[0].row, 0, (N + 1) * sizeof(int), stream_));
-        CK(cudaMemsetAsync(h_.L[0].brow, 0, (N + 1) * sizeof(int), stream_));
+        // the first list is empty: rows of zeros (the slab is zeroed)
         int one = 1;
         copy_(h_.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice);
         push_dev();
@@ -817,53 +825,89 @@ class EngineT final : public EngineBase {
     static size_t hist_bytes(long long cap) { return (size_t)cap * (2 * sizeof(R4<R>) + sizeof(R)); }
 
     double slack() const { return opt_.pair_slack >= 1.0 ? opt_.pair_slack : 1.6; }
-    // capacity of the pair buffers at the first list: slack x its pairs; with
-    // the default slack at least the reference's own list capacity, the sum
-    // over scenes of n_sub x BranchLmtLen/2, as far as 30% of the free device
-    // memory allows (growing later costs a host round trip and re-allocation)
-    long long first_capacity(long long need) {
-        long long cap = std::max<long long>(1024, (long long)(need * slack()));
+    // Bytes of the pair buffers per pair slot.
+    static double bytes_per_pair() {
+        return 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) +
+               2 * sizeof(int) + 1;
+    }
+    // Region capacities for the first lists: slack x each scene's pairs; with
+    // the default slack at least the reference's own list capacity, n_sub x
+    // BranchLmtLen/2, as far as 30% of the free device memory allows (growing
+    // later costs a host round trip and a re-layout).
+    std::vector<long long> first_capacities(const std::vector<long long>& need) {
+        std::vector<long long> cap(S_);
+        for (int s = 0; s < S_; s++) cap[s] = std::max<long long>(16, (long long)std::ceil(need[s] * slack()));
         if (opt_.pair_slack >= 1.0) return cap;
-        long long ref = 0;
-        for (const ScenePar& P : hpar_) ref += (long long)P.nsub * (P.bl / 2);
+        double want = 0, have = 0;
+        for (int s = 0; s < S_; s++) {
+            have += (double)cap[s];
+            want += std::max(0.0, (double)hpar_[s].nsub * (hpar_[s].bl / 2) - (double)cap[s]);
+        }
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const double per_pair = 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) + 2 * sizeof(int) + 1;
-        const long long budget = (long long)(0.3 * (double)fr / per_pair);
-        return std::min<long long>(std::max(cap, std::min(ref, budget)), 2000000000LL);
+        const double budget = 0.3 * (double)fr / bytes_per_pair() - have;
+        if (budget <= 0 || want <= 0) return cap;
+        const double f = std::min(1.0, budget / want);
+        for (int s = 0; s < S_; s++) {
+            const double extra = std::max(0.0, (double)hpar_[s].nsub * (hpar_[s].bl / 2) - (double)cap[s]);
+            cap[s] += (long long)(f * extra);
+        }
+        return cap;
     }
-    // grow the pair buffers, keeping the current list and history generation
-    void grow_pairs(long long need) {
-        refresh_dev();
-        resize_pairs(std::max<long long>((long long)(need * slack()), (long long)h_.cap + 1024));
+    // the regions after an overflow: every scene whose new list does not fit
+    // gets slack x its pairs (at least 1,024 more slots)
+    std::vector<long long> grown_capacities(const std::vector<int>& need, const std::vector<SceneDyn>& y) {
+        std::vector<long long> cap(S_);
+        for (int s = 0; s < S_; s++) {
+            cap[s] = y[s].pcap;
+            if (need[s] > y[s].pcap)
+                cap[s] = std::max<long long>((long long)std::ceil(need[s] * slack()), (long long)y[s].pcap + 1024);
+        }
+        return cap;
     }
-    void resize_pairs(long long cap) {
+    std::vector<SceneDyn> read_dyn_all() {
+        std::vector<SceneDyn> y(S_);
+        copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
+        return y;
+    }
+    // New pair regions of the given capacities: the pair buffers are
+    // re-allocated and every scene's current list, the history generation
+    // the next contact pass reads, touch and near flags move to its new
+    // region (rows shifted).  The build list and the other generation need
+    // nothing: a rebuild writes them before reading.
+    void layout_pairs(const std::vector<long long>& pcap) {
         refresh_dev();
+        std::vector<SceneDyn> y = read_dyn_all();
+        std::vector<int4> map(S_);
+        long long total = 0;
+        int moved = 0;
+        for (int s = 0; s < S_; s++) {
+            map[s].x = y[s].pair_off;
+            map[s].y = (int)total;
+            map[s].z = y[s].npairs;
+            map[s].w = moved;
+            moved += y[s].npairs;
+            y[s].pair_off = (int)total;
+            y[s].pcap = (int)pcap[s];
+            total += pcap[s];
+            if (total > 2000000000LL) throw CudaError("pair capacity above 2^31");
+        }
+        const int hg = read_int(h_.hgen);
         Dev old = h_;
-        int lc = read_int(h_.lcur), hg = read_int(h_.hgen);
-        const PairList& Lo = old.L[lc & 1];
-        int np_f = 0, np_b = 0;
-        copy_(&np_f, Lo.row + N_, sizeof(int), cudaMemcpyDeviceToHost);
-        copy_(&np_b, Lo.brow + N_, sizeof(int), cudaMemcpyDeviceToHost);
         char* old_slab = pslab_;
         const size_t old_bytes = pslab_bytes_;
-        alloc_pairs(cap);
-        PairList& Ln = h_.L[lc & 1];
-        copy_(Ln.nbr, Lo.nbr, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice);
-        copy_(Ln.own, Lo.own, (size_t)np_f * sizeof(int), cudaMemcpyDeviceToDevice);
-        copy_(Ln.bnbr, Lo.bnbr, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice);
-        copy_(Ln.bpair, Lo.bpair, (size_t)np_b * sizeof(int), cudaMemcpyDeviceToDevice);
-        const int g = hg & 1;
-        char* ho = (char*)old.H[g];
-        char* hn = (char*)h_.H[g];
-        copy_(hn, ho, (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice);
-        copy_(hn + (size_t)h_.cap * sizeof(R4<R>), ho + (size_t)old.cap * sizeof(R4<R>),
-              (size_t)np_f * sizeof(R4<R>), cudaMemcpyDeviceToDevice);
-        copy_(hn + (size_t)h_.cap * 2 * sizeof(R4<R>), ho + (size_t)old.cap * 2 * sizeof(R4<R>),
-              (size_t)np_f * sizeof(R), cudaMemcpyDeviceToDevice);
-        copy_(h_.touch[g], old.touch[g], (size_t)np_f, cudaMemcpyDeviceToDevice);
-        mem_.release(old_slab, old_bytes);
+        alloc_pairs(std::max<long long>(total, 1));
+        copy_(h_.dyn, y.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice);
+        copy_(relmap_, map.data(), S_ * sizeof(int4), cudaMemcpyHostToDevice);
         push_dev();
+        const int B = 256;
+        if (moved > 0)
+            k_relayout<R><<<std::min(148 * 8, cdiv(moved, B)), B, 0, stream_>>>(
+                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.cap, relmap_, moved);
+        k_shift_rows<<<std::min(148 * 8, cdiv((long long)N_ + S_, B)), B, 0, stream_>>>(d_, relmap_);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream_));
+        mem_.release(old_slab, old_bytes);
     }
 
     // Every copy goes through the engine's own stream.  cudaMemcpy would run
@@ -881,7 +925,7 @@ class EngineT final : public EngineBase {
         CK(cudaStreamSynchronize(stream_));
         copy_(d_, &h_, sizeof(Dev), cudaMemcpyHostToDevice);
     }
-    // the device swaps buffer pointers in k_commit: refresh the host copy
+    // the host copy of the pointer table, as the device has it
     void refresh_dev() {
         CK(cudaStreamSynchronize(stream_));
         copy_(&h_, d_, sizeof(Dev), cudaMemcpyDeviceToHost);
@@ -913,8 +957,8 @@ class EngineT final : public EngineBase {
         RowData rd;
         rd.row.resize(P.nsub + 1);
         rd.brow.resize(P.nsub + 1);
-        copy_(rd.row.data(), Lc.row + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
-        copy_(rd.brow.data(), Lc.brow + P.sub_off, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(rd.row.data(), Lc.row + P.sub_off + s, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
+        copy_(rd.brow.data(), Lc.brow + P.sub_off + s, (P.nsub + 1) * sizeof(int), cudaMemcpyDeviceToHost);
         int nf = rd.row[P.nsub] - rd.row[0], nb = rd.brow[P.nsub] - rd.brow[0];
         rd.nbr.resize(nf);
         rd.bnbr.resize(nb);
@@ -958,8 +1002,11 @@ class EngineT final : public EngineBase {
         mark(4, stream2_);
         CK(cudaEventRecord(ev_join_, stream2_));
         // grid-stride over the pairs: a fixed grid stays valid as the list grows
-        if (exp) k_pairs<R, true><<<148 * 12, PR_THREADS, 0, stream_>>>(d_);
-        else k_pairs<R, false><<<148 * 12, PR_THREADS, 0, stream_>>>(d_);
+        // grid-stride over the near pairs (a device count); a small scene gets
+        // a small grid so that other scenes' kernels run beside it
+        const int pg = std::min(148 * 12, cdiv(3LL * N_, PR_THREADS));
+        if (exp) k_pairs<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
+        else k_pairs<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
         CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
         const dim3 g(cdiv(N_ * lanes_, CT_THREADS));
 #define NBC_CT(L)                                                                   \
@@ -976,64 +1023,82 @@ class EngineT final : public EngineBase {
         mark(6, stream_);
         if (!capturing_ && timing_) launches_ += 3;
     }
-    void scan(int* a, int n) {
-        int nb = cdiv(n, SC_TILE);
-        k_scan_tiles<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp);
-        k_scan_sums<<<1, SC_THREADS, 0, stream_>>>(h_.scan_tmp, nb);
-        k_scan_add<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp);
+    // exclusive scan of a[0, n) (or of a[0, *dn) when dn is given, n then
+    // bounds it)
+    void scan(int* a, int n, const int* dn = nullptr) {
+        const int nb = std::min(cdiv(n, SC_TILE), 148 * 8);
+        k_scan_tiles<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp, dn);
+        k_scan_sums<<<1, SC_THREADS, 0, stream_>>>(h_.scan_tmp, cdiv(n, SC_TILE), dn);
+        k_scan_add<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp, dn);
     }
-    // the rebuild block of src/dem_simulation_clump.cu:124-176
+    // The rebuild block of src/dem_simulation_clump.cu:124-176, over the
+    // scenes whose rebuild flag is set: every kernel but the near rows walks
+    // the rebuilt scenes only (grid-stride over counts the plan puts on the
+    // device), so a batch pays for the scenes it rebuilds.
     void launch_rebuild(bool eager) {
         const int B = 128;
-        k_hash<<<cdiv(N_, B), B, 0, stream_>>>(d_);
+        const int gN = std::min(cdiv(N_, B), 148 * 16);         // grid-stride grids
+        const int sl = search_lanes_;
+        const int gS = std::min(cdiv(N_, SEARCH_THREADS / sl), 148 * 16);
+        const int* pl = h_.plan;
+        k_plan<<<1, SC_THREADS, 0, stream_>>>(d_);
+        k_hash<<<gN, B, 0, stream_>>>(d_);
         int *ki = h_.kA, *vi = h_.vA, *ko = h_.kB, *vo = h_.vB;
+        const int gR = std::min(rs_blocks_, 148 * 8);
         for (int p = 0; p < passes_; p++) {
-            k_rs_hist<<<rs_blocks_, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, rs_blocks_);
-            scan(h_.hist, 256 * rs_blocks_);
-            k_rs_scatter<<<rs_blocks_, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, rs_blocks_);
+            k_rs_hist<<<gR, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, pl + PL_T);
+            scan(h_.hist, 256 * rs_blocks_, pl + PL_HIST);
+            k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T);
             std::swap(ki, ko);
             std::swap(vi, vo);
         }
-        k_cellrange<<<cdiv(N_, B), B, 0, stream_>>>(d_, ki, vi);
-        k_cellstart<<<std::min(cdiv(h_.cells + 1, 256), 148 * 16), 256, 0, stream_>>>(d_);
-        k_reorder<R><<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        const int sl = search_lanes_;
-        const int sb = cdiv(N_, SEARCH_THREADS / sl);
-        k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, N_ + 1, 0);
-        k_fill_i<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, N_ + 1, 0);
-        if (sl == 16) k_search<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 32) k_search<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else k_search<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.cnt_f, N_ + 1);
-        scan(h_.cnt_b, N_ + 1);
+        k_cellrange<<<gN, B, 0, stream_>>>(d_, ki, vi);
+        k_cellstart<<<std::min(cdiv(h_.cells + S_, 256), 148 * 16), 256, 0, stream_>>>(d_);
+        k_reorder<R><<<gN, B, 0, stream_>>>(d_);
+        k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, pl + PL_T1, 0);
+        k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, pl + PL_T1, 0);
+        if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_search<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        scan(h_.cnt_f, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
         CK(cudaGetLastError());
         if (eager) {
-            CK(cudaMemcpyAsync(hflag_, h_.cnt_f + N_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
-            CK(cudaMemcpyAsync(hflag_ + 1, h_.cnt_b + N_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            // size the regions to the first lists, or grow the ones that overflow
+            k_check_cap<<<1, 256, 0, stream_>>>(d_, 0);
             CK(cudaStreamSynchronize(stream_));
-            long long need = std::max(hflag_[0], hflag_[1]);
+            std::vector<int> need(S_);
+            copy_(need.data(), h_.need, S_ * sizeof(int), cudaMemcpyDeviceToHost);
+            std::vector<SceneDyn> y = read_dyn_all();
             if (first_list_) {
-                // size the pair buffers to the first list: capacity = slack x pairs
-                resize_pairs(first_capacity(need));
+                std::vector<long long> nd(S_);
+                for (int s = 0; s < S_; s++) nd[s] = need[s] >= 0 ? need[s] : y[s].npairs;
+                layout_pairs(first_capacities(nd));
                 first_list_ = false;
-            } else if (need > h_.cap) {
-                grow_pairs(need);
+            } else {
+                bool grow = false;
+                for (int s = 0; s < S_; s++) grow |= need[s] > y[s].pcap;
+                if (grow) layout_pairs(grown_capacities(need, y));
             }
         }
-        k_check_cap<<<1, 1, 0, stream_>>>(d_);
-        if (hgrid_) k_fill_i<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, N_, 0);
-        if (sl == 16) k_compact<16><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 32) k_compact<32><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        else k_compact<8><<<sb, SEARCH_THREADS, 0, stream_>>>(d_);
-        if (hgrid_) k_xsort<<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        k_backref<<<cdiv(N_, B), B, 0, stream_>>>(d_);
-        k_carry<R><<<148 * 8, 256, 0, stream_>>>(d_);
-        // near rows of the new list
+        k_check_cap<<<1, 256, 0, stream_>>>(d_, 1);
+        if (hgrid_) k_fill_n<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, pl + PL_T, 0);
+        if (sl == 16) k_compact<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 32) k_compact<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        else k_compact<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        if (hgrid_) k_xsort<<<gN, B, 0, stream_>>>(d_);
+        k_backref<<<gN, B, 0, stream_>>>(d_);
+        const int gP = std::min(148 * 8, cdiv(8LL * N_, 256));
+        k_carry<R><<<gP, 256, 0, stream_>>>(d_);
+        k_writeback<R><<<gN, B, 0, stream_>>>(d_);
+        k_writeback_pairs<R><<<gP, 256, 0, stream_>>>(d_);
+        k_swap<<<1, 1, 0, stream_>>>(d_);
+        // near rows of every scene (offsets over the whole batch)
         k_near<false, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
         scan(h_.nrow, N_ + 1);
         scan(h_.nbrow, N_ + 1);
         k_near<true, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
-        k_commit<<<cdiv(K_ + S_ + 1, B), B, 0, stream_>>>(d_);
+        k_commit<<<std::min(cdiv((long long)K_ + S_ + 1, B), 148 * 8), B, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
 
@@ -1119,12 +1184,13 @@ class EngineT final : public EngineBase {
     // finish that step's rebuild and contact pass on the host path
     void recover_halt() {
         refresh_dev();
-        long long need = std::max(read_int(h_.cnt_f + N_), read_int(h_.cnt_b + N_));
-        grow_pairs(need);
+        std::vector<int> need(S_);
+        copy_(need.data(), h_.need, S_ * sizeof(int), cudaMemcpyDeviceToHost);
+        std::vector<SceneDyn> y = read_dyn_all();
+        layout_pairs(grown_capacities(need, y));
         int zero = 0;
         copy_(h_.halt, &zero, sizeof(int), cudaMemcpyHostToDevice);
-        std::vector<SceneDyn> y(S_);
-        copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
+        y = read_dyn_all();
         for (auto& v : y) v.err &= ~ERR_LIST_OVERFLOW;
         copy_(h_.dyn, y.data(), S_ * sizeof(SceneDyn), cudaMemcpyHostToDevice);
         launch_rebuild(true);

@@ -326,101 +326,29 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// GetParticleCellIndex_cuk (src/dem_grid.cu:155-202); hierarchical variant
-// GetParticleCellIndex_hGrid_cuk (src/dem_hgrid.cu:205-242) with the
-// out-of-box bucket kept inside the scene's cell range.
-static __global__ void k_hash(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    const int s = d.sid[i];
-    const ScenePar& P = d.par[s];
-    d.vA[i] = i;
-    if (!d.dyn[s].rebuild) { d.kA[i] = d.key[i]; return; }
-    double4 p = d.posr[i];
-    int local;
-    if (P.levels <= 1) {
-        if (p.z >= P.box_hi[2] || p.y >= P.box_hi[1] || p.x >= P.box_hi[0] ||
-            p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
-            local = P.cellnum - 1;
-        } else {
-            int cx = (int)floor((p.x - P.origin[0]) / P.cell[0]);
-            int cy = (int)floor((p.y - P.origin[1]) / P.cell[1]);
-            int cz = (int)floor((p.z - P.origin[2]) / P.cell[2]);
-            cx = clampi(cx, 0, P.gdim[0] - 1);
-            cy = clampi(cy, 0, P.gdim[1] - 1);
-            cz = clampi(cz, 0, P.gdim[2] - 1);
-            local = cz * P.gdim[1] * P.gdim[0] + cy * P.gdim[0] + cx;
-            local = clampi(local, 0, P.cellnum - 1);
-        }
-    } else {
-        if (p.z > P.box_hi[2] || p.y > P.box_hi[1] || p.x > P.box_hi[0] ||
-            p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
-            local = P.cellnum - 1;
-        } else {
-            int t = d.level[i];
-            double c = P.lcell[t];
-            int cx = clampi((int)floor((p.x - P.origin[0]) / c), 0, P.ldim[t][0] - 1);
-            int cy = clampi((int)floor((p.y - P.origin[1]) / c), 0, P.ldim[t][1] - 1);
-            int cz = clampi((int)floor((p.z - P.origin[2]) / c), 0, P.ldim[t][2] - 1);
-            local = P.loff[t] + (cz * P.ldim[t][1] * P.ldim[t][0] + cy * P.ldim[t][0] + cx);
-        }
+// A rebuild runs over the rebuilt scenes only.  k_plan lists them (ascending)
+// with prefix sums of their subsphere, cell-table and clump counts; a rebuild
+// kernel walks the concatenation of the rebuilt scenes with a grid-stride
+// loop and finds the scene of an element by binary search in the prefix.
+// Scenes that are not rebuilt keep their order, list region and histories
+// untouched, so a rebuild costs in proportion to the scenes it rebuilds.
+//
+// plan_find: the k in [0, n) with pre[k] <= t < pre[k + 1] (empty scenes are
+// passed over).
+__device__ __forceinline__ int plan_find(const int* __restrict__ pre, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int m = (lo + hi + 1) >> 1;
+        if (pre[m] <= t) lo = m;
+        else hi = m - 1;
     }
-    d.kA[i] = P.cell_off + local;
-}
-
-// --- LSD radix sort, 8-bit digits, stable (the reference sorts with CUB's
-// stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
-constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
-
-static __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ keys, int n, int shift,
-                                                        int* __restrict__ hist, int nblk) {
-    __shared__ int h[256];
-    const int tid = threadIdx.x, blk = blockIdx.x;
-    h[tid] = 0;
-    __syncthreads();
-    for (int it = 0; it < RS_ITEMS; it++) {
-        int idx = blk * RS_TILE + it * RS_THREADS + tid;
-        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255], 1);
-    }
-    __syncthreads();
-    hist[tid * nblk + blk] = h[tid];
-}
-
-static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
-                                                           int* __restrict__ kout, int* __restrict__ vout, int n,
-                                                           int shift, const int* __restrict__ hist, int nblk) {
-    __shared__ int base[256];
-    __shared__ int wcnt[RS_THREADS / 32][257];
-    const int tid = threadIdx.x, blk = blockIdx.x, lane = tid & 31, warp = tid >> 5;
-    base[tid] = hist[tid * nblk + blk];
-    for (int it = 0; it < RS_ITEMS; it++) {
-        for (int w = 0; w < RS_THREADS / 32; w++) wcnt[w][tid] = 0;
-        __syncthreads();
-        const int idx = blk * RS_TILE + it * RS_THREADS + tid;
-        const bool valid = idx < n;
-        const int k = valid ? kin[idx] : 0;
-        const int dig = valid ? ((k >> shift) & 255) : 256;
-        const unsigned peers = __match_any_sync(0xffffffffu, dig);
-        const int rank = __popc(peers & ((1u << lane) - 1u));
-        if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
-        __syncthreads();
-        if (valid) {
-            int off = base[dig] + rank;
-            for (int w = 0; w < warp; w++) off += wcnt[w][dig];
-            kout[off] = k;
-            vout[off] = vin[idx];
-        }
-        __syncthreads();
-        int add = 0;
-        for (int w = 0; w < RS_THREADS / 32; w++) add += wcnt[w][tid];
-        base[tid] += add;
-        __syncthreads();
-    }
+    return lo;
 }
 
 // --- exclusive scan of ints (three passes) --------------------------------
+// The length is n, or *dn when dn is given (a count computed on the device);
+// the kernels walk the tiles with grid-stride loops, so a fixed grid serves
+// any length.
 constexpr int SC_THREADS = 256, SC_ITEMS = 4, SC_TILE = SC_THREADS * SC_ITEMS;
 
 __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
@@ -448,22 +376,28 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
     return warp_base + x - v;
 }
 
-static __global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, int n, int* __restrict__ sums) {
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(int* __restrict__ a, int n, int* __restrict__ sums,
+                                                           const int* __restrict__ dn) {
     __shared__ int sh[SC_THREADS / 32];
-    const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
-    int v[SC_ITEMS], s = 0;
-    for (int j = 0; j < SC_ITEMS; j++) { v[j] = base + j < n ? a[base + j] : 0; s += v[j]; }
-    int total;
-    int ex = block_excl_scan(s, sh, total);
-    for (int j = 0; j < SC_ITEMS; j++) {
-        if (base + j < n) a[base + j] = ex;
-        ex += v[j];
+    const int nn = dn ? *dn : n;
+    const int tiles = (nn + SC_TILE - 1) / SC_TILE;
+    for (int b = blockIdx.x; b < tiles; b += gridDim.x) {
+        const int base = b * SC_TILE + threadIdx.x * SC_ITEMS;
+        int v[SC_ITEMS], s = 0;
+        for (int j = 0; j < SC_ITEMS; j++) { v[j] = base + j < nn ? a[base + j] : 0; s += v[j]; }
+        int total;
+        int ex = block_excl_scan(s, sh, total);
+        for (int j = 0; j < SC_ITEMS; j++) {
+            if (base + j < nn) a[base + j] = ex;
+            ex += v[j];
+        }
+        if (threadIdx.x == 0) sums[b] = total;
     }
-    if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
-static __global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums, int nb) {
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict__ sums, int nb, const int* __restrict__ dn) {
     __shared__ int sh[SC_THREADS / 32];
+    if (dn) nb = (*dn + SC_TILE - 1) / SC_TILE;
     int carry = 0;
     for (int off = 0; off < nb; off += SC_THREADS) {
         int i = off + threadIdx.x;
@@ -475,60 +409,238 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan_sums(int* __restrict
     }
 }
 
-static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums) {
-    const int base = blockIdx.x * SC_TILE + threadIdx.x * SC_ITEMS;
-    const int add = sums[blockIdx.x];
-    for (int j = 0; j < SC_ITEMS; j++)
-        if (base + j < n) a[base + j] += add;
+static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict__ a, int n, const int* __restrict__ sums,
+                                                         const int* __restrict__ dn) {
+    const int nn = dn ? *dn : n;
+    const int tiles = (nn + SC_TILE - 1) / SC_TILE;
+    for (int b = blockIdx.x; b < tiles; b += gridDim.x) {
+        const int base = b * SC_TILE + threadIdx.x * SC_ITEMS;
+        const int add = sums[b];
+        for (int j = 0; j < SC_ITEMS; j++)
+            if (base + j < nn) a[base + j] += add;
+    }
+}
+
+// --- LSD radix sort, 8-bit digits, stable (the reference sorts with CUB's
+// stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
+constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
+
+// The plan of a rebuild (one block).  Rebuilt scenes are listed in ascending
+// order; their cell keys (cell_off + local cell) ascend with the scene, so
+// sorting the concatenation of their subspheres keeps every scene in its own
+// range.
+static __global__ void __launch_bounds__(SC_THREADS) k_plan(const Dev* __restrict__ dp) {
+    __shared__ int sh[SC_THREADS / 32];
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int ns = 0, nsub = 0, ncell = 0, nclump = 0;
+    for (int b = 0; b < d.S; b += SC_THREADS) {
+        const int s = b + threadIdx.x;
+        const bool f = s < d.S && d.dyn[s].rebuild;
+        int a1 = 0, a2 = 0, a3 = 0;
+        if (f) {
+            const ScenePar& P = d.par[s];
+            a1 = P.nsub;
+            a2 = P.cellnum + 1;
+            a3 = P.nclump;
+        }
+        if (s < d.S) d.need[s] = -1;
+        int t0, t1, t2, t3;
+        const int e0 = block_excl_scan(f ? 1 : 0, sh, t0);
+        const int e1 = block_excl_scan(a1, sh, t1);
+        const int e2 = block_excl_scan(a2, sh, t2);
+        const int e3 = block_excl_scan(a3, sh, t3);
+        if (f) {
+            d.pscene[ns + e0] = s;
+            d.psub[ns + e0] = nsub + e1;
+            d.pcell[ns + e0] = ncell + e2;
+            d.pclump[ns + e0] = nclump + e3;
+        }
+        ns += t0;
+        nsub += t1;
+        ncell += t2;
+        nclump += t3;
+    }
+    if (threadIdx.x == 0) {
+        d.psub[ns] = nsub;
+        d.pcell[ns] = ncell;
+        d.pclump[ns] = nclump;
+        d.plan[PL_NS] = ns;
+        d.plan[PL_T] = nsub;
+        d.plan[PL_TC] = ncell;
+        d.plan[PL_T1] = nsub + 1;
+        d.plan[PL_HIST] = 256 * ((nsub + RS_TILE - 1) / RS_TILE);
+        d.plan[PL_TK] = nclump;
+        d.plan[PL_CS] = 0;
+        d.plan[PL_CC] = 0;
+    }
+}
+
+#define NBC_GRID_STRIDE(t, n) for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (n); t += gridDim.x * blockDim.x)
+
+// GetParticleCellIndex_cuk (src/dem_grid.cu:155-202); hierarchical variant
+// GetParticleCellIndex_hGrid_cuk (src/dem_hgrid.cu:205-242) with the
+// out-of-box bucket kept inside the scene's cell range.  Element t of the
+// rebuilt concatenation: key kA[t], value vA[t] = its subsphere.
+static __global__ void k_hash(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    NBC_GRID_STRIDE(t, T) {
+        const int k = plan_find(d.psub, ns, t);
+        const ScenePar& P = d.par[d.pscene[k]];
+        const int i = P.sub_off + (t - d.psub[k]);
+        d.vA[t] = i;
+        const double4 p = d.posr[i];
+        int local;
+        if (P.levels <= 1) {
+            if (p.z >= P.box_hi[2] || p.y >= P.box_hi[1] || p.x >= P.box_hi[0] ||
+                p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
+                local = P.cellnum - 1;
+            } else {
+                int cx = (int)floor((p.x - P.origin[0]) / P.cell[0]);
+                int cy = (int)floor((p.y - P.origin[1]) / P.cell[1]);
+                int cz = (int)floor((p.z - P.origin[2]) / P.cell[2]);
+                cx = clampi(cx, 0, P.gdim[0] - 1);
+                cy = clampi(cy, 0, P.gdim[1] - 1);
+                cz = clampi(cz, 0, P.gdim[2] - 1);
+                local = cz * P.gdim[1] * P.gdim[0] + cy * P.gdim[0] + cx;
+                local = clampi(local, 0, P.cellnum - 1);
+            }
+        } else {
+            if (p.z > P.box_hi[2] || p.y > P.box_hi[1] || p.x > P.box_hi[0] ||
+                p.z < P.box_lo[2] || p.y < P.box_lo[1] || p.x < P.box_lo[0]) {
+                local = P.cellnum - 1;
+            } else {
+                const int lv = d.level[i];
+                const double c = P.lcell[lv];
+                const int cx = clampi((int)floor((p.x - P.origin[0]) / c), 0, P.ldim[lv][0] - 1);
+                const int cy = clampi((int)floor((p.y - P.origin[1]) / c), 0, P.ldim[lv][1] - 1);
+                const int cz = clampi((int)floor((p.z - P.origin[2]) / c), 0, P.ldim[lv][2] - 1);
+                local = P.loff[lv] + (cz * P.ldim[lv][1] * P.ldim[lv][0] + cy * P.ldim[lv][0] + cx);
+            }
+        }
+        d.kA[t] = P.cell_off + local;
+    }
+}
+
+// Tiles of RS_TILE keys, n keys (or *dn); the histogram of tile b, digit v
+// sits at hist[v * tiles + b].  Grid-stride over the tiles.
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __restrict__ keys, int n, int shift,
+                                                        int* __restrict__ hist, const int* __restrict__ dn) {
+    __shared__ int h[256];
+    const int tid = threadIdx.x;
+    const int nn = dn ? *dn : n;
+    const int tiles = (nn + RS_TILE - 1) / RS_TILE;
+    for (int blk = blockIdx.x; blk < tiles; blk += gridDim.x) {
+        h[tid] = 0;
+        __syncthreads();
+        for (int it = 0; it < RS_ITEMS; it++) {
+            const int idx = blk * RS_TILE + it * RS_THREADS + tid;
+            if (idx < nn) atomicAdd(&h[(keys[idx] >> shift) & 255], 1);
+        }
+        __syncthreads();
+        hist[tid * tiles + blk] = h[tid];
+        __syncthreads();
+    }
+}
+
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
+                                                           int* __restrict__ kout, int* __restrict__ vout, int n,
+                                                           int shift, const int* __restrict__ hist,
+                                                           const int* __restrict__ dn) {
+    __shared__ int base[256];
+    __shared__ int wcnt[RS_THREADS / 32][257];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nn = dn ? *dn : n;
+    const int tiles = (nn + RS_TILE - 1) / RS_TILE;
+    for (int blk = blockIdx.x; blk < tiles; blk += gridDim.x) {
+        base[tid] = hist[tid * tiles + blk];
+        for (int it = 0; it < RS_ITEMS; it++) {
+            for (int w = 0; w < RS_THREADS / 32; w++) wcnt[w][tid] = 0;
+            __syncthreads();
+            const int idx = blk * RS_TILE + it * RS_THREADS + tid;
+            const bool valid = idx < nn;
+            const int k = valid ? kin[idx] : 0;
+            const int dig = valid ? ((k >> shift) & 255) : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, dig);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            if (valid && lane == __ffs(peers) - 1) wcnt[warp][dig] = __popc(peers);
+            __syncthreads();
+            if (valid) {
+                int off = base[dig] + rank;
+                for (int w = 0; w < warp; w++) off += wcnt[w][dig];
+                kout[off] = k;
+                vout[off] = vin[idx];
+            }
+            __syncthreads();
+            int add = 0;
+            for (int w = 0; w < RS_THREADS / 32; w++) add += wcnt[w][tid];
+            base[tid] += add;
+            __syncthreads();
+        }
+    }
 }
 
 // --- cell ranges, reorder ------------------------------------------------
 static __global__ void k_fill_i(int* __restrict__ a, int n, int v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
 }
+// a[0, *dn) = v
+static __global__ void k_fill_n(int* __restrict__ a, const int* __restrict__ dn, int v) {
+    const int n = *dn;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
+}
 
-// The permutation of the sort, its inverse and the sorted keys (into key2).
-// The cell table is built from key2 by k_cellstart (FindBegEndInCell_cuk,
-// src/dem_grid.cu:105-153, as one start offset per cell: cell c holds the
-// sorted slots [cstart[c], cstart[c + 1])).
+// The permutation of the sort, its inverse and the sorted keys (into key2),
+// at the subsphere slots of the rebuilt scenes.  The cell table is built
+// from key2 by k_cellstart (FindBegEndInCell_cuk, src/dem_grid.cu:105-153, as
+// one start offset per cell: cell c holds the sorted slots
+// [cstart[c], cstart[c + 1])).
 static __global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    int k = skey[i];
-    d.inv[perm[i]] = i;
-    d.perm[i] = perm[i];
-    d.key2[i] = k;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    NBC_GRID_STRIDE(t, T) {
+        const int k = plan_find(d.psub, ns, t);
+        const int i = d.par[d.pscene[k]].sub_off + (t - d.psub[k]);
+        const int o = perm[t];
+        d.inv[o] = i;
+        d.perm[i] = o;
+        d.key2[i] = skey[t];
+    }
 }
 
 // SortArray_*_cuk (src/dem_grid.cu:336-437) for every persistent per-subsphere
-// array at once, into the alternate buffers.  The displacement accumulator
-// restarts at zero in rebuilt scenes (src/dem_simulation_clump.cu:172).
+// array at once, into the alternate buffers (written back by k_writeback).
+// The displacement accumulator restarts at zero (src/dem_simulation_clump.cu:172).
 template <typename R>
 __global__ void k_reorder(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    const int o = d.perm[i];
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const size_t N = (size_t)d.N;
-    d.posr2[i] = d.posr[o];
-    d.lom2[i] = d.lom[o];
-    d.cum2[i] = d.dyn[d.sid[i]].rebuild ? make_double4(0, 0, 0, 0) : d.cum[o];
-    d.clump_id2[i] = d.clump_id[o];
-    d.part_fix2[i] = d.part_fix[o];
-    d.level2[i] = d.level[o];
-    d.bbits2[i] = d.bbits[o];
-    const R4<R>* k1 = (const R4<R>*)d.kin;
-    R4<R>* k2 = (R4<R>*)d.kin2;
-    for (int c = 0; c < 3; c++) k2[c * N + i] = k1[c * N + o];
-    const R4<R>* b1 = (const R4<R>*)d.bhist;
-    R4<R>* b2 = (R4<R>*)d.bhist2;
-    const uint16_t bits = d.bbits[o];
-    for (int sl = 0; sl < NB_SLOTS; sl++) {
-        if (!(bits & (1u << sl))) continue;  // only live histories are ever read
-        for (int c = 0; c < 3; c++) b2[((size_t)sl * 3 + c) * N + i] = b1[((size_t)sl * 3 + c) * N + o];
+    NBC_GRID_STRIDE(t, T) {
+        const int k = plan_find(d.psub, ns, t);
+        const int i = d.par[d.pscene[k]].sub_off + (t - d.psub[k]);
+        const int o = d.perm[i];
+        d.posr2[i] = d.posr[o];
+        d.lom2[i] = d.lom[o];
+        d.cum2[i] = make_double4(0, 0, 0, 0);
+        d.clump_id2[i] = d.clump_id[o];
+        d.part_fix2[i] = d.part_fix[o];
+        d.level2[i] = d.level[o];
+        d.bbits2[i] = d.bbits[o];
+        const R4<R>* k1 = (const R4<R>*)d.kin;
+        R4<R>* k2 = (R4<R>*)d.kin2;
+        for (int c = 0; c < 3; c++) k2[c * N + i] = k1[c * N + o];
+        const R4<R>* b1 = (const R4<R>*)d.bhist;
+        R4<R>* b2 = (R4<R>*)d.bhist2;
+        const uint16_t bits = d.bbits[o];
+        for (int sl = 0; sl < NB_SLOTS; sl++) {
+            if (!(bits & (1u << sl))) continue;  // only live histories are ever read
+            for (int c = 0; c < 3; c++) b2[((size_t)sl * 3 + c) * N + i] = b1[((size_t)sl * 3 + c) * N + o];
+        }
     }
 }
 
@@ -569,10 +681,13 @@ struct SearchShared {
 // FILL = false: count the hits and store them in subsphere i's scratch rows,
 // count cross-level entries into the coarser partner's cnt_f.  FILL = true:
 // write the hits into the list rows at the scanned offsets and claim the
-// cross-level slots of the coarser partners.
+// cross-level slots of the coarser partners.  The counts of subsphere j sit
+// at j + tb (its element of the rebuilt concatenation); a front row starts at
+// slot cnt_f[j + tb] + poff, a back row at cnt_b[j + tb] + boff.
 template <bool FILL, int SL>
 __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, const PairList& Nw, int i, int lane,
-                                             int* __restrict__ rs, int* __restrict__ pre, int& nf_out, int& nb_out) {
+                                             int* __restrict__ rs, int* __restrict__ pre, int tb, int poff, int boff,
+                                             int& nf_out, int& nb_out) {
     // buffer pointers in registers: the stores below could otherwise alias
     // the pointer table and force it to be re-read on every candidate
     const double4* __restrict__ posr = d.posr2;
@@ -586,6 +701,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     int* __restrict__ bnbr = Nw.bnbr;
     const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
     const int gshift = (threadIdx.x & 31) & ~(SL - 1);
+    __syncwarp(gm);  // the group's previous subsphere is done with rs / pre
     const double4 pi = posr[i];
     const int ci = cid[i];
     const int my = P.levels > 1 ? d.level2[i] : 0;
@@ -643,7 +759,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     // positions are loaded before the current batch is tested
     const unsigned lt = (1u << lane) - 1u;
     int nf = 0, nb = 0;
-    const int rf = FILL ? cnt_f[i] : 0, rb = FILL ? d.cnt_b[i] : 0;
+    const int rf = FILL ? cnt_f[i + tb] + poff : 0, rb = FILL ? d.cnt_b[i + tb] + boff : 0;
     int* __restrict__ scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
     int* __restrict__ scr_b = scr_f + SCR_CAP;
     int r = 0;
@@ -688,7 +804,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
                     if (cross) {
                         // the coarser partner owns the pair: claim a slot after
                         // its same-level front entries (sorted afterwards)
-                        const int q = cnt_f[j] + sfc[j] + atomicAdd(&xcnt[j], 1);
+                        const int q = cnt_f[j + tb] + poff + sfc[j + tb] + atomicAdd(&xcnt[j + tb], 1);
                         nbr[q] = i | flag;
                         own[q] = j;
                     }
@@ -700,7 +816,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
                 } else {
                     const int q = nb + __popc(bm & lt);
                     if (q < SCR_CAP) scr_b[q] = j | flag | (cross ? CROSS_TAG : 0);
-                    if (cross) atomicAdd(&cnt_f[j], 1);
+                    if (cross) atomicAdd(&cnt_f[j + tb], 1);
                 }
             }
         }
@@ -711,14 +827,19 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     nb_out = nb;
 }
 
-// cstart[c] = first sorted slot whose cell key is >= c, for c in [0, cells]
+// cstart[c] = first sorted slot whose cell key is >= c, for the cells of the
+// rebuilt scenes and the entry after each one's last cell (the next scene's
+// first slot, which every writer of that entry agrees on)
 static __global__ void k_cellstart(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int n = d.N;
+    const int TC = d.plan[PL_TC], ns = d.plan[PL_NS];
     const int* __restrict__ key = d.key2;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= d.cells; c += gridDim.x * blockDim.x) {
-        int lo = 0, len = n;
+    NBC_GRID_STRIDE(u, TC) {
+        const int k = plan_find(d.pcell, ns, u);
+        const ScenePar& P = d.par[d.pscene[k]];
+        const int c = P.cell_off + (u - d.pcell[k]);
+        int lo = P.sub_off, len = P.nsub;
         while (len > 0) {
             const int h = len >> 1;
             if (key[lo + h] < c) { lo += h + 1; len -= h + 1; }
@@ -728,99 +849,138 @@ static __global__ void k_cellstart(const Dev* __restrict__ dp) {
     }
 }
 
-// The fused search: counts (cnt_f[i] = same-level front entries + cross-level
-// entries found by finer partners, cnt_b[i] = back entries) and the hits in
-// scratch rows.  Scenes that are not rebuilt keep their rows.
+// the subsphere of element t of the rebuilt concatenation and its scene
+struct PlanItem {
+    int k, s, i;
+};
+__device__ __forceinline__ PlanItem plan_item(const Dev& d, int ns, int t) {
+    PlanItem r;
+    r.k = plan_find(d.psub, ns, t);
+    r.s = d.pscene[r.k];
+    r.i = d.par[r.s].sub_off + (t - d.psub[r.k]);
+    return r;
+}
+
+// The next chunk of a block's work: the search and the compaction cost
+// differ a lot between subspheres (finer levels search more rows), so
+// blocks claim chunks of one element per lane group from a counter instead
+// of taking fixed strides; a block that drew cheap subspheres takes more.
+__device__ __forceinline__ int claim_chunk(int* ctr, int n, int* sh) {
+    if (threadIdx.x == 0) *sh = atomicAdd(ctr, n);
+    __syncthreads();
+    const int b = *sh;
+    __syncthreads();
+    return b;
+}
+
+// The fused search: counts (cnt_f[t] = same-level front entries + cross-level
+// entries found by finer partners, cnt_b[t] = back entries) and the hits in
+// scratch rows.  A group of SL lanes per subsphere, grid-stride.
 template <int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_search(const Dev* __restrict__ dp) {
     __shared__ SearchShared<SL> sh;
+    __shared__ int s_claim;
     const Dev& d = *dp;
     if (*d.halt) return;
     const int g = threadIdx.x / SL;
-    const int i = blockIdx.x * (SEARCH_THREADS / SL) + g;
     const int lane = threadIdx.x % SL;
-    if (i >= d.N) return;
-    const int s = d.sid[i];
-    const ScenePar& P = d.par[s];
-    if (!d.dyn[s].rebuild) {
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    for (;;) {
+        const int c0 = claim_chunk(d.plan + PL_CS, SEARCH_THREADS / SL, &s_claim);
+        if (c0 >= T) break;
+        const int t = c0 + g;
+        if (t >= T) continue;
+        const PlanItem it = plan_item(d, ns, t);
+        const ScenePar& P = d.par[it.s];
+        int nf = 0, nb = 0;
+        if (d.key2[it.i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
+            group_search<false, SL>(d, P, d.L[1], it.i, lane, sh.rs[g], sh.pre[g], t - it.i, 0, 0, nf, nb);
         if (lane == 0) {
-            const PairList& O = d.L[*d.lcur & 1];
-            atomicAdd(&d.cnt_f[i], O.row[i + 1] - O.row[i]);
-            d.cnt_b[i] = O.brow[i + 1] - O.brow[i];
-            d.sfc[i] = 0;
+            atomicAdd(&d.cnt_f[t], nf);
+            d.cnt_b[t] = nb;
+            d.sfc[t] = nf;
+            if (nf > P.bl / 2 || nb > P.bl / 2) atomicOr(&d.dyn[it.s].err, ERR_ROW_OVERFLOW);
         }
-        return;
-    }
-    int nf = 0, nb = 0;
-    if (d.key2[i] != P.cell_off + P.cellnum - 1)  // out-of-box subspheres do not search
-        group_search<false, SL>(d, P, d.L[0], i, lane, sh.rs[g], sh.pre[g], nf, nb);
-    if (lane == 0) {
-        atomicAdd(&d.cnt_f[i], nf);
-        d.cnt_b[i] = nb;
-        d.sfc[i] = nf;
-        if (nf > P.bl / 2 || nb > P.bl / 2) atomicOr(&d.dyn[s].err, ERR_ROW_OVERFLOW);
     }
 }
 
-// the pair totals are cnt_f[N] / cnt_b[N] after the scans
-static __global__ void k_check_cap(const Dev* __restrict__ dp) {
+// After the scans: the pairs of each rebuilt scene's new list (front and
+// back entries are equally many: every pair is one owner entry and one
+// partner entry) into need[s], their prefix over the rebuilt scenes into
+// ppair; with stop set, a list longer than its scene's region stops the
+// step (the host grows the regions and runs the rebuild again).  One block.
+static __global__ void k_check_cap(const Dev* __restrict__ dp, int stop) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    if (d.cnt_f[d.N] > d.cap || d.cnt_b[d.N] > d.cap) {
-        *d.halt = 1;
-        for (int s = 0; s < d.S; s++) atomicOr(&d.dyn[s].err, ERR_LIST_OVERFLOW);
+    const int ns = d.plan[PL_NS];
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        const int s = d.pscene[k];
+        const int a = d.psub[k], b = d.psub[k + 1];
+        const int nf = d.cnt_f[b] - d.cnt_f[a], nb = d.cnt_b[b] - d.cnt_b[a];
+        const int need = max(nf, nb);
+        d.need[s] = need;
+        d.ppair[k] = d.cnt_f[a];
+        if (stop && need > d.dyn[s].pcap) {
+            *d.halt = 1;
+            atomicOr(&d.dyn[s].err, ERR_LIST_OVERFLOW);
+        }
     }
+    if (threadIdx.x == 0) d.ppair[ns] = d.cnt_f[d.psub[ns]];
 }
 
-// The list rows at their scanned offsets: copied from the scratch rows (and
-// the cross-level slots of coarser partners claimed), searched again for rows
-// longer than the scratch, or copied from the previous list for scenes that
-// were not rebuilt.
+// The new rows in the build list L[1], in the scene's region: copied from
+// the scratch rows (and the cross-level slots of coarser partners claimed),
+// or searched again for rows longer than the scratch.
 template <int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_compact(const Dev* __restrict__ dp) {
     __shared__ SearchShared<SL> sh;
+    __shared__ int s_claim;
     const Dev& d = *dp;
     if (*d.halt) return;
     const int g = threadIdx.x / SL;
-    const int i = blockIdx.x * (SEARCH_THREADS / SL) + g;
     const int lane = threadIdx.x % SL;
-    if (i >= d.N) return;
-    const int s = d.sid[i];
-    const ScenePar& P = d.par[s];
-    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
-    const int rf = d.cnt_f[i], rb = d.cnt_b[i];
-    if (lane == 0) {
-        if (i == d.N - 1) { Nw.row[d.N] = d.cnt_f[d.N]; Nw.brow[d.N] = d.cnt_b[d.N]; }
-        Nw.row[i] = rf;
-        Nw.brow[i] = rb;
-    }
-    if (!d.dyn[s].rebuild) {
-        const PairList& O = d.L[*d.lcur & 1];
-        const int of = O.row[i], nf = O.row[i + 1] - of;
-        for (int k = lane; k < nf; k += SL) { Nw.nbr[rf + k] = O.nbr[of + k]; Nw.own[rf + k] = i; }
-        const int ob = O.brow[i], nb = O.brow[i + 1] - ob;
-        for (int k = lane; k < nb; k += SL) Nw.bnbr[rb + k] = O.bnbr[ob + k];
-        return;
-    }
-    if (d.key2[i] == P.cell_off + P.cellnum - 1) return;
-    const int nf = d.sfc[i], nb = d.cnt_b[i + 1] - rb;
-    if (nf <= SCR_CAP && nb <= SCR_CAP) {
-        const int* scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
-        const int* scr_b = scr_f + SCR_CAP;
-        for (int k = lane; k < nf; k += SL) { Nw.nbr[rf + k] = scr_f[k]; Nw.own[rf + k] = i; }
-        for (int k = lane; k < nb; k += SL) {
-            const int v = scr_b[k];
-            Nw.bnbr[rb + k] = v & ~CROSS_TAG;
-            if (v & CROSS_TAG) {
-                const int j = v & (IDX_MASK & ~CROSS_TAG);
-                const int q = d.cnt_f[j] + d.sfc[j] + atomicAdd(&d.xcnt[j], 1);
-                Nw.nbr[q] = i | (v & INTRA);
-                Nw.own[q] = j;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    const PairList& Nw = d.L[1];
+    for (;;) {
+        const int c0 = claim_chunk(d.plan + PL_CC, SEARCH_THREADS / SL, &s_claim);
+        if (c0 >= T) break;
+        const int t = c0 + g;
+        if (t >= T) continue;
+        const PlanItem it = plan_item(d, ns, t);
+        const int i = it.i, s = it.s, tb = t - i;
+        const ScenePar& P = d.par[s];
+        const int t0 = d.psub[it.k];
+        const int base = d.dyn[s].pair_off;
+        const int poff = base - d.cnt_f[t0], boff = base - d.cnt_b[t0];
+        const int rf = d.cnt_f[t] + poff, rb = d.cnt_b[t] + boff;
+        if (lane == 0) {
+            Nw.row[i + s] = rf;
+            Nw.brow[i + s] = rb;
+            if (i == P.sub_off + P.nsub - 1) {
+                Nw.row[i + s + 1] = d.cnt_f[t + 1] + poff;
+                Nw.brow[i + s + 1] = d.cnt_b[t + 1] + boff;
             }
         }
-    } else {
-        int f2, b2;
-        group_search<true, SL>(d, P, Nw, i, lane, sh.rs[g], sh.pre[g], f2, b2);
+        if (d.key2[i] == P.cell_off + P.cellnum - 1) continue;
+        const int nf = d.sfc[t], nb = d.cnt_b[t + 1] - d.cnt_b[t];
+        if (nf <= SCR_CAP && nb <= SCR_CAP) {
+            const int* scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
+            const int* scr_b = scr_f + SCR_CAP;
+            for (int k = lane; k < nf; k += SL) { Nw.nbr[rf + k] = scr_f[k]; Nw.own[rf + k] = i; }
+            for (int k = lane; k < nb; k += SL) {
+                const int v = scr_b[k];
+                Nw.bnbr[rb + k] = v & ~CROSS_TAG;
+                if (v & CROSS_TAG) {
+                    const int tj = (v & (IDX_MASK & ~CROSS_TAG)) + tb;
+                    const int q = d.cnt_f[tj] + poff + d.sfc[tj] + atomicAdd(&d.xcnt[tj], 1);
+                    Nw.nbr[q] = i | (v & INTRA);
+                    Nw.own[q] = tj - tb;
+                }
+            }
+        } else {
+            int f2, b2;
+            group_search<true, SL>(d, P, Nw, i, lane, sh.rs[g], sh.pre[g], tb, poff, boff, f2, b2);
+        }
     }
 }
 
@@ -829,43 +989,50 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_compact(const Dev* __restric
 static __global__ void k_xsort(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N || !d.dyn[d.sid[i]].rebuild) return;
-    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
-    const int b = Nw.row[i] + d.sfc[i], e = Nw.row[i + 1];
-    for (int m = b + 1; m < e; m++) {
-        const int v = Nw.nbr[m];
-        int q = m - 1;
-        while (q >= b && (Nw.nbr[q] & IDX_MASK) > (v & IDX_MASK)) { Nw.nbr[q + 1] = Nw.nbr[q]; q--; }
-        Nw.nbr[q + 1] = v;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    const PairList& Nw = d.L[1];
+    NBC_GRID_STRIDE(t, T) {
+        const PlanItem it = plan_item(d, ns, t);
+        const int b = Nw.row[it.i + it.s] + d.sfc[t], e = Nw.row[it.i + it.s + 1];
+        for (int m = b + 1; m < e; m++) {
+            const int v = Nw.nbr[m];
+            int q = m - 1;
+            while (q >= b && (Nw.nbr[q] & IDX_MASK) > (v & IDX_MASK)) { Nw.nbr[q + 1] = Nw.nbr[q]; q--; }
+            Nw.nbr[q + 1] = v;
+        }
     }
 }
 
 // The reverse map of CreateContList_cuk (src/dem_grid.cu:561-601): for each
-// back entry of i (owner j), the index of the pair (j, i) in j's front row.
+// back entry of i (owner j), the slot of the pair (j, i) in j's front row.
 static __global__ void k_backref(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.N) return;
-    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
-    for (int k = Nw.brow[i]; k < Nw.brow[i + 1]; k++) {
-        const int j = Nw.bnbr[k] & IDX_MASK;
-        int found = -1;
-        for (int q = Nw.row[j]; q < Nw.row[j + 1]; q++)
-            if ((Nw.nbr[q] & IDX_MASK) == i) { found = q; break; }
-        Nw.bpair[k] = found;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    const PairList& Nw = d.L[1];
+    NBC_GRID_STRIDE(t, T) {
+        const PlanItem it = plan_item(d, ns, t);
+        const int s = it.s;
+        for (int k = Nw.brow[it.i + s]; k < Nw.brow[it.i + s + 1]; k++) {
+            const int j = Nw.bnbr[k] & IDX_MASK;
+            int found = -1;
+            for (int q = Nw.row[j + s]; q < Nw.row[j + s + 1]; q++)
+                if ((Nw.nbr[q] & IDX_MASK) == it.i) { found = q; break; }
+            Nw.bpair[k] = found;
+        }
     }
 }
 
 // InheritContHistory_cuk (src/dem_grid.cu:603-647): each new pair copies the
-// spring history of the same pair in the previous list, negated when the
-// owner changed.  Pairs absent from the previous list start from zero.
+// spring history of the same pair in the current list, negated when the
+// owner changed; pairs absent from it start from zero.  The new history and
+// touch flag go to the generation the next contact pass writes (free now) and
+// are written back by k_writeback_pairs.
 template <typename R>
-__device__ __forceinline__ void carry_one(const Dev& d, int p) {
-    const int lc = *d.lcur, hg = *d.hgen;
-    const PairList& O = d.L[lc & 1];
-    const PairList& Nw = d.L[(lc + 1) & 1];
+__device__ __forceinline__ void carry_one(const Dev& d, int p, int s) {
+    const int hg = *d.hgen;
+    const PairList& O = d.L[0];
+    const PairList& Nw = d.L[1];
     const size_t cap = (size_t)d.cap;
     const R4<R>* Hi = (const R4<R>*)d.H[hg & 1];
     R4<R>* Ho = (R4<R>*)d.H[(hg + 1) & 1];
@@ -874,30 +1041,23 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p) {
     const int jr = Nw.nbr[p];
     if (jr < 0) { to[p] = 0; d.nearf[p] = 0; return; }  // pair inside one clump
     const int i = Nw.own[p], j = jr;
-    const int s = d.sid[i];
     const ScenePar& P = d.par[s];
-    // near flag of the new pair (see k_near): distance below ri + rj + m, with
-    // m = 2 Thresh in a scene rebuilt now and 4 Thresh in one that is not (its
-    // subspheres are up to Thresh from their last rebuild already)
+    // near flag of the new pair (see k_near): distance below ri + rj + 2 Thresh
     {
         const double4 pi = d.posr2[i], pj = d.posr2[j];
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        const double m = (d.dyn[s].rebuild ? 2.0 : 4.0) * P.thresh * (1.0 + 1e-6) + 1e-12;
+        const double m = 2.0 * P.thresh * (1.0 + 1e-6) + 1e-12;
         const double lim = (pi.w + pj.w) + m;
         const bool nr = dx * dx + dy * dy + dz * dz < lim * lim;
         d.nearf[p] = nr;
         if (!nr) {
-            // cannot touch before the next rebuild: no live history (the
-            // other touch buffer is still read here and is cleared by k_near)
-            to[p] = 0;
+            to[p] = 0;  // cannot touch before the next rebuild: no live history
             return;
         }
     }
     int q = -1;
     R sign = R(1);
-    if (!d.dyn[s].rebuild) {
-        q = p - Nw.row[P.sub_off] + O.row[P.sub_off];
-    } else {
+    {
         const int io = d.perm[i], jo = d.perm[j];
         int oo, ot;
         if (P.levels > 1 && d.level2[i] != d.level2[j]) {
@@ -909,7 +1069,7 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p) {
             ot = io < jo ? jo : io;
         }
         sign = oo == io ? R(1) : R(-1);
-        for (int r = O.row[oo]; r < O.row[oo + 1]; r++)
+        for (int r = O.row[oo + s]; r < O.row[oo + s + 1]; r++)
             if ((O.nbr[r] & IDX_MASK) == ot) { q = r; break; }
     }
     if (q >= 0 && ti[q]) {
@@ -927,28 +1087,122 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p) {
     }
 }
 
+// the pairs of the rebuilt scenes' new lists (element u of their
+// concatenation is slot pair_off + u - ppair[k] of its scene's region)
 template <typename R>
 __global__ void k_carry(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    // grid-stride: the launch is captured once and the list may have grown since
-    const int np = d.cnt_f[d.N];
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-        carry_one<R>(d, p);
+    const int ns = d.plan[PL_NS];
+    const int np = d.ppair[ns];
+    NBC_GRID_STRIDE(u, np) {
+        const int k = plan_find(d.ppair, ns, u);
+        const int s = d.pscene[k];
+        carry_one<R>(d, d.dyn[s].pair_off + (u - d.ppair[k]), s);
+    }
+}
+
+// The rebuilt scenes' gathered per-subsphere state and new rows, written
+// back into the current buffers.
+template <typename R>
+__global__ void k_writeback(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    if (ns == d.S) return;  // every scene rebuilt: k_swap exchanges the buffers instead
+    const size_t N = (size_t)d.N;
+    const PairList& Lc = d.L[0];
+    const PairList& Nw = d.L[1];
+    NBC_GRID_STRIDE(t, T) {
+        const PlanItem it = plan_item(d, ns, t);
+        const int i = it.i, s = it.s;
+        d.posr[i] = d.posr2[i];
+        d.lom[i] = d.lom2[i];
+        d.cum[i] = d.cum2[i];
+        d.clump_id[i] = d.clump_id2[i];
+        d.part_fix[i] = d.part_fix2[i];
+        d.level[i] = d.level2[i];
+        d.key[i] = d.key2[i];
+        const R4<R>* k2 = (const R4<R>*)d.kin2;
+        R4<R>* k1 = (R4<R>*)d.kin;
+        for (int c = 0; c < 3; c++) k1[c * N + i] = k2[c * N + i];
+        const uint16_t bits = d.bbits2[i];
+        d.bbits[i] = bits;
+        const R4<R>* b2 = (const R4<R>*)d.bhist2;
+        R4<R>* b1 = (R4<R>*)d.bhist;
+        for (int sl = 0; sl < NB_SLOTS; sl++) {
+            if (!(bits & (1u << sl))) continue;
+            for (int c = 0; c < 3; c++) b1[((size_t)sl * 3 + c) * N + i] = b2[((size_t)sl * 3 + c) * N + i];
+        }
+        Lc.row[i + s] = Nw.row[i + s];
+        Lc.brow[i + s] = Nw.brow[i + s];
+        if (i == d.par[s].sub_off + d.par[s].nsub - 1) {
+            Lc.row[i + s + 1] = Nw.row[i + s + 1];
+            Lc.brow[i + s + 1] = Nw.brow[i + s + 1];
+        }
+    }
+}
+
+// the rebuilt scenes' new list entries, carried histories and touch flags,
+// written back into the current list and the generation the next contact
+// pass reads (both generations then agree on the region)
+template <typename R>
+__global__ void k_writeback_pairs(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int ns = d.plan[PL_NS];
+    if (ns == d.S) return;
+    const int np = d.ppair[ns];
+    const int hg = *d.hgen;
+    const size_t cap = (size_t)d.cap;
+    const PairList& Lc = d.L[0];
+    const PairList& Nw = d.L[1];
+    R4<R>* Hc = (R4<R>*)d.H[hg & 1];
+    const R4<R>* Hn = (const R4<R>*)d.H[(hg + 1) & 1];
+    uint8_t* tc = d.touch[hg & 1];
+    const uint8_t* tn = d.touch[(hg + 1) & 1];
+    NBC_GRID_STRIDE(u, np) {
+        const int k = plan_find(d.ppair, ns, u);
+        const int p = d.dyn[d.pscene[k]].pair_off + (u - d.ppair[k]);
+        Lc.nbr[p] = Nw.nbr[p];
+        Lc.own[p] = Nw.own[p];
+        Lc.bnbr[p] = Nw.bnbr[p];
+        Lc.bpair[p] = Nw.bpair[p];
+        const uint8_t f = tn[p];
+        tc[p] = f;
+        if (f) {
+            Hc[p] = Hn[p];
+            Hc[cap + p] = Hn[cap + p];
+            ((R*)(Hc + 2 * cap))[p] = ((const R*)(Hn + 2 * cap))[p];
+        }
+    }
+}
+
+// When every scene was rebuilt (always for a single scene) the gathered
+// buffers, the build list and the carried history generation become the
+// current ones by exchanging pointers in the table instead of copying back;
+// k_near then clears the other touch generation for the pairs that are not
+// near (it still holds the flags of the previous list).
+static __global__ void k_swap(Dev* __restrict__ dp) {
+    Dev& d = *dp;
+    if (*d.halt || d.plan[PL_NS] != d.S) return;
+#define NBC_SWAP(a, b) { auto tmp_ = d.a; d.a = d.b; d.b = tmp_; }
+    NBC_SWAP(posr, posr2) NBC_SWAP(lom, lom2) NBC_SWAP(cum, cum2) NBC_SWAP(clump_id, clump_id2)
+    NBC_SWAP(part_fix, part_fix2) NBC_SWAP(level, level2) NBC_SWAP(key, key2) NBC_SWAP(kin, kin2)
+    NBC_SWAP(bhist, bhist2) NBC_SWAP(bbits, bbits2)
+    NBC_SWAP(L[0], L[1]) NBC_SWAP(H[0], H[1]) NBC_SWAP(touch[0], touch[1])
+#undef NBC_SWAP
 }
 
 // Near rows.  Between two rebuilds of a scene every subsphere stays within
 // Thresh of where it was at the rebuild (a larger displacement triggers the
 // next one), so a pair whose distance at a rebuild is at least ri + rj +
-// 2 Thresh cannot touch before the next one (4 Thresh for a scene of the
-// batch that is not rebuilt now: its subspheres are up to Thresh from their
-// last rebuild already).  k_carry flags the near pairs of the new list and
-// clears the touch flag it writes for the others, k_near the other flag (the
-// one k_carry reads), as every contact pass in the interval would have
-// cleared them; the near rows list the near entries
-// (front: pair index in row order, back: the pair index of each near back
-// entry) and the contact pass visits only them, with the same results as
-// visiting the whole list.
+// 2 Thresh cannot touch before the next one.  k_carry flags the near pairs
+// of a rebuilt scene and clears the touch flag of the others (in both
+// generations, after the write-back); the near rows list the near entries of
+// every scene (front: pair slot in row order, back: the pair slot of each
+// near back entry) and the contact pass visits only them, with the same
+// results as visiting the whole list.
 template <bool FILL, int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -959,22 +1213,24 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
     const int gshift = (threadIdx.x & 31) & ~(SL - 1);
     const unsigned lt = (1u << lane) - 1u;
-    const PairList& Nw = d.L[(*d.lcur + 1) & 1];
+    const PairList& Lc = d.L[0];
     const uint8_t* __restrict__ nearf = d.nearf;
-    const int* __restrict__ bpair = Nw.bpair;
-    uint8_t* __restrict__ tprev = d.touch[*d.hgen & 1];   // read by k_carry, free now
+    const int* __restrict__ bpair = Lc.bpair;
+    const int s = d.sid[i];
+    // after k_swap: the other touch generation still holds the old list's flags
+    uint8_t* __restrict__ tother = !FILL && d.plan[PL_NS] == d.S ? d.touch[(*d.hgen + 1) & 1] : nullptr;
     int nf = 0, nb = 0;
     const int rf = FILL ? d.nrow[i] : 0, rb = FILL ? d.nbrow[i] : 0;
-    const int rs = Nw.row[i], re = Nw.row[i + 1];
+    const int rs = Lc.row[i + s], re = Lc.row[i + s + 1];
     for (int k0 = rs; k0 < re; k0 += SL) {
         const int k = k0 + lane;
         const bool nr = k < re && nearf[k];
-        if (!FILL && k < re && !nr) tprev[k] = 0;
+        if (tother && k < re && !nr) tother[k] = 0;
         const unsigned m = __ballot_sync(gm, nr) >> gshift;
         if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
         nf += __popc(m);
     }
-    const int bs = Nw.brow[i], be = Nw.brow[i + 1];
+    const int bs = Lc.brow[i + s], be = Lc.brow[i + s + 1];
     for (int k0 = bs; k0 < be; k0 += SL) {
         const int k = k0 + lane;
         int q = -1;
@@ -991,38 +1247,94 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     }
 }
 
-// Finishes a rebuild: per-clump member lists in ascending subsphere order
-// (the order thrust::sort_by_key gives reduce_by_key, src/dem_clumpsphere.cu:
-// 123-147), scene bookkeeping, and the swap of list, history generation and
-// persistent per-subsphere buffers.
-static __global__ void k_commit(Dev* __restrict__ dp) {
-    Dev& d = *dp;
+// Finishes a rebuild: per-clump member lists of the rebuilt scenes in
+// ascending subsphere order (the order thrust::sort_by_key gives
+// reduce_by_key, src/dem_clumpsphere.cu:123-147) and the scene bookkeeping.
+static __global__ void k_commit(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
     if (*d.halt) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < d.K) {
-        const int mb = d.mem_start[t], me = d.mem_start[t + 1];
-        for (int m = mb; m < me; m++) d.mem_idx[m] = d.inv[d.mem_idx[m]];
-        for (int m = mb + 1; m < me; m++) {
-            int v = d.mem_idx[m], q = m - 1;
-            while (q >= mb && d.mem_idx[q] > v) { d.mem_idx[q + 1] = d.mem_idx[q]; q--; }
-            d.mem_idx[q + 1] = v;
+    const int ns = d.plan[PL_NS], TK = d.plan[PL_TK];
+    NBC_GRID_STRIDE(u, TK + ns + 1) {
+        if (u < TK) {
+            const int k = plan_find(d.pclump, ns, u);
+            const int c = d.par[d.pscene[k]].clump_off + (u - d.pclump[k]);
+            const int mb = d.mem_start[c], me = d.mem_start[c + 1];
+            for (int m = mb; m < me; m++) d.mem_idx[m] = d.inv[d.mem_idx[m]];
+            for (int m = mb + 1; m < me; m++) {
+                int v = d.mem_idx[m], q = m - 1;
+                while (q >= mb && d.mem_idx[q] > v) { d.mem_idx[q + 1] = d.mem_idx[q]; q--; }
+                d.mem_idx[q + 1] = v;
+            }
+        } else if (u < TK + ns) {
+            const int k = u - TK;
+            SceneDyn& y = d.dyn[d.pscene[k]];
+            y.npairs = d.ppair[k + 1] - d.ppair[k];
+            y.nrebuild++;
+            y.rebuild = 0;
+        } else {
+            *d.any_rebuild = 0;
         }
-    } else if (t < d.K + d.S) {
-        const int s = t - d.K;
-        SceneDyn& y = d.dyn[s];
-        const int so = d.par[s].sub_off, ns = d.par[s].nsub;
-        y.pair_off = d.cnt_f[so];
-        y.npairs = d.cnt_f[so + ns] - d.cnt_f[so];
-        if (y.rebuild) { y.nrebuild++; y.rebuild = 0; }
-    } else if (t == d.K + d.S) {
-        *d.lcur += 1;
-        *d.hgen += 1;
-        *d.any_rebuild = 0;
-#define NBC_SWAP(a, b) { auto tmp_ = d.a; d.a = d.b; d.b = tmp_; }
-        NBC_SWAP(posr, posr2) NBC_SWAP(lom, lom2) NBC_SWAP(cum, cum2) NBC_SWAP(clump_id, clump_id2)
-        NBC_SWAP(part_fix, part_fix2) NBC_SWAP(level, level2) NBC_SWAP(key, key2) NBC_SWAP(kin, kin2)
-        NBC_SWAP(bhist, bhist2) NBC_SWAP(bbits, bbits2)
-#undef NBC_SWAP
+    }
+}
+
+// Moves every scene's list to a new layout of the pair regions (the host
+// grows them): entries, back references, the history generation the next
+// contact pass reads, touch and near flags.  map[s] = (old first slot, new
+// first slot, pairs, prefix of the pairs over the scenes); d holds the new
+// buffers.
+template <typename R>
+__global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* __restrict__ oh,
+                           const uint8_t* __restrict__ ot, const uint8_t* __restrict__ onear, int ocap,
+                           const int4* __restrict__ map, int total) {
+    const Dev& d = *dp;
+    const int hg = *d.hgen;
+    const size_t cap = (size_t)d.cap, oc = (size_t)ocap;
+    const R4<R>* Ho = (const R4<R>*)oh;
+    R4<R>* Hn = (R4<R>*)d.H[hg & 1];
+    const PairList& Lc = d.L[0];
+    NBC_GRID_STRIDE(u, total) {
+        int lo = 0, hi = d.S - 1;
+        while (lo < hi) {
+            const int m = (lo + hi + 1) >> 1;
+            if (map[m].w <= u) lo = m;
+            else hi = m - 1;
+        }
+        const int4 m = map[lo];
+        const int po = m.x + (u - m.w), pn = m.y + (u - m.w);
+        Lc.nbr[pn] = ol.nbr[po];
+        Lc.own[pn] = ol.own[po];
+        Lc.bnbr[pn] = ol.bnbr[po];
+        const int bq = ol.bpair[po];
+        Lc.bpair[pn] = bq >= 0 ? bq + (m.y - m.x) : bq;
+        const uint8_t f = ot[po];
+        d.touch[hg & 1][pn] = f;
+        d.nearf[pn] = onear[po];
+        if (f) {
+            Hn[pn] = Ho[po];
+            Hn[cap + pn] = Ho[oc + po];
+            ((R*)(Hn + 2 * cap))[pn] = ((const R*)(Ho + 2 * oc))[po];
+        }
+    }
+}
+
+// the current rows follow their scene's region: every row offset of scene s
+// moves by its region's move (the subsphere threads take the row starts,
+// one thread per scene the end entry)
+static __global__ void k_shift_rows(const Dev* __restrict__ dp, const int4* __restrict__ map) {
+    const Dev& d = *dp;
+    const PairList& Lc = d.L[0];
+    NBC_GRID_STRIDE(u, d.N + d.S) {
+        int s, r;
+        if (u < d.N) {
+            s = d.sid[u];
+            r = u + s;
+        } else {
+            s = u - d.N;
+            r = d.par[s].sub_off + d.par[s].nsub + s;
+        }
+        const int delta = map[s].y - map[s].x;
+        Lc.row[r] += delta;
+        Lc.brow[r] += delta;
     }
 }
 

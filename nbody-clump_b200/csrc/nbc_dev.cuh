@@ -68,18 +68,34 @@ struct SceneDyn {
     int step;                      // completed steps
     int nrebuild;
     int npairs;                    // pairs in the current list
-    int pair_off;                  // first pair of this scene in the current list
+    int pair_off;                  // first pair slot of this scene's region of the pair buffers
+    int pcap;                      // pair slots of that region (set by the host, grown on overflow)
     long long ifix[6];             // fixed-point sums of intruder force (2^-40 N) and torque (2^-44 N m)
 };
 
+// Pair list of a batch: scene s owns the pair slots [pair_off, pair_off +
+// pcap) of every per-pair buffer, so a scene's rebuild rewrites its own region
+// only.  Row offsets are absolute slots, one row array per scene with its end
+// entry: subsphere i of scene s starts at row[i + s], ends at row[i + s + 1].
 struct PairList {
-    int* row;     // [N+1] exclusive scan of front counts (owner rows)
-    int* brow;    // [N+1] exclusive scan of back counts
+    int* row;     // [N+S] front (owner) row offsets
+    int* brow;    // [N+S] back row offsets
     int* nbr;     // [cap] front partner, bit 31 set for pairs inside one clump
     int* own;     // [cap] owner of each pair (the reference's Lpa)
     int* bnbr;    // [cap] back partner (the owner), bit 31 set inside one clump
     int* bpair;   // [cap] pair index of each back entry (the reference's Aref)
 };
+
+// entries of Dev::plan
+constexpr int PL_NS = 0;     // rebuilt scenes
+constexpr int PL_T = 1;      // their subspheres
+constexpr int PL_TC = 2;     // their cell-table entries
+constexpr int PL_T1 = 3;     // PL_T + 1 (scan length of the counts)
+constexpr int PL_HIST = 4;   // radix histogram entries (256 per tile)
+constexpr int PL_TK = 5;     // their clumps
+constexpr int PL_CS = 6;     // work counter of k_search (subspheres claimed)
+constexpr int PL_CC = 7;     // work counter of k_compact
+constexpr int PL_SIZE = 8;
 
 struct Dev {
     int S, N, K;
@@ -93,8 +109,9 @@ struct Dev {
     int* sid;         // [N] scene of each subsphere
     int* csid;        // [K] scene of each clump
     // subspheres, sorted order.  Each persistent array has an alternate
-    // buffer (suffix 2): a rebuild gathers into the alternates and k_commit
-    // swaps the pointers in this table, so nothing changes if it stops early.
+    // buffer (suffix 2): a rebuild gathers the rebuilt scenes into the
+    // alternates and writes them back once the new list is complete, so
+    // nothing changes if it stops early.
     double4* posr;    double4* posr2;    // x y z r
     double4* lom;     double4* lom2;     // local offset (body frame) xyz, mass
     double4* cum;     double4* cum2;     // displacement since the last rebuild
@@ -130,10 +147,21 @@ struct Dev {
     int* xcnt;                            // [N] cross-level entries placed so far (hierarchical grid)
     int* scan_tmp;                        // block sums
     int* any_rebuild;                     // device flag: some scene rebuilds this step
+    // rebuild plan (k_plan): the scenes rebuilt at this step in ascending
+    // order and prefix sums over them; every rebuild kernel runs over the
+    // concatenation of the rebuilt scenes only
+    int* plan;        // [PL_SIZE] counts, see PL_*
+    int* pscene;      // [S] rebuilt scenes
+    int* psub;        // [S+1] prefix of their subsphere counts
+    int* pcell;       // [S+1] prefix of their cell-table entries (cellnum + 1)
+    int* pclump;      // [S+1] prefix of their clump counts
+    int* ppair;       // [S+1] prefix of the pairs of their new lists
+    int* need;        // [S] pairs of the new list of each rebuilt scene, -1 for the others
     int* halt;                            // device flag: pair capacity exceeded, kernels stand still
-    // pair lists and histories (ping-pong)
+    // pair lists: the current one and the one a rebuild builds (written
+    // back into the current one), histories ping-pong between steps
     PairList L[2];
-    int* lcur;        // index of the current list
+    int* lcur;        // index of the current list (0)
     void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
     void* ctb;        // Real4 [4][cap]: per pair force and torque on the owner, then on the partner

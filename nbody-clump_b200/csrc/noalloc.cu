@@ -70,9 +70,9 @@ __global__ void k_hash_plain(const double* __restrict__ pos, int n, nbc_grid_des
 
 void scan_ints(int* a, int n, int* sums, cudaStream_t st) {
     const int nb = (n + nbc::SC_TILE - 1) / nbc::SC_TILE;
-    nbc::k_scan_tiles<<<nb, nbc::SC_THREADS, 0, st>>>(a, n, sums);
-    nbc::k_scan_sums<<<1, nbc::SC_THREADS, 0, st>>>(sums, nb);
-    nbc::k_scan_add<<<nb, nbc::SC_THREADS, 0, st>>>(a, n, sums);
+    nbc::k_scan_tiles<<<nb, nbc::SC_THREADS, 0, st>>>(a, n, sums, nullptr);
+    nbc::k_scan_sums<<<1, nbc::SC_THREADS, 0, st>>>(sums, nb, nullptr);
+    nbc::k_scan_add<<<nb, nbc::SC_THREADS, 0, st>>>(a, n, sums, nullptr);
 }
 
 }  // namespace
@@ -123,9 +123,9 @@ extern "C" nbc_status nbc_cell_sort_noalloc(const double* pos_dev, int n, const 
     else { ki = key_dev; vi = perm_dev; ko = kB; vo = vB; }
     k_hash_plain<<<(n + 127) / 128, 128, 0, st>>>(pos_dev, n, *grid, ki, vi);
     for (int p = 0; p < passes; p++) {
-        nbc::k_rs_hist<<<tiles, nbc::RS_THREADS, 0, st>>>(ki, n, 8 * p, hist, tiles);
+        nbc::k_rs_hist<<<tiles, nbc::RS_THREADS, 0, st>>>(ki, n, 8 * p, hist, nullptr);
         scan_ints(hist, 256 * tiles, sums, st);
-        nbc::k_rs_scatter<<<tiles, nbc::RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, 8 * p, hist, tiles);
+        nbc::k_rs_scatter<<<tiles, nbc::RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, 8 * p, hist, nullptr);
         int* t = ki; ki = ko; ko = t;
         t = vi; vi = vo; vo = t;
     }

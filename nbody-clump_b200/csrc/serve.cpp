@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -254,7 +255,8 @@ nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_active, int* n_qu
             }
             double b = 0, ms = 0;
             h->eng->info(&b, &ms);
-            r.bytes = std::max(b, r.est_bytes);
+            // whole bytes, so that the sum over running requests stays exact
+            r.bytes = std::ceil(std::max(b, r.est_bytes));
             s->used += r.bytes;
             r.eng = std::move(h);
             r.state = 1;
