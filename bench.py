@@ -316,9 +316,10 @@ def cpu_baseline(args):
 def run_batch(args):
     """cfg3: n independent cfg1-style scenes (clump counts log-uniform in
     [500, 50,000], friction U[0.2, 0.8], own seeds), advanced together
-    (nbc_batch: one engine, stream and graph per scene, launches interleaved)
-    against the same scenes one at a time on the plain engine.  Both timings
-    include engine creation (upload) and the first list build."""
+    (nbc_batch: one engine over all scenes, one launch per kernel and step,
+    rebuilds over the scenes that need one) against the same scenes one at a
+    time on the plain engine.  Both timings include engine creation (upload)
+    and the first list build."""
     import nbc
     scenes = [nbc.with_levels(s) for s in sg.make_cfg3(args.scenes, steps=args.steps)]
     n_sub = sum(int(s["params"]["NumberBody"]) for s in scenes)
@@ -327,8 +328,7 @@ def run_batch(args):
     b = nbc.Batch(scenes, **opts)
     t1 = time.perf_counter()
     b.step(args.steps)
-    for e in b.engines:
-        e.sync()
+    b.sync()
     t2 = time.perf_counter()
     b.close()
     bc, bs = t1 - t0, t2 - t1

@@ -182,20 +182,22 @@ nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 
 /* --- batches of independent scenes ---------------------------------------
- * No reference counterpart (the reference runs one scene per process).  Each
- * scene gets its own engine, stream and step graph; nbc_batch_step enqueues a
- * chunk of steps on every scene's stream before it waits for any, so the
- * scenes' kernels overlap on the GPU.  Each scene rebuilds its list on its
- * own schedule: its results are bitwise those of the scene run alone.  For
- * the streams to run concurrently set CUDA_DEVICE_MAX_CONNECTIONS (e.g. 32)
- * in the environment before the process first uses CUDA. */
+ * No reference counterpart (the reference runs one scene per process).  A
+ * batch is one engine over all its scenes, concatenated: every kernel of a
+ * step covers every scene in one launch, and a rebuild covers only the
+ * scenes whose own rebuild test fired (each scene keeps its own rebuild
+ * schedule and its own region of the pair buffers), so each scene's results
+ * are bitwise those of the scene run alone.  nbc_create with several scenes
+ * makes the same engine; the batch calls exist for callers that think in
+ * batches. */
 typedef struct nbc_batch nbc_batch;
 nbc_status nbc_batch_create(const nbc_scene_desc* const* scenes, int n_scenes, const nbc_options* opt,
                             nbc_batch** out);
 nbc_status nbc_batch_step(nbc_batch* b, int nsteps);
-/* the engine of scene i, for the getters above; owned by the batch (do not
- * pass it to nbc_destroy), valid until nbc_batch_destroy */
-nbc_status nbc_batch_engine(nbc_batch* b, int i, nbc_engine** e);
+/* the batch's engine, for the getters above: scene i of the batch is scene i
+ * of this engine; owned by the batch (do not pass it to nbc_destroy), valid
+ * until nbc_batch_destroy */
+nbc_status nbc_batch_engine(nbc_batch* b, nbc_engine** e);
 nbc_status nbc_batch_destroy(nbc_batch* b);
 
 /* --- request server (continuous batching) ---------------------------------

@@ -1,18 +1,18 @@
 // serve.cpp -- batches of independent scenes and a request server, on top of
-// the engine's asynchronous stepping.
+// the engine.
 //
 // The reference runs one scene per process (DEMClumpMain::RunSimulationClump,
 // src/dem_simulation_clump.cu:110-259).  Here many scenes share one GPU:
-//   nbc_batch_*   a fixed set of scenes advanced together.  Each scene has its
-//                 own engine, stream and step graph; the host enqueues a chunk
-//                 of steps on every scene's stream before waiting for any, so
-//                 the scenes' kernels overlap on the GPU.  Each scene rebuilds
-//                 its list on its own schedule, so a scene's results in a
-//                 batch are bitwise those of the scene run alone.
+//   nbc_batch_*   a fixed set of scenes in one engine: every kernel of a step
+//                 covers all of them in one launch, a rebuild covers the
+//                 scenes whose own rebuild test fired, and each scene's
+//                 results are bitwise those of the scene run alone.
 //   nbc_server_*  continuous batching: requests (a scene and a step count)
 //                 are queued, admitted in arrival order while the device-
 //                 memory budget and the slot limit allow, advanced together in
-//                 chunks, and retired when their steps are done, which frees
+//                 chunks (each request has its own engine and stream, the
+//                 host enqueues a chunk on every stream before waiting for
+//                 any), and retired when their steps are done, which frees
 //                 their memory for the next admissions.  The result of a
 //                 request is the intruder's reaction force and torque sampled
 //                 every `sample_every` steps (the reference's fc output,
@@ -39,37 +39,8 @@ using nbc::guard;
 // ---------------------------------------------------------------------------
 
 struct nbc_batch {
-    std::vector<std::unique_ptr<nbc_engine>> eng;
+    std::unique_ptr<nbc_engine> eng;
 };
-
-namespace {
-
-// advance every engine by nsteps, chunk steps at a time, all chunks
-// enqueued before any is waited for
-void advance_all(const std::vector<nbc_engine*>& engines, const std::vector<int>& nsteps, int chunk,
-                 std::vector<int>* done_out) {
-    std::vector<int> left(nsteps);
-    std::vector<int> done(engines.size(), 0);
-    for (;;) {
-        bool any = false;
-        std::vector<int> launched(engines.size(), 0);
-        for (size_t k = 0; k < engines.size(); k++)
-            if (left[k] > 0) {
-                launched[k] = engines[k]->eng->enqueue(std::min(chunk, left[k]));
-                any = true;
-            }
-        if (!any) break;
-        for (size_t k = 0; k < engines.size(); k++)
-            if (launched[k] > 0) {
-                const int d = engines[k]->eng->wait_steps();
-                left[k] -= d;
-                done[k] += d;
-            }
-    }
-    if (done_out) *done_out = done;
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -82,13 +53,11 @@ nbc_status nbc_batch_create(const nbc_scene_desc* const* scenes, int n, const nb
     if (opt) o = *opt; else nbc_default_options(&o);
     std::unique_ptr<nbc_batch> b(new nbc_batch());
     nbc_status st = guard([&] {
-        for (int s = 0; s < n; s++) {
-            std::unique_ptr<nbc_engine> h(new nbc_engine());
-            h->opt = o;
-            std::vector<const nbc_scene_desc*> v(1, scenes[s]);
-            h->eng.reset(nbc::make_engine(v, o));
-            b->eng.push_back(std::move(h));
-        }
+        std::unique_ptr<nbc_engine> h(new nbc_engine());
+        h->opt = o;
+        std::vector<const nbc_scene_desc*> v(scenes, scenes + n);
+        h->eng.reset(nbc::make_engine(v, o));
+        b->eng = std::move(h);
     });
     if (st == NBC_OK) *out = b.release();
     return st;
@@ -96,16 +65,12 @@ nbc_status nbc_batch_create(const nbc_scene_desc* const* scenes, int n, const nb
 
 nbc_status nbc_batch_step(nbc_batch* b, int nsteps) {
     if (!b || nsteps < 0) return fail(NBC_ERR_ARG, "nbc_batch_step: bad arguments");
-    return guard([&] {
-        std::vector<nbc_engine*> v;
-        for (auto& e : b->eng) v.push_back(e.get());
-        advance_all(v, std::vector<int>(v.size(), nsteps), 64, nullptr);
-    });
+    return guard([&] { b->eng->eng->step(nsteps, false); });
 }
 
-nbc_status nbc_batch_engine(nbc_batch* b, int i, nbc_engine** e) {
-    if (!b || !e || i < 0 || i >= (int)b->eng.size()) return fail(NBC_ERR_ARG, "nbc_batch_engine: bad index");
-    *e = b->eng[i].get();
+nbc_status nbc_batch_engine(nbc_batch* b, nbc_engine** e) {
+    if (!b || !e) return fail(NBC_ERR_ARG, "nbc_batch_engine: bad arguments");
+    *e = b->eng.get();
     return NBC_OK;
 }
 

@@ -240,13 +240,13 @@ class Engine:
         _check(lib().nbc_run(self.h))
 
     @classmethod
-    def borrowed(cls, handle, scene):
-        """A view of an engine owned by a Batch (not destroyed by close)."""
+    def borrowed(cls, handle, scenes):
+        """A view of an engine owned by a Batch or a Server (not destroyed by close)."""
         self = cls.__new__(cls)
         self._descs = []
-        self.N = [int(scene["params"]["NumberBody"])]
-        self.K = [int(scene["params"]["ClumpNum"])]
-        self.BL = [int(scene["params"]["BranchLmtLen"])]
+        self.N = [int(sc["params"]["NumberBody"]) for sc in scenes]
+        self.K = [int(sc["params"]["ClumpNum"]) for sc in scenes]
+        self.BL = [int(sc["params"]["BranchLmtLen"]) for sc in scenes]
         self.h = handle
         self._owner = False
         return self
@@ -400,10 +400,30 @@ def _options(precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.
     return o
 
 
+class SceneView:
+    """Scene s of a multi-scene engine: the per-scene getters of Engine with
+    the scene index bound."""
+
+    _PER_SCENE = ("stats", "subspheres", "clumps", "sub_forces", "force_parts", "pairs", "rows", "chain",
+                  "intruder", "intruder_diag", "intruder_history", "restart_scene")
+
+    def __init__(self, engine, s):
+        self.engine, self.s = engine, s
+
+    def sync(self):
+        self.engine.sync()
+
+    def __getattr__(self, name):
+        if name in SceneView._PER_SCENE:
+            f = getattr(self.engine, name)
+            return lambda *a, **k: f(*a, s=self.s, **k)
+        raise AttributeError(name)
+
+
 class Batch:
-    """Independent scenes advanced together (nbc_batch_*): one engine, stream
-    and step graph per scene, their launches interleaved; each scene's
-    results equal those of the scene run alone."""
+    """Independent scenes advanced together (nbc_batch_*): one engine over
+    all of them, one launch per kernel and step; each scene's results equal
+    those of the scene run alone.  engines[i] is scene i's view."""
 
     def __init__(self, scenes, **opts):
         self._descs = [scene_desc(s) for s in scenes]
@@ -412,19 +432,20 @@ class Batch:
         h = C.c_void_p()
         _check(lib().nbc_batch_create(arr, len(scenes), C.byref(o), C.byref(h)))
         self.h = h
-        self.engines = []
-        for i, sc in enumerate(scenes):
-            e = C.c_void_p()
-            _check(lib().nbc_batch_engine(self.h, i, C.byref(e)))
-            self.engines.append(Engine.borrowed(e, sc))
+        e = C.c_void_p()
+        _check(lib().nbc_batch_engine(self.h, C.byref(e)))
+        self.engine = Engine.borrowed(e, scenes)
+        self.engines = [SceneView(self.engine, i) for i in range(len(scenes))]
 
     def step(self, n=1):
         _check(lib().nbc_batch_step(self.h, int(n)))
 
+    def sync(self):
+        self.engine.sync()
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
-            for e in self.engines:
-                e.h = None
+            self.engine.h = None
             lib().nbc_batch_destroy(self.h)
             self.h = None
 

@@ -1,8 +1,9 @@
 """Batches of independent scenes and the request server (continuous
 batching): every scene's result in a batch or in the server's mix equals the
-same scene run alone, bitwise (each scene keeps its own engine, stream, graph
-and rebuild schedule), and admission respects the slot limit and the
-device-memory budget."""
+same scene run alone, bitwise (a batch is one engine over its scenes, each
+with its own rebuild schedule and pair region; a request has its own
+engine), and admission respects the slot limit and the device-memory
+budget."""
 import os
 
 import numpy as np
