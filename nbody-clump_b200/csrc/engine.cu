@@ -239,15 +239,19 @@ class EngineT final : public EngineBase {
     // those of them that touched at the last contact pass, over all scenes
     void contact_counts(long long* nnear, long long* ntouch) override {
         refresh_dev();
-        const int nn = read_int(h_.nrow + N_);
         const int hg = read_int(h_.hgen);
-        std::vector<int> idx(nn);
+        std::vector<SceneDyn> y = read_dyn_all();
         std::vector<uint8_t> t(h_.cap);
-        if (nn) copy_(idx.data(), h_.nfp, (size_t)nn * sizeof(int), cudaMemcpyDeviceToHost);
         copy_(t.data(), h_.touch[(hg + 1) & 1], (size_t)h_.cap, cudaMemcpyDeviceToHost);
-        long long c = 0;
-        for (int p : idx) c += t[p] != 0;
-        if (nnear) *nnear = nn;
+        long long n = 0, c = 0;
+        for (int s = 0; s < S_; s++) {
+            std::vector<int> idx(y[s].nnear);
+            if (y[s].nnear)
+                copy_(idx.data(), h_.nfp + y[s].pair_off, (size_t)y[s].nnear * sizeof(int), cudaMemcpyDeviceToHost);
+            for (int p : idx) c += t[p] != 0;
+            n += y[s].nnear;
+        }
+        if (nnear) *nnear = n;
         if (ntouch) *ntouch = c;
     }
     void get_subspheres(int s, int* fix, int* cid, double* pos, double* rad) override {
@@ -741,8 +745,9 @@ class EngineT final : public EngineBase {
             h_.cstart = m.take<int>(cells + 1);
             h_.scr = m.take<int>((size_t)N * 2 * SCR_CAP);
             h_.cnt_f = m.take<int>(N + 1);
-            h_.nrow = m.take<int>(N + 1);
-            h_.nbrow = m.take<int>(N + 1);
+            h_.nrow = m.take<int>(N + S_);
+            h_.nbrow = m.take<int>(N + S_);
+            h_.nprefix = m.take<int>(S_ + 1);
             h_.cnt_b = m.take<int>(N + 1);
             h_.sfc = m.take<int>(N);
             h_.xcnt = m.take<int>(N);
@@ -903,7 +908,7 @@ class EngineT final : public EngineBase {
         const int B = 256;
         if (moved > 0)
             k_relayout<R><<<std::min(148 * 8, cdiv(moved, B)), B, 0, stream_>>>(
-                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.cap, relmap_, moved);
+                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.nfp, old.nbq, old.cap, relmap_, moved);
         k_shift_rows<<<std::min(148 * 8, cdiv((long long)N_ + S_, B)), B, 0, stream_>>>(d_, relmap_);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
@@ -1093,12 +1098,14 @@ class EngineT final : public EngineBase {
         k_writeback<R><<<gN, B, 0, stream_>>>(d_);
         k_writeback_pairs<R><<<gP, 256, 0, stream_>>>(d_);
         k_swap<<<1, 1, 0, stream_>>>(d_);
-        // near rows of every scene (offsets over the whole batch)
-        k_near<false, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.nrow, N_ + 1);
-        scan(h_.nbrow, N_ + 1);
-        k_near<true, 4><<<cdiv(N_, SEARCH_THREADS / 4), SEARCH_THREADS, 0, stream_>>>(d_);
+        // near rows of the rebuilt scenes (counts, scans, rows)
+        const int gNr = std::min(cdiv(N_, SEARCH_THREADS / 4), 148 * 16);
+        k_near<false, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
+        scan(h_.cnt_f, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
+        k_near<true, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
         k_commit<<<std::min(cdiv((long long)K_ + S_ + 1, B), 148 * 8), B, 0, stream_>>>(d_);
+        k_nprefix<<<1, SC_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
 

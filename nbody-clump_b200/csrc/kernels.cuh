@@ -1199,52 +1199,87 @@ static __global__ void k_swap(Dev* __restrict__ dp) {
 // next one), so a pair whose distance at a rebuild is at least ri + rj +
 // 2 Thresh cannot touch before the next one.  k_carry flags the near pairs
 // of a rebuilt scene and clears the touch flag of the others (in both
-// generations, after the write-back); the near rows list the near entries of
-// every scene (front: pair slot in row order, back: the pair slot of each
-// near back entry) and the contact pass visits only them, with the same
-// results as visiting the whole list.
+// generations, after the write-back); the near rows list a rebuilt scene's
+// near entries in its pair region (front: pair slot in row order, back: the
+// pair slot of each near back entry) and the contact pass visits only them,
+// with the same results as visiting the whole list.  FILL = false counts
+// them into cnt_f / cnt_b of the rebuilt concatenation; FILL = true writes
+// the rows at the scanned offsets.
 template <bool FILL, int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const int lane = threadIdx.x % SL;
-    if (i >= d.N) return;
     const unsigned gm = SL == 32 ? 0xffffffffu : (((1u << SL) - 1u) << ((threadIdx.x & 31) & ~(SL - 1)));
     const int gshift = (threadIdx.x & 31) & ~(SL - 1);
     const unsigned lt = (1u << lane) - 1u;
     const PairList& Lc = d.L[0];
     const uint8_t* __restrict__ nearf = d.nearf;
     const int* __restrict__ bpair = Lc.bpair;
-    const int s = d.sid[i];
     // after k_swap: the other touch generation still holds the old list's flags
-    uint8_t* __restrict__ tother = !FILL && d.plan[PL_NS] == d.S ? d.touch[(*d.hgen + 1) & 1] : nullptr;
-    int nf = 0, nb = 0;
-    const int rf = FILL ? d.nrow[i] : 0, rb = FILL ? d.nbrow[i] : 0;
-    const int rs = Lc.row[i + s], re = Lc.row[i + s + 1];
-    for (int k0 = rs; k0 < re; k0 += SL) {
-        const int k = k0 + lane;
-        const bool nr = k < re && nearf[k];
-        if (tother && k < re && !nr) tother[k] = 0;
-        const unsigned m = __ballot_sync(gm, nr) >> gshift;
-        if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
-        nf += __popc(m);
+    uint8_t* __restrict__ tother = !FILL && ns == d.S ? d.touch[(*d.hgen + 1) & 1] : nullptr;
+    if (!FILL && blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
+    for (int t = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL; t < T;
+         t += gridDim.x * (SEARCH_THREADS / SL)) {
+        const PlanItem it = plan_item(d, ns, t);
+        const int i = it.i, s = it.s;
+        int nf = 0, nb = 0, rf = 0, rb = 0;
+        if (FILL) {
+            const int t0 = d.psub[it.k], base = d.dyn[s].pair_off;
+            rf = base + d.cnt_f[t] - d.cnt_f[t0];
+            rb = base + d.cnt_b[t] - d.cnt_b[t0];
+            if (lane == 0) {
+                d.nrow[i + s] = rf;
+                d.nbrow[i + s] = rb;
+                if (i == d.par[s].sub_off + d.par[s].nsub - 1) {
+                    d.nrow[i + s + 1] = base + d.cnt_f[t + 1] - d.cnt_f[t0];
+                    d.nbrow[i + s + 1] = base + d.cnt_b[t + 1] - d.cnt_b[t0];
+                }
+            }
+        }
+        const int rs = Lc.row[i + s], re = Lc.row[i + s + 1];
+        for (int k0 = rs; k0 < re; k0 += SL) {
+            const int k = k0 + lane;
+            const bool nr = k < re && nearf[k];
+            if (tother && k < re && !nr) tother[k] = 0;
+            const unsigned m = __ballot_sync(gm, nr) >> gshift;
+            if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
+            nf += __popc(m);
+        }
+        const int bs = Lc.brow[i + s], be = Lc.brow[i + s + 1];
+        for (int k0 = bs; k0 < be; k0 += SL) {
+            const int k = k0 + lane;
+            int q = -1;
+            if (k < be) q = bpair[k];
+            const bool nr = q >= 0 && nearf[q];
+            const unsigned m = __ballot_sync(gm, nr) >> gshift;
+            if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = q;
+            nb += __popc(m);
+        }
+        if (!FILL && lane == 0) {
+            d.cnt_f[t] = nf;
+            d.cnt_b[t] = nb;
+        }
     }
-    const int bs = Lc.brow[i + s], be = Lc.brow[i + s + 1];
-    for (int k0 = bs; k0 < be; k0 += SL) {
-        const int k = k0 + lane;
-        int q = -1;
-        if (k < be) q = bpair[k];
-        const bool nr = q >= 0 && nearf[q];
-        const unsigned m = __ballot_sync(gm, nr) >> gshift;
-        if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = q;
-        nb += __popc(m);
+}
+
+// the contact pass's work items: near pairs of every scene, scene by scene
+// (one block)
+static __global__ void __launch_bounds__(SC_THREADS) k_nprefix(const Dev* __restrict__ dp) {
+    __shared__ int sh[SC_THREADS / 32];
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    int run = 0;
+    for (int b = 0; b < d.S; b += SC_THREADS) {
+        const int s = b + threadIdx.x;
+        const int v = s < d.S ? d.dyn[s].nnear : 0;
+        int tot;
+        const int ex = block_excl_scan(v, sh, tot);
+        if (s < d.S) d.nprefix[s] = run + ex;
+        run += tot;
     }
-    if (!FILL && lane == 0) {
-        d.nrow[i] = nf;
-        d.nbrow[i] = nb;
-        if (i == d.N - 1) { d.nrow[d.N] = 0; d.nbrow[d.N] = 0; }
-    }
+    if (threadIdx.x == 0) d.nprefix[d.S] = run;
 }
 
 // Finishes a rebuild: per-clump member lists of the rebuilt scenes in
@@ -1269,6 +1304,7 @@ static __global__ void k_commit(const Dev* __restrict__ dp) {
             const int k = u - TK;
             SceneDyn& y = d.dyn[d.pscene[k]];
             y.npairs = d.ppair[k + 1] - d.ppair[k];
+            y.nnear = d.cnt_f[d.psub[k + 1]] - d.cnt_f[d.psub[k]];
             y.nrebuild++;
             y.rebuild = 0;
         } else {
@@ -1284,7 +1320,8 @@ static __global__ void k_commit(const Dev* __restrict__ dp) {
 // buffers.
 template <typename R>
 __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* __restrict__ oh,
-                           const uint8_t* __restrict__ ot, const uint8_t* __restrict__ onear, int ocap,
+                           const uint8_t* __restrict__ ot, const uint8_t* __restrict__ onear,
+                           const int* __restrict__ onfp, const int* __restrict__ onbq, int ocap,
                            const int4* __restrict__ map, int total) {
     const Dev& d = *dp;
     const int hg = *d.hgen;
@@ -1309,6 +1346,8 @@ __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* 
         const uint8_t f = ot[po];
         d.touch[hg & 1][pn] = f;
         d.nearf[pn] = onear[po];
+        d.nfp[pn] = onfp[po] + (m.y - m.x);   // slots past the near count carry nothing
+        d.nbq[pn] = onbq[po] + (m.y - m.x);
         if (f) {
             Hn[pn] = Ho[po];
             Hn[cap + pn] = Ho[oc + po];
@@ -1317,7 +1356,7 @@ __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* 
     }
 }
 
-// the current rows follow their scene's region: every row offset of scene s
+// the current rows and near rows follow their scene's region: every offset of scene s
 // moves by its region's move (the subsphere threads take the row starts,
 // one thread per scene the end entry)
 static __global__ void k_shift_rows(const Dev* __restrict__ dp, const int4* __restrict__ map) {
@@ -1335,6 +1374,8 @@ static __global__ void k_shift_rows(const Dev* __restrict__ dp, const int4* __re
         const int delta = map[s].y - map[s].x;
         Lc.row[r] += delta;
         Lc.brow[r] += delta;
+        d.nrow[r] += delta;
+        d.nbrow[r] += delta;
     }
 }
 
@@ -1822,13 +1863,14 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     if (*d.halt) return;
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& Lst = d.L[lc & 1];
-    const int np = d.nrow[d.N];
+    const int S = d.S;
+    const int* __restrict__ npre = d.nprefix;
+    const int np = npre[S];
     const int* __restrict__ nfp = d.nfp;
     const int* __restrict__ nbr = Lst.nbr;
     const int* __restrict__ own = Lst.own;
     const double4* __restrict__ posr = d.posr;
     const R4<R>* __restrict__ kin = (const R4<R>*)d.kin;
-    const int* __restrict__ sid = d.sid;
     const size_t N = (size_t)d.N;
     const size_t cap = (size_t)d.cap;
     const R4<R>* __restrict__ Hi = (const R4<R>*)d.H[hg & 1];
@@ -1836,9 +1878,10 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     const uint8_t* __restrict__ ti = d.touch[hg & 1];
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
     R4<R>* __restrict__ ct = (R4<R>*)d.ctb;
-    const bool one_scene = d.S == 1;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
-        const int p = nfp[w];
+        // work item w: near pair w - nprefix[s] of scene s
+        const int s = S == 1 ? 0 : plan_find(npre, S, w);
+        const int p = nfp[d.dyn[s].pair_off + (w - npre[s])];
         const int jr = nbr[p];
         if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
         const int i = own[p];
@@ -1850,7 +1893,7 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         load_kin<R>(kin, N, jr, b);
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         if (ti[p]) hist_read<R>(Hi, cap, p, hs, ht, hr);
-        const ScenePar& P = d.par[one_scene ? 0 : sid[i]];
+        const ScenePar& P = d.par[s];
         Law<R> L;
         L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
         L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
@@ -1895,14 +1938,15 @@ __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) 
     const int* __restrict__ nfp = d.nfp;
     const int* __restrict__ nbq = d.nbq;
     V3<R> F = v3<R>(0, 0, 0), T = F;
-    const int rs = d.nrow[i], re = d.nrow[i + 1];
+    const int s = d.S == 1 ? 0 : d.sid[i];
+    const int rs = d.nrow[i + s], re = d.nrow[i + s + 1];
     for (int e = rs + lane; e < re; e += LANES) {
         const int k = nfp[e];
         if (!to[k]) continue;
         F = F + xyz<R>(ct[k]);
         T = T + xyz<R>(ct[cap + k]);
     }
-    const int bs = d.nbrow[i], be = d.nbrow[i + 1];
+    const int bs = d.nbrow[i + s], be = d.nbrow[i + s + 1];
     for (int e = bs + lane; e < be; e += LANES) {
         const int q = nbq[e];
         if (!to[q]) continue;
@@ -1927,7 +1971,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) 
         fs[N + i] = pack<R>(T, R(0));
         if (!(isfinite((double)F.x) && isfinite((double)F.y) && isfinite((double)F.z) &&
               isfinite((double)T.x) && isfinite((double)T.y) && isfinite((double)T.z)))
-            atomicOr(&d.dyn[d.sid[i]].err, ERR_NONFINITE);
+            atomicOr(&d.dyn[s].err, ERR_NONFINITE);
     }
 }
 

@@ -70,6 +70,7 @@ struct SceneDyn {
     int npairs;                    // pairs in the current list
     int pair_off;                  // first pair slot of this scene's region of the pair buffers
     int pcap;                      // pair slots of that region (set by the host, grown on overflow)
+    int nnear;                     // near pairs of the current list (see k_near)
     long long ifix[6];             // fixed-point sums of intruder force (2^-40 N) and torque (2^-44 N m)
 };
 
@@ -166,10 +167,13 @@ struct Dev {
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
     void* ctb;        // Real4 [4][cap]: per pair force and torque on the owner, then on the partner
     // near rows (the entries that can touch before the next rebuild)
-    int* nrow;        // [N+1] near front offsets
-    int* nbrow;       // [N+1] near back offsets
-    int* nfp;         // [cap] near front entries: pair index
-    int* nbq;         // [cap] near back entries: pair index
+    // (kept in each scene's pair region like the list: rows [N+S] with
+    // absolute slots, one row array per scene with its end entry)
+    int* nrow;        // [N+S] near front offsets
+    int* nbrow;       // [N+S] near back offsets
+    int* nfp;         // [cap] near front entries: pair slot
+    int* nbq;         // [cap] near back entries: pair slot
+    int* nprefix;     // [S+1] prefix over the scenes of their near pairs (the contact pass's work items)
     uint8_t* nearf;   // [cap] pair can touch before the next rebuild
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
     int* gstep;       // steps started by k_clump (counts steps across graph launches)
