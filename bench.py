@@ -324,6 +324,25 @@ def run_batch(args):
     scenes = [nbc.with_levels(s) for s in sg.make_cfg3(args.scenes, steps=args.steps)]
     n_sub = sum(int(s["params"]["NumberBody"]) for s in scenes)
     opts = dict(precision=args.precision, pair_slack=1.6)
+    if args.profile_window is not None:
+        # for a launch list: eager launches (kernel nodes of a graph with a
+        # conditional node are not profiled), the profiler range around
+        # --steps steps after --profile-window steps
+        import torch
+        b = nbc.Batch(scenes, use_graph=False, **opts)
+        b.step(args.profile_window)
+        b.sync()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        b.step(args.steps)
+        b.sync()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_run": True, "scenes": len(scenes), "subspheres": n_sub,
+                          "window": [args.profile_window, args.profile_window + args.steps],
+                          "rebuilds": sum(v.stats()["rebuilds"] for v in b.engines)}), flush=True)
+        b.close()
+        return
     # process start-up (CUDA context, lazy kernel loading) stays out of both arms
     w = nbc.Engine([scenes[0]], **opts)
     w.step(3)
@@ -455,7 +474,8 @@ def run_serve(args):
     sizes, reqs = serve_requests(args)
     work = sum(int(sc["params"]["NumberBody"]) * n for _, sc, n in reqs)
     # served: arrivals replayed in real time
-    srv = nbc.Server(budget_bytes=args.budget_gb * 1e9, max_active=args.slots, precision=args.precision)
+    srv = nbc.Server(budget_bytes=args.budget_gb * 1e9, max_active=args.slots, cohort=args.cohort,
+                     precision=args.precision)
     t0 = time.perf_counter()
     nxt, ids, done_at, failed = 0, {}, {}, []
     while len(done_at) < len(reqs):
@@ -510,7 +530,7 @@ def run_serve(args):
                       "requests_per_s": len(reqs) / sum(svc), "subsphere_steps_per_s": work / sum(svc)},
             "throughput_ratio": (work / makespan) / (work / sum(svc)),
             "failed": failed, "failed_plain": failed_plain,
-            "slots": args.slots, "budget_gb": args.budget_gb,
+            "slots": args.slots, "cohort": args.cohort, "budget_gb": args.budget_gb,
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy beds settled by the engine)"}
     print(json.dumps(line), flush=True)
@@ -574,6 +594,8 @@ def main():
     ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--settle2", type=int, default=150_000, help="cfg2: settling steps of the bed")
     ap.add_argument("--scenes", type=int, default=256, help="cfg3: number of scenes")
+    ap.add_argument("--profile-window", type=int, default=None,
+                    help="cfg3: eager batch only, profiler range around --steps steps after this many")
     ap.add_argument("--requests", type=int, default=200, help="cfg4: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="cfg4: mean arrivals per second")
     ap.add_argument("--bank", type=int, default=8, help="cfg4: pre-settled beds in the bank")
@@ -582,6 +604,7 @@ def main():
     ap.add_argument("--slots", type=int, default=64, help="cfg4: requests running at once at most")
     ap.add_argument("--budget-gb", type=float, default=120.0, help="cfg4: device memory for requests")
     ap.add_argument("--chunk", type=int, default=256, help="cfg4: steps per server round")
+    ap.add_argument("--cohort", type=int, default=1, help="cfg4: requests per server cohort (shared engine) at most")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)

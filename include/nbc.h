@@ -180,6 +180,14 @@ nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launc
 nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
+/* No reference counterpart (the reference runs one scene until EndStep).
+ * Scene `scene` takes `nsteps` steps counted from the engine's creation and
+ * then stands still while the engine's other scenes go on: its state, forces
+ * and intruder record are exactly those of the scene run alone for nsteps
+ * steps, and it costs no contact or boundary work afterwards.  0 removes the
+ * limit.  Call between steps; nsteps below the steps already started is an
+ * NBC_ERR_ARG. */
+nbc_status nbc_set_scene_steps(nbc_engine* e, int scene, int nsteps);
 
 /* --- batches of independent scenes ---------------------------------------
  * No reference counterpart (the reference runs one scene per process).  A
@@ -202,11 +210,14 @@ nbc_status nbc_batch_destroy(nbc_batch* b);
 
 /* --- request server (continuous batching) ---------------------------------
  * No reference counterpart.  A request is a scene (copied at submission) and
- * a step count.  nbc_server_advance admits queued requests in arrival order
+ * a step count.  nbc_server_advance advances every running request by up to
+ * `chunk` steps (at most 1024) and admits queued requests in arrival order
  * while the head fits the device-memory budget (estimated before creation,
- * actual after) and fewer than max_active run, advances every running request
- * by up to `chunk` steps (at most 1024) with their kernels overlapping, and
- * retires the finished ones, freeing their memory.  A request's result is
+ * actual after) and fewer than max_active run.  The requests admitted in one
+ * call share one engine (a cohort: one launch per kernel and step for all of
+ * them, each standing still at its own step count, nbc_set_scene_steps);
+ * cohorts run concurrently on their own streams, and a cohort's memory is
+ * returned when its last request finishes.  A request's result is
  * the intruder reaction force and torque every sample_every steps and at its
  * last step ([n_samples][6], the reference's fc record,
  * src/dem_integrate_penetrator.cu:108-109) and the intruder's final position;
@@ -222,6 +233,9 @@ nbc_status nbc_server_result(nbc_server* s, int id, int* state, int* steps_done,
 nbc_status nbc_server_release(nbc_server* s, int id);
 nbc_status nbc_server_memory(nbc_server* s, double* used_bytes, double* budget_bytes);
 nbc_status nbc_server_destroy(nbc_server* s);
+/* requests per cohort at most (default 1: an engine per request); the
+ * requests admitted in one call are grouped by step count, within 2x */
+nbc_status nbc_server_set_cohort(nbc_server* s, int max_requests);
 
 /* Hierarchical-grid levels for a radius distribution (replaces the grid.bt
  * level table the reference's sphere path reads, src/dem_io.cu:204-248):

@@ -166,6 +166,11 @@ nbc_status nbc_engine_info(nbc_engine* e, double* bytes, double* ms) {
     return guard([&] { e->eng->info(bytes, ms); });
 }
 
+nbc_status nbc_set_scene_steps(nbc_engine* e, int scene, int nsteps) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "null engine");
+    return guard([&] { e->eng->set_stop(scene, nsteps); });
+}
+
 // --- drop-in entry point ----------------------------------------------------
 
 nbc_status nbc_open(const char* workdir, const nbc_options* opt, nbc_engine** out) {

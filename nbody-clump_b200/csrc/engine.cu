@@ -445,6 +445,17 @@ class EngineT final : public EngineBase {
         harvest_events();
         for (int k = 0; k < NPH; k++) ms[k] = t_contact_n_ ? t_phase_ms_[k] / t_contact_n_ : 0.0;
     }
+    // scene s stands still after nsteps steps counted from the engine's creation
+    void set_stop(int s, int nsteps) override {
+        if (s < 0 || s >= S_) throw ArgError("scene index out of range");
+        if (nsteps < 0) throw ArgError("scene step count is negative");
+        const int started = read_int(h_.lstep);
+        if (nsteps != 0 && nsteps < started)
+            throw ArgError("scene " + std::to_string(s) + " has started " + std::to_string(started) + " steps already");
+        SceneDyn y = read_dyn(s);
+        y.stop = nsteps;
+        copy_(h_.dyn + s, &y, sizeof(SceneDyn), cudaMemcpyHostToDevice);
+    }
     void info(double* bytes, double* ms) override {
         if (bytes) *bytes = mem_.bytes;
         if (ms) *ms = last_ms_;
@@ -738,6 +749,7 @@ class EngineT final : public EngineBase {
             h_.hgen = flags + 4;
             h_.gstep = flags + 5;
             h_.kc_done = flags + 6;
+            h_.lstep = flags + 7;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
             h_.hist = m.take<int>((size_t)256 * rs_blocks_);
             h_.perm = m.take<int>(N);

@@ -37,6 +37,7 @@ class EngineBase {
     virtual void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) = 0;
     virtual void get_intruder_history(int s, int count, double* out) = 0;
     virtual void info(double* bytes, double* ms) = 0;
+    virtual void set_stop(int s, int nsteps) = 0;
     virtual void timing_enable(int level) = 0;
     virtual void timing_read(double* contact_ms, int* contact_launches, long long* kernel_launches, int* rebuilds) = 0;
     virtual void timing_phases(double* phase_ms) = 0;

@@ -47,7 +47,17 @@ constexpr int INTRA = (int)0x80000000u;
 //
 // A step (do_pre) also advances the spring-history generation so the next
 // contact pass reads what the previous one wrote, and counts itself; the last
-// block to finish sets the graph's rebuild condition (when given a handle).
+// block to finish sets the graph's rebuild condition (when given a handle)
+// and counts the step in lstep.  A scene with a stop s takes the steps started
+// at lstep = 0 .. s-1 and closes the last one at lstep = s; afterwards it
+// stands still (frozen) while the other scenes go on, so its state is
+// exactly that of the scene run alone for s steps.
+__device__ __forceinline__ bool scene_pre(const SceneDyn& y, int do_pre, int L) {
+    return do_pre && (y.stop == 0 || L < y.stop);
+}
+__device__ __forceinline__ bool scene_post(const SceneDyn& y, int post, int L) {
+    return post && (y.stop == 0 || L <= y.stop);
+}
 constexpr int CL_THREADS = 128;
 constexpr int CL_WARPS = CL_THREADS / 32;
 constexpr int CL_CHUNK = 128;   // members staged in shared memory per warp at a time
@@ -59,17 +69,27 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
     __shared__ double s_cl[CL_WARPS][13][32];        // clump position, velocity, angular velocity, quaternion
     __shared__ int s_ms[CL_WARPS][33];               // member-list offsets of the warp's clumps
     __shared__ int s_sc[CL_WARPS][32];               // scene of each of the warp's clumps
+    __shared__ int s_pre[CL_WARPS][32];              // the clump's scene takes this step
     const Dev& d = *dp;
     if (*d.halt) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k0 = (blockIdx.x * CL_WARPS + warp) * 32;
     const int t = k0 + lane;
     const int post = *d.post_pending;
+    const int L = *d.lstep;   // written only by the last block, after every block has read it
     if (do_pre && blockIdx.x == 0 && threadIdx.x == 0) {
         *d.hgen += 1;
         *d.gstep += 1;
     }
-    if (k0 < d.K) {   // warp-uniform: this warp holds clumps
+    // warp-uniform: this warp holds clumps of a scene that moves (a warp whose
+    // clumps all belong to scenes standing still skips its work)
+    bool warp_live = false;
+    if (k0 < d.K) {
+        const int nq = min(32, d.K - k0);
+        const SceneDyn& yq = d.dyn[d.csid[lane < nq ? t : k0 + nq - 1]];
+        warp_live = __any_sync(0xffffffffu, lane < nq && (scene_pre(yq, do_pre, L) || scene_post(yq, post, L)));
+    }
+    if (warp_live) {
         const int* __restrict__ mem_start = d.mem_start;
         const int* __restrict__ mem_idx = d.mem_idx;
         const double4* __restrict__ posr = d.posr;
@@ -80,7 +100,9 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
         if (lane == 0) s_ms[warp][32] = mem_start[k0 + nk];
         const int sc = d.csid[k];
         double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cprop[k];
+        const bool pre_k = scene_pre(d.dyn[sc], do_pre, L), post_k = scene_post(d.dyn[sc], post, L);
         s_sc[warp][lane] = sc;
+        s_pre[warp][lane] = isc && pre_k;
         s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
         __syncwarp();
         const int M0 = s_ms[warp][0], M1 = s_ms[warp][nk];
@@ -149,7 +171,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
                 }
                 __syncwarp();
             }
-            if (isc) {
+            if (isc && post_k) {
                 if (mb < me) {
                     if (!(isfinite(F.x) && isfinite(F.y) && isfinite(F.z) && isfinite(T.x) && isfinite(T.y) &&
                           isfinite(T.z)))
@@ -161,16 +183,19 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
                     T = xyzd(d.cT[k]);
                 }
             }
-            V3<double> ac = (1.0 / pr.w) * F;
-            ac.z = ac.z + P.gravity;
-            V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
-            cv.x += (0.5 * Dt) * ac.x; cv.y += (0.5 * Dt) * ac.y; cv.z += (0.5 * Dt) * ac.z;
-            cw.x += (0.5 * Dt) * al.x; cw.y += (0.5 * Dt) * al.y; cw.z += (0.5 * Dt) * al.z;
+            if (post_k) {
+                V3<double> ac = (1.0 / pr.w) * F;
+                ac.z = ac.z + P.gravity;
+                V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
+                cv.x += (0.5 * Dt) * ac.x; cv.y += (0.5 * Dt) * ac.y; cv.z += (0.5 * Dt) * ac.z;
+                cw.x += (0.5 * Dt) * al.x; cw.y += (0.5 * Dt) * al.y; cw.z += (0.5 * Dt) * al.z;
+            }
         } else {
             F = xyzd(d.cF[k]);
             T = xyzd(d.cT[k]);
         }
         if (do_pre) {
+            const double4 cp_old = cp;
             V3<double> ac = (1.0 / pr.w) * F;
             ac.z = ac.z + P.gravity;
             V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
@@ -197,7 +222,13 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             q.w = (q.w + Dt * qd.w) + h2 * qdd.w;
             const double inv = 1.0 / sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
             q.x *= inv; q.y *= inv; q.z *= inv; q.w *= inv;
-            if (isc) {
+            if (!pre_k) {   // the scene stands still: keep the clump as it is
+                cp = cp_old;
+                v = xyzd(cv);
+                w = xyzd(cw);
+                q = cq;
+            }
+            if (isc && pre_k) {
                 d.cpos[k] = cp;
                 d.cvel[k] = make_double4(v.x, v.y, v.z, 0.0);
                 d.cw[k] = make_double4(w.x, w.y, w.z, 0.0);
@@ -240,6 +271,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
                     if (idx[j] < 0) continue;
                     const int i = idx[j];
                     const int kk = owner(c0 + 32 * j + lane);
+                    if (!s_pre[warp][kk]) continue;
                     const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
                                                     s_cl[warp][12][kk]);
                     const V3<double> arm = rot_b2w(qk, v3(lo[j].x, lo[j].y, lo[j].z));
@@ -262,7 +294,8 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
                     }
                 }
             }
-        } else if (post && isc) {
+        }
+        if (isc && post_k && !pre_k) {   // closing half-kick only (sync, or the scene's last step)
             d.cvel[k] = cv;
             d.cw[k] = cw;
         }
@@ -272,7 +305,8 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
         const ScenePar& P = d.par[s];
         SceneDyn& y = d.dyn[s];
         const double Dt = P.dt;
-        if (post) {
+        const bool pre_s = scene_pre(y, do_pre, L), post_s = scene_post(y, post, L);
+        if (post_s) {
             long long* fx = (long long*)&y.ifix[0];
             V3<double> tf = v3(fx[0] / FIX_F, fx[1] / FIX_F, fx[2] / FIX_F);
             V3<double> tt = v3(fx[3] / FIX_T, fx[4] / FIX_T, fx[5] / FIX_T);
@@ -295,7 +329,8 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             }
             y.step += 1;
         }
-        if (do_pre && P.has_intr) {
+        if (do_pre) y.frozen = !pre_s;
+        if (pre_s && P.has_intr) {
             if (P.intr_motion == 1 && (!P.intr_wait || y.intr_state != 0)) {
                 V3<double> a = (-1.0 / P.intr_mass) * v3(y.totF[0], y.totF[1], y.totF[2]);
                 a.z = a.z + P.gravity;
@@ -308,14 +343,13 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             }
         }
     }
-    if (use_cond) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            if (atomicAdd(d.kc_done, 1) == (int)gridDim.x - 1) {
-                *d.kc_done = 0;
-                cudaGraphSetConditional(cond, atomicAdd(d.any_rebuild, 0) ? 1u : 0u);
-            }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(d.kc_done, 1) == (int)gridDim.x - 1) {
+            *d.kc_done = 0;
+            if (do_pre) *d.lstep = L + 1;
+            if (use_cond) cudaGraphSetConditional(cond, atomicAdd(d.any_rebuild, 0) ? 1u : 0u);
         }
     }
 }
@@ -1628,6 +1662,7 @@ __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__
     const int i = blockIdx.x * BD_THREADS + threadIdx.x;
     if (i >= d.N) return;
     const int s = d.sid[i];
+    if (d.dyn[s].frozen) return;   // a scene past its stop stands still
     const ScenePar& P = d.par[s];
     const size_t N = (size_t)d.N;
     const double4 pp = d.posr[i];
@@ -1881,7 +1916,9 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
         // work item w: near pair w - nprefix[s] of scene s
         const int s = S == 1 ? 0 : plan_find(npre, S, w);
-        const int p = nfp[d.dyn[s].pair_off + (w - npre[s])];
+        const SceneDyn& ys = d.dyn[s];
+        if (ys.frozen) continue;
+        const int p = nfp[ys.pair_off + (w - npre[s])];
         const int jr = nbr[p];
         if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
         const int i = own[p];
@@ -1939,6 +1976,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) 
     const int* __restrict__ nbq = d.nbq;
     V3<R> F = v3<R>(0, 0, 0), T = F;
     const int s = d.S == 1 ? 0 : d.sid[i];
+    if (d.dyn[s].frozen) return;
     const int rs = d.nrow[i + s], re = d.nrow[i + s + 1];
     for (int e = rs + lane; e < re; e += LANES) {
         const int k = nfp[e];

@@ -71,6 +71,8 @@ struct SceneDyn {
     int pair_off;                  // first pair slot of this scene's region of the pair buffers
     int pcap;                      // pair slots of that region (set by the host, grown on overflow)
     int nnear;                     // near pairs of the current list (see k_near)
+    int stop;                      // steps the scene takes before it stands still (0: no limit)
+    int frozen;                    // the scene took no step at the last k_clump (its stop was reached)
     long long ifix[6];             // fixed-point sums of intruder force (2^-40 N) and torque (2^-44 N m)
 };
 
@@ -178,6 +180,7 @@ struct Dev {
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
     int* gstep;       // steps started by k_clump (counts steps across graph launches)
     int* kc_done;     // blocks of k_clump finished (last-block detection)
+    int* lstep;       // steps started by k_clump, counted by its last block (per-scene stops)
     // export (per pair), written by the export variant of the contact kernel
     void* xfcn;       // Real4 [cap] normal force on the owner (CacheFcn)
     void* xcpt;       // double4 [cap] contact point (CacheCpt)

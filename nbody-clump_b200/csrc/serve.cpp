@@ -114,14 +114,27 @@ struct SceneCopy {
 };
 
 struct Request {
-    int id = 0, state = 0;  // 0 queued, 1 active, 2 done, 3 failed
+    int id = 0, state = 0;  // 0 queued, 1 running, 2 done, 3 failed
     int nsteps = 0, sample_every = 1, done = 0;
-    double est_bytes = 0, bytes = 0;
-    std::unique_ptr<SceneCopy> scene;
-    std::unique_ptr<nbc_engine> eng;
+    double est_bytes = 0;
+    std::unique_ptr<SceneCopy> scene;   // until its cohort is created
+    int cohort = -1, slot = 0;          // its cohort and its scene there
     std::vector<double> curve;  // [samples][6]: reaction force, reaction torque
     double intr_pos[3] = {0, 0, 0};
     std::string error;
+};
+
+// The requests admitted in one round share one engine: one launch per kernel
+// and step covers all of them, and each request's scene stands still once its
+// own step count is reached (nbc_set_scene_steps) while the others go on.
+// The engine and its memory are released when its last request finishes.
+struct Cohort {
+    std::unique_ptr<nbc_engine> eng;
+    std::vector<int> ids;   // the request of each scene
+    int started = 0;        // steps the engine has taken
+    int longest = 0;        // the largest step count of its requests
+    int open = 0;           // requests still running
+    double bytes = 0;
 };
 
 // device bytes a scene is expected to take before it is created: per
@@ -139,10 +152,12 @@ double estimate_bytes(const nbc_scene_desc& s, const nbc_options& o) {
 struct nbc_server {
     nbc_options opt;
     double budget = 0, used = 0;
-    int max_active = 1, next_id = 1;
+    int max_active = 1, next_id = 1, next_cohort = 1;
+    int cohort_max = 1;              // requests per cohort at most
     std::map<int, std::unique_ptr<Request>> req;
-    std::deque<int> queue;     // ids waiting for admission, in arrival order
-    std::vector<int> active;   // ids being advanced
+    std::deque<int> queue;           // ids waiting for admission, in arrival order
+    std::map<int, Cohort> cohorts;   // running cohorts
+    int running = 0;                 // requests admitted and not finished
 };
 
 extern "C" {
@@ -173,108 +188,154 @@ nbc_status nbc_server_submit(nbc_server* s, const nbc_scene_desc* scene, int nst
     });
 }
 
-// Admit queued requests (in arrival order, while the head fits the budget
-// and a slot is free), advance every active request by up to chunk steps
-// (concurrently), record their samples and retire the finished ones.
+// Advance every running cohort by up to chunk steps (all cohorts' chunks
+// are enqueued before any is waited for), admit queued requests (arrival
+// order, while the head fits the budget and a slot is free) into one new
+// cohort created while the others run, record the new samples of every
+// running request and retire the finished ones.
 nbc_status nbc_server_advance(nbc_server* s, int chunk, int* n_active, int* n_queued, int* n_done) {
     if (!s || chunk < 1) return fail(NBC_ERR_ARG, "nbc_server_advance: bad arguments");
     chunk = std::min(chunk, 1024);  // the engine's intruder ring keeps the last 1024 steps at least
     nbc_status st = guard([&] {
-        // one chunk of every running request is put on its stream first, so
-        // the GPU works while new requests are admitted and created
-        const std::vector<int> running = s->active;
-        std::vector<int> launched(running.size(), 0), want(running.size(), 0), did(running.size(), 0);
-        // a request whose engine fails (non-finite force, device memory) is
-        // retired with its error; the others go on
-        auto retire_failed = [&](Request& r, const std::exception& e) {
-            r.state = 3;
-            r.error = e.what();
-            s->used -= r.bytes;
-            r.eng.reset();
-            r.scene.reset();
-        };
-        for (size_t k = 0; k < running.size(); k++) {
-            Request& r = *s->req[running[k]];
-            want[k] = std::min(chunk, r.nsteps - r.done);
-            try {
-                launched[k] = r.eng->eng->enqueue(want[k]);
-            } catch (const std::exception& e) {
-                retire_failed(r, e);
-            }
-        }
-        // admission: arrival order, while the head fits and a slot is free
-        while (!s->queue.empty() && (int)s->active.size() < s->max_active) {
-            Request& r = *s->req[s->queue.front()];
-            if (!s->active.empty() && s->used + r.est_bytes > s->budget) break;
-            s->queue.pop_front();
-            std::unique_ptr<nbc_engine> h(new nbc_engine());
-            h->opt = s->opt;
-            std::vector<const nbc_scene_desc*> v(1, &r.scene->d);
-            try {
-                h->eng.reset(nbc::make_engine(v, s->opt));
-            } catch (const std::exception& e) {
+        // a cohort whose engine fails (non-finite force, device memory) is
+        // retired with its error on every request still running in it; the
+        // other cohorts go on
+        auto fail_cohort = [&](Cohort& c, const std::exception& e) {
+            for (int id : c.ids) {
+                auto f = s->req.find(id);   // finished requests may have been released
+                if (f == s->req.end() || f->second->state != 1) continue;
+                Request& r = *f->second;
                 r.state = 3;
                 r.error = e.what();
-                r.scene.reset();
-                continue;
+                s->running--;
             }
-            double b = 0, ms = 0;
-            h->eng->info(&b, &ms);
-            // whole bytes, so that the sum over running requests stays exact
-            r.bytes = std::ceil(std::max(b, r.est_bytes));
-            s->used += r.bytes;
-            r.eng = std::move(h);
-            r.state = 1;
-            s->active.push_back(r.id);
-        }
-        // the rest of each running request's chunk (a capacity overflow can
-        // stop a chunk early), waited for in turn
-        for (size_t k = 0; k < running.size(); k++) {
-            Request& r = *s->req[running[k]];
-            if (r.state != 1) continue;
+            c.open = 0;
+        };
+        std::vector<int> old;
+        std::map<int, int> want, launched;
+        for (auto& kv : s->cohorts) {
+            Cohort& c = kv.second;
+            old.push_back(kv.first);
+            want[kv.first] = std::min(chunk, c.longest - c.started);
             try {
-                if (launched[k] > 0) did[k] = r.eng->eng->wait_steps();
-                while (did[k] < want[k]) {
-                    r.eng->eng->enqueue(want[k] - did[k]);
-                    did[k] += r.eng->eng->wait_steps();
+                launched[kv.first] = c.eng->eng->enqueue(want[kv.first]);
+            } catch (const std::exception& e) {
+                fail_cohort(c, e);
+            }
+        }
+        // admission into one new cohort, created while the others run
+        std::vector<int> adm;
+        double add = 0;
+        while (!s->queue.empty() && s->running + (int)adm.size() < s->max_active) {
+            Request& r = *s->req[s->queue.front()];
+            if ((s->running > 0 || !adm.empty()) && s->used + add + r.est_bytes > s->budget) break;
+            s->queue.pop_front();
+            adm.push_back(r.id);
+            add += r.est_bytes;
+        }
+        // the admitted requests, in order of their step counts, form cohorts
+        // of at most cohort_max requests whose step counts are within 2x
+        std::stable_sort(adm.begin(), adm.end(), [&](int a, int b) { return s->req[a]->nsteps < s->req[b]->nsteps; });
+        std::vector<std::vector<int>> groups;
+        for (int id : adm) {
+            if (groups.empty() || (int)groups.back().size() >= s->cohort_max ||
+                s->req[id]->nsteps > 2 * s->req[groups.back().front()]->nsteps)
+                groups.emplace_back();
+            groups.back().push_back(id);
+        }
+        for (std::vector<int>& adm : groups) {
+            double add = 0;
+            for (int id : adm) add += s->req[id]->est_bytes;
+            Cohort c;
+            std::vector<const nbc_scene_desc*> v;
+            for (int id : adm) v.push_back(&s->req[id]->scene->d);
+            try {
+                c.eng.reset(new nbc_engine());
+                c.eng->opt = s->opt;
+                c.eng->eng.reset(nbc::make_engine(v, s->opt));
+                for (size_t k = 0; k < adm.size(); k++) {
+                    Request& r = *s->req[adm[k]];
+                    c.eng->eng->set_stop((int)k, r.nsteps);
+                    c.longest = std::max(c.longest, r.nsteps);
+                }
+                double b = 0, ms = 0;
+                c.eng->eng->info(&b, &ms);
+                // whole bytes, so that the sum over running cohorts stays exact
+                c.bytes = std::ceil(std::max(b, add));
+                for (size_t k = 0; k < adm.size(); k++) {
+                    Request& r = *s->req[adm[k]];
+                    r.state = 1;
+                    r.cohort = s->next_cohort;
+                    r.slot = (int)k;
+                    r.scene.reset();
+                }
+                c.ids = adm;
+                c.open = (int)adm.size();
+                s->used += c.bytes;
+                s->running += (int)adm.size();
+                s->cohorts[s->next_cohort++] = std::move(c);
+            } catch (const std::exception& e) {
+                for (int id : adm) {
+                    Request& r = *s->req[id];
+                    r.state = 3;
+                    r.error = e.what();
+                    r.scene.reset();
+                }
+            }
+        }
+        // the rest of each old cohort's chunk (a capacity overflow can stop a
+        // chunk early), then the new samples of its requests
+        for (int cid : old) {
+            Cohort& c = s->cohorts[cid];
+            if (c.open == 0) continue;
+            try {
+                int did = launched[cid] > 0 ? c.eng->eng->wait_steps() : 0;
+                while (did < want[cid]) {
+                    c.eng->eng->enqueue(want[cid] - did);
+                    did += c.eng->eng->wait_steps();
+                }
+                c.started += did;
+                if (did == 0) continue;
+                c.eng->eng->sync();  // the last step's reaction is recorded by its closing half-kick
+                for (int id : c.ids) {
+                    auto f = s->req.find(id);   // finished requests may have been released
+                    if (f == s->req.end() || f->second->state != 1) continue;
+                    Request& r = *f->second;
+                    const int now = std::min(c.started, r.nsteps), n = now - r.done;
+                    if (n > 0) {
+                        // samples at the new steps that are multiples of sample_every
+                        std::vector<double> hist((size_t)n * 6);
+                        c.eng->eng->get_intruder_history(r.slot, n, hist.data());
+                        for (int k = r.done + 1; k <= now; k++)
+                            if (k % r.sample_every == 0 || k == r.nsteps)
+                                r.curve.insert(r.curve.end(), &hist[(size_t)(k - r.done - 1) * 6],
+                                               &hist[(size_t)(k - r.done - 1) * 6 + 6]);
+                        r.done = now;
+                    }
+                    if (r.done >= r.nsteps) {
+                        double v[3], reac[3], tq[3];
+                        int state = 0;
+                        c.eng->eng->get_intruder(r.slot, r.intr_pos, v, reac, tq, &state);
+                        r.state = 2;
+                        c.open--;
+                        s->running--;
+                    }
                 }
             } catch (const std::exception& e) {
-                retire_failed(r, e);
+                fail_cohort(c, e);
             }
         }
-        std::vector<int> still;
-        for (size_t k = 0; k < running.size(); k++) {
-            Request& r = *s->req[running[k]];
-            if (r.state != 1) continue;
-            // samples at the steps of this chunk that are multiples of sample_every
-            const int first = r.done + 1, last = r.done + did[k];
-            if (did[k] > 0) {
-                r.eng->eng->sync();  // the last step's reaction is recorded by its closing half-kick
-                std::vector<double> hist((size_t)did[k] * 6);
-                r.eng->eng->get_intruder_history(0, did[k], hist.data());
-                for (int st = first; st <= last; st++)
-                    if (st % r.sample_every == 0 || st == r.nsteps)
-                        r.curve.insert(r.curve.end(), &hist[(size_t)(st - first) * 6], &hist[(size_t)(st - first) * 6 + 6]);
-            }
-            r.done = last;
-            if (r.done >= r.nsteps) {
-                r.eng->eng->sync();
-                double v[3], reac[3], tq[3];
-                int state = 0;
-                r.eng->eng->get_intruder(0, r.intr_pos, v, reac, tq, &state);
-                s->used -= r.bytes;
-                r.eng.reset();
-                r.scene.reset();
-                r.state = 2;
+        // cohorts without running requests release their engine and memory
+        for (auto it = s->cohorts.begin(); it != s->cohorts.end();) {
+            if (it->second.open == 0) {
+                s->used -= it->second.bytes;
+                it = s->cohorts.erase(it);
             } else {
-                still.push_back(r.id);
+                ++it;
             }
         }
-        // the requests admitted in this round run from the next one
-        for (size_t k = running.size(); k < s->active.size(); k++) still.push_back(s->active[k]);
-        s->active = still;
     });
-    if (n_active) *n_active = (int)s->active.size();
+    if (n_active) *n_active = s->running;
     if (n_queued) *n_queued = (int)s->queue.size();
     if (n_done) {
         int c = 0;
@@ -312,6 +373,12 @@ nbc_status nbc_server_memory(nbc_server* s, double* used_bytes, double* budget_b
     if (!s) return fail(NBC_ERR_ARG, "nbc_server_memory: null server");
     if (used_bytes) *used_bytes = s->used;
     if (budget_bytes) *budget_bytes = s->budget;
+    return NBC_OK;
+}
+
+nbc_status nbc_server_set_cohort(nbc_server* s, int max_requests) {
+    if (!s || max_requests < 1) return fail(NBC_ERR_ARG, "nbc_server_set_cohort: bad arguments");
+    s->cohort_max = max_requests;
     return NBC_OK;
 }
 

@@ -98,10 +98,10 @@ EXPORTED = [
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
     "nbc_timing_phases",
-    "nbc_engine_info", "nbc_cell_sort_noalloc", "nbc_choose_levels",
+    "nbc_engine_info", "nbc_set_scene_steps", "nbc_cell_sort_noalloc", "nbc_choose_levels",
     "nbc_batch_create", "nbc_batch_step", "nbc_batch_engine", "nbc_batch_destroy",
     "nbc_server_create", "nbc_server_submit", "nbc_server_advance", "nbc_server_result",
-    "nbc_server_release", "nbc_server_memory", "nbc_server_destroy",
+    "nbc_server_release", "nbc_server_memory", "nbc_server_destroy", "nbc_server_set_cohort",
 ]
 
 _lib = None
@@ -385,6 +385,10 @@ class Engine:
         _check(lib().nbc_timing_phases(self.h, _p(a, P_D)))
         return dict(zip(("clump", "rebuild", "boundary", "contact", "step"), a.tolist()))
 
+    def set_steps(self, nsteps, s=0):
+        """Scene s stands still after nsteps steps from the engine's creation (0: no limit)."""
+        _check(lib().nbc_set_scene_steps(self.h, int(s), int(nsteps)))
+
     def info(self):
         b, ms = C.c_double(), C.c_double()
         _check(lib().nbc_engine_info(self.h, C.byref(b), C.byref(ms)))
@@ -405,7 +409,7 @@ class SceneView:
     the scene index bound."""
 
     _PER_SCENE = ("stats", "subspheres", "clumps", "sub_forces", "force_parts", "pairs", "rows", "chain",
-                  "intruder", "intruder_diag", "intruder_history", "restart_scene")
+                  "intruder", "intruder_diag", "intruder_history", "restart_scene", "set_steps")
 
     def __init__(self, engine, s):
         self.engine, self.s = engine, s
@@ -461,11 +465,12 @@ class Server:
     and a step count; its result is the intruder reaction sampled every
     sample_every steps and the intruder's final position."""
 
-    def __init__(self, budget_bytes, max_active=64, **opts):
+    def __init__(self, budget_bytes, max_active=64, cohort=1, **opts):
         o = _options(**opts)
         h = C.c_void_p()
         _check(lib().nbc_server_create(C.byref(o), C.c_double(budget_bytes), int(max_active), C.byref(h)))
         self.h = h
+        _check(lib().nbc_server_set_cohort(self.h, int(cohort)))
 
     def submit(self, scene, nsteps, sample_every=100):
         d, keep = scene_desc(scene)

@@ -1,9 +1,9 @@
 """Batches of independent scenes and the request server (continuous
 batching): every scene's result in a batch or in the server's mix equals the
 same scene run alone, bitwise (a batch is one engine over its scenes, each
-with its own rebuild schedule and pair region; a request has its own
-engine), and admission respects the slot limit and the device-memory
-budget."""
+with its own rebuild schedule and pair region; the requests admitted together
+share one engine, each standing still at its own step count), and admission
+respects the slot limit and the device-memory budget."""
 import os
 
 import numpy as np
@@ -40,6 +40,38 @@ def test_batch_equals_alone():
     b.close()
 
 
+def test_scene_step_limits_equal_alone():
+    """Scenes of one engine with their own step limits: each stands still at
+    its limit (inside graph launches) while the others go on, with the state
+    and intruder record of the scene run alone for that many steps."""
+    scenes = _scenes()
+    stops = [40, 95, 0]
+    b = nbc.Batch(scenes, precision="mixed")
+    for v, n in zip(b.engines, stops):
+        if n:
+            v.set_steps(n)
+    b.step(70)
+    b.step(60)
+    b.sync()
+    with pytest.raises(nbc.NbcError):
+        b.engines[0].set_steps(100)   # 130 steps have started
+    for sc, v, n in zip(scenes, b.engines, stops):
+        n = n or 130
+        a = nbc.Engine([sc], precision="mixed")
+        a.step(n)
+        a.sync()
+        ca, cb = a.clumps(), v.clumps()
+        for k in ("pos", "vel", "angvel", "quat"):
+            assert np.array_equal(ca[k], cb[k]), (n, k)
+        assert v.stats()["steps"] == n and a.stats()["rebuilds"] == v.stats()["rebuilds"]
+        if sc.get("intruder") is not None:
+            ia, ib = a.intruder(), v.intruder()
+            assert np.array_equal(ia["pos"], ib["pos"]) and np.array_equal(ia["reaction"], ib["reaction"])
+            assert np.array_equal(a.intruder_history(count=n), v.intruder_history(count=n))
+        a.close()
+    b.close()
+
+
 def _requests():
     out = []
     for i, (n, r_i, v, mu) in enumerate([(1500, 4e-3, 0.3, 0.3), (4000, 6e-3, 0.5, 0.6),
@@ -64,23 +96,28 @@ def _alone_curve(scene, nsteps, every):
 def test_server_results_equal_alone_and_respect_slots():
     reqs = _requests()
     nsteps, every = [300, 410, 250, 333], 50
-    srv = nbc.Server(budget_bytes=64e9, max_active=2, precision="mixed")
+    srv = nbc.Server(budget_bytes=64e9, max_active=2, cohort=2, precision="mixed")
     ids = [srv.submit(sc, n, every) for sc, n in zip(reqs, nsteps)]
-    seen_running = 0
+    seen_running, results = 0, {}
     for _ in range(1000):
         st = srv.advance(chunk=37)
         seen_running = max(seen_running, st["running"])
         assert st["running"] <= 2
-        if st["finished"] == len(ids):
+        # results are taken and released as soon as they are ready, while
+        # requests admitted with them may still run
+        for rid in ids:
+            if rid not in results and srv.state(rid)[0] == 2:
+                results[rid] = srv.result(rid)
+                srv.release(rid)
+        if len(results) == len(ids):
             break
     assert seen_running == 2
     for rid, sc, n in zip(ids, reqs, nsteps):
-        res = srv.result(rid)
+        res = results[rid]
         assert res is not None and res["steps"] == n
         curve, pos = _alone_curve(sc, n, every)
         assert np.array_equal(res["curve"], curve), rid
         assert np.array_equal(res["intr_pos"], pos), rid
-        srv.release(rid)
     assert srv.memory()[0] == 0.0
     srv.close()
 
