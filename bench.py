@@ -416,6 +416,29 @@ def run_cfg2(args):
     import nbc
     bed = nbc.with_levels(sg.make_cfg2())
     N = int(bed["params"]["NumberBody"])
+    if args.profile_window is not None:
+        # for a launch list: settle --profile-window steps, then restart the
+        # state in an eager engine (kernel nodes of a graph with a conditional
+        # node are not profiled) and put the profiler range around --steps steps
+        import torch
+        e = nbc.Engine([bed], precision=args.precision)
+        e.step(args.profile_window)
+        state = e.restart_scene(bed)
+        e.close()
+        e = nbc.Engine([state], precision=args.precision, use_graph=False)
+        e.step(3)
+        e.sync()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        e.step(args.steps)
+        e.sync()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        st = e.stats()
+        print(json.dumps({"profile_run": True, "subspheres": N, "window": [args.profile_window, args.steps],
+                          "rebuilds": st["rebuilds"], "pairs": st["npairs"]}), flush=True)
+        e.close()
+        return
     e = nbc.Engine([bed], precision=args.precision)
     t0 = time.perf_counter()
     e.step(args.settle2)
@@ -595,7 +618,7 @@ def main():
     ap.add_argument("--settle2", type=int, default=150_000, help="cfg2: settling steps of the bed")
     ap.add_argument("--scenes", type=int, default=256, help="cfg3: number of scenes")
     ap.add_argument("--profile-window", type=int, default=None,
-                    help="cfg3: eager batch only, profiler range around --steps steps after this many")
+                    help="cfg2/cfg3: eager run for a profiler range of --steps steps after this many")
     ap.add_argument("--requests", type=int, default=200, help="cfg4: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="cfg4: mean arrivals per second")
     ap.add_argument("--bank", type=int, default=8, help="cfg4: pre-settled beds in the bank")

@@ -696,7 +696,11 @@ class EngineT final : public EngineBase {
                 cid[g] = P.clump_off + D.clump_id[i];
                 fix[g] = i;
                 sid[g] = s;
-                if (P.levels > 1) lev[g] = D.level[i];
+                if (P.levels > 1) {
+                    if (D.level[i] < 0 || D.level[i] >= P.levels)
+                        throw ArgError("scene " + std::to_string(s) + ": grid level out of range at row " + std::to_string(i));
+                    lev[g] = D.level[i];
+                }
                 mstart[cid[g] + 1]++;
             }
             for (int k = 0; k < D.n_clump; k++) {

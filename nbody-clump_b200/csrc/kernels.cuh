@@ -1039,6 +1039,20 @@ static __global__ void k_xsort(const Dev* __restrict__ dp) {
 
 // The reverse map of CreateContList_cuk (src/dem_grid.cu:561-601): for each
 // back entry of i (owner j), the slot of the pair (j, i) in j's front row.
+// A front row is two ascending runs of partners: the same-level entries
+// (the search visits the stencil's cells in ascending cell order, and the
+// subspheres are sorted by cell), then the cross-level entries (k_xsort), so
+// the slot is found by binary search in the run of i's level.
+__device__ __forceinline__ int find_partner(const int* __restrict__ nbr, int lo, int hi, int key) {
+    int len = hi - lo;
+    while (len > 0) {
+        const int h = len >> 1;
+        if ((nbr[lo + h] & IDX_MASK) < key) { lo += h + 1; len -= h + 1; }
+        else len = h;
+    }
+    return lo < hi && (nbr[lo] & IDX_MASK) == key ? lo : -1;
+}
+
 static __global__ void k_backref(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
@@ -1046,12 +1060,15 @@ static __global__ void k_backref(const Dev* __restrict__ dp) {
     const PairList& Nw = d.L[1];
     NBC_GRID_STRIDE(t, T) {
         const PlanItem it = plan_item(d, ns, t);
-        const int s = it.s;
-        for (int k = Nw.brow[it.i + s]; k < Nw.brow[it.i + s + 1]; k++) {
+        const int s = it.s, i = it.i, tb = t - i;
+        for (int k = Nw.brow[i + s]; k < Nw.brow[i + s + 1]; k++) {
             const int j = Nw.bnbr[k] & IDX_MASK;
-            int found = -1;
-            for (int q = Nw.row[j + s]; q < Nw.row[j + s + 1]; q++)
-                if ((Nw.nbr[q] & IDX_MASK) == it.i) { found = q; break; }
+            const int rs = Nw.row[j + s], re = Nw.row[j + s + 1], mid = rs + d.sfc[j + tb];
+            const bool same = d.level2[i] == d.level2[j];
+            int found = same ? find_partner(Nw.nbr, rs, mid, i) : find_partner(Nw.nbr, mid, re, i);
+            if (found < 0)   // not where the order puts it: scan the row
+                for (int q = rs; q < re; q++)
+                    if ((Nw.nbr[q] & IDX_MASK) == i) { found = q; break; }
             Nw.bpair[k] = found;
         }
     }
