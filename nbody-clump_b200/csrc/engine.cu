@@ -1001,7 +1001,7 @@ class EngineT final : public EngineBase {
     void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
         k_clump<R><<<cdiv(K_ + S_, CL_THREADS), CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond);
         CK(cudaGetLastError());
-        if (!capturing_ && timing_) launches_ += 1;
+        if (!capturing_) launches_ += 1;
     }
     bool capturing_ = false;
     // the contact pass: k_pairs, with k_boundary beside it on the second
@@ -1042,7 +1042,7 @@ class EngineT final : public EngineBase {
 #undef NBC_CT
         CK(cudaGetLastError());
         mark(6, stream_);
-        if (!capturing_ && timing_) launches_ += 3;
+        if (!capturing_) launches_ += 3;
     }
     // exclusive scan of a[0, n) (or of a[0, *dn) when dn is given, n then
     // bounds it)
@@ -1198,8 +1198,8 @@ class EngineT final : public EngineBase {
             for (int k = 0; k < NMARK; k++)
                 if (mark_on(timing_, k))
                     CK(cudaGraphExecEventRecordNodeSetEvent(gexec_[timing_], gev_node_[timing_][k], r[k]));
-            launches_ += 4;
         }
+        launches_ += 4;
         CK(cudaGraphLaunch(gexec_[timing_], stream_));
     }
 
