@@ -455,6 +455,11 @@ class EngineT final : public EngineBase {
         SceneDyn y = read_dyn(s);
         y.stop = nsteps;
         copy_(h_.dyn + s, &y, sizeof(SceneDyn), cudaMemcpyHostToDevice);
+        if (nsteps && !h_.has_stops) {
+            refresh_dev();
+            h_.has_stops = 1;
+            push_dev();
+        }
     }
     void info(double* bytes, double* ms) override {
         if (bytes) *bytes = mem_.bytes;

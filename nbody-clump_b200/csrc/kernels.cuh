@@ -83,8 +83,9 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
     }
     // warp-uniform: this warp holds clumps of a scene that moves (a warp whose
     // clumps all belong to scenes standing still skips its work)
-    bool warp_live = false;
-    if (k0 < d.K) {
+    const bool stops = d.has_stops;
+    bool warp_live = k0 < d.K && !stops;
+    if (k0 < d.K && stops) {
         const int nq = min(32, d.K - k0);
         const SceneDyn& yq = d.dyn[d.csid[lane < nq ? t : k0 + nq - 1]];
         warp_live = __any_sync(0xffffffffu, lane < nq && (scene_pre(yq, do_pre, L) || scene_post(yq, post, L)));
@@ -100,7 +101,8 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
         if (lane == 0) s_ms[warp][32] = mem_start[k0 + nk];
         const int sc = d.csid[k];
         double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cprop[k];
-        const bool pre_k = scene_pre(d.dyn[sc], do_pre, L), post_k = scene_post(d.dyn[sc], post, L);
+        const bool pre_k = stops ? scene_pre(d.dyn[sc], do_pre, L) : do_pre != 0;
+        const bool post_k = stops ? scene_post(d.dyn[sc], post, L) : post != 0;
         s_sc[warp][lane] = sc;
         s_pre[warp][lane] = isc && pre_k;
         s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
@@ -1679,13 +1681,13 @@ __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__
     const int i = blockIdx.x * BD_THREADS + threadIdx.x;
     if (i >= d.N) return;
     const int s = d.sid[i];
-    if (d.dyn[s].frozen) return;   // a scene past its stop stands still
+    const double4 pp = d.posr[i];   // issued before the scene's flag is known
+    const uint16_t bb_old = d.bbits[i];
+    if (d.has_stops && d.dyn[s].frozen) return;   // a scene past its stop stands still
     const ScenePar& P = d.par[s];
     const size_t N = (size_t)d.N;
-    const double4 pp = d.posr[i];
     const double r = pp.w;
     const int nwall = P.wall == WALL_CUBE ? 6 : (P.wall == WALL_CYL ? 3 : 0);
-    const uint16_t bb_old = d.bbits[i];
     {
         // conservative early-out: clearly inside every wall and outside the
         // intruder's bounding sphere (margins of 1e-9 relative cover rounding)
@@ -1934,7 +1936,7 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         // work item w: near pair w - nprefix[s] of scene s
         const int s = S == 1 ? 0 : plan_find(npre, S, w);
         const SceneDyn& ys = d.dyn[s];
-        if (ys.frozen) continue;
+        if (d.has_stops && ys.frozen) continue;
         const int p = nfp[ys.pair_off + (w - npre[s])];
         const int jr = nbr[p];
         if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
@@ -1993,15 +1995,15 @@ __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) 
     const int* __restrict__ nbq = d.nbq;
     V3<R> F = v3<R>(0, 0, 0), T = F;
     const int s = d.S == 1 ? 0 : d.sid[i];
-    if (d.dyn[s].frozen) return;
-    const int rs = d.nrow[i + s], re = d.nrow[i + s + 1];
+    const int rs = d.nrow[i + s], re = d.nrow[i + s + 1];   // issued before the scene's flag is known
+    const int bs = d.nbrow[i + s], be = d.nbrow[i + s + 1];
+    if (d.has_stops && d.dyn[s].frozen) return;
     for (int e = rs + lane; e < re; e += LANES) {
         const int k = nfp[e];
         if (!to[k]) continue;
         F = F + xyz<R>(ct[k]);
         T = T + xyz<R>(ct[cap + k]);
     }
-    const int bs = d.nbrow[i + s], be = d.nbrow[i + s + 1];
     for (int e = bs + lane; e < be; e += LANES) {
         const int q = nbq[e];
         if (!to[q]) continue;

@@ -107,6 +107,7 @@ struct Dev {
     int sort_bits;    // key bits for the radix sort
     int cblocks;      // total contact-kernel blocks
     int nthreads_sub; // subsphere-parallel grid stride helpers
+    int has_stops;    // some scene has a step limit (nbc_set_scene_steps): the kernels check for frozen scenes
     ScenePar* par;
     SceneDyn* dyn;
     int* sid;         // [N] scene of each subsphere
