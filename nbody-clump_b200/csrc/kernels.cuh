@@ -913,7 +913,7 @@ __device__ __forceinline__ int claim_chunk(int* ctr, int n, int* sh) {
 // entries found by finer partners, cnt_b[t] = back entries) and the hits in
 // scratch rows.  A group of SL lanes per subsphere, grid-stride.
 template <int SL>
-__global__ void __launch_bounds__(SEARCH_THREADS) k_search(const Dev* __restrict__ dp) {
+__global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search(const Dev* __restrict__ dp) {
     __shared__ SearchShared<SL> sh;
     __shared__ int s_claim;
     const Dev& d = *dp;
