@@ -123,6 +123,14 @@ def barrier(world):
         dist.barrier()
 
 
+def replica_throughput(n_sub, steps, world, local_seconds, backend):
+    """Whole-job throughput of `world` independent replicas (one scene per
+    rank, the same work on each): the slowest rank's time, taken by an
+    all-reduce, and units = n_sub x steps x world.  Returns (seconds, value)."""
+    secs = reduce_max(local_seconds, world, backend)
+    return secs, n_sub * steps * world / secs
+
+
 def run_b200(args, world, rank, local):
     import nbc
     backend = None
@@ -163,8 +171,7 @@ def run_b200(args, world, rank, local):
     st1 = eng.stats()
     barrier(world)
     local_s = t1 - t0
-    secs = reduce_max(local_s, world, backend)
-    value = N * args.steps * world / secs
+    secs, value = replica_throughput(N, args.steps, world, local_s, backend)
     launches = tm["kernel_launches"]
     if not args.profile:
         # the contact pass's CUDA-event time over a replay of the timed region
