@@ -453,11 +453,11 @@ def run_cfg2(args):
         # state in an eager engine (kernel nodes of a graph with a conditional
         # node are not profiled) and put the profiler range around --steps steps
         import torch
-        e = nbc.Engine([bed], precision=args.precision)
+        e = nbc.Engine([bed], precision=args.precision, search_lanes=args.search_lanes)
         e.step(args.profile_window)
         state = e.restart_scene(bed)
         e.close()
-        e = nbc.Engine([state], precision=args.precision, use_graph=False)
+        e = nbc.Engine([state], precision=args.precision, use_graph=False, search_lanes=args.search_lanes)
         e.step(3)
         e.sync()
         torch.cuda.synchronize()
@@ -471,7 +471,7 @@ def run_cfg2(args):
                           "rebuilds": st["rebuilds"], "pairs": st["npairs"]}), flush=True)
         e.close()
         return
-    e = nbc.Engine([bed], precision=args.precision)
+    e = nbc.Engine([bed], precision=args.precision, search_lanes=args.search_lanes)
     t0 = time.perf_counter()
     e.step(args.settle2)
     e.sync()
@@ -486,7 +486,7 @@ def run_cfg2(args):
     dt = float(sc["params"]["StepSize"])
     total = int(round(0.5 / dt))
     nchunk = 100
-    e = nbc.Engine([sc], precision=args.precision)
+    e = nbc.Engine([sc], precision=args.precision, search_lanes=args.search_lanes)
     z0 = float(sc["intruder"]["pos"][2])
     curve, done = [[0.0, 0.0, 0.0, 0.0]], 0
     t0 = time.perf_counter()
