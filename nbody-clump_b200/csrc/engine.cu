@@ -31,8 +31,9 @@ thread_local std::string g_last_error;
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
-struct ArgError : std::runtime_error {
-    using std::runtime_error::runtime_error;
+// an argument the caller can fix; the C ABI reports it as NBC_ERR_ARG
+struct ArgError : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
 };
 
 #define CK(call)                                                                             \
