@@ -127,6 +127,48 @@ struct PinnedSlots {
 };
 static PinnedSlots g_pinned;
 
+// A scene's arrays are checked before anything reaches the device: missing
+// arrays, non-finite values, non-positive radii, masses and inertias, clump
+// ids and grid levels out of range are argument errors (the reference reads
+// its inputs unchecked, src/dem_subsphere_io.cu:151-193).
+static void validate_scene(const nbc_scene_desc& D, int s) {
+    const std::string at = "scene " + std::to_string(s) + ": ";
+    if (D.n_sub <= 0 || D.n_clump <= 0 || !D.pos || !D.radius || !D.clump_id || !D.local || !D.mass ||
+        !D.clump_pos || !D.clump_vel || !D.clump_quat || !D.clump_angvel || !D.clump_prop)
+        throw ArgError(at + "empty or missing arrays");
+    if (!(std::isfinite(D.dt) && D.dt > 0)) throw ArgError(at + "time step not positive");
+    if (!(std::isfinite(D.thresh) && D.thresh >= 0)) throw ArgError(at + "Thresh negative or not finite");
+    if (D.levels > 1 && (!D.level || !D.level_cell)) throw ArgError(at + "grid levels without level arrays");
+    auto fin = [](const double* p, int n) {
+        for (int k = 0; k < n; k++)
+            if (!std::isfinite(p[k])) return false;
+        return true;
+    };
+    for (int i = 0; i < D.n_sub; i++) {
+        if (!fin(D.pos + 3 * i, 3) || !fin(D.local + 3 * i, 3))
+            throw ArgError(at + "non-finite position at row " + std::to_string(i));
+        if (!(std::isfinite(D.radius[i]) && D.radius[i] > 0) || !(std::isfinite(D.mass[i]) && D.mass[i] > 0))
+            throw ArgError(at + "radius or mass not positive at row " + std::to_string(i));
+        if (D.clump_id[i] < 0 || D.clump_id[i] >= D.n_clump)
+            throw ArgError(at + "clump id out of range at row " + std::to_string(i));
+        if (D.levels > 1 && (D.level[i] < 0 || D.level[i] >= D.levels))
+            throw ArgError(at + "grid level out of range at row " + std::to_string(i));
+    }
+    for (int k = 0; k < D.n_clump; k++) {
+        const double* q = D.clump_quat + 4 * k;
+        const double* pr = D.clump_prop + 4 * k;
+        if (!fin(D.clump_pos + 3 * k, 3) || !fin(D.clump_vel + 3 * k, 3) || !fin(D.clump_angvel + 3 * k, 3) ||
+            !fin(q, 4) || q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3] == 0)
+            throw ArgError(at + "non-finite or zero clump state at clump " + std::to_string(k));
+        for (int c = 0; c < 4; c++)
+            if (!(std::isfinite(pr[c]) && pr[c] > 0))
+                throw ArgError(at + "clump inertia or mass not positive at clump " + std::to_string(k));
+    }
+    for (int l = 0; D.levels > 1 && l < D.levels; l++)
+        if (!(std::isfinite(D.level_cell[l]) && D.level_cell[l] > 0))
+            throw ArgError(at + "grid cell size not positive on level " + std::to_string(l));
+}
+
 template <typename R>
 class EngineT final : public EngineBase {
    public:
@@ -565,6 +607,7 @@ class EngineT final : public EngineBase {
 
     // ---- setup --------------------------------------------------------------
     void setup(const std::vector<const nbc_scene_desc*>& sc) {
+        for (size_t s = 0; s < sc.size(); s++) validate_scene(*sc[s], (int)s);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw CudaError("no CUDA device");
         CK(cudaSetDevice(opt_.device));

@@ -135,3 +135,27 @@ def test_server_admits_by_memory_budget():
             break
     assert all(srv.state(i)[0] == 2 for i in ids)
     srv.close()
+
+
+def test_server_retires_a_bad_request_and_serves_the_others():
+    """A request whose scene fails the engine's input checks (here a radius
+    of zero) is retired with its error at admission; the requests around it
+    run and give the results they give alone."""
+    reqs = _requests()[:3]
+    bad = dict(reqs[1])
+    bad["sub"] = {k: np.array(v, copy=True) for k, v in reqs[1]["sub"].items()}
+    bad["sub"]["radius"][0] = 0.0
+    srv = nbc.Server(budget_bytes=64e9, max_active=3, precision="mixed")
+    ids = [srv.submit(sc, 60, 20) for sc in (reqs[0], bad, reqs[2])]
+    for _ in range(100):
+        st = srv.advance(chunk=30)
+        if st["finished"] == 3:
+            break
+    assert srv.state(ids[1])[0] == 3
+    with pytest.raises(nbc.NbcError, match="radius or mass not positive"):
+        srv.result(ids[1])
+    for rid, sc in ((ids[0], reqs[0]), (ids[2], reqs[2])):
+        res = srv.result(rid)
+        curve, pos = _alone_curve(sc, 60, 20)
+        assert np.array_equal(res["curve"], curve) and np.array_equal(res["intr_pos"], pos)
+    srv.close()

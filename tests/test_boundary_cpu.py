@@ -58,6 +58,35 @@ def test_create_rejects_bad_arguments():
     assert L.nbc_step(None, 1) == -1
 
 
+def _copy_scene(sc):
+    out = dict(sc)
+    for k in ("sub", "clump"):
+        out[k] = {kk: np.array(vv, copy=True) for kk, vv in sc[k].items()}
+    return out
+
+
+@pytest.mark.parametrize("where,index,value,needle", [
+    ("sub.pos", (0, 0), float("nan"), "non-finite position"),
+    ("sub.radius", 1, 0.0, "radius or mass not positive"),
+    ("sub.mass", 2, -1.0, "radius or mass not positive"),
+    ("clump.prop", (2, 3), -1.0, "clump inertia or mass not positive"),
+    ("clump.vel", (3, 1), float("inf"), "non-finite or zero clump state"),
+])
+def test_create_rejects_invalid_values_before_the_device(where, index, value, needle):
+    """A scene's values are checked on the host before any device call, so
+    a bad scene is an argument error (on a machine without a GPU too) and
+    never reaches a kernel."""
+    sc = _copy_scene(sg.make_test_spheres(n=64, seed=3))
+    part, key = where.split(".")
+    sc[part][key][index] = value
+    d, keep = nbc.scene_desc(sc)
+    arr = (C.POINTER(nbc.SceneDesc) * 1)(C.pointer(d))
+    h = C.c_void_p()
+    rc = nbc.lib().nbc_create(arr, 1, None, C.byref(h))
+    assert nbc.STATUS[rc] == "ERR_ARG"
+    assert needle in nbc.lib().nbc_last_error().decode()
+
+
 def _workdir(scene, d):
     sg.write_reference_inputs(scene, d)
     return d
