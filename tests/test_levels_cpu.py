@@ -41,3 +41,28 @@ def test_oracle_hgrid_pairs_equal_single_level_set():
     # same physics: clump states after the step agree to rounding
     ca, cb = one.clumps(), multi.clumps()
     assert np.abs(ca["vel"] - cb["vel"]).max() <= 1e-9 * np.abs(ca["vel"]).max()
+
+
+def test_owner_rows_are_two_ascending_runs():
+    """The order the back references rely on (binary search in k_backref):
+    an owner row lists its same-level partners first, in ascending index
+    order (the stencil's cells are visited in ascending cell order and the
+    subspheres are sorted by cell), then its cross-level partners in
+    ascending order.  Checked on the oracle's lists, which follow the
+    reference's order, after several rebuilds."""
+    sc = nbc.with_levels(sg.make_test_poly(n_clumps=120, seed=5))
+    assert sc["levels"] is not None and len(sc["levels"]["cell"]) > 1
+    o = oracle.OracleScene(sc)
+    o.step(40)
+    assert o.rebuilds >= 2
+    lv = np.asarray(sc["levels"]["level"])[o.sub()["part_fix"]]
+    anei, ng, _ = o.rows()
+    runs = 0
+    for i in range(len(ng)):
+        row = anei[i, :ng[i]]
+        same = lv[row] == lv[i]
+        k = int(np.argmin(same)) if not same.all() else len(row)
+        assert same[:k].all() and not same[k:].any(), i      # same-level entries form a prefix
+        assert np.all(np.diff(row[:k]) > 0) and np.all(np.diff(row[k:]) > 0), i
+        runs += k < len(row)
+    assert runs > 10
