@@ -86,3 +86,21 @@ def test_oracle_damping_matches_restitution_formula():
     ln = np.log(e)
     ref = 2.0 * np.sqrt(5.0 / 6.0) * ln / np.sqrt(ln * ln + 3.14159265359 ** 2)
     assert abs(sg.damping_from_restitution(e) - ref) < 1e-15
+
+
+def test_oracle_threads_do_not_change_results():
+    """The reference arm of the benchmark runs the oracle on every host
+    thread, the parity tests mostly on one: its lists and states are the
+    same bit for bit on 1 and 4 threads (each subsphere's sums run in a
+    fixed order whatever the thread that owns it)."""
+    import nbc
+    sc = nbc.with_levels(sg.make_test_poly(n_clumps=120, seed=5))
+    a, b = oracle.OracleScene(sc, threads=1), oracle.OracleScene(sc, threads=4)
+    a.step(60)
+    b.step(60)
+    assert a.rebuilds == b.rebuilds and a.rebuilds > 5
+    ca, cb = a.clumps(), b.clumps()
+    for k in ca:
+        assert np.array_equal(ca[k], cb[k]), k
+    for x, y in zip(a.pairs(), b.pairs()):
+        assert np.array_equal(x, y)
