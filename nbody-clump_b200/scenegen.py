@@ -302,8 +302,9 @@ def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000, 
               fit_box: bool = False) -> dict:
     """50,000 tetrahedral clumps (4 subspheres, r = 1 mm, centre offset 0.6 r,
     log-normal(0, 0.2) size scale, random orientation) seeded in layers inside
-    a closed cylinder wall (R = 60 mm, half-height 300 mm, axis z, floor at
-    z = 0) and settling under gravity.  mu overrides the friction; fit_box
+    a closed cylinder wall (R = 60 mm, height 300 mm = half-height 150 mm,
+    axis z, floor at z = 0; the layers reach z = 0.19 m) and settling under
+    gravity.  mu overrides the friction; fit_box
     ends the hashing box a few clump sizes above the seeded bed (the bed only
     falls) instead of at the cylinder top, so small beds get small grids."""
     rng = np.random.default_rng(seed)
@@ -311,7 +312,7 @@ def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000, 
     scales = rng.lognormal(0.0, 0.2, n_clumps)
     locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
     diam = 2.0 * np.array([np.linalg.norm(l, axis=1).max() + rr.max() for l, rr in zip(locals_, radii)])
-    R, H = 0.06, 0.30
+    R, H = 0.06, 0.15
     pts = layered_packing(rng, diam, R, 0.0)
     q = random_unit_quaternions(rng, n_clumps)
     rmin = min(rr.min() for rr in radii)
@@ -326,6 +327,71 @@ def make_cfg1(n_clumps: int = 50_000, seed: int = 20260828, steps: int = 20000, 
     return assemble(params, pts, q, np.zeros((K, 3)), np.zeros((K, 3)), props,
                     locals_, radii, masses,
                     cylinder=make_cylinder(R, H, (0, 0, H)))
+
+
+def tetra_scales(n_clumps: int = 50_000, seed: int = 20260828) -> np.ndarray:
+    """The per-clump size scales make_cfg1 draws for (n_clumps, seed): the
+    first draw of its generator."""
+    return np.random.default_rng(seed).lognormal(0.0, 0.2, n_clumps)
+
+
+def tetra_state_to_npz(scene: dict, scales: np.ndarray, path: str, **meta):
+    """A compact snapshot of a scene of tetrahedral clumps (the cfg1 family):
+    its parameters and walls, each clump's size scale, pose (FP64) and
+    velocities (FP32), and the hierarchical-grid level of every subsphere.
+    The members are rebuilt from the scales by the template, so the file
+    stays a few MB for 50,000 clumps."""
+    local, radius = _tetra_members(scales, 1e-3, 0.6, MATERIAL["rho"])[:2]
+    if not (np.array_equal(np.concatenate(radius), scene["sub"]["radius"])
+            and np.array_equal(np.concatenate(local), scene["sub"]["local"])):
+        raise ValueError("scales do not rebuild the scene's members")
+    flat = {}
+    for k, v in scene["params"].items():
+        flat["param/" + k] = np.array(v)
+    for grp in ("cube", "cylinder"):
+        if scene.get(grp) is not None:
+            for k, v in scene[grp].items():
+                flat[f"{grp}/{k}"] = np.array(v)
+    c = scene["clump"]
+    flat["clump/scale"] = np.asarray(scales, np.float64)
+    flat["clump/pos"] = c["pos"]
+    flat["clump/quat"] = c["quat"]
+    flat["clump/vel"] = c["vel"].astype(np.float32)
+    flat["clump/angvel"] = c["angvel"].astype(np.float32)
+    lv = scene.get("levels")
+    if lv is not None:
+        flat["levels/level"] = np.asarray(lv["level"], np.uint8)
+        flat["levels/cell"] = np.asarray(lv["cell"], np.float64)
+    for k, v in meta.items():
+        flat["meta/" + k] = np.array(v)
+    np.savez_compressed(path, **flat)
+
+
+def tetra_state_from_npz(path: str) -> dict:
+    """The scene a tetra_state_to_npz snapshot holds: subsphere positions are
+    the clump poses applied to the rebuilt members (X + C_bn(q) local)."""
+    z = np.load(path)
+    params = {}
+    for k in z.files:
+        if k.startswith("param/"):
+            v = z[k]
+            params[k[6:]] = v.item() if v.dtype.kind != "U" else str(v)
+    scales = z["clump/scale"]
+    locals_, radii, masses, props = _tetra_members(scales, 1e-3, 0.6, MATERIAL["rho"])
+    grp = {}
+    for g in ("cube", "cylinder"):
+        keys = [k for k in z.files if k.startswith(g + "/")]
+        if keys:
+            grp[g] = {k.split("/", 1)[1]: (z[k].item() if z[k].ndim == 0 else z[k].copy()) for k in keys}
+    sc = assemble(params, z["clump/pos"], z["clump/quat"], z["clump/vel"].astype(np.float64),
+                  z["clump/angvel"].astype(np.float64), props, locals_, radii, masses,
+                  cube=grp.get("cube"), cylinder=grp.get("cylinder"))
+    if "levels/level" in z.files:
+        sc["levels"] = {"level": z["levels/level"].astype(np.int32), "cell": z["levels/cell"].copy()}
+    else:
+        sc["levels"] = None
+    sc["meta"] = {k[5:]: z[k].item() for k in z.files if k.startswith("meta/")}
+    return sc
 
 
 def make_cfg3(n_scenes: int = 256, seed: int = 20260828, steps: int = 20000, kmin: int = 500,
@@ -734,6 +800,137 @@ def scene_from_npz(path: str) -> dict:
                     v = str(v)
             scene[grp][k] = v
     return scene
+
+
+def _cyl_wall_sphere_sites(rng, r, Rc, H, spacing, n_side, n_cap, n_interior):
+    """Sphere centres (relative to the cylinder centre, axis z) for a closed
+    cylinder of radius Rc and half-height H: n_cap on each cap, n_side on
+    the side, a ring at each cap edge, and n_interior clear of every wall.
+    Returns (centres, kind) with kind 0 bottom cap, 1 top cap, 2 side,
+    3 bottom edge, 4 top edge, 5 interior; the overlap with the wall is
+    drawn later per sphere.  Sites are at least `spacing` apart."""
+    sites, kind = [], []
+
+    def put(p, k):
+        if all(np.linalg.norm(p - q) >= spacing for q in sites):
+            sites.append(p)
+            kind.append(k)
+            return True
+        return False
+
+    for k in (3, 4):  # edge rings
+        n = int(2 * math.pi * (Rc - r) / spacing)
+        for j in range(n):
+            a = 2 * math.pi * (j + 0.5 * (k - 3)) / n
+            put(np.array([(Rc - r) * math.cos(a), (Rc - r) * math.sin(a), (-1 if k == 3 else 1) * (H - r)]), k)
+    for k, cnt in ((0, n_cap), (1, n_cap), (2, n_side), (5, n_interior)):
+        placed, tries = 0, 0
+        while placed < cnt and tries < 200 * cnt:
+            tries += 1
+            if k in (0, 1):
+                rho, a = (Rc - 3 * r) * math.sqrt(rng.random()), 2 * math.pi * rng.random()
+                p = np.array([rho * math.cos(a), rho * math.sin(a), (-1 if k == 0 else 1) * (H - r)])
+            elif k == 2:
+                a, z = 2 * math.pi * rng.random(), rng.uniform(-(H - 3 * r), H - 3 * r)
+                p = np.array([(Rc - r) * math.cos(a), (Rc - r) * math.sin(a), z])
+            else:
+                rho, a = (Rc - 3.5 * r) * math.sqrt(rng.random()), 2 * math.pi * rng.random()
+                p = np.array([rho * math.cos(a), rho * math.sin(a), rng.uniform(-(H - 3.5 * r), H - 3.5 * r)])
+            placed += put(p, k)
+    return np.array(sites), np.array(kind)
+
+
+def make_test_cyl(kind="spheres", seed=31, r=1e-3, Rc=12e-3, H=9e-3, overlap=(0.005, 0.04), vel=0.2,
+                  angvel=300.0, dt=2e-6, steps=24, thresh_ratio=3e-4, bl=64, sigma=0.1, squeeze=0.8):
+    """Clumps in a closed cylinder wall (axis z) in contact with its bottom
+    cap, top cap, side and both cap edges from the first step.
+
+    kind "spheres": one-sphere clumps (LocalPos = 0, radius r x LogNormal(0,
+    sigma) clipped to [0.8, 1.25] r) at least 2.6 r_max apart, so the only
+    contacts are with the wall: the scene the reference's sphere-only driver
+    runs (its cylinder wall, src/dem_force_cylind_wall.cu:152-237) and the
+    clump path must match.  Each sphere on a wall site is pushed into the
+    wall by overlap x r (uniform in the given range; at an edge into both),
+    random linear and angular velocities stretch, break and make wall
+    contacts over the run, and a small Thresh rebuilds the list every few
+    steps.
+
+    kind "tetra": tetrahedral clumps on a lattice clipped to the cylinder,
+    packed closer than their extent (inter-clump contacts); every clump of
+    the outer ring, the top layer and the bottom layer is moved until its
+    farthest subsphere presses into the wall by overlap x r, so the side,
+    both caps and the rings where they meet carry contacts."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    if kind == "spheres":
+        rmax = 1.25 * r
+        sites, skind = _cyl_wall_sphere_sites(rng, rmax, Rc, H, 2.6 * rmax, 16, 12, 12)
+        K = len(sites)
+        rad = r * np.clip(np.exp(sigma * rng.standard_normal(K)), 0.8, 1.25)
+        ov = rng.uniform(overlap[0], overlap[1], (K, 2)) * rad[:, None]
+        pts = sites.copy()
+        for i in range(K):
+            ri, k = rad[i], skind[i]
+            rho_xy = math.hypot(pts[i, 0], pts[i, 1])
+            if k in (0, 3):
+                pts[i, 2] = -(H - ri + ov[i, 0])
+            elif k in (1, 4):
+                pts[i, 2] = H - ri + ov[i, 0]
+            if k in (2, 3, 4):
+                f = (Rc - ri + ov[i, 1]) / rho_xy
+                pts[i, 0] *= f
+                pts[i, 1] *= f
+        m = rho * 4 / 3 * math.pi * rad ** 3
+        I = 0.4 * m * rad ** 2
+        props = np.stack([I, I, I, m], axis=1)
+        locals_ = [np.zeros((1, 3))] * K
+        radii = [np.array([x]) for x in rad]
+        masses = [np.array([x]) for x in m]
+        rmin = float(rad.min())
+        quats = random_unit_quaternions(rng, K)
+    elif kind == "tetra":
+        n_side = 6
+        scales = rng.lognormal(0.0, sigma, 4 * n_side ** 3)
+        rmed = r * float(np.median(scales))
+        ext = 2 * 1.6 * rmed * squeeze
+        g = (np.arange(n_side) - (n_side - 1) / 2.0) * ext
+        gx, gy, gz = np.meshgrid(g, g, g, indexing="ij")
+        keep = gx ** 2 + gy ** 2 <= (g.max() + 1e-12) ** 2
+        pts = np.stack([gx[keep], gy[keep], gz[keep]], axis=1)
+        pts = pts + rng.uniform(-0.03 * ext, 0.03 * ext, pts.shape)
+        K = len(pts)
+        scales = scales[:K]
+        locals_, radii, masses, props = _tetra_members(scales, r, 0.6, rho)
+        quats = random_unit_quaternions(rng, K)
+        Rm = quat_to_body2world(quats)
+        cid = np.repeat(np.arange(K), 4)
+        arm = np.einsum("nij,nj->ni", Rm[cid], np.concatenate(locals_))
+        sr = np.concatenate(radii)
+        rho_k = np.hypot(pts[:, 0], pts[:, 1])
+        Rc = float(rho_k.max() + 1.4 * rmed)
+        H = float(np.abs(pts[:, 2]).max() + 1.4 * rmed)
+        dl = rng.uniform(overlap[0], overlap[1], (K, 2)) * r
+        zmax = np.abs(pts[:, 2]).max()
+        for k in range(K):
+            sub = slice(4 * k, 4 * k + 4)
+            if rho_k[k] > rho_k.max() - 0.5 * ext:
+                u = pts[k, :2] / rho_k[k]
+                reach = np.max((pts[k, :2] + arm[sub, :2]) @ u + sr[sub])
+                pts[k, :2] += (Rc - reach + dl[k, 0]) * u
+            if abs(pts[k, 2]) > zmax - 0.5 * ext:
+                sgn = 1.0 if pts[k, 2] > 0 else -1.0
+                reach = np.max(sgn * (pts[k, 2] + arm[sub, 2]) + sr[sub])
+                pts[k, 2] += sgn * (H - reach + dl[k, 1])
+        rmin = r * float(scales.min())
+        rmax = r * float(scales.max())
+    else:
+        raise ValueError(kind)
+    c = np.array([Rc + 2 * rmax, Rc + 2 * rmax, H + 2 * rmax])
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=1, Thresh=thresh_ratio * rmin,
+                            BranchLmtLen=bl)
+    set_world_box(params, np.zeros(3), 2 * c)
+    return assemble(params, pts + c, quats, rng.uniform(-vel, vel, (K, 3)), rng.uniform(-angvel, angvel, (K, 3)),
+                    props, locals_, radii, masses, cylinder=make_cylinder(Rc, H, c))
 
 
 def make_test_converging(n_side=8, seed=5, r=1e-3, loose=1.6, shrink=0.45, steps=1500, sigma=0.15):

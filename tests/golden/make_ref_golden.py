@@ -18,6 +18,15 @@ Two phases:
     ``OutForce/*.bin``; layouts of ``src/dem_binary_io.h``) and stores a
     compact ``<case>.ref.npz`` in ``--out``.
 
+Cases in SPHERE_PATH run the reference's sphere-only driver instead
+(``oracle/_ref/nbody_sphere_ref``: ``DEMmain::RunSimulation``,
+``src/dem_simulation_cylind.cu:3-211``, the only driver of the reference
+with a closed cylinder wall).  Their scenes are one-sphere clumps with
+LocalPos = 0, written in the sphere format (``ph`` with 21 columns,
+``src/dem_io.cu:155-193``) plus ``Rocks/CylindWall.bt``; the sphere
+driver's ``OutPart/ph.*.bin`` (``src/dem_io.cu:313-329``) gives positions,
+velocities, quaternions and angular velocities at every step.
+
 The ``.ref.npz`` files are committed next to this script and read by
 ``tests/test_oracle_golden.py`` and the GPU parity tests.
 """
@@ -52,13 +61,16 @@ CASES = {
                                                 motion="gravity_after_contact", wall="cube",
                                                 steps=24),
     "cfg0_settle": None,
+    "cyl_spheres": lambda: sg.make_test_cyl("spheres", seed=31, steps=24, thresh_ratio=1e-3),
 }
+SPHERE_PATH = {"cyl_spheres"}
 STEPS = 24
 FORCE_STEPS = (2, 12, 24)
 
 
-def prepare(ref_dir: str | None):
-    for name, build in CASES.items():
+def prepare(ref_dir: str | None, names):
+    for name in names:
+        build = CASES[name]
         path = os.path.join(HERE, f"{name}.scene.npz")
         if name == "ref_fixture":
             if ref_dir is None:
@@ -77,6 +89,67 @@ def prepare(ref_dir: str | None):
             sc["params"]["OutputInterval"] = 1
         sg.scene_to_npz(sc, path)
         print("wrote", path, sc["params"]["NumberBody"], "subspheres")
+
+
+def write_sphere_inputs(scene: dict, d: str):
+    """The sphere driver's inputs for a scene of one-sphere clumps: world.par
+    (the same 38 keys), the 21-column ph file (id, id, Type, pos, vel, quat,
+    angular velocity, Ixx Iyy Izz M, radius; src/dem_io.cu:183-185) and
+    Rocks/ (CylindWall.bt, src/dem_cylind_wall_io.cu:41-49; an inert
+    Penetrator.bt, which the driver always reads)."""
+    s, c = scene["sub"], scene["clump"]
+    if len(s["radius"]) != len(c["pos"]) or np.abs(s["local"]).max() != 0.0:
+        raise ValueError("the sphere driver takes one-sphere clumps with LocalPos = 0")
+    if np.any(s["clump_id"] != np.arange(len(c["pos"]))):
+        raise ValueError("sphere k must be clump k")
+    sg.write_reference_inputs(scene, d)   # world.par and Rocks/, as for the clump path
+    with open(os.path.join(d, scene["params"]["IniConFile"]), "w") as f:
+        for k in range(len(c["pos"])):
+            cols = np.concatenate([c["pos"][k], c["vel"][k], c["quat"][k], c["angvel"][k], c["prop"][k],
+                                   [s["radius"][k]]])
+            f.write("%d %d 0 %s\n" % (k, k, " ".join(sg._g(v) for v in cols)))
+
+
+def read_sphere_ph(path: str) -> dict:
+    """OutPart/ph.N.bin of the sphere driver (src/dem_io.cu:313-329): int32 n,
+    int32 sortedParticleID[n], ParticleID[n], Type[n], then double3 Pos, Vel,
+    double4 Quat, double3 AngSpd, double4 Property, double Radius."""
+    b = open(path, "rb").read()
+    n = int(np.frombuffer(b, np.int32, 1, 0)[0])
+    o = 4
+    out = {}
+    for key, dt, w in (("sorted_id", np.int32, 1), ("part_fix", np.int32, 1), ("type", np.int32, 1),
+                       ("pos", np.float64, 3), ("vel", np.float64, 3), ("quat", np.float64, 4),
+                       ("angvel", np.float64, 3), ("prop", np.float64, 4), ("radius", np.float64, 1)):
+        a = np.frombuffer(b, dt, n * w, o)
+        o += a.nbytes
+        out[key] = a.reshape(n, w) if w > 1 else a.copy()
+    if o != len(b):
+        raise ValueError(f"{path}: {len(b) - o} trailing bytes")
+    return out
+
+
+def run_sphere_case(binary: str, name: str, out: str, keep: bool):
+    sc = sg.scene_from_npz(os.path.join(HERE, f"{name}.scene.npz"))
+    work = tempfile.mkdtemp(prefix=f"ref_{name}_")
+    write_sphere_inputs(sc, work)
+    t0 = time.time()
+    r = subprocess.run([binary], cwd=work, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, timeout=900)
+    wall = time.time() - t0
+    if r.returncode != 0:
+        print(r.stdout.decode(errors="replace")[-3000:])
+        raise SystemExit(f"reference sphere driver failed on {name}: rc={r.returncode}")
+    p = sc["params"]
+    steps = p["EndStep"] - p["StartStep"]
+    res = {"wall_s": np.array(wall), "steps": np.array(steps)}
+    for s in range(p["OutputInterval"], steps + 1, p["OutputInterval"]):
+        ph = read_sphere_ph(os.path.join(work, "OutPart", "ph.%08d.bin" % s))
+        for k in ("part_fix", "pos", "vel", "quat", "angvel"):
+            res[f"s{s}/{k}"] = ph[k]
+    np.savez_compressed(os.path.join(out, f"{name}.ref.npz"), **res)
+    print(f"{name}: {steps} steps in {wall:.2f} s wall (reference sphere driver, incl. file IO)")
+    if not keep:
+        shutil.rmtree(work, ignore_errors=True)
 
 
 def run_case(binary: str, name: str, out: str, keep: bool):
@@ -129,16 +202,21 @@ def main():
     ap.add_argument("phase", choices=["prepare", "run"])
     ap.add_argument("--ref", default=None, help="reference tree (prepare)")
     ap.add_argument("--binary", default=os.path.join(REPO, "oracle", "_ref", "nbody_clump_ref"))
+    ap.add_argument("--sphere-binary", default=os.path.join(REPO, "oracle", "_ref", "nbody_sphere_ref"))
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--cases", default=",".join(CASES))
     ap.add_argument("--keep", action="store_true")
     a = ap.parse_args()
     if a.phase == "prepare":
-        prepare(a.ref)
+        prepare(a.ref, a.cases.split(","))
         return
     os.makedirs(a.out, exist_ok=True)
     for name in a.cases.split(","):
-        if os.path.exists(os.path.join(HERE, f"{name}.scene.npz")):
+        if not os.path.exists(os.path.join(HERE, f"{name}.scene.npz")):
+            continue
+        if name in SPHERE_PATH:
+            run_sphere_case(a.sphere_binary, name, a.out, a.keep)
+        else:
             run_case(a.binary, name, a.out, a.keep)
 
 
