@@ -259,10 +259,13 @@ int nbc_choose_levels(const double* radius, int n, int max_levels, int* level, d
  *   key_dev   device out [n]: its cell, ascending
  *   stream    cudaStream_t to launch on (NULL: the default stream); the
  *             call returns after launching, the caller synchronises.
- * n above NBC_NOALLOC_MAX_N returns NBC_ERR_ARG.  The first call on a device
- * looks up the scratch array's device address, so make that first call
- * before any stream capture.  Calls share the scratch array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * n above NBC_NOALLOC_MAX_N returns NBC_ERR_ARG.  A call made outside a
+ * stream capture looks up the scratch array's device address (again on
+ * every such call, so a device reset is followed); a captured call reuses
+ * the address the last uncaptured call on that device found, so make the
+ * first call on a device before any stream capture (a captured first call
+ * returns NBC_ERR_STATE).  Calls share the scratch array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
 #define NBC_NOALLOC_MAX_N 262144
 typedef struct {
     double origin[3];

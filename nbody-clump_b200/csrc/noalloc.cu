@@ -92,17 +92,28 @@ extern "C" nbc_status nbc_cell_sort_noalloc(const double* pos_dev, int n, const 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(NBC_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= MAX_DEVICES) return fail(NBC_ERR_ARG, "device ordinal too large");
+    cudaStream_t st = (cudaStream_t)stream;
     int* scratch;
     {
-        // once per device, with that device current: the scratch array's
-        // device address (the first call on a device does this look-up)
+        // The scratch array's device address, with the device current.  It
+        // is looked up again on every call made outside a stream capture (a
+        // device reset rebuilds the context and may move the array); a call
+        // inside a capture uses the address the last uncaptured call on this
+        // device found, so the first call on a device must come before any
+        // capture.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        e = cudaStreamIsCapturing(st, &cs);
+        if (e != cudaSuccess)
+            return fail(NBC_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
         std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_addr[dev]) {
+        if (cs == cudaStreamCaptureStatusNone) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_sort_scratch);
             if (e != cudaSuccess)
                 return fail(NBC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             g_scratch_addr[dev] = (int*)p;
+        } else if (!g_scratch_addr[dev]) {
+            return fail(NBC_ERR_STATE, "nbc_cell_sort_noalloc: the first call on a device must not be captured");
         }
         scratch = g_scratch_addr[dev];
     }
@@ -110,7 +121,6 @@ extern "C" nbc_status nbc_cell_sort_noalloc(const double* pos_dev, int n, const 
     int* vB = kB + MAX_N;
     int* hist = vB + MAX_N;
     int* sums = hist + HIST;
-    cudaStream_t st = (cudaStream_t)stream;
     int bits = 1;
     while ((1LL << bits) < cells) bits++;
     const int passes = (bits + 7) / 8;

@@ -60,6 +60,56 @@ def test_noalloc_sort_matches_engine_sort_twice():
     eng.close()
 
 
+def numpy_cell_sort(pos, g):
+    """The cell hash of GetParticleCellIndex_cuk (src/dem_grid.cu:155-202,
+    the engine's padded grid: positions outside the box go to the last
+    cell, cell coordinates clamped to the grid) and a stable sort by cell."""
+    dims = np.array(g.dims[:], np.int64)
+    cellnum = int(np.prod(dims))
+    lo, hi = np.array(g.box_lo[:]), np.array(g.box_hi[:])
+    out = np.any((pos >= hi) | (pos < lo), axis=1)
+    c = np.floor((pos - np.array(g.origin[:])) / g.cell).astype(np.int64)
+    c = np.clip(c, 0, dims - 1)
+    key = np.clip(c[:, 2] * dims[1] * dims[0] + c[:, 1] * dims[0] + c[:, 0], 0, cellnum - 1)
+    key[out] = cellnum - 1
+    perm = np.argsort(key, kind="stable")
+    return perm.astype(np.int32), key[perm].astype(np.int32)
+
+
+@pytest.mark.parametrize("dims,n", [((6, 6, 6), 3001), ((20, 20, 91), 20000 + 777), ((50, 50, 40), 70001)])
+def test_noalloc_sort_matches_numpy_for_one_two_three_passes(dims, n):
+    """216 cells (one 8-bit radix pass: the hash lands in the library's
+    scratch array and the pass in the caller's buffers), 36,400 cells (two
+    passes) and 100,000 cells (three passes), n not a multiple of the radix
+    tile, some positions outside the box and some on cell faces: permutation
+    and keys bit-exact with a numpy hash and stable sort, on two calls in a
+    row."""
+    import torch
+
+    rng = np.random.default_rng(n)
+    g = nbc.GridDesc()
+    g.cell = 1e-3
+    for a in range(3):
+        g.origin[a] = -g.cell
+        g.dims[a] = dims[a]
+        g.box_lo[a] = 0.0
+        g.box_hi[a] = (dims[a] - 2) * g.cell
+    span = np.array([(d - 2) * g.cell for d in dims])
+    pos = rng.uniform(-0.05, 1.05, (n, 3)) * span           # about 15% outside the box
+    pos[: n // 10] = np.round(pos[: n // 10] / g.cell) * g.cell   # some exactly on cell faces
+    want_p, want_k = numpy_cell_sort(pos, g)
+    bits = int(np.ceil(np.log2(np.prod(dims))))
+    assert (bits + 7) // 8 == {216: 1, 36400: 2, 100000: 3}[int(np.prod(dims))]
+    dpos = torch.from_numpy(pos).cuda()
+    for call in range(2):
+        perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        key = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        nbc.cell_sort_noalloc(dpos.data_ptr(), n, g, perm.data_ptr(), key.data_ptr(), 0)
+        torch.cuda.synchronize()
+        assert np.array_equal(perm.cpu().numpy(), want_p), f"call {call}: permutation"
+        assert np.array_equal(key.cpu().numpy(), want_k), f"call {call}: keys"
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     grid = nbc.GridDesc()
     grid.cell = 1.0
