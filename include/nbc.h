@@ -88,12 +88,14 @@ typedef struct {
 
 typedef struct {
     int precision;      /* NBC_PREC_* */
-    int lanes;          /* lanes per subsphere in the contact sum: 1, 2, 4, 8, 16 or 32 (0 = 2) */
+    int lanes;          /* reserved, ignored: each subsphere's contact sum runs in the clump pass */
     int use_graph;      /* 1: one CUDA graph per step with a conditional rebuild node */
     int device;         /* CUDA device ordinal */
     double pair_slack;  /* pair capacity = slack * pairs of the first list; 0 = 1.6 and at least
                            the reference's own n_sub * BranchLmtLen/2 as far as 30% of free memory allows */
     int search_lanes;   /* lanes per subsphere in the neighbour search: 8, 16 or 32 (0 = 8) */
+    int clump_batch;    /* members each lane of the clump pass loads at a time: 1, 2 or 4 (0 = 2) */
+    int pair_blocks;    /* blocks per SM of the pair kernel's grid: 2 .. 16 (0 = 12) */
 } nbc_options;
 
 typedef struct nbc_engine nbc_engine;
@@ -154,6 +156,11 @@ nbc_status nbc_get_rows(nbc_engine* e, int scene, int bl, int* anei, int* ng, in
  * (CalFcnChain_cuk, src/dem_force_particle.cu:238-268): normal force and
  * contact point per row slot, [n_sub][bl][3] each */
 nbc_status nbc_get_chain(nbc_engine* e, int scene, int bl, double* fcn, double* cpt);
+/* after nbc_step_export: the normal force on the owner of every pair of the
+ * half list, in list order (the reference's CacheFcn, src/dem_force_clump.cu:
+ * 114-116; zero where the pair does not touch), [npairs][3]; *npairs in/out
+ * as for nbc_get_pairs */
+nbc_status nbc_get_pair_forces(nbc_engine* e, int scene, int* npairs, double* fcn);
 /* intruder position, velocity, last reaction force/torque, contact state */
 nbc_status nbc_get_intruder(nbc_engine* e, int scene, double* pos, double* vel, double* reaction,
                             double* torque, int* state);
@@ -180,6 +187,21 @@ nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launc
 nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
+/* Exact checkpoint, replacing the reference's restart from StartStep
+ * (src/world.par:28, the step loop of src/dem_simulation_clump.cu:110),
+ * which restarts from ph/ch snapshots and loses the spring histories.  write
+ * waits for the device, applies the pending half-kick (as nbc_sync) and
+ * saves the whole state the next step needs: scene bookkeeping, every
+ * subsphere in its current sort order with its wall and intruder spring
+ * histories, every clump, each scene's current pair list with its spring
+ * histories, touch flags and near rows, and the intruder force record.
+ * read loads such a file into an engine created (nbc_create / nbc_open)
+ * from the same scenes with the same precision, before its first step or
+ * after; stepping on then gives bitwise the results of the run that was
+ * saved.  Writing before the first step is NBC_ERR_STATE; a file of other
+ * scenes or precision is NBC_ERR_ARG; a missing file NBC_ERR_IO. */
+nbc_status nbc_checkpoint_write(nbc_engine* e, const char* path);
+nbc_status nbc_checkpoint_read(nbc_engine* e, const char* path);
 /* No reference counterpart (the reference runs one scene until EndStep).
  * Scene `scene` takes `nsteps` steps counted from the engine's creation and
  * then stands still while the engine's other scenes go on: its state, forces
@@ -236,6 +258,19 @@ nbc_status nbc_server_destroy(nbc_server* s);
 /* requests per cohort at most (default 1: an engine per request); the
  * requests admitted in one call are grouped by step count, within 2x */
 nbc_status nbc_server_set_cohort(nbc_server* s, int max_requests);
+
+/* Autotuner (no reference counterpart): times trial_steps steps (after a
+ * short warm-up) of engines made from these scenes with candidate launch
+ * shapes -- lanes per subsphere of the neighbour search, members per lane
+ * of the clump pass, blocks per SM of the pair kernel -- by coordinate
+ * descent from the defaults, a candidate replacing the incumbent only when
+ * it is at least 3% faster, and writes the fastest into opt (other fields
+ * untouched).  The shapes change no result: every candidate computes the
+ * same lists and forces bit for bit.  The choice is cached in the process
+ * by scene shape (scenes, subspheres, clumps, grid levels, precision) and
+ * trial length; best_ms_per_step (may be NULL) receives its time. */
+nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n_scenes, nbc_options* opt, int trial_steps,
+                        double* best_ms_per_step);
 
 /* Hierarchical-grid levels for a radius distribution (replaces the grid.bt
  * level table the reference's sphere path reads, src/dem_io.cu:204-248):

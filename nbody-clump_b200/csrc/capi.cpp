@@ -6,9 +6,13 @@
 // src/dem_force_cube_wall_clump.cu:322-331).
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -35,6 +39,8 @@ void nbc_default_options(nbc_options* o) {
     o->device = 0;
     o->pair_slack = 0.0;
     o->search_lanes = 0;
+    o->clump_batch = 0;
+    o->pair_blocks = 0;
 }
 
 nbc_status nbc_create(const nbc_scene_desc* const* scenes, int n, const nbc_options* opt, nbc_engine** out) {
@@ -129,6 +135,11 @@ nbc_status nbc_get_rows(nbc_engine* e, int s, int bl, int* anei, int* ng, int* n
 nbc_status nbc_get_chain(nbc_engine* e, int s, int bl, double* fcn, double* cpt) {
     if (bad_scene(e, s) || bl <= 0 || !fcn || !cpt) return fail(NBC_ERR_ARG, "bad arguments");
     return guard([&] { e->eng->get_chain(s, bl, fcn, cpt); });
+}
+
+nbc_status nbc_get_pair_forces(nbc_engine* e, int s, int* npairs, double* fcn) {
+    if (bad_scene(e, s) || !npairs) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->get_pair_forces(s, npairs, fcn); });
 }
 
 nbc_status nbc_get_intruder(nbc_engine* e, int s, double* pos, double* vel, double* reac, double* tq, int* state) {
@@ -284,3 +295,115 @@ nbc_status nbc_run(nbc_engine* e) {
 }
 
 }  // extern "C"
+
+// ---- exact checkpoint ---------------------------------------------------
+nbc_status nbc_checkpoint_write(nbc_engine* e, const char* path) {
+    if (!e || !e->eng || !path) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] {
+        std::vector<char> b = e->eng->checkpoint_save();
+        FILE* f = std::fopen(path, "wb");
+        if (!f) throw std::invalid_argument(std::string("cannot write ") + path);
+        const size_t w = std::fwrite(b.data(), 1, b.size(), f);
+        const int c = std::fclose(f);
+        if (w != b.size() || c != 0) throw std::invalid_argument(std::string("short write to ") + path);
+    });
+}
+
+nbc_status nbc_checkpoint_read(nbc_engine* e, const char* path) {
+    if (!e || !e->eng || !path) return fail(NBC_ERR_ARG, "bad arguments");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(NBC_ERR_IO, std::string("cannot open ") + path);
+    std::vector<char> b;
+    char buf[1 << 16];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) b.insert(b.end(), buf, buf + n);
+    std::fclose(f);
+    return guard([&] { e->eng->checkpoint_load(b.data(), b.size()); });
+}
+
+// ---- autotuner ------------------------------------------------------------
+// Coordinate descent over the launch shapes from the defaults: each trial
+// makes an engine from the scenes, takes a short warm-up (the first list
+// build included) and times trial_steps steps on the host clock around a
+// synchronised nbc_step; a candidate replaces the incumbent only when it is
+// at least 3% faster, so timing noise between equal shapes keeps the
+// defaults.  Cached per process by scene shape.
+namespace {
+struct Tuned {
+    int search_lanes, clump_batch, pair_blocks;
+    double ms;
+};
+std::map<std::string, Tuned> g_tuned;
+std::mutex g_tuned_mu;
+}  // namespace
+
+nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n, nbc_options* opt, int trial_steps,
+                        double* best_ms) {
+    if (!scenes || n <= 0 || !opt || trial_steps <= 0) return fail(NBC_ERR_ARG, "nbc_autotune: bad arguments");
+    for (int i = 0; i < n; i++)
+        if (!scenes[i]) return fail(NBC_ERR_ARG, "nbc_autotune: null scene");
+    long long nsub = 0, ncl = 0;
+    int lv = 1;
+    for (int i = 0; i < n; i++) {
+        nsub += scenes[i]->n_sub;
+        ncl += scenes[i]->n_clump;
+        lv = std::max(lv, scenes[i]->levels);
+    }
+    const std::string key = std::to_string(n) + "|" + std::to_string(nsub) + "|" + std::to_string(ncl) + "|" +
+                            std::to_string(lv) + "|" + std::to_string(opt->precision) + "|" +
+                            std::to_string(trial_steps) + "|" + std::to_string(opt->device);
+    {
+        std::lock_guard<std::mutex> lock(g_tuned_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            opt->search_lanes = it->second.search_lanes;
+            opt->clump_batch = it->second.clump_batch;
+            opt->pair_blocks = it->second.pair_blocks;
+            if (best_ms) *best_ms = it->second.ms;
+            return NBC_OK;
+        }
+    }
+    return guard([&] {
+        std::vector<const nbc_scene_desc*> v(scenes, scenes + n);
+        const int warm = std::max(20, trial_steps / 5);
+        auto trial = [&](const nbc_options& o) {
+            std::unique_ptr<nbc::EngineBase> e(nbc::make_engine(v, o));
+            e->step(warm, false);
+            const auto t0 = std::chrono::steady_clock::now();
+            e->step(trial_steps, false);
+            const auto t1 = std::chrono::steady_clock::now();
+            return std::chrono::duration<double, std::milli>(t1 - t0).count() / trial_steps;
+        };
+        nbc_options best = *opt;
+        best.search_lanes = 8;
+        best.clump_batch = 2;
+        best.pair_blocks = 12;
+        best.use_graph = 1;
+        double tb = trial(best);
+        const int lanes[] = {16, 32}, batch[] = {1, 4}, blocks[] = {4, 8, 16};
+        for (int x : lanes) {
+            nbc_options o = best;
+            o.search_lanes = x;
+            const double t = trial(o);
+            if (t < 0.97 * tb) { best = o; tb = t; }
+        }
+        for (int x : batch) {
+            nbc_options o = best;
+            o.clump_batch = x;
+            const double t = trial(o);
+            if (t < 0.97 * tb) { best = o; tb = t; }
+        }
+        for (int x : blocks) {
+            nbc_options o = best;
+            o.pair_blocks = x;
+            const double t = trial(o);
+            if (t < 0.97 * tb) { best = o; tb = t; }
+        }
+        opt->search_lanes = best.search_lanes;
+        opt->clump_batch = best.clump_batch;
+        opt->pair_blocks = best.pair_blocks;
+        if (best_ms) *best_ms = tb;
+        std::lock_guard<std::mutex> lock(g_tuned_mu);
+        g_tuned[key] = Tuned{best.search_lanes, best.clump_batch, best.pair_blocks, tb};
+    });
+}

@@ -178,6 +178,8 @@ class EngineT final : public EngineBase {
             if (gexec_[t]) cudaGraphExecDestroy(gexec_[t]);
             if (graph_[t]) cudaGraphDestroy(graph_[t]);
         }
+        if (gexec_loop_) cudaGraphExecDestroy(gexec_loop_);
+        if (graph_loop_) cudaGraphDestroy(graph_loop_);
         for (cudaEvent_t e : ev_) cudaEventDestroy(e);
         for (auto& row : gev_)
             for (cudaEvent_t e : row) if (e) cudaEventDestroy(e);
@@ -223,9 +225,14 @@ class EngineT final : public EngineBase {
             n--;
         }
         if (n <= 0) return pend_eager_;
-        if (!gexec_[timing_]) capture(timing_);
+        if (timing_ == 0 && !loop_tried_) capture_loop();
         pend_before_ = read_gstep();
-        for (int i = 0; i < n; i++) launch_graph();
+        if (timing_ == 0 && gexec_loop_) {
+            launch_loop(n);
+        } else {
+            if (!gexec_[timing_]) capture(timing_);
+            for (int i = 0; i < n; i++) launch_graph();
+        }
         pend_ = n;
         return pend_eager_ + n;
     }
@@ -234,6 +241,7 @@ class EngineT final : public EngineBase {
         if (pend_ > 0) {
             CK(cudaStreamSynchronize(stream_));
             const int started = read_gstep() - pend_before_;
+            launches_ += 3LL * started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
             if (read_int(h_.halt)) {
                 // the last step started stopped at its rebuild: finish it on the host path
                 steps_done_ += started - 1;
@@ -359,6 +367,7 @@ class EngineT final : public EngineBase {
     }
     void get_sub_forces(int s, double* f, double* t) override {
         refresh_dev();
+        launch_sum(false);
         const ScenePar& P = hpar_[s];
         pull_r4(h_.fsum, P.sub_off, P.nsub, f);
         pull_r4((char*)h_.fsum + (size_t)N_ * sizeof(R4<R>), P.sub_off, P.nsub, t);
@@ -443,6 +452,22 @@ class EngineT final : public EngineBase {
             }
         }
     }
+    // the normal force on the owner of every listed pair, list order (the
+    // reference's CacheFcn, src/dem_force_clump.cu:114-116), from the export
+    // step; zero for pairs that do not touch
+    void get_pair_forces(int s, int* np, double* fcn) override {
+        refresh_dev();
+        SceneDyn y = read_dyn(s);
+        const int cap_in = *np;
+        *np = y.npairs;
+        if (!fcn) return;
+        if (cap_in < y.npairs) throw ArgError("pair buffer too small");
+        std::vector<R4<R>> xf(y.npairs);
+        copy_(xf.data(), (R4<R>*)h_.xfcn + y.pair_off, y.npairs * sizeof(R4<R>), cudaMemcpyDeviceToHost);
+        for (int p = 0; p < y.npairs; p++) {
+            fcn[3 * p] = xf[p].x; fcn[3 * p + 1] = xf[p].y; fcn[3 * p + 2] = xf[p].z;
+        }
+    }
     void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) override {
         SceneDyn y = read_dyn(s);
         for (int c = 0; c < 3; c++) {
@@ -504,6 +529,174 @@ class EngineT final : public EngineBase {
             push_dev();
         }
     }
+    // ---- exact checkpoint -------------------------------------------------
+    // The state a step leaves for the next one, after nbc_sync (the pending
+    // half-kick applied): every scene's bookkeeping (SceneDyn: steps, intruder
+    // state, pair region, step limit), the history generation and step
+    // counters, every subsphere in the current sort order (position and
+    // radius, body offset and mass, displacement since the last rebuild,
+    // clump, original index, grid level, cell key, contact kinematics, wall
+    // and intruder spring histories and their contact bits, boundary
+    // candidates), every clump's state and member list, and each scene's
+    // pair region: the current half list with its back references, spring
+    // histories and touch flags, the near rows and their contact slots, and
+    // the intruder force ring.  Rebuild scratch is not saved: a rebuild
+    // writes it before reading it.  Loading this into an engine made from
+    // the same scenes and options and stepping on gives bitwise the run that
+    // never stopped (the reference restarts from StartStep, src/world.par:28
+    // and src/dem_simulation_clump.cu:110, with its spring histories lost).
+    struct CkHeader {
+        char magic[8];
+        int version, S, N, K, cells, real_bytes, steps_done, hgen, gstep, lstep, ring_len;
+        long long total_cap;
+    };
+    std::vector<char> checkpoint_save() override {
+        if (steps_done_ < 1) throw StateError("checkpoint before the first step (there is no list yet)");
+        sync();
+        refresh_dev();
+        CkHeader hd{};
+        memcpy(hd.magic, "NBCCKPT", 8);
+        hd.version = 1;
+        hd.S = S_; hd.N = N_; hd.K = K_; hd.cells = h_.cells;
+        hd.real_bytes = (int)sizeof(R);
+        hd.steps_done = steps_done_;
+        hd.hgen = read_int(h_.hgen);
+        hd.gstep = read_int(h_.gstep);
+        hd.lstep = read_int(h_.lstep);
+        hd.ring_len = ring_len_;
+        hd.total_cap = h_.cap;
+        std::vector<char> out((const char*)&hd, (const char*)&hd + sizeof(hd));
+        ck_blocks(out, nullptr, 0, hd);
+        return out;
+    }
+    void checkpoint_load(const char* data, size_t bytes) override {
+        if (bytes < sizeof(CkHeader)) throw ArgError("checkpoint too short");
+        CkHeader hd;
+        memcpy(&hd, data, sizeof(hd));
+        if (memcmp(hd.magic, "NBCCKPT", 8) != 0 || hd.version != 1) throw ArgError("not an engine checkpoint");
+        if (hd.S != S_ || hd.N != N_ || hd.K != K_ || hd.cells != h_.cells || hd.ring_len != ring_len_)
+            throw ArgError("checkpoint of different scenes");
+        if (hd.real_bytes != (int)sizeof(R)) throw ArgError("checkpoint of the other precision");
+        if (bytes < sizeof(hd) + S_ * sizeof(SceneDyn)) throw ArgError("checkpoint too short");
+        CK(cudaStreamSynchronize(stream_));
+        // pair regions as saved (their sizes are in the saved SceneDyn)
+        refresh_dev();
+        mem_.release(pslab_, pslab_bytes_);
+        alloc_pairs(std::max<long long>(hd.total_cap, 1));
+        push_dev();
+        std::vector<char> in(data, data + bytes);
+        ck_blocks(in, &in, sizeof(hd), hd);
+        steps_done_ = hd.steps_done;
+        first_list_ = false;
+        post_done_ = false;
+        pend_ = pend_eager_ = 0;
+        bool stops = false;
+        for (const SceneDyn& v : read_dyn_all()) stops |= v.stop != 0;
+        if (stops && !h_.has_stops) {
+            h_.has_stops = 1;
+            push_dev();
+        }
+        CK(cudaStreamSynchronize(stream_));
+    }
+    // Writes (src == nullptr: appends to out) or reads (from src at offset
+    // off) the checkpoint's blocks in one fixed order.
+    void ck_blocks(std::vector<char>& out, const std::vector<char>* src, size_t off, const CkHeader& hd) {
+        const size_t N = N_;
+        auto blk = [&](void* dev, size_t n) {
+            if (!n) return;
+            if (!src) {
+                const size_t at = out.size();
+                out.resize(at + n);
+                copy_(out.data() + at, dev, n, cudaMemcpyDeviceToHost);
+            } else {
+                if (off + n > src->size()) throw ArgError("checkpoint truncated");
+                copy_(dev, src->data() + off, n, cudaMemcpyHostToDevice);
+                off += n;
+            }
+        };
+        // scene bookkeeping first (its pair regions size the rest)
+        blk(h_.dyn, S_ * sizeof(SceneDyn));
+        std::vector<SceneDyn> y = read_dyn_all();
+        // counters; the pending half-kick was applied by sync, so the next
+        // step must not repeat it (post_pending saved as 0)
+        int flags[4] = {hd.hgen, hd.gstep, hd.lstep, 0};
+        if (!src) {
+            const size_t at = out.size();
+            out.resize(at + sizeof(flags));
+            memcpy(out.data() + at, flags, sizeof(flags));
+        } else {
+            if (off + sizeof(flags) > src->size()) throw ArgError("checkpoint truncated");
+            memcpy(flags, src->data() + off, sizeof(flags));
+            off += sizeof(flags);
+            copy_(h_.hgen, &flags[0], sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.gstep, &flags[1], sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.lstep, &flags[2], sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.post_pending, &flags[3], sizeof(int), cudaMemcpyHostToDevice);
+            int zero = 0;
+            copy_(h_.any_rebuild, &zero, sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.halt, &zero, sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.lcur, &zero, sizeof(int), cudaMemcpyHostToDevice);
+            copy_(h_.kc_done, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        }
+        // subspheres, current sort order
+        blk(h_.posr, N * sizeof(double4));
+        blk(h_.lom, N * sizeof(double4));
+        blk(h_.cum, N * sizeof(double4));
+        blk(h_.clump_id, N * sizeof(int));
+        blk(h_.part_fix, N * sizeof(int));
+        blk(h_.level, N * sizeof(int));
+        blk(h_.key, N * sizeof(int));
+        blk(h_.kin, 3 * N * sizeof(R4<R>));
+        blk(h_.bhist, (size_t)NB_SLOTS * 3 * N * sizeof(R4<R>));
+        blk(h_.bbits, N * sizeof(uint16_t));
+        blk(h_.fbnd, 2 * N * sizeof(R4<R>));
+        blk(h_.bidx, N * sizeof(int));
+        // clumps
+        blk(h_.cpos, K_ * sizeof(double4));
+        blk(h_.cvel, K_ * sizeof(double4));
+        blk(h_.cw, K_ * sizeof(double4));
+        blk(h_.cq, K_ * sizeof(double4));
+        blk(h_.cprop, K_ * sizeof(double4));
+        blk(h_.cF, K_ * sizeof(double4));
+        blk(h_.cT, K_ * sizeof(double4));
+        blk(h_.mem_start, (K_ + 1) * sizeof(int));
+        blk(h_.mem_idx, N * sizeof(int));
+        // rows and work-item prefixes
+        blk(h_.L[0].row, (N + S_) * sizeof(int));
+        blk(h_.L[0].brow, (N + S_) * sizeof(int));
+        blk(h_.nrow, (N + S_) * sizeof(int));
+        blk(h_.nbrow, (N + S_) * sizeof(int));
+        blk(h_.nprefix, (S_ + 1) * sizeof(int));
+        blk(h_.bprefix, (S_ + 1) * sizeof(int));
+        blk(h_.ring, (size_t)S_ * ring_len_ * 6 * sizeof(double));
+        // each scene's pair region: the history generation the next contact
+        // pass reads is (hgen + 1) & 1 (k_clump advances hgen first)
+        const int g = (hd.hgen + 1) & 1;
+        const size_t cap = h_.cap;
+        for (int s = 0; s < S_; s++) {
+            const size_t o = y[s].pair_off, np = y[s].npairs, nn = y[s].nnear;
+            blk(h_.L[0].nbr + o, np * sizeof(int));
+            blk(h_.L[0].own + o, np * sizeof(int));
+            blk(h_.L[0].bnbr + o, np * sizeof(int));
+            blk(h_.L[0].bpair + o, np * sizeof(int));
+            R4<R>* H = (R4<R>*)h_.H[g];
+            blk(H + o, np * sizeof(R4<R>));
+            blk(H + cap + o, np * sizeof(R4<R>));
+            blk((R*)(H + 2 * cap) + o, np * sizeof(R));
+            blk(h_.touch[g] + o, np);
+            blk(h_.nearf + o, np);
+            blk(h_.nbpos + o, np * sizeof(int));
+            blk(h_.nfp + o, nn * sizeof(int));
+            blk(h_.nbq + o, nn * sizeof(int));
+            R4<R>* fs = (R4<R>*)h_.nfs;
+            R4<R>* bs = (R4<R>*)h_.nbs;
+            blk(fs + o, nn * sizeof(R4<R>));
+            blk(fs + cap + o, nn * sizeof(R4<R>));
+            blk(bs + o, nn * sizeof(R4<R>));
+            blk(bs + cap + o, nn * sizeof(R4<R>));
+        }
+        if (src && off != src->size()) throw ArgError("checkpoint has trailing bytes");
+    }
     void info(double* bytes, double* ms) override {
         if (bytes) *bytes = mem_.bytes;
         if (ms) *ms = last_ms_;
@@ -520,10 +713,13 @@ class EngineT final : public EngineBase {
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Dev h_{};            // host copy of the device table
     Dev* d_ = nullptr;   // device table
-    int S_ = 0, N_ = 0, K_ = 0, lanes_ = 16, passes_ = 0, rs_blocks_ = 0;
+    int S_ = 0, N_ = 0, K_ = 0, passes_ = 0, rs_blocks_ = 0;
     bool hgrid_ = false;
     bool first_list_ = true;
     int search_lanes_ = 8;
+    int clump_batch_ = 2;    // members per lane per load batch of the clump pass
+    int pair_bps_ = 12;      // blocks per SM of the pair kernel's grid
+    int sm_count_ = 148;
     int ring_len_ = 1;
     std::vector<ScenePar> hpar_;
     std::vector<int> start_step_;
@@ -536,6 +732,12 @@ class EngineT final : public EngineBase {
     // contact pass (k_pairs + k_sum), [2] event nodes at every mark
     cudaGraph_t graph_[3] = {nullptr, nullptr, nullptr};
     cudaGraphExec_t gexec_[3] = {nullptr, nullptr, nullptr};
+    // the untimed graph with a device-side step loop (capture_loop)
+    cudaGraph_t graph_loop_ = nullptr;
+    cudaGraphExec_t gexec_loop_ = nullptr;
+    cudaGraphNode_t loop_init_node_ = nullptr;
+    bool loop_tried_ = false;
+    std::string loop_error_;
     // kernel timing: one record of NMARK events per step, at the marks
     //   0 step start  1 after k_clump  2 after the rebuild node
     //   3/4 around k_boundary and 5 start of the contact pass (second branch)
@@ -562,7 +764,7 @@ class EngineT final : public EngineBase {
         return n;
     }
     // kernels one rebuild launches (launch_rebuild)
-    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4 + 8; }
+    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4 + 8 + 5; }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -618,15 +820,15 @@ class EngineT final : public EngineBase {
         hflag_ = g_pinned.get();
         mem_.stream = stream_;
         DevMem::keep_pool(opt_.device);
-        lanes_ = opt_.lanes == 1 || opt_.lanes == 2 || opt_.lanes == 4 || opt_.lanes == 8 || opt_.lanes == 16 ||
-                         opt_.lanes == 32 ? opt_.lanes : 2;
         search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
-        const int spb = CT_THREADS / lanes_;
+        clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
+        pair_bps_ = opt_.pair_blocks >= 2 && opt_.pair_blocks <= 16 ? opt_.pair_blocks : 12;
+        CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
         S_ = (int)sc.size();
         hpar_.resize(S_);
         start_step_.resize(S_);
         std::vector<SceneDyn> hdyn(S_);
-        int cells = 0, cblk = 0;
+        int cells = 0;
         for (int s = 0; s < S_; s++) {
             const nbc_scene_desc& D = *sc[s];
             if (D.n_sub <= 0 || D.n_clump <= 0 || !D.pos || !D.radius || !D.clump_id)
@@ -676,9 +878,6 @@ class EngineT final : public EngineBase {
             P.nsub = D.n_sub;
             P.clump_off = K_;
             P.nclump = D.n_clump;
-            P.cblk_off = cblk;
-            P.cblk_n = cdiv(D.n_sub, spb);
-            cblk += P.cblk_n;
             N_ += D.n_sub;
             K_ += D.n_clump;
             // walls
@@ -721,7 +920,6 @@ class EngineT final : public EngineBase {
         if ((long long)N_ >= (1LL << 30)) throw ArgError("more than 2^30 subspheres in one engine");
         h_.S = S_; h_.N = N_; h_.K = K_;
         h_.cells = cells;
-        h_.cblocks = cblk;
         int bits = 1;
         while ((1LL << bits) < (long long)cells) bits++;
         h_.sort_bits = bits;
@@ -732,7 +930,6 @@ class EngineT final : public EngineBase {
         std::vector<double4> posr(N_), lom(N_);
         std::vector<int> cid(N_), fix(N_), lev(N_, 0), sid(N_), csid(K_), mstart(K_ + 1, 0), midx(N_);
         std::vector<double4> cpos(K_), cvel(K_), cw(K_), cq(K_), cprop(K_);
-        std::vector<int> sblk(cblk);
         for (int s = 0; s < S_; s++) {
             const nbc_scene_desc& D = *sc[s];
             const ScenePar& P = hpar_[s];
@@ -761,7 +958,6 @@ class EngineT final : public EngineBase {
                 cq[g] = make_double4(D.clump_quat[4 * k], D.clump_quat[4 * k + 1], D.clump_quat[4 * k + 2], D.clump_quat[4 * k + 3]);
                 cprop[g] = make_double4(D.clump_prop[4 * k], D.clump_prop[4 * k + 1], D.clump_prop[4 * k + 2], D.clump_prop[4 * k + 3]);
             }
-            for (int b = 0; b < P.cblk_n; b++) sblk[P.cblk_off + b] = s;
         }
         for (int k = 0; k < K_; k++) mstart[k + 1] += mstart[k];
         {
@@ -803,6 +999,7 @@ class EngineT final : public EngineBase {
             h_.gstep = flags + 5;
             h_.kc_done = flags + 6;
             h_.lstep = flags + 7;
+            h_.loop_left = flags + 8;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
             h_.hist = m.take<int>((size_t)256 * rs_blocks_);
             h_.perm = m.take<int>(N);
@@ -813,6 +1010,8 @@ class EngineT final : public EngineBase {
             h_.nrow = m.take<int>(N + S_);
             h_.nbrow = m.take<int>(N + S_);
             h_.nprefix = m.take<int>(S_ + 1);
+            h_.bidx = m.take<int>(N);
+            h_.bprefix = m.take<int>(S_ + 1);
             h_.cnt_b = m.take<int>(N + 1);
             h_.sfc = m.take<int>(N);
             h_.xcnt = m.take<int>(N);
@@ -833,7 +1032,6 @@ class EngineT final : public EngineBase {
             h_.xintr = m.take<R4<R>>(4 * N);
             h_.ring_len = ring_len_;
             h_.ring = m.take<double>((size_t)S_ * ring_len_ * 6);
-            h_.sblk_scene = m.take<int>(cblk);
             d_ = m.take<Dev>(1);
         };
         Carver sz;
@@ -859,7 +1057,6 @@ class EngineT final : public EngineBase {
         copy_(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
         copy_(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice);
         copy_(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice);
-        copy_(h_.sblk_scene, sblk.data(), cblk * sizeof(int), cudaMemcpyHostToDevice);
         // the first list is empty: rows of zeros (the slab is zeroed)
         int one = 1;
         copy_(h_.any_rebuild, &one, sizeof(int), cudaMemcpyHostToDevice);
@@ -878,7 +1075,9 @@ class EngineT final : public EngineBase {
                 h_.H[l] = m.take<char>(hist_bytes(cap));
                 h_.touch[l] = m.take<uint8_t>(cap);
             }
-            h_.ctb = m.take<R4<R>>(4 * cap);
+            h_.nfs = m.take<R4<R>>(2 * cap);
+            h_.nbs = m.take<R4<R>>(2 * cap);
+            h_.nbpos = m.take<int>(cap);
             h_.nfp = m.take<int>(cap);
             h_.nbq = m.take<int>(cap);
             h_.nearf = m.take<uint8_t>(cap);
@@ -898,7 +1097,7 @@ class EngineT final : public EngineBase {
     // Bytes of the pair buffers per pair slot.
     static double bytes_per_pair() {
         return 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) +
-               2 * sizeof(int) + 1;
+               3 * sizeof(int) + 1;
     }
     // Region capacities for the first lists: slack x each scene's pairs; with
     // the default slack at least the reference's own list capacity, n_sub x
@@ -973,7 +1172,8 @@ class EngineT final : public EngineBase {
         const int B = 256;
         if (moved > 0)
             k_relayout<R><<<std::min(148 * 8, cdiv(moved, B)), B, 0, stream_>>>(
-                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.nfp, old.nbq, old.cap, relmap_, moved);
+                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.nfp, old.nbq, old.nbpos, old.cap,
+                relmap_, moved);
         k_shift_rows<<<std::min(148 * 8, cdiv((long long)N_ + S_, B)), B, 0, stream_>>>(d_, relmap_);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream_));
@@ -1047,8 +1247,12 @@ class EngineT final : public EngineBase {
     }
 
     // ---- launches -------------------------------------------------------------
-    void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0) {
-        k_clump<R><<<cdiv(K_ + S_, CL_THREADS), CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond);
+    void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0,
+                      cudaGraphConditionalHandle loop = 0, int use_loop = 0) {
+        const int g = cdiv(K_ + S_, CL_THREADS);
+        if (clump_batch_ == 1) k_clump<R, 1><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        else if (clump_batch_ == 4) k_clump<R, 4><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        else k_clump<R, 2><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         CK(cudaGetLastError());
         if (!capturing_) launches_ += 1;
     }
@@ -1060,6 +1264,9 @@ class EngineT final : public EngineBase {
         if (exp) {
             CK(cudaMemsetAsync(h_.xfcn, 0, (size_t)h_.cap * sizeof(R4<R>), stream_));
             CK(cudaMemsetAsync(h_.xcpt, 0, (size_t)h_.cap * sizeof(double4), stream_));
+            // wall and intruder parts: k_boundary writes its candidates only
+            CK(cudaMemsetAsync((R4<R>*)h_.xparts + 2 * (size_t)N_, 0, 4 * (size_t)N_ * sizeof(R4<R>), stream_));
+            CK(cudaMemsetAsync(h_.xintr, 0, 4 * (size_t)N_ * sizeof(R4<R>), stream_));
         }
         CK(cudaEventRecord(ev_fork_, stream_));
         CK(cudaStreamWaitEvent(stream2_, ev_fork_, 0));
@@ -1067,31 +1274,31 @@ class EngineT final : public EngineBase {
         // dependencies), so only its end mark sits on the critical path
         mark(5, stream2_);
         mark(3, stream2_);
-        if (exp) k_boundary<R, true><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream2_>>>(d_);
-        else k_boundary<R, false><<<cdiv(N_, BD_THREADS), BD_THREADS, 0, stream2_>>>(d_);
+        // grid-stride over the boundary candidates (a device count)
+        const int bg = std::min(sm_count_ * 8, cdiv(N_, BD_THREADS));
+        if (exp) k_boundary<R, true><<<bg, BD_THREADS, 0, stream2_>>>(d_);
+        else k_boundary<R, false><<<bg, BD_THREADS, 0, stream2_>>>(d_);
         mark(4, stream2_);
         CK(cudaEventRecord(ev_join_, stream2_));
-        // grid-stride over the pairs: a fixed grid stays valid as the list grows
-        // grid-stride over the near pairs (a device count); a small scene gets
-        // a small grid so that other scenes' kernels run beside it
-        const int pg = std::min(148 * 12, cdiv(3LL * N_, PR_THREADS));
+        // grid-stride over the near pairs (a device count), so a fixed grid
+        // stays valid as the list grows; a small scene gets a small grid so
+        // that other scenes' kernels run beside it
+        const int pg = std::min(sm_count_ * pair_bps_, cdiv(3LL * N_, PR_THREADS));
         if (exp) k_pairs<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
         else k_pairs<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
         CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
-        const dim3 g(cdiv(N_ * lanes_, CT_THREADS));
-#define NBC_CT(L)                                                                   \
-    if (exp) k_sum<R, L, true><<<g, CT_THREADS, 0, stream_>>>(d_);                 \
-    else k_sum<R, L, false><<<g, CT_THREADS, 0, stream_>>>(d_);
-        if (lanes_ == 1) { NBC_CT(1) }
-        else if (lanes_ == 2) { NBC_CT(2) }
-        else if (lanes_ == 4) { NBC_CT(4) }
-        else if (lanes_ == 16) { NBC_CT(16) }
-        else if (lanes_ == 32) { NBC_CT(32) }
-        else { NBC_CT(8) }
-#undef NBC_CT
         CK(cudaGetLastError());
         mark(6, stream_);
-        if (!capturing_) launches_ += 3;
+        if (!capturing_) launches_ += 2;
+        // the export step also records the per-subsphere pair part
+        if (exp) launch_sum(true);
+    }
+    // per-subsphere totals of the last contact pass into fsum (the clump
+    // pass sums the same slots itself; this runs for getters and exports)
+    void launch_sum(bool exp) {
+        if (exp) k_sum<R, true><<<cdiv(N_, CT_THREADS), CT_THREADS, 0, stream_>>>(d_);
+        else k_sum<R, false><<<cdiv(N_, CT_THREADS), CT_THREADS, 0, stream_>>>(d_);
+        CK(cudaGetLastError());
     }
     // exclusive scan of a[0, n) (or of a[0, *dn) when dn is given, n then
     // bounds it)
@@ -1170,6 +1377,10 @@ class EngineT final : public EngineBase {
         scan(h_.cnt_b, N_ + 1, pl + PL_T1);
         k_near<true, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
         k_commit<<<std::min(cdiv((long long)K_ + S_ + 1, B), 148 * 8), B, 0, stream_>>>(d_);
+        // boundary candidates of the rebuilt scenes (flags, scan, list)
+        k_bflag<false><<<std::min(cdiv((long long)N_ + 1, B), 148 * 16), B, 0, stream_>>>(d_);
+        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
+        k_bflag<true><<<gN, B, 0, stream_>>>(d_);
         k_nprefix<<<1, SC_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
@@ -1248,8 +1459,85 @@ class EngineT final : public EngineBase {
                 if (mark_on(timing_, k))
                     CK(cudaGraphExecEventRecordNodeSetEvent(gexec_[timing_], gev_node_[timing_][k], r[k]));
         }
-        launches_ += 4;
         CK(cudaGraphLaunch(gexec_[timing_], stream_));
+    }
+
+    // Many steps in one graph launch: a while node whose body is one step
+    // (k_clump, the rebuild under an if node, the contact pass).  The step
+    // count goes to the kernel node ahead of the loop; the last block of each
+    // step's k_clump counts it down and ends the loop at zero, or at once
+    // when a rebuild has run out of pair capacity (the host then finishes
+    // that step, as after a per-step graph).  Step graphs with timing event
+    // nodes stay one step per launch (an event node in a loop body would be
+    // overwritten by every iteration).  If the loop graph cannot be built the
+    // engine keeps launching one step per graph.
+    void capture_loop() {
+        loop_tried_ = true;
+        capturing_ = true;
+        capture_timed_ = 0;
+        try {
+            CK(cudaGraphCreate(&graph_loop_, 0));
+            cudaGraphConditionalHandle hw;
+            CK(cudaGraphConditionalHandleCreate(&hw, graph_loop_, 1, cudaGraphCondAssignDefault));
+            CK(cudaStreamBeginCaptureToGraph(stream_, graph_loop_, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+            k_loop_init<<<1, 1, 0, stream_>>>(h_.loop_left, 1);
+            CK(cudaGetLastError());
+            loop_init_node_ = last_captured_node(stream_);
+            cudaGraph_t body = add_conditional(graph_loop_, hw, cudaGraphCondTypeWhile);
+            cudaGraph_t g2 = nullptr;
+            CK(cudaStreamEndCapture(stream_, &g2));
+            cudaGraphConditionalHandle hif;
+            CK(cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault));
+            CK(cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            launch_clump(1, hif, 1, hw, 1);
+            cudaGraph_t rbody = add_conditional(body, hif, cudaGraphCondTypeIf);
+            launch_contact(false);
+            CK(cudaStreamEndCapture(stream_, &g2));
+            CK(cudaStreamBeginCaptureToGraph(stream_, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            launch_rebuild(false);
+            CK(cudaStreamEndCapture(stream_, &g2));
+            CK(cudaGraphInstantiate(&gexec_loop_, graph_loop_, 0));
+        } catch (const CudaError& e) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(stream_, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(stream_, &g);
+            }
+            (void)cudaGetLastError();
+            if (gexec_loop_) cudaGraphExecDestroy(gexec_loop_);
+            if (graph_loop_) cudaGraphDestroy(graph_loop_);
+            gexec_loop_ = nullptr;
+            graph_loop_ = nullptr;
+            loop_error_ = e.what();
+        }
+        capturing_ = false;
+    }
+    // a conditional node after the capture's current dependencies; returns its body
+    cudaGraph_t add_conditional(cudaGraph_t graph, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type) {
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, nullptr, &deps, &ndeps));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = type;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, graph, deps, ndeps, &cp));
+        CK(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+        return cp.conditional.phGraph_out[0];
+    }
+    void launch_loop(int n) {
+        int* left = h_.loop_left;
+        void* args[] = {&left, &n};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void*)k_loop_init;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(1);
+        kp.kernelParams = args;
+        CK(cudaGraphExecKernelNodeSetParams(gexec_loop_, loop_init_node_, &kp));
+        CK(cudaGraphLaunch(gexec_loop_, stream_));
     }
 
     // a graph launch stopped at a rebuild whose pairs did not fit: grow and

@@ -12,6 +12,10 @@ namespace nbc {
 struct NonFinite : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+// a call that is not valid in the engine's state (NBC_ERR_STATE)
+struct StateError : std::logic_error {
+    using std::logic_error::logic_error;
+};
 
 // One batch of scenes resident on one GPU.
 class EngineBase {
@@ -34,6 +38,7 @@ class EngineBase {
     virtual void get_pairs(int s, int* np, int* lpa, int* lpb) = 0;
     virtual void get_rows(int s, int bl, int* anei, int* ng, int* ni) = 0;
     virtual void get_chain(int s, int bl, double* fcn, double* cpt) = 0;
+    virtual void get_pair_forces(int s, int* np, double* fcn) = 0;
     virtual void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) = 0;
     virtual void get_intruder_history(int s, int count, double* out) = 0;
     virtual void info(double* bytes, double* ms) = 0;
@@ -41,6 +46,11 @@ class EngineBase {
     virtual void timing_enable(int level) = 0;
     virtual void timing_read(double* contact_ms, int* contact_launches, long long* kernel_launches, int* rebuilds) = 0;
     virtual void timing_phases(double* phase_ms) = 0;
+    // exact checkpoint of the state after the last completed step (see
+    // EngineT::checkpoint_save); load into an engine made from the same
+    // scenes and options
+    virtual std::vector<char> checkpoint_save() = 0;
+    virtual void checkpoint_load(const char* data, size_t bytes) = 0;
 };
 
 EngineBase* make_engine(const std::vector<const nbc_scene_desc*>& scenes, const nbc_options& opt);

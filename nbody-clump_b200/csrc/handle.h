@@ -34,6 +34,8 @@ nbc_status guard(F&& f) {
         return NBC_OK;
     } catch (const NonFinite& e) {
         return fail(NBC_ERR_NONFINITE, e.what());
+    } catch (const StateError& e) {
+        return fail(NBC_ERR_STATE, e.what());
     } catch (const std::bad_alloc& e) {
         return fail(NBC_ERR_MEMORY, e.what());
     } catch (const std::invalid_argument& e) {

@@ -10,10 +10,11 @@
 //                ranges, reorder, count/scan/fill of the half pair list in
 //                the reference's traversal order, back references, history
 //                carry, clump member lists.
-//   k_pairs      per listed pair: overlap test, the law once for both
-//                subspheres of a touching pair, the new spring history
-//   k_boundary   per subsphere: walls and intruder (beside k_pairs)
-//   k_sum        per subsphere: its pair slots, then walls and intruder
+//   k_pairs      per near pair: overlap test, the law once for both
+//                subspheres of a touching pair, the new spring history, the
+//                force and torque on each side into its near-row slot
+//   k_boundary   per boundary candidate: walls and intruder (beside k_pairs)
+//   (the next step's k_clump sums each member's slots and boundary force)
 #pragma once
 #include "nbc_dev.cuh"
 #include "nbc_math.cuh"
@@ -24,6 +25,28 @@ constexpr double FIX_F = 1099511627776.0;    // 2^40: fixed-point scale of intru
 constexpr double FIX_T = 17592186044416.0;   // 2^44: fixed-point scale of intruder torque sums
 constexpr int IDX_MASK = 0x7fffffff;
 constexpr int INTRA = (int)0x80000000u;
+
+// The contact slots of one subsphere (its near front entries, then its near
+// back entries, in row order; SumContForce_clump, src/dem_force_clump.cu:
+// 165-191, sums a subsphere's front entries, then its back entries).
+template <typename R>
+__device__ __forceinline__ void slot_sum(const R4<R>* __restrict__ fs, const R4<R>* __restrict__ bs, size_t cap,
+                                         int rs, int re, int bs0, int be, V3<R>& F, V3<R>& T) {
+    F = v3<R>(0, 0, 0);
+    T = F;
+    // not unrolled: a subsphere has a few near entries at most, and unrolled
+    // copies cost the clump pass registers (and warps per SM)
+#pragma unroll 1
+    for (int e = rs; e < re; e++) {
+        F = F + xyz<R>(fs[e]);
+        T = T + xyz<R>(fs[cap + e]);
+    }
+#pragma unroll 1
+    for (int e = bs0; e < be; e++) {
+        F = F + xyz<R>(bs[e]);
+        T = T + xyz<R>(bs[cap + e]);
+    }
+}
 
 // ===========================================================================
 // clump pass
@@ -60,18 +83,27 @@ __device__ __forceinline__ bool scene_post(const SceneDyn& y, int post, int L) {
 }
 constexpr int CL_THREADS = 128;
 constexpr int CL_WARPS = CL_THREADS / 32;
-constexpr int CL_CHUNK = 128;   // members staged in shared memory per warp at a time
-
-template <typename R>
-__global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp, int do_pre,
-                                                      cudaGraphConditionalHandle cond, int use_cond) {
+// J: members each lane keeps in flight per batch of loads (a launch shape
+// the autotuner picks; results do not depend on it); a warp stages 32 J
+// members in shared memory at a time.  J <= 2 fits 128 registers (4 blocks,
+// 16 warps per SM) with a few bytes of spill; J = 4 keeps 3 blocks per SM.
+template <typename R, int J>
+__global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev* __restrict__ dp, int do_pre,
+                                                      cudaGraphConditionalHandle cond, int use_cond,
+                                                      cudaGraphConditionalHandle loop, int use_loop) {
+    constexpr int CL_CHUNK = 32 * J;
     __shared__ double s_mf[CL_WARPS][6][CL_CHUNK];   // member force xyz, torque xyz
     __shared__ double s_cl[CL_WARPS][13][32];        // clump position, velocity, angular velocity, quaternion
     __shared__ int s_ms[CL_WARPS][33];               // member-list offsets of the warp's clumps
     __shared__ int s_sc[CL_WARPS][32];               // scene of each of the warp's clumps
     __shared__ int s_pre[CL_WARPS][32];              // the clump's scene takes this step
     const Dev& d = *dp;
-    if (*d.halt) return;
+    if (*d.halt) {
+        // a rebuild ran out of pair capacity: the host finishes that step, so
+        // a device-side step loop ends here
+        if (use_loop && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(loop, 0u);
+        return;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k0 = (blockIdx.x * CL_WARPS + warp) * 32;
     const int t = k0 + lane;
@@ -122,43 +154,60 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
         const double Dt = P.dt;
         V3<double> F, T;
         if (post) {
-            // ---- member sums, CL_CHUNK members of the warp's range at a time
-            const R4<R>* __restrict__ fs = (const R4<R>*)d.fsum;
-            const size_t N = (size_t)d.N;
-            constexpr int J = CL_CHUNK / 32;
+            // ---- member sums, CL_CHUNK members of the warp's range at a time:
+            // each member's contact slots (the contact pass of the last step),
+            // its wall and intruder force, and its lever-arm torque
+            const R4<R>* __restrict__ fsl = (const R4<R>*)d.nfs;
+            const R4<R>* __restrict__ bsl = (const R4<R>*)d.nbs;
+            const R4<R>* __restrict__ fbd = (const R4<R>*)d.fbnd;
+            const int* __restrict__ nrow = d.nrow;
+            const int* __restrict__ nbrow = d.nbrow;
+            const uint16_t* __restrict__ bbits = d.bbits;
+            const size_t N = (size_t)d.N, cap = (size_t)d.cap;
             F = v3(0.0, 0.0, 0.0);
             T = F;
             for (int c0 = M0; c0 < M1; c0 += CL_CHUNK) {
-                int idx[J];
+                int idx[J], own[J];
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     const int m = c0 + 32 * j + lane;
                     idx[j] = m < M1 ? mem_idx[m] : -1;
+                    own[j] = m < M1 ? owner(m) : 0;
                 }
                 double4 ps[J];
-                R4<R> f4[J], t4[J];
+                int r0[J], r1[J], q0[J], q1[J];
+                uint16_t bb[J];
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     const int i = idx[j] < 0 ? 0 : idx[j];
+                    const int ro = i + s_sc[warp][own[j]];
                     ps[j] = posr[i];
-                    f4[j] = fs[i];
-                    t4[j] = fs[N + i];
+                    r0[j] = nrow[ro];
+                    r1[j] = nrow[ro + 1];
+                    q0[j] = nbrow[ro];
+                    q1[j] = nbrow[ro + 1];
+                    bb[j] = bbits[i];
                 }
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     if (idx[j] < 0) continue;
-                    const int kk = owner(c0 + 32 * j + lane);
-                    const R4<R> a = f4[j], b = t4[j];
+                    const int kk = own[j];
+                    V3<R> fr, tr;
+                    slot_sum<R>(fsl, bsl, cap, r0[j], r1[j], q0[j], q1[j], fr, tr);
+                    if (bb[j]) {
+                        fr = fr + xyz<R>(fbd[idx[j]]);
+                        tr = tr + xyz<R>(fbd[N + idx[j]]);
+                    }
                     const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
                                             ps[j].z - s_cl[warp][2][kk]);
-                    const V3<double> f = v3((double)a.x, (double)a.y, (double)a.z);
+                    const V3<double> f = v3((double)fr.x, (double)fr.y, (double)fr.z);
                     const int q = 32 * j + lane;
                     s_mf[warp][0][q] = f.x;
                     s_mf[warp][1][q] = f.y;
                     s_mf[warp][2][q] = f.z;
-                    s_mf[warp][3][q] = (double)b.x + (r.y * f.z - r.z * f.y);
-                    s_mf[warp][4][q] = (double)b.y + (r.z * f.x - r.x * f.z);
-                    s_mf[warp][5][q] = (double)b.z + (r.x * f.y - r.y * f.x);
+                    s_mf[warp][3][q] = (double)tr.x + (r.y * f.z - r.z * f.y);
+                    s_mf[warp][4][q] = (double)tr.y + (r.z * f.x - r.x * f.z);
+                    s_mf[warp][5][q] = (double)tr.z + (r.x * f.y - r.y * f.x);
                 }
                 __syncwarp();
                 if (isc) {
@@ -252,7 +301,7 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             double4* __restrict__ posw = d.posr;
             // J members per lane at a time: all indices, then all member
             // records, in flight together
-            constexpr int JP = CL_CHUNK / 32;
+            constexpr int JP = J;
             for (int c0 = M0; c0 < M1; c0 += 32 * JP) {
                 int idx[JP];
 #pragma unroll
@@ -352,9 +401,18 @@ __global__ void __launch_bounds__(CL_THREADS) k_clump(const Dev* __restrict__ dp
             *d.kc_done = 0;
             if (do_pre) *d.lstep = L + 1;
             if (use_cond) cudaGraphSetConditional(cond, atomicAdd(d.any_rebuild, 0) ? 1u : 0u);
+            if (use_loop) {
+                const int left = *d.loop_left - 1;
+                *d.loop_left = left;
+                cudaGraphSetConditional(loop, left > 0 ? 1u : 0u);
+            }
         }
     }
 }
+
+// The steps a graph launch with a device-side step loop takes (the first
+// node of that graph; its argument is set before each launch).
+static __global__ void k_loop_init(int* __restrict__ left, int n) { *left = n; }
 
 // ===========================================================================
 // broad phase
@@ -1307,7 +1365,11 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
             if (k < be) q = bpair[k];
             const bool nr = q >= 0 && nearf[q];
             const unsigned m = __ballot_sync(gm, nr) >> gshift;
-            if (FILL && nr) d.nbq[rb + nb + __popc(m & lt)] = q;
+            if (FILL && nr) {
+                const int e = rb + nb + __popc(m & lt);
+                d.nbq[e] = q;
+                d.nbpos[q] = e;
+            }
             nb += __popc(m);
         }
         if (!FILL && lane == 0) {
@@ -1323,16 +1385,71 @@ static __global__ void __launch_bounds__(SC_THREADS) k_nprefix(const Dev* __rest
     __shared__ int sh[SC_THREADS / 32];
     const Dev& d = *dp;
     if (*d.halt) return;
-    int run = 0;
+    int run = 0, brun = 0;
     for (int b = 0; b < d.S; b += SC_THREADS) {
         const int s = b + threadIdx.x;
-        const int v = s < d.S ? d.dyn[s].nnear : 0;
         int tot;
-        const int ex = block_excl_scan(v, sh, tot);
+        const int ex = block_excl_scan(s < d.S ? d.dyn[s].nnear : 0, sh, tot);
         if (s < d.S) d.nprefix[s] = run + ex;
         run += tot;
+        const int bx = block_excl_scan(s < d.S ? d.dyn[s].nbound : 0, sh, tot);
+        if (s < d.S) d.bprefix[s] = brun + bx;
+        brun += tot;
     }
-    if (threadIdx.x == 0) d.nprefix[d.S] = run;
+    if (threadIdx.x == 0) {
+        d.nprefix[d.S] = run;
+        d.bprefix[d.S] = brun;
+    }
+}
+
+// Boundary candidates.  Walls do not move (their velocity enters only the
+// contact law), and between two rebuilds of a scene every subsphere stays
+// within Thresh of where it was at the rebuild, so a subsphere farther than
+// 2 Thresh from every wall region at a rebuild cannot touch a wall before
+// the next one.  At each rebuild k_bflag flags, per rebuilt subsphere (new
+// order), whether it is within that margin of a wall -- every subsphere of a
+// scene with an intruder is a candidate, the intruder moves -- and clears
+// the wall contact bits of the others (they are not in contact now); the
+// FILL pass lists the candidates in the scene's range of bidx, and
+// k_boundary visits only them.  FILL = false writes the flags into cnt_b of
+// the rebuilt concatenation (free after k_commit); FILL = true writes the
+// list at the scanned offsets and the scene's count.
+template <bool FILL>
+__global__ void k_bflag(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
+    NBC_GRID_STRIDE(t, T + (FILL ? 0 : 1)) {
+        if (!FILL && t == T) { d.cnt_b[T] = 0; continue; }
+        const PlanItem it = plan_item(d, ns, t);
+        const int i = it.i, s = it.s;
+        const ScenePar& P = d.par[s];
+        if (FILL) {
+            const int t0 = d.psub[it.k];
+            const int c = d.cnt_b[t] - d.cnt_b[t0];
+            if (d.cnt_b[t + 1] - d.cnt_b[t]) d.bidx[P.sub_off + c] = i;
+            if (i == P.sub_off + P.nsub - 1) d.dyn[s].nbound = d.cnt_b[t + 1] - d.cnt_b[t0];
+            continue;
+        }
+        bool cand = P.has_intr;
+        if (!cand && P.wall != WALL_NONE) {
+            const double4 pp = d.posr[i];
+            const double m = 2.0 * P.thresh * (1.0 + 1e-6) + 1e-12;
+            const double r = pp.w + m;
+            const double ex = pp.x - P.w_c[0], ey = pp.y - P.w_c[1], ez = pp.z - P.w_c[2];
+            if (P.wall == WALL_CUBE) {
+                cand = fabs(ex) + r >= P.w_half[0] * (1 - 1e-9) || fabs(ey) + r >= P.w_half[1] * (1 - 1e-9) ||
+                       fabs(ez) + r >= P.w_half[2] * (1 - 1e-9);
+            } else {
+                const double ax = ex * P.cyl_axis[0] + ey * P.cyl_axis[1] + ez * P.cyl_axis[2];
+                const double rr = ex * ex + ey * ey + ez * ez - ax * ax;
+                const double in = P.cyl_R - r;
+                cand = fabs(ax) + r >= P.cyl_H * (1 - 1e-9) || in <= 0 || rr >= in * in * (1 - 1e-9);
+            }
+        }
+        if (!cand) d.bbits[i] = 0;
+        d.cnt_b[t] = cand ? 1 : 0;
+    }
 }
 
 // Finishes a rebuild: per-clump member lists of the rebuilt scenes in
@@ -1374,7 +1491,8 @@ static __global__ void k_commit(const Dev* __restrict__ dp) {
 template <typename R>
 __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* __restrict__ oh,
                            const uint8_t* __restrict__ ot, const uint8_t* __restrict__ onear,
-                           const int* __restrict__ onfp, const int* __restrict__ onbq, int ocap,
+                           const int* __restrict__ onfp, const int* __restrict__ onbq,
+                           const int* __restrict__ onbpos, int ocap,
                            const int4* __restrict__ map, int total) {
     const Dev& d = *dp;
     const int hg = *d.hgen;
@@ -1401,6 +1519,7 @@ __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* 
         d.nearf[pn] = onear[po];
         d.nfp[pn] = onfp[po] + (m.y - m.x);   // slots past the near count carry nothing
         d.nbq[pn] = onbq[po] + (m.y - m.x);
+        d.nbpos[pn] = onear[po] ? onbpos[po] + (m.y - m.x) : -1;
         if (f) {
             Hn[pn] = Ho[po];
             Hn[cap + pn] = Ho[oc + po];
@@ -1650,23 +1769,10 @@ __device__ __forceinline__ void hist_write(R4<R>* H, size_t cap, size_t q, V3<R>
     ((R*)(H + 2 * cap))[q] = hr.z;
 }
 
-template <int LANES>
-__device__ __forceinline__ unsigned group_mask() {
-    if (LANES == 32) return 0xffffffffu;
-    const int g = (threadIdx.x & 31) / LANES;
-    return ((1u << LANES) - 1u) << (g * LANES);
-}
-
-template <typename R, int LANES>
-__device__ __forceinline__ R group_sum(R v, unsigned mask) {
-    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
-    return v;
-}
-
 constexpr int CT_THREADS = 256;
 constexpr int BD_THREADS = 128;
 
-// Walls and intruder, one thread per subsphere: the face tests of
+// Walls and intruder, one thread per boundary candidate: the face tests of
 // CubeWallInteraction_clump_cuk (src/dem_force_cube_wall_clump.cu:185-298),
 // the region tests of CylindWallInteraction_cuk (src/dem_force_cylind_wall.cu:
 // 152-237) with clump kinematics, PrePenetrator / GetSphereIntruderContact /
@@ -1675,12 +1781,25 @@ constexpr int BD_THREADS = 128;
 // Writes the summed boundary force/torque where some slot is in contact and
 // the slot mask; the intruder totals go to fixed-point accumulators.
 template <typename R, bool EXPORT>
+__device__ __forceinline__ void boundary_one(const Dev& d, int i, int s);
+
+template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int i = blockIdx.x * BD_THREADS + threadIdx.x;
-    if (i >= d.N) return;
-    const int s = d.sid[i];
+    const int S = d.S;
+    const int* __restrict__ bpre = d.bprefix;
+    const int nb = bpre[S];
+    for (int w = blockIdx.x * BD_THREADS + threadIdx.x; w < nb; w += gridDim.x * BD_THREADS) {
+        // work item w: boundary candidate w - bprefix[s] of scene s
+        const int s = S == 1 ? 0 : plan_find(bpre, S, w);
+        const int i = d.bidx[d.par[s].sub_off + (w - bpre[s])];
+        boundary_one<R, EXPORT>(d, i, s);
+    }
+}
+
+template <typename R, bool EXPORT>
+__device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
     const double4 pp = d.posr[i];   // issued before the scene's flag is known
     const uint16_t bb_old = d.bbits[i];
     if (d.has_stops && d.dyn[s].frozen) return;   // a scene past its stop stands still
@@ -1903,24 +2022,29 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
     return a.w + b.w - sqrt(d2) > 0.0;
 }
 
-// Pairs, one thread per near owner pair (grid-stride, so a captured launch
+// Pairs, one thread per near front entry (grid-stride, so a captured launch
 // covers a list that has grown since): the overlap test, and for touching
 // pairs the law once (ContactForce_clump_cuk, src/dem_force_clump.cu:3-163,
-// for both particles of the pair), the owner's new spring history, and the
-// force and torque on each of the two subspheres into per-pair slots.
-// k_sum adds the slots per subsphere in a fixed order.
+// for both particles of the pair) and the owner's new spring history.  The
+// force and torque on the owner go to the entry's front slot, those on the
+// partner to the pair's near back slot (zero when the pair does not touch),
+// so the clump pass sums every subsphere's contacts from two contiguous slot
+// ranges in row order.  Block 0 marks this step's closing half-kick as
+// pending.
 constexpr int PR_THREADS = 256;
 
 template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
     const int lc = *d.lcur, hg = *d.hgen;
     const PairList& Lst = d.L[lc & 1];
     const int S = d.S;
     const int* __restrict__ npre = d.nprefix;
     const int np = npre[S];
     const int* __restrict__ nfp = d.nfp;
+    const int* __restrict__ nbpos = d.nbpos;
     const int* __restrict__ nbr = Lst.nbr;
     const int* __restrict__ own = Lst.own;
     const double4* __restrict__ posr = d.posr;
@@ -1931,20 +2055,34 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     R4<R>* __restrict__ Ho = (R4<R>*)d.H[(hg + 1) & 1];
     const uint8_t* __restrict__ ti = d.touch[hg & 1];
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
-    R4<R>* __restrict__ ct = (R4<R>*)d.ctb;
+    R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
+    R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
+    const R4<R> zero = pack<R>(v3<R>(0, 0, 0), R(0));
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
-        // work item w: near pair w - nprefix[s] of scene s
+        // work item w: near front entry w - nprefix[s] of scene s
         const int s = S == 1 ? 0 : plan_find(npre, S, w);
         const SceneDyn& ys = d.dyn[s];
         if (d.has_stops && ys.frozen) continue;
-        const int p = nfp[ys.pair_off + (w - npre[s])];
+        const int ef = ys.pair_off + (w - npre[s]);
+        const int p = nfp[ef];
+        const int eb = nbpos[p];
         const int jr = nbr[p];
-        if (jr < 0) { to[p] = 0; continue; }  // pair inside one clump (src/dem_force_clump.cu:18-19)
         const int i = own[p];
         Body<R> a, b;
-        a.p = posr[i];
-        b.p = posr[jr];
-        if (!overlaps(a.p, b.p)) { to[p] = 0; continue; }
+        bool on = jr >= 0;   // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)
+        if (on) {
+            a.p = posr[i];
+            b.p = posr[jr];
+            on = overlaps(a.p, b.p);
+        }
+        if (!on) {
+            to[p] = 0;
+            fs[ef] = zero;
+            fs[cap + ef] = zero;
+            bs[eb] = zero;
+            bs[cap + eb] = zero;
+            continue;
+        }
         load_kin<R>(kin, N, i, a);
         load_kin<R>(kin, N, jr, b);
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
@@ -1960,10 +2098,10 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         pair_contact2<R>(L, (R)P.cohesion, a, b, hs, hr, ht, fa, ta, tb, o, Ap, nd);
         hist_write<R>(Ho, cap, p, o.hs, o.ht, o.hr);
         to[p] = 1;
-        ct[p] = pack<R>(fa, R(0));
-        ct[cap + p] = pack<R>(ta, R(0));
-        ct[2 * cap + p] = pack<R>(-fa, R(0));
-        ct[3 * cap + p] = pack<R>(tb, R(0));
+        fs[ef] = pack<R>(fa, R(0));
+        fs[cap + ef] = pack<R>(ta, R(0));
+        bs[eb] = pack<R>(-fa, R(0));
+        bs[cap + eb] = pack<R>(tb, R(0));
         if (EXPORT) {
             R4<R>* xf = (R4<R>*)d.xfcn;
             double4* xc = (double4*)d.xcpt;
@@ -1973,63 +2111,45 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     }
 }
 
-// Per subsphere, one lane group: the pair slots of its near front entries,
-// then those of its near back entries (by their pair index), summed in
-// registers, then the wall and intruder force of k_boundary where a boundary
-// is touched; the sum written once (the force and torque k_clump reduces).
-template <typename R, int LANES, bool EXPORT>
+// The contact force and torque on subsphere i: its contact slots, then the
+// wall and intruder force where a boundary slot is in contact -- the sum the
+// clump pass forms, so the per-subsphere totals read back are bitwise the
+// ones it integrates.
+template <typename R>
+__device__ __forceinline__ void contact_sum(const Dev& d, int i, int s, V3<R>& F, V3<R>& T, V3<R>* pairF = nullptr,
+                                            V3<R>* pairT = nullptr) {
+    const size_t N = (size_t)d.N;
+    slot_sum<R>((const R4<R>*)d.nfs, (const R4<R>*)d.nbs, (size_t)d.cap, d.nrow[i + s], d.nrow[i + s + 1],
+                d.nbrow[i + s], d.nbrow[i + s + 1], F, T);
+    if (pairF) { *pairF = F; *pairT = T; }
+    if (d.bbits[i]) {
+        const R4<R>* fb = (const R4<R>*)d.fbnd;
+        F = F + xyz<R>(fb[i]);
+        T = T + xyz<R>(fb[N + i]);
+    }
+}
+
+// Per subsphere, on request (the force getters and the export step): the
+// totals of contact_sum into fsum, the pair part into the export record.
+template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(CT_THREADS) k_sum(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int grp = (blockIdx.x * CT_THREADS + threadIdx.x) / LANES, lane = threadIdx.x % LANES;
-    const int i = grp;
+    const int i = blockIdx.x * CT_THREADS + threadIdx.x;
     if (i >= d.N) return;
-    const unsigned mask = group_mask<LANES>();
-    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-    const int hg = *d.hgen;
     const size_t N = (size_t)d.N;
-    const size_t cap = (size_t)d.cap;
-    const uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
-    const R4<R>* __restrict__ ct = (const R4<R>*)d.ctb;
-    const int* __restrict__ nfp = d.nfp;
-    const int* __restrict__ nbq = d.nbq;
-    V3<R> F = v3<R>(0, 0, 0), T = F;
     const int s = d.S == 1 ? 0 : d.sid[i];
-    const int rs = d.nrow[i + s], re = d.nrow[i + s + 1];   // issued before the scene's flag is known
-    const int bs = d.nbrow[i + s], be = d.nbrow[i + s + 1];
     if (d.has_stops && d.dyn[s].frozen) return;
-    for (int e = rs + lane; e < re; e += LANES) {
-        const int k = nfp[e];
-        if (!to[k]) continue;
-        F = F + xyz<R>(ct[k]);
-        T = T + xyz<R>(ct[cap + k]);
+    V3<R> F, T, pF, pT;
+    contact_sum<R>(d, i, s, F, T, &pF, &pT);
+    if (EXPORT) {
+        R4<R>* xp = (R4<R>*)d.xparts;
+        xp[i] = pack<R>(pF, R(0));
+        xp[N + i] = pack<R>(pT, R(0));
     }
-    for (int e = bs + lane; e < be; e += LANES) {
-        const int q = nbq[e];
-        if (!to[q]) continue;
-        F = F + xyz<R>(ct[2 * cap + q]);
-        T = T + xyz<R>(ct[3 * cap + q]);
-    }
-    F.x = group_sum<R, LANES>(F.x, mask); F.y = group_sum<R, LANES>(F.y, mask); F.z = group_sum<R, LANES>(F.z, mask);
-    T.x = group_sum<R, LANES>(T.x, mask); T.y = group_sum<R, LANES>(T.y, mask); T.z = group_sum<R, LANES>(T.z, mask);
-    if (lane == 0) {
-        if (EXPORT) {
-            R4<R>* xp = (R4<R>*)d.xparts;
-            xp[i] = pack<R>(F, R(0));
-            xp[N + i] = pack<R>(T, R(0));
-        }
-        if (d.bbits[i]) {
-            const R4<R>* fb = (const R4<R>*)d.fbnd;
-            F = F + xyz<R>(fb[i]);
-            T = T + xyz<R>(fb[N + i]);
-        }
-        R4<R>* fs = (R4<R>*)d.fsum;
-        fs[i] = pack<R>(F, R(0));
-        fs[N + i] = pack<R>(T, R(0));
-        if (!(isfinite((double)F.x) && isfinite((double)F.y) && isfinite((double)F.z) &&
-              isfinite((double)T.x) && isfinite((double)T.y) && isfinite((double)T.z)))
-            atomicOr(&d.dyn[s].err, ERR_NONFINITE);
-    }
+    R4<R>* fo = (R4<R>*)d.fsum;
+    fo[i] = pack<R>(F, R(0));
+    fo[N + i] = pack<R>(T, R(0));
 }
 
 }  // namespace nbc

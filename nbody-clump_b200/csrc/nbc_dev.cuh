@@ -47,7 +47,6 @@ struct ScenePar {
     int loff[MAX_LEVELS];
     // ranges
     int sub_off, nsub, clump_off, nclump;
-    int cblk_off, cblk_n;  // contact-kernel blocks of this scene
     int bl;                // BranchLmtLen of the reference (row capacity of the export)
     // walls
     int wall;       // WALL_*
@@ -71,6 +70,7 @@ struct SceneDyn {
     int pair_off;                  // first pair slot of this scene's region of the pair buffers
     int pcap;                      // pair slots of that region (set by the host, grown on overflow)
     int nnear;                     // near pairs of the current list (see k_near)
+    int nbound;                    // boundary candidates of the current list (see k_bflag)
     int stop;                      // steps the scene takes before it stands still (0: no limit)
     int frozen;                    // the scene took no step at the last k_clump (its stop was reached)
     long long ifix[6];             // fixed-point sums of intruder force (2^-40 N) and torque (2^-44 N m)
@@ -105,8 +105,6 @@ struct Dev {
     int cap;          // pair capacity of each list buffer
     int cells;        // total global cells (sum over scenes)
     int sort_bits;    // key bits for the radix sort
-    int cblocks;      // total contact-kernel blocks
-    int nthreads_sub; // subsphere-parallel grid stride helpers
     int has_stops;    // some scene has a step limit (nbc_set_scene_steps): the kernels check for frozen scenes
     ScenePar* par;
     SceneDyn* dyn;
@@ -126,7 +124,8 @@ struct Dev {
     void* kin;        void* kin2;        // Real4 [3][N]: clump velocity + mass, clump angular velocity, world arm
     void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][3][N] boundary histories (Dv, Dt, Dr)
     uint16_t* bbits;  uint16_t* bbits2;  // [N] boundary slots in contact at the last step
-    void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder)
+    void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder),
+                      // written on request only (getters, export): the clump pass sums the slots itself
     void* fbnd;       // Real4 [2][N]: wall + intruder force and torque, valid where bbits != 0
     // clumps
     double4* cpos;    // xyz
@@ -168,7 +167,13 @@ struct Dev {
     int* lcur;        // index of the current list (0)
     void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
-    void* ctb;        // Real4 [4][cap]: per pair force and torque on the owner, then on the partner
+    // contact slots, one per near row entry (see k_near), written by every
+    // contact pass (zero for a pair that does not touch) and summed by the
+    // next clump pass in row order: front entries hold the force and torque
+    // on the row's subsphere as owner, back entries as partner
+    void* nfs;        // Real4 [2][cap]: force, then torque, per near front entry
+    void* nbs;        // Real4 [2][cap]: force, then torque, per near back entry
+    int* nbpos;       // [cap] the near back entry of each near pair
     // near rows (the entries that can touch before the next rebuild)
     // (kept in each scene's pair region like the list: rows [N+S] with
     // absolute slots, one row array per scene with its end entry)
@@ -177,11 +182,14 @@ struct Dev {
     int* nfp;         // [cap] near front entries: pair slot
     int* nbq;         // [cap] near back entries: pair slot
     int* nprefix;     // [S+1] prefix over the scenes of their near pairs (the contact pass's work items)
+    int* bidx;        // [N] boundary candidates of scene s at [sub_off, sub_off + nbound) (see k_bflag)
+    int* bprefix;     // [S+1] prefix over the scenes of their boundary candidates (k_boundary's work items)
     uint8_t* nearf;   // [cap] pair can touch before the next rebuild
     int* hgen;        // history generation: read H[hgen&1], write H[(hgen+1)&1]
     int* gstep;       // steps started by k_clump (counts steps across graph launches)
     int* kc_done;     // blocks of k_clump finished (last-block detection)
     int* lstep;       // steps started by k_clump, counted by its last block (per-scene stops)
+    int* loop_left;   // steps left in a graph launch with a device-side step loop
     // export (per pair), written by the export variant of the contact kernel
     void* xfcn;       // Real4 [cap] normal force on the owner (CacheFcn)
     void* xcpt;       // double4 [cap] contact point (CacheCpt)
@@ -190,7 +198,6 @@ struct Dev {
     // intruder force history ring (per scene), reaction force and torque
     double* ring;     // [S][ring_len][6]
     int ring_len;
-    int* sblk_scene;  // [cblocks] scene of each contact block
 };
 
 }  // namespace nbc

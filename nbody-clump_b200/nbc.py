@@ -88,17 +88,20 @@ def with_levels(scene: dict, max_levels=6) -> dict:
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("lanes", C.c_int), ("use_graph", C.c_int),
-                ("device", C.c_int), ("pair_slack", C.c_double), ("search_lanes", C.c_int)]
+                ("device", C.c_int), ("pair_slack", C.c_double), ("search_lanes", C.c_int),
+                ("clump_batch", C.c_int), ("pair_blocks", C.c_int)]
 
 
 EXPORTED = [
     "nbc_last_error", "nbc_default_options", "nbc_open", "nbc_run", "nbc_create", "nbc_destroy",
     "nbc_step", "nbc_step_export", "nbc_sync", "nbc_num_scenes", "nbc_scene_stats", "nbc_contact_counts",
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
-    "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_intruder",
+    "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_pair_forces",
+    "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
     "nbc_timing_phases",
     "nbc_engine_info", "nbc_set_scene_steps", "nbc_cell_sort_noalloc", "nbc_choose_levels",
+    "nbc_checkpoint_write", "nbc_checkpoint_read", "nbc_autotune",
     "nbc_batch_create", "nbc_batch_step", "nbc_batch_engine", "nbc_batch_destroy",
     "nbc_server_create", "nbc_server_submit", "nbc_server_advance", "nbc_server_result",
     "nbc_server_release", "nbc_server_memory", "nbc_server_destroy", "nbc_server_set_cohort",
@@ -205,19 +208,15 @@ def scene_desc(scene: dict):
 class Engine:
     """A batch of scenes resident on one GPU."""
 
-    def __init__(self, scenes, precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0,
-                 search_lanes=0):
+    def __init__(self, scenes, precision="mixed", use_graph=True, device=0, pair_slack=0.0,
+                 search_lanes=0, clump_batch=0, pair_blocks=0, tuned=None):
         L = lib()
         self._descs = [scene_desc(s) for s in scenes]
         self.N = [int(s["params"]["NumberBody"]) for s in scenes]
         self.K = [int(s["params"]["ClumpNum"]) for s in scenes]
         self.BL = [int(s["params"]["BranchLmtLen"]) for s in scenes]
         arr = (C.POINTER(SceneDesc) * len(scenes))(*[C.pointer(d) for d, _ in self._descs])
-        o = Options()
-        L.nbc_default_options(C.byref(o))
-        o.precision, o.lanes, o.use_graph, o.device = PREC[precision], lanes, int(use_graph), device
-        o.pair_slack = pair_slack
-        o.search_lanes = search_lanes
+        o = _options(precision, use_graph, device, pair_slack, search_lanes, clump_batch, pair_blocks, tuned)
         h = C.c_void_p()
         _check(L.nbc_create(arr, len(scenes), C.byref(o), C.byref(h)))
         self.h = h
@@ -351,6 +350,24 @@ class Engine:
         _check(lib().nbc_get_chain(self.h, s, bl, _p(f), _p(c)))
         return f, c
 
+    def checkpoint(self, path):
+        """nbc_checkpoint_write: the exact state after the last step."""
+        _check(lib().nbc_checkpoint_write(self.h, os.fsencode(path)))
+
+    def restore(self, path):
+        """nbc_checkpoint_read into this engine (made from the same scenes and
+        precision); stepping on continues the saved run bit for bit."""
+        _check(lib().nbc_checkpoint_read(self.h, os.fsencode(path)))
+
+    def pair_forces(self, s=0):
+        """After step_export: the normal force on the owner of every listed
+        pair, in list order (zero where the pair does not touch)."""
+        n = C.c_int(0)
+        _check(lib().nbc_get_pair_forces(self.h, s, C.byref(n), None))
+        f = np.zeros((n.value, 3))
+        _check(lib().nbc_get_pair_forces(self.h, s, C.byref(n), _p(f)))
+        return f
+
     def intruder(self, s=0):
         o = {k: np.zeros(3) for k in ("pos", "vel", "reaction", "torque")}
         st = C.c_int()
@@ -395,20 +412,57 @@ class Engine:
         return {"device_bytes": b.value, "last_step_ms": ms.value}
 
 
-def _options(precision="mixed", lanes=0, use_graph=True, device=0, pair_slack=0.0, search_lanes=0):
+TUNED_KEYS = ("search_lanes", "clump_batch", "pair_blocks")
+
+
+def _options(precision="mixed", use_graph=True, device=0, pair_slack=0.0, search_lanes=0, clump_batch=0,
+             pair_blocks=0, tuned=None):
+    """nbc_options; `tuned` (a dict from autotune) overrides the launch shapes."""
     o = Options()
     lib().nbc_default_options(C.byref(o))
-    o.precision, o.lanes, o.use_graph, o.device = PREC[precision], lanes, int(use_graph), device
+    o.precision, o.use_graph, o.device = PREC[precision], int(use_graph), device
     o.pair_slack = pair_slack
-    o.search_lanes = search_lanes
+    o.search_lanes, o.clump_batch, o.pair_blocks = search_lanes, clump_batch, pair_blocks
+    for k in TUNED_KEYS:
+        if tuned and k in tuned:
+            setattr(o, k, int(tuned[k]))
     return o
+
+
+def autotune(scenes, precision="mixed", device=0, trial_steps=200, cache=None):
+    """nbc_autotune: the fastest launch shapes for these scenes (a dict of
+    TUNED_KEYS plus ms_per_step).  `cache`, a JSON file, keeps the choice by
+    scene shape across processes, so a shape is measured once."""
+    import json
+    key = "|".join(str(x) for x in (len(scenes), sum(int(s["params"]["NumberBody"]) for s in scenes),
+                                    sum(int(s["params"]["ClumpNum"]) for s in scenes),
+                                    max(len(s["levels"]["cell"]) if s.get("levels") else 1 for s in scenes),
+                                    precision, trial_steps))
+    book = {}
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            book = json.load(f)
+        if key in book:
+            return dict(book[key], cached=True)
+    descs = [scene_desc(s) for s in scenes]
+    arr = (C.POINTER(SceneDesc) * len(scenes))(*[C.pointer(d) for d, _ in descs])
+    o = _options(precision, True, device)
+    ms = C.c_double(0.0)
+    _check(lib().nbc_autotune(arr, len(scenes), C.byref(o), int(trial_steps), C.byref(ms)))
+    out = {k: int(getattr(o, k)) for k in TUNED_KEYS}
+    out["ms_per_step"] = ms.value
+    if cache:
+        book[key] = out
+        with open(cache, "w") as f:
+            json.dump(book, f, indent=1, sort_keys=True)
+    return dict(out, cached=False)
 
 
 class SceneView:
     """Scene s of a multi-scene engine: the per-scene getters of Engine with
     the scene index bound."""
 
-    _PER_SCENE = ("stats", "subspheres", "clumps", "sub_forces", "force_parts", "pairs", "rows", "chain",
+    _PER_SCENE = ("stats", "subspheres", "clumps", "sub_forces", "force_parts", "pairs", "rows", "chain", "pair_forces",
                   "intruder", "intruder_diag", "intruder_history", "restart_scene", "set_steps")
 
     def __init__(self, engine, s):
