@@ -1,18 +1,26 @@
 """Benchmark: subsphere-steps/s of the NBodyClump step on a B200.
 
-Workload (one GPU): 50,000 tetrahedral clumps = 200,000 subspheres
-(r = 1 mm x LogNormal(0, 0.2), centre offset 0.6 r, random orientation)
-settling under gravity in a closed cylinder wall (R = 60 mm, half-height
-300 mm), contact law in FP32 with FP64 positions and quaternions, dt = 0.2 of
-the Rayleigh step, Thresh = 0.2 r_min.  One step = one pass of the clump step
-(kick/drift/attitude/pose, list rebuild when triggered, contacts, clump
-reduction).  The bed is generated by seeded numpy and settles from a loose
-layered packing; the timed steps are the first W+1..W+K steps of that settle.
+Workload (one GPU): the cfg1 bed -- 50,000 tetrahedral clumps = 200,000
+subspheres (r = 1 mm x LogNormal(0, 0.2), centre offset 0.6 r, random
+orientation) in a closed cylinder wall (R = 60 mm, half-height 150 mm),
+contact law in FP32 with FP64 positions and quaternions, dt = 0.2 of the
+Rayleigh step, Thresh = 0.2 r_min, 5 hierarchical-grid levels -- started from
+its engine-settled state after 20,000 steps of settling under gravity
+(tests/golden/cfg1_settled.npz, made by tests/golden/make_cfg1_state.py), so
+every timed step has touching pairs, wall contacts and list rebuilds.  One
+step = one pass of the clump step (kick/drift/attitude/pose, list rebuild
+when triggered, contacts, clump reduction).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Under torchrun each rank runs its own independent scene (different seed):
-weak scaling, no collective on the data path; timing is the max over ranks.
+The default line also carries a `batched` record: the first 64 scenes of
+the cfg3 draw (cfg1-style beds, clump counts log-uniform in [500, 50,000],
+friction U[0.2, 0.8]), settled together for 2,000 steps, then advanced 300
+steps as one batch against the same scenes one at a time on the plain
+engine (the batched-vs-plain metric on a fixed subset).
+
+Under torchrun each rank runs its own replica of the workload: weak
+scaling, no collective on the data path; timing is the max over ranks.
 Prints one JSON line (rank 0).
 """
 from __future__ import annotations
@@ -38,7 +46,9 @@ sys.path.insert(0, os.path.join(REPO, "nbody-clump_b200"))
 import scenegen as sg  # noqa: E402
 
 METRIC = "subsphere-steps/sec"
-WORKLOAD = "cfg1: 50,000 tetra clumps (200,000 subspheres) settling in a cylinder wall"
+SNAPSHOT = os.path.join(REPO, "tests", "golden", "cfg1_settled.npz")
+WORKLOAD = ("cfg1: 50,000 tetra clumps (200,000 subspheres) in a closed cylinder wall (R 60 mm, half-height "
+            "150 mm), from the engine-settled state after {steps} steps of settling")
 
 
 def peaks():
@@ -131,6 +141,33 @@ def replica_throughput(n_sub, steps, world, local_seconds, backend):
     return secs, n_sub * steps * world / secs
 
 
+def workload(args):
+    """The benchmarked scene: the engine-settled cfg1 snapshot (its grid
+    levels are stored with it, so neither arm needs the level chooser); with
+    --scene, a scene saved by --save-state; with --from-seed, the cfg1 bed as
+    seeded (falling, levels from nbc_choose_levels).  Returns (scene, config)
+    where config describes the workload identically for both arms."""
+    if args.scene:
+        scene = sg.scene_from_npz(args.scene)
+        start = f"scene file {os.path.basename(args.scene)}"
+    elif args.from_seed:
+        import nbc
+        scene = nbc.with_levels(sg.make_cfg1(n_clumps=args.clumps, seed=20260828))
+        start = "as seeded (loose layers, falling)"
+    else:
+        scene = sg.tetra_state_from_npz(SNAPSHOT)
+        start = f"engine-settled state after {int(scene['meta']['steps'])} steps ({os.path.relpath(SNAPSHOT, REPO)})"
+    N, K = int(scene["params"]["NumberBody"]), int(scene["params"]["ClumpNum"])
+    lv = scene.get("levels")
+    steps = int(scene.get("meta", {}).get("steps", 0))
+    config = {"workload": WORKLOAD.format(steps=steps) if steps else WORKLOAD.split(", from")[0],
+              "subspheres": N, "clumps": K, "grid_levels": 1 if lv is None else len(lv["cell"]),
+              "start_state": start,
+              "l2": "not flushed between steps: each step reads the state the previous step wrote "
+                    "(~60 MB, resident in the 126 MB L2 as in real use)"}
+    return scene, config
+
+
 def run_b200(args, world, rank, local):
     import nbc
     backend = None
@@ -141,69 +178,72 @@ def run_b200(args, world, rank, local):
         torch.cuda.set_device(local)
         from datetime import timedelta
         dist.init_process_group(backend, timeout=timedelta(seconds=120))
-    seed = 20260828 + rank
-    scene = workload(args, seed)
-    N, K = scene["params"]["NumberBody"], scene["params"]["ClumpNum"]
-    levels = 1 if scene.get("levels") is None else len(scene["levels"]["cell"])
+    scene, config = workload(args)
+    N, K = config["subspheres"], config["clumps"]
+    clk = ClockSampler(local)
+    clk.__enter__()       # sampled over every GPU leg of the run (tuning, warm-up, timed region, replay, e2e)
+    tuned = None
+    if args.autotune:
+        # launch shapes measured on this scene (results do not depend on them)
+        tuned = nbc.autotune([scene], precision=args.precision, device=local, trial_steps=200)
+    opts = dict(precision=args.precision, use_graph=args.graph, device=local, pair_slack=args.pair_slack,
+                search_lanes=args.search_lanes, tuned=tuned)
 
     # ---- device-resident throughput -----------------------------------
-    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local,
-                     pair_slack=args.pair_slack, search_lanes=args.search_lanes)
+    eng = nbc.Engine([scene], **opts)
     eng.step(args.warmup)
     eng.sync()
     st0 = eng.stats()
-    # the timed region: no timing event nodes in the step graph and no host
+    # the timed region: no timing event nodes in the step graphs and no host
     # queries between its chunks (launches are still counted)
     eng.timing_enable(2 if args.profile else 0)
     barrier(world)
     pair_samples = []
-    with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        left = args.steps
-        while left > 0:           # each call returns after the device finished (stream synchronised)
-            c = min(left, 1000)
-            eng.step(c)
-            if args.profile:
-                pair_samples.append((c, eng.stats()["npairs"]) + eng.contact_counts())
-            left -= c
-        t1 = time.perf_counter()
+    t0 = time.perf_counter()
+    left = args.steps
+    while left > 0:           # each call returns after the device finished (stream synchronised)
+        c = min(left, 1000)
+        eng.step(c)
+        if args.profile:
+            pair_samples.append((c, eng.stats()["npairs"]) + eng.contact_counts())
+        left -= c
+    t1 = time.perf_counter()
     tm = eng.timing_read()
     st1 = eng.stats()
     barrier(world)
     local_s = t1 - t0
     secs, value = replica_throughput(N, args.steps, world, local_s, backend)
     launches = tm["kernel_launches"]
-    if not args.profile:
-        # the contact pass's CUDA-event time over a replay of the timed region
-        # (the same scene, warm-up and steps on a second engine: runs are
-        # deterministic, so it does the same work), with the timing event nodes
-        # in its step graph and the near and touching pair counts sampled every
-        # 1,000 steps
-        eng.close()
-        eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph,
-                         device=local, pair_slack=args.pair_slack, search_lanes=args.search_lanes)
-        eng.step(args.warmup)
-        eng.sync()
-        eng.timing_enable(1)
-        left = args.steps
-        while left > 0:
-            c = min(left, 1000)
-            eng.step(c)
-            pair_samples.append((c, eng.stats()["npairs"]) + eng.contact_counts())
-            left -= c
-        tm = eng.timing_read()
-        eng.close()
-
     if args.profile:
+        clk.__exit__()
         if rank == 0:
+            nt = eng.contact_counts()
             print(json.dumps({"profile_run": True, "ms_per_step": secs * 1e3 / args.steps,
                               "contact_ms_avg": tm["contact_ms"] / max(1, tm["contact_launches"]),
                               "npairs": st1["npairs"], "rebuilds": st1["rebuilds"] - st0["rebuilds"],
-                              "phases_ms": eng.timing_phases(),
-                              "near_touching": eng.contact_counts(),
-                              "alg_bytes": algorithmic_contact_bytes(N, *eng.contact_counts(), args.precision)}),
-                  flush=True)
+                              "phases_ms": eng.timing_phases(), "near_touching": nt,
+                              "alg_bytes": algorithmic_contact_bytes(N, *nt, args.precision)}), flush=True)
         return
+    # the kernels' CUDA-event times over a replay of the timed region (the
+    # same scene, warm-up and steps on a second engine: runs are
+    # deterministic, so it does the same work), with timing event nodes in
+    # its step graphs, and the near and touching pair counts sampled every
+    # chunk
+    eng.close()
+    eng = nbc.Engine([scene], **opts)
+    eng.step(args.warmup)
+    eng.sync()
+    eng.timing_enable(2)
+    left = args.steps
+    chunk = max(1, min(1000, args.steps // 4))
+    while left > 0:
+        c = min(left, chunk)
+        eng.step(c)
+        pair_samples.append((c, eng.stats()["npairs"]) + eng.contact_counts())
+        left -= c
+    tm = eng.timing_read()
+    phases = eng.timing_phases()
+    eng.close()
 
     # ---- end to end through the C ABI with host buffers -----------------
     # create (H2D of the scene from host arrays), K steps, sync, D2H of the
@@ -212,8 +252,7 @@ def run_b200(args, world, rank, local):
         sum(np.asarray(v).nbytes for v in scene["clump"].values())
     barrier(world)
     te0 = time.perf_counter()
-    e2 = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=args.graph, device=local,
-                    pair_slack=args.pair_slack, search_lanes=args.search_lanes)
+    e2 = nbc.Engine([scene], **opts)
     e2.step(args.warmup + args.steps)
     e2.sync()
     out = e2.clumps()
@@ -224,51 +263,73 @@ def run_b200(args, world, rank, local):
     e2e_steps = args.warmup + args.steps
     e2e_value = N * e2e_steps * world / e2e_s
 
-    # ---- roofline of the contact kernel -----------------------------------
+    # ---- the benchmarked law's per-contact forces at the start state (the
+    # CPU-baseline leg compares them with the FP64 oracle) ----------------
+    ex = nbc.Engine([scene], precision=args.precision, use_graph=False, device=local)
+    ex.step_export(1)
+    first_step = {"pairs": ex.pairs(), "fcn": ex.pair_forces()}
+    ex.close()
+
+    batched = None
+    if rank == 0 and args.batch_scenes > 0:
+        batched = batched_record(args)
+    clk.__exit__()
+
+    # ---- rooflines: the contact kernel and the clump pass --------------
     pk, pk_kind = peaks()
-    wsum = max(1, sum(s[0] for s in pair_samples))
-    npairs, nnear, ntouch = (sum(s[0] * s[q] for s in pair_samples) / wsum for q in (1, 2, 3))
+    wsum = max(1, sum(q[0] for q in pair_samples))
+    npairs, nnear, ntouch = (sum(q[0] * q[i] for q in pair_samples) / wsum for i in (1, 2, 3))
     alg = algorithmic_contact_bytes(N, nnear, ntouch, args.precision)
     avg_ms = tm["contact_ms"] / max(1, tm["contact_launches"])
     achieved = alg / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    clump_ms = phases[0]
+    alg_clump = algorithmic_clump_bytes(N, K, nnear, args.precision)
+    clump_gbs = alg_clump / (clump_ms * 1e-3) / 1e9 if clump_ms > 0 else 0.0
     traffic, traffic_note = None, None
     tp = os.path.join(REPO, "profiles", "contact_traffic.json")
     if os.path.exists(tp):
         tj = json.load(open(tp))
-        if (tj.get("kernels") == ["k_pairs", "k_sum"] and tj.get("lanes") == eng_lanes(args)
-                and tj.get("precision") == args.precision):
-            # captured on a smaller list state; scaled to this run's mean
-            # listed pairs by the ratio of algorithmic bytes
+        if tj.get("kernel") == "k_pairs" and tj.get("precision") == args.precision and tj.get("slots") == "entry":
+            # captured on the same start state; scaled to this run's mean near
+            # and touching pairs by the ratio of algorithmic bytes
             traffic = tj["dram_bytes_per_launch"] * alg / tj["algorithmic_bytes_at_capture"]
             traffic_note = tj["note"]
 
-    cpu = cpu_baseline(args) if (rank == 0 and not args.no_cpu_baseline) else None
+    cpu = cpu_baseline(args, scene, first_step) if (rank == 0 and not args.no_cpu_baseline) else None
     clocks = clk.summary()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "subsphere-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
-            "data": "synthetic (seeded numpy bed, no dataset)",
-            "config": {"workload": WORKLOAD, "subspheres": N, "clumps": K, "precision": args.precision,
-                       "lanes": eng_lanes(args), "graph": bool(args.graph), "grid_levels": levels,
+            "vs_baseline": None,
+            "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded numpy bed settled by the engine, no dataset)",
+            "config": config,
+            "engine": {"precision": args.precision, "graph": bool(args.graph), "autotuned": tuned,
                        "pairs_listed_end": st1["npairs"],
                        "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
-                       "l2": "working set 60+ MB per step; not flushed between steps (state is resident by design)",
-                       "parallelism": f"replicas x{world} (independent scenes)"},
+                       "mean_pairs_near": nnear, "mean_pairs_touching": ntouch,
+                       "parallelism": f"replicas x{world} (independent scenes)",
+                       "phases_ms_per_step_replay": dict(zip(("clump", "rebuild_node", "boundary", "contact", "step"),
+                                                             phases))},
             "e2e": {"value": e2e_value, "unit": "subsphere-steps/s", "h2d_bytes_per_step": host_in / e2e_steps,
                     "d2h_bytes_per_step": host_out / e2e_steps, "steps": e2e_steps,
-                    "includes": "nbc_create (upload) + steps + sync + clump-state download"},
+                    "includes": "nbc_create (upload) + first list build + steps + sync + clump-state download"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
                          "frac": achieved / pk if pk else None, "traffic": traffic,
-                         "kernel": "contact pass (k_pairs + k_sum)", "avg_launch_ms": avg_ms,
+                         "kernel": "contact pass (k_pairs)", "avg_launch_ms": avg_ms,
                          "alg_bytes_per_launch": alg, "mean_pairs_listed": npairs,
                          "mean_pairs_near": nnear, "mean_pairs_touching": ntouch, "peak_kind": pk_kind,
-                         "window": "a replay of the timed region (same scene, warm-up and steps) with CUDA events on the engine's stream",
+                         "window": "a replay of the timed region (same scene, warm-up and steps) with CUDA events "
+                                   "on the engine's stream",
                          "traffic_note": traffic_note},
+            "roofline_clump": {"bound": "hbm", "achieved": clump_gbs, "peak": pk, "unit": "GB/s",
+                               "frac": clump_gbs / pk if pk else None, "kernel": "clump pass (k_clump)",
+                               "avg_launch_ms": clump_ms, "alg_bytes_per_launch": alg_clump, "peak_kind": pk_kind},
             "cpu_baseline": cpu,
+            "batched": batched,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -277,61 +338,121 @@ def run_b200(args, world, rank, local):
         dist.destroy_process_group()
 
 
-def eng_lanes(args):
-    return args.lanes if args.lanes in (1, 2, 4, 8, 16, 32) else 2
-
-
-def workload(args, seed):
-    """The cfg1 scene with the hierarchical-grid levels nbc_choose_levels picks
-    (or, with --scene, a scene saved by --save-state)."""
+def batched_record(args):
+    """cfg3 on a fixed subset: the first --batch-scenes scenes of the cfg3
+    draw, settled together for --batch-settle steps (untimed, so both arms
+    start from the same contact-rich states), then --batch-steps steps as
+    one batch (nbc_batch, launch shapes from the autotuner) against the same
+    scenes one at a time on the plain engine (default shapes).  scenes/s
+    includes engine creation (upload) and the first list build in both arms;
+    subsphere-steps/s counts the stepping only."""
     import nbc
-    if args.scene:
-        scene = sg.scene_from_npz(args.scene)
-    else:
-        scene = sg.make_cfg1(n_clumps=args.clumps, seed=seed, steps=args.warmup + args.steps)
-    return nbc.with_levels(scene) if args.levels else scene
+    scenes = [nbc.with_levels(x) for x in sg.make_cfg3(args.batch_scenes, steps=args.batch_steps)]
+    n_sub = sum(int(x["params"]["NumberBody"]) for x in scenes)
+    opts = dict(precision=args.precision, pair_slack=1.6)
+    b = nbc.Batch(scenes, **opts)
+    b.step(args.batch_settle)
+    b.sync()
+    states = [b.engines[i].restart_scene(scenes[i]) for i in range(len(scenes))]
+    b.close()
+    tuned = nbc.autotune(states, precision=args.precision, trial_steps=100) if args.autotune else None
+    t0 = time.perf_counter()
+    b = nbc.Batch(states, tuned=tuned, **opts)
+    t1 = time.perf_counter()
+    b.step(args.batch_steps)
+    b.sync()
+    t2 = time.perf_counter()
+    reb_b = sum(v.stats()["rebuilds"] for v in b.engines)
+    b.close()
+    bc, bs = t1 - t0, t2 - t1
+    pc = ps = 0.0
+    for sc in states:
+        t0 = time.perf_counter()
+        e = nbc.Engine([sc], **opts)
+        t1 = time.perf_counter()
+        e.step(args.batch_steps)
+        e.sync()
+        ps += time.perf_counter() - t1
+        pc += t1 - t0
+        e.close()
+    work = n_sub * args.batch_steps
+    arm = lambda c, st: {"create_s": c, "step_s": st, "scenes_per_s": len(states) / (c + st),
+                         "subsphere_steps_per_s": work / st}
+    return {"metric": "subsphere-steps/s and scenes/s, batched vs plain (one at a time), same B200",
+            "workload": f"first {len(states)} scenes of the cfg3 draw ({n_sub} subspheres), settled "
+                        f"{args.batch_settle} steps together, then {args.batch_steps} steps timed",
+            "batched": arm(bc, bs), "plain": arm(pc, ps), "rebuilds_batched": reb_b, "autotuned_batch": tuned,
+            "speedup_steps": ps / bs, "speedup_scenes_per_s": (pc + ps) / (bc + bs)}
 
 
 def save_state(args):
     """Advance the workload --advance steps and save the state it reached as a
-    scene file (a late-settle starting point for short profiler runs)."""
+    scene file (a starting point for short profiler runs)."""
     import nbc
-    scene = workload(args, 20260828)
-    eng = nbc.Engine([scene], precision=args.precision, lanes=args.lanes, use_graph=True)
+    scene, _ = workload(args)
+    eng = nbc.Engine([scene], precision=args.precision, use_graph=True)
     eng.step(args.advance)
     out = eng.restart_scene(scene)
-    out.pop("levels", None)
     sg.scene_to_npz(out, args.save_state)
     print(json.dumps({"saved": args.save_state, "steps": args.advance, "npairs": eng.stats()["npairs"]}), flush=True)
 
 
 def algorithmic_contact_bytes(N, nnear, ntouch, precision):
-    """Unique bytes the contact pass (k_pairs + k_sum) must move per step.
+    """Unique bytes the contact kernel (k_pairs) must move per step.
 
-    Per near pair (the pairs that can touch before the next rebuild): its
-    index in the near front and back rows 4 + 4 B, partner and owner 4 + 4 B,
-    the touch flag written 1 B and read twice by the sum 2 B.  Per touching
-    pair: the previous touch flag 1 B, the spring history read and written
-    (2 Real4 + 1 Real each way) and the four per-pair force slots written and
-    read (4 Real4 each way).  Per subsphere: FP64 position and radius 32 B,
-    contact kinematics 3 Real4, near-row offsets 16 B, boundary bits 2 B,
-    force and torque out 2 Real4."""
+    Per near pair (the pairs that can touch before the next rebuild, each
+    visited once): its near front slot index, near back slot index, partner
+    and owner 4 B each, the touch flag written 1 B, both subspheres' FP64
+    position and radius 2 x 32 B, and the four contact slots written (force
+    and torque on each side, 4 Real4).  Per touching pair: the previous touch
+    flag 1 B, the spring history read and written (2 Real4 + 1 Real each way)
+    and both subspheres' contact kinematics (3 Real4 each).  N is unused: the
+    per-subsphere sums are part of the clump pass."""
     r = 4 if precision == "mixed" else 8
     r4 = 4 * r
-    per_near = 4 + 4 + 4 + 4 + 1 + 2
-    per_touch = 1 + 2 * (2 * r4 + r) + 2 * 4 * r4
-    per_sub = 32 + 3 * r4 + 16 + 2 + 2 * r4
-    return per_near * nnear + per_touch * ntouch + per_sub * N
+    per_near = 4 * 4 + 1 + 2 * 32 + 4 * r4
+    per_touch = 1 + 2 * (2 * r4 + r) + 2 * 3 * r4
+    return per_near * nnear + per_touch * ntouch
 
 
-def cpu_baseline(args):
-    """The FP64 CPU oracle on a bounded sample of the same workload."""
+def algorithmic_clump_bytes(N, K, nnear, precision):
+    """Unique bytes the clump pass (k_clump) must move per step: per clump
+    its position, velocity, angular velocity, quaternion and properties read
+    (5 x 32 B) and position, velocity, angular velocity, quaternion, force and
+    torque written (6 x 32 B) plus its member offset 4 B; per member its index
+    4 B, FP64 position read and written 2 x 32 B, body offset and mass 32 B,
+    displacement since the rebuild read and written 2 x 32 B, contact
+    kinematics written 3 Real4, near-row offsets 16 B and boundary bits 2 B;
+    per near pair its two contact-slot pairs read (4 Real4)."""
+    r4 = 16 if precision == "mixed" else 32
+    per_clump = 5 * 32 + 6 * 32 + 4
+    per_sub = 4 + 2 * 32 + 32 + 2 * 32 + 3 * r4 + 16 + 2
+    return per_clump * K + per_sub * N + 4 * r4 * nnear
+
+
+def cpu_baseline(args, scene, first_step):
+    """The FP64 CPU oracle on a bounded sample of the same workload, single
+    thread.  Its first step (the list build) also checks the benchmarked
+    engine's first step from the same state: the pair list bit for bit and
+    every contact's normal force against FP64."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    scene = workload(args, 20260828)
     threads = 1
     o = oracle.OracleScene(scene, threads=threads)
     o.step(1)  # first step includes the initial list build, like the GPU warm-up
+    oa, ob = o.pairs()
+    ea, eb = first_step["pairs"]
+    same = bool(np.array_equal(oa, ea) and np.array_equal(ob, eb))
+    err = None
+    if same:
+        fo = o.pair_caches()["cfcn"]
+        fe = first_step["fcn"]
+        mag = np.linalg.norm(fo, axis=1)
+        big = mag > 1e-6 * mag.max() if mag.size else mag > 0
+        rel = np.linalg.norm(fe - fo, axis=1)[big] / mag[big]
+        err = {"max_rel_per_contact": float(rel.max()) if rel.size else 0.0, "contacts": int(big.sum()),
+               "p99_rel": float(np.percentile(rel, 99)) if rel.size else 0.0, "tolerance": 1e-5,
+               "law": args.precision}
     n = 0
     t0 = time.perf_counter()
     while True:
@@ -342,7 +463,9 @@ def cpu_baseline(args):
     dt = time.perf_counter() - t0
     N = scene["params"]["NumberBody"]
     return {"value": N * n / dt, "unit": "subsphere-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{n} steps of the same 200,000-subsphere scene after its first step, single thread"}
+            "sample": f"{n} steps of the benchmarked {N}-subsphere scene from its start state, after its first "
+                      "step (list build), single thread",
+            "first_step_vs_engine": {"pair_list_bitexact": same, "force_error_vs_fp64": err}}
 
 
 def run_batch(args):
@@ -592,16 +715,18 @@ def run_serve(args):
 
 
 def run_reference(args, world, rank, local):
-    """The reference arm: the project's FP64 CPU restatement of the
-    reference's clump step (the reference itself has no CPU implementation),
-    with every host thread, on the same workload."""
+    """The reference arm: the reference's clump step restated in C (oracle/,
+    FP64, OpenMP over every host thread; the reference itself is a GPU
+    program with no CPU implementation), on the same workload and start
+    state, each step of a sample bounded to a few minutes.  It loads nothing
+    of the engine."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
-    scene = workload(args, 20260828)
-    N = scene["params"]["NumberBody"]
+    scene, config = workload(args)
+    N = config["subspheres"]
     o = oracle.OracleScene(scene, threads=threads)
     t = time.perf_counter()
     o.step(max(1, args.warmup))
@@ -616,11 +741,12 @@ def run_reference(args, world, rank, local):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "subsphere-steps/s",
         "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded numpy bed, no dataset)",
-        "config": {"workload": WORKLOAD, "subspheres": N, "precision": "f64",
-                   "note": "CPU restatement of the reference clump step (oracle/), OpenMP threads"},
+        "data": "synthetic (seeded numpy bed settled by the engine, no dataset)",
+        "config": config,
+        "engine": {"implementation": "CPU restatement of the reference clump step (oracle/), FP64, OpenMP"},
         "cpu_baseline": {"value": v, "unit": "subsphere-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} steps of the {N}-subsphere scene after {max(1, args.warmup)} warm-up steps"},
+                         "sample": f"{steps} steps of the {N}-subsphere scene after {max(1, args.warmup)} warm-up "
+                                   "steps from the same start state"},
         "e2e": {"value": v, "unit": "subsphere-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -632,12 +758,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
-    ap.add_argument("--lanes", type=int, default=0, help="lanes per subsphere in the contact kernel (0 = engine default)")
-    ap.add_argument("--clumps", type=int, default=50_000)
+    ap.add_argument("--clumps", type=int, default=50_000, help="with --from-seed: clumps of the cfg1 bed")
+    ap.add_argument("--from-seed", action="store_true", help="start from the seeded (falling) cfg1 bed")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--graph", type=int, default=1, help="1: CUDA graph per step; 0: eager launches (for ncu)")
-    ap.add_argument("--levels", type=int, default=1, help="1: hierarchical grid chosen by nbc_choose_levels")
+    ap.add_argument("--graph", type=int, default=1, help="1: CUDA graphs; 0: eager launches (for ncu)")
+    ap.add_argument("--autotune", type=int, default=1, help="1: launch shapes from nbc_autotune (untimed)")
+    ap.add_argument("--batch-scenes", type=int, default=64, help="batched record: cfg3 scenes (0: skip)")
+    ap.add_argument("--batch-settle", type=int, default=2000, help="batched record: settling steps (untimed)")
+    ap.add_argument("--batch-steps", type=int, default=300, help="batched record: timed steps")
     ap.add_argument("--profile", action="store_true",
                     help="short run for profilers: warm-up + timed steps only, no e2e / CPU legs")
     ap.add_argument("--pair-slack", type=float, default=0.0,
