@@ -282,7 +282,7 @@ def run_b200(args, world, rank, local):
     alg = algorithmic_contact_bytes(N, nnear, ntouch, args.precision)
     avg_ms = tm["contact_ms"] / max(1, tm["contact_launches"])
     achieved = alg / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
-    clump_ms = phases[0]
+    clump_ms = phases["clump"]
     alg_clump = algorithmic_clump_bytes(N, K, nnear, args.precision)
     clump_gbs = alg_clump / (clump_ms * 1e-3) / 1e9 if clump_ms > 0 else 0.0
     traffic, traffic_note = None, None
@@ -311,8 +311,7 @@ def run_b200(args, world, rank, local):
                        "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
                        "mean_pairs_near": nnear, "mean_pairs_touching": ntouch,
                        "parallelism": f"replicas x{world} (independent scenes)",
-                       "phases_ms_per_step_replay": dict(zip(("clump", "rebuild_node", "boundary", "contact", "step"),
-                                                             phases))},
+                       "phases_ms_per_step_replay": phases},
             "e2e": {"value": e2e_value, "unit": "subsphere-steps/s", "h2d_bytes_per_step": host_in / e2e_steps,
                     "d2h_bytes_per_step": host_out / e2e_steps, "steps": e2e_steps,
                     "includes": "nbc_create (upload) + first list build + steps + sync + clump-state download"},

@@ -293,8 +293,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             s_cl[warp][12][lane] = q.w;
             __syncwarp();
             // ---- poses of the members, 32 at a time
-            R4<R>* __restrict__ kv = (R4<R>*)d.kin;
-            R4<R>* __restrict__ kw = kv + d.N;
+            double4* __restrict__ kv = (double4*)d.kin;
+            R4<R>* __restrict__ kw = (R4<R>*)(kv + d.N);
             R4<R>* __restrict__ ka = kw + d.N;
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
                     cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
                     posw[i] = make_double4(p.x, p.y, p.z, o.w);
-                    kv[i] = pack<R>(cvt<R>(vk), (R)lo[j].w);
+                    kv[i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
                     kw[i] = pack<R>(cvt<R>(wk), R(0));
                     ka[i] = pack<R>(cvt<R>(arm), R(0));
                     const int sk = s_sc[warp][kk];
@@ -725,9 +725,10 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
         d.part_fix2[i] = d.part_fix[o];
         d.level2[i] = d.level[o];
         d.bbits2[i] = d.bbits[o];
-        const R4<R>* k1 = (const R4<R>*)d.kin;
-        R4<R>* k2 = (R4<R>*)d.kin2;
-        for (int c = 0; c < 3; c++) k2[c * N + i] = k1[c * N + o];
+        ((double4*)d.kin2)[i] = ((const double4*)d.kin)[o];
+        const R4<R>* k1 = (const R4<R>*)((const double4*)d.kin + N);
+        R4<R>* k2 = (R4<R>*)((double4*)d.kin2 + N);
+        for (int c = 0; c < 2; c++) k2[c * N + i] = k1[c * N + o];
         const R4<R>* b1 = (const R4<R>*)d.bhist;
         R4<R>* b2 = (R4<R>*)d.bhist2;
         const uint16_t bits = d.bbits[o];
@@ -1234,9 +1235,10 @@ __global__ void k_writeback(const Dev* __restrict__ dp) {
         d.part_fix[i] = d.part_fix2[i];
         d.level[i] = d.level2[i];
         d.key[i] = d.key2[i];
-        const R4<R>* k2 = (const R4<R>*)d.kin2;
-        R4<R>* k1 = (R4<R>*)d.kin;
-        for (int c = 0; c < 3; c++) k1[c * N + i] = k2[c * N + i];
+        ((double4*)d.kin)[i] = ((const double4*)d.kin2)[i];
+        const R4<R>* k2 = (const R4<R>*)((const double4*)d.kin2 + N);
+        R4<R>* k1 = (R4<R>*)((double4*)d.kin + N);
+        for (int c = 0; c < 2; c++) k1[c * N + i] = k2[c * N + i];
         const uint16_t bits = d.bbits2[i];
         d.bbits[i] = bits;
         const R4<R>* b2 = (const R4<R>*)d.bhist2;
@@ -1626,43 +1628,35 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vto
     o.Mt = tm;
 }
 
+// The contact kinematics of a subsphere: its clump's velocity in FP64 (a
+// bed moving as a whole gives touching subspheres nearly equal velocities,
+// so their difference is taken before rounding to the law's precision), the
+// clump's angular velocity and the subsphere's world arm in the law's
+// precision.  Buffer layout: N double4 (velocity, mass), then N Real4
+// (angular velocity), then N Real4 (arm).
 template <typename R> struct Body {
     double4 p;         // position, radius
-    V3<R> v, w, arm;   // clump velocity, clump angular velocity, world arm
+    V3<double> v;      // clump velocity
+    V3<R> w, arm;      // clump angular velocity, world arm
     R m;
 };
 
 template <typename R>
+__device__ __forceinline__ void load_kin(const void* __restrict__ kin, size_t N, int i, Body<R>& b) {
+    const double4 a = ((const double4*)kin)[i];
+    const R4<R>* kw = (const R4<R>*)((const double4*)kin + N);
+    const R4<R> w = kw[i], r = kw[N + i];
+    b.v = v3(a.x, a.y, a.z);
+    b.m = (R)a.w;
+    b.w = xyz<R>(w);
+    b.arm = xyz<R>(r);
+}
+
+template <typename R>
 __device__ __forceinline__ void load_kin(const Dev& d, int i, Body<R>& b) {
-    const R4<R>* kv = (const R4<R>*)d.kin;
-    R4<R> a = kv[i], w = kv[d.N + i], r = kv[2 * d.N + i];
-    b.v = xyz<R>(a);
-    b.m = a.w;
-    b.w = xyz<R>(w);
-    b.arm = xyz<R>(r);
+    load_kin<R>(d.kin, (size_t)d.N, i, b);
 }
 
-template <typename R>
-__device__ __forceinline__ void load_kin(const R4<R>* __restrict__ kv, size_t N, int i, Body<R>& b) {
-    const R4<R> a = kv[i], w = kv[N + i], r = kv[2 * N + i];
-    b.v = xyz<R>(a);
-    b.m = a.w;
-    b.w = xyz<R>(w);
-    b.arm = xyz<R>(r);
-}
-
-template <typename R>
-__device__ __forceinline__ Body<R> load_body(const Dev& d, int i) {
-    const R4<R>* kv = (const R4<R>*)d.kin;
-    Body<R> b;
-    b.p = d.posr[i];
-    R4<R> a = kv[i], w = kv[d.N + i], r = kv[2 * d.N + i];
-    b.v = xyz<R>(a);
-    b.m = a.w;
-    b.w = xyz<R>(w);
-    b.arm = xyz<R>(r);
-    return b;
-}
 
 // Pair contact seen from body a (the pair law of ContactForce_clump_cuk,
 // src/dem_force_clump.cu:3-163, with a in the role of particleI).  Returns
@@ -1686,7 +1680,7 @@ __device__ __forceinline__ bool pair_contact(const Law<R>& L, R cohesion, const 
     const R Mij = a.m * b.m / (a.m + b.m);
     const V3<R> ARMa = a.arm + (R)Ap * n;
     const V3<R> ARMb = b.arm - (R)An * n;
-    const V3<R> Vtot = (b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
+    const V3<R> Vtot = cvt<R>(b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
     const V3<R> Dth = L.dt * (a.w - b.w);
     hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
     const R br = L.beta * Rij;
@@ -1722,7 +1716,7 @@ __device__ __forceinline__ bool pair_contact2(const Law<R>& L, R cohesion, const
     const R Mij = a.m * b.m / (a.m + b.m);
     const V3<R> ARMa = a.arm + (R)Ap * n;
     const V3<R> ARMb = b.arm - (R)An * n;
-    const V3<R> Vtot = (b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
+    const V3<R> Vtot = cvt<R>(b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
     const V3<R> Dth = L.dt * (a.w - b.w);
     hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
     const R br = L.beta * Rij;
@@ -1744,7 +1738,8 @@ __device__ __forceinline__ void boundary_contact(const Law<R>& L, const Body<R>&
                                                  LawOut<R>& o, V3<R>& arm_out) {
     const V3<R> Arm = (-a.arm) + Ap * n;
     const V3<R> Vwall = cross(ww, RVo);
-    const V3<R> Vtot = (a.v - wv) + (cross(Arm, a.w) - Vwall);
+    const V3<R> Vrel = cvt<R>(v3(a.v.x - (double)wv.x, a.v.y - (double)wv.y, a.v.z - (double)wv.z));
+    const V3<R> Vtot = Vrel + (cross(Arm, a.w) - Vwall);
     const V3<R> Dth = L.dt * (a.w - ww);
     hm_law<R>(L, n, Dn, Vtot, Dth, Rij, Mij, cs_mult, H, Mr, Mt, o);
     f = o.Fn + o.Ft;
@@ -2048,7 +2043,7 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
     const int* __restrict__ nbr = Lst.nbr;
     const int* __restrict__ own = Lst.own;
     const double4* __restrict__ posr = d.posr;
-    const R4<R>* __restrict__ kin = (const R4<R>*)d.kin;
+    const void* __restrict__ kin = d.kin;
     const size_t N = (size_t)d.N;
     const size_t cap = (size_t)d.cap;
     const R4<R>* __restrict__ Hi = (const R4<R>*)d.H[hg & 1];
