@@ -502,12 +502,15 @@ def run_batch(args):
     w.step(3)
     w.sync()
     w.close()
+    # launch shapes for the batch measured on it (untimed); the plain arm keeps the defaults
+    tuned = nbc.autotune(scenes, precision=args.precision, trial_steps=100) if args.autotune else None
     t0 = time.perf_counter()
-    b = nbc.Batch(scenes, **opts)
+    b = nbc.Batch(scenes, tuned=tuned, **opts)
     t1 = time.perf_counter()
     b.step(args.steps)
     b.sync()
     t2 = time.perf_counter()
+    last = b.engines[0].clumps()
     b.close()
     bc, bs = t1 - t0, t2 - t1
     pc = ps = 0.0
@@ -523,10 +526,20 @@ def run_batch(args):
     work = n_sub * args.steps
     arm = lambda c, st: {"create_s": c, "step_s": st, "scenes_per_s": args.scenes / (c + st),
                          "subsphere_steps_per_s": work / st}
+    # the FP64 oracle on the first scene: its first step against the batched
+    # engine's export step from the same state, and its speed
+    ex = nbc.Engine([scenes[0]], precision=args.precision, use_graph=False)
+    ex.step_export(1)
+    first = {"pairs": ex.pairs(), "fcn": ex.pair_forces()}
+    ex.close()
+    cpu = None if args.no_cpu_baseline else cpu_baseline(args, scenes[0], first)
     line = {"metric": "scenes/s and subsphere-steps/s, batched vs plain (cfg3)",
             "workload": f"cfg3: {args.scenes} settling scenes, clumps log-uniform in [500, 50000], {args.steps} steps each",
-            "subspheres_total": n_sub, "batched": arm(bc, bs), "plain": arm(pc, ps),
+            "subspheres_total": n_sub, "batched": arm(bc, bs), "plain": arm(pc, ps), "autotuned_batch": tuned,
             "speedup_steps": ps / bs, "speedup_scenes_per_s": (pc + ps) / (bc + bs),
+            "scene0_after": {"mean_height_m": float(last["pos"][:, 2].mean()),
+                             "mean_speed_m_s": float(np.linalg.norm(last["vel"], axis=1).mean())},
+            "cpu_baseline_scene0": cpu,
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy beds)"}
     print(json.dumps(line), flush=True)
@@ -603,6 +616,12 @@ def run_cfg2(args):
     st = e.stats()
     settled = e.restart_scene(bed)
     top = float((settled["sub"]["pos"][:, 2] + settled["sub"]["radius"]).max())
+    rmax = float(settled["sub"]["radius"].max())
+    cube = settled["cube"]
+    lo = cube["centre"] - cube["half"] + 3 * rmax
+    hi = np.array(cube["centre"] + cube["half"] - 3 * rmax)
+    hi[2] = top - 3 * rmax
+    phi = bulk_packing_fraction(settled["sub"]["pos"], settled["sub"]["radius"], lo, hi)
     e.close()
     sc = sg.with_sphere_intruder(settled, 0.02, 0.1)
     dt = float(sc["params"]["StepSize"])
@@ -627,6 +646,8 @@ def run_cfg2(args):
                         f"({total} steps of {dt:.3e} s)",
             "settle": {"steps": args.settle2, "seconds": settle_s, "subsphere_steps_per_s": N * args.settle2 / settle_s,
                        "rebuilds": st["rebuilds"], "pairs": st["npairs"], "bed_top_m": top,
+                       "bulk_packing_fraction": phi,
+                       "bulk_region": "at least 3 r_max from every wall and below the bed top (seeded Monte Carlo)",
                        "clump_speed_mean": float(speed.mean()), "clump_speed_max": float(speed.max())},
             "penetration": {"steps": total, "seconds": pen_s, "subsphere_steps_per_s": N * total / pen_s,
                             "rebuilds": st2["rebuilds"], "pairs": st2["npairs"], "err": st2["err"]},
@@ -635,6 +656,22 @@ def run_cfg2(args):
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy bed settled by the engine)"}
     print(json.dumps(line), flush=True)
+
+
+def bulk_packing_fraction(pos, radius, lo, hi, n=400_000, seed=3):
+    """Solid fraction of the box [lo, hi] by seeded Monte Carlo: a point is
+    solid when some sphere contains it (neighbours within the largest radius
+    from a k-d tree)."""
+    from scipy.spatial import cKDTree
+    pts = np.random.default_rng(seed).uniform(lo, hi, (n, 3))
+    tree = cKDTree(pos)
+    rmax = float(radius.max())
+    inside = np.zeros(n, dtype=bool)
+    for k, cand in enumerate(tree.query_ball_point(pts, rmax)):
+        if cand:
+            c = np.asarray(cand)
+            inside[k] = bool((((pos[c] - pts[k]) ** 2).sum(1) <= radius[c] ** 2).any())
+    return float(inside.mean())
 
 
 def run_serve(args):
