@@ -658,7 +658,7 @@ def run_cfg2(args):
     print(json.dumps(line), flush=True)
 
 
-def bulk_packing_fraction(pos, radius, lo, hi, n=400_000, seed=3):
+def bulk_packing_fraction(pos, radius, lo, hi, n=100_000, seed=3):
     """Solid fraction of the box [lo, hi] by seeded Monte Carlo: a point is
     solid when some sphere contains it (neighbours within the largest radius
     from a k-d tree)."""
