@@ -196,6 +196,7 @@ def run_b200(args, world, rank, local):
     st0 = eng.stats()
     # the timed region: no timing event nodes in the step graphs and no host
     # queries between its chunks (launches are still counted)
+    launch = eng.launch_info()
     eng.timing_enable(2 if args.profile else 0)
     barrier(world)
     pair_samples = []
@@ -306,7 +307,7 @@ def run_b200(args, world, rank, local):
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy bed settled by the engine, no dataset)",
             "config": config,
-            "engine": {"precision": args.precision, "graph": bool(args.graph), "autotuned": tuned,
+            "engine": {"precision": args.precision, "graph": bool(args.graph), "autotuned": tuned, "launch": launch,
                        "pairs_listed_end": st1["npairs"],
                        "rebuilds_in_timed_region": st1["rebuilds"] - st0["rebuilds"],
                        "mean_pairs_near": nnear, "mean_pairs_touching": ntouch,

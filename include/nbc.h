@@ -185,6 +185,11 @@ nbc_status nbc_timing_read(nbc_engine* e, double* contact_ms, int* contact_launc
  * its first kernel to its last (k_boundary runs beside k_contact); no
  * reference counterpart */
 nbc_status nbc_timing_phases(nbc_engine* e, double* phase_ms);
+/* the launch shapes an engine uses (see nbc_options) and whether its
+ * untimed steps run as a device-side loop in one graph launch (1) or one
+ * step per graph launch (0, e.g. when use_graph is 0); no reference
+ * counterpart */
+nbc_status nbc_launch_info(nbc_engine* e, int* step_loop, int* search_lanes, int* clump_batch, int* pair_blocks);
 /* device memory in use and wall time of the last nbc_step in ms */
 nbc_status nbc_engine_info(nbc_engine* e, double* device_bytes, double* last_step_ms);
 /* Exact checkpoint, replacing the reference's restart from StartStep

@@ -407,3 +407,8 @@ nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n, nbc_options*
         g_tuned[key] = Tuned{best.search_lanes, best.clump_batch, best.pair_blocks, tb};
     });
 }
+
+nbc_status nbc_launch_info(nbc_engine* e, int* step_loop, int* search_lanes, int* clump_batch, int* pair_blocks) {
+    if (!e || !e->eng) return fail(NBC_ERR_ARG, "bad arguments");
+    return guard([&] { e->eng->launch_info(step_loop, search_lanes, clump_batch, pair_blocks); });
+}

@@ -697,6 +697,15 @@ class EngineT final : public EngineBase {
         }
         if (src && off != src->size()) throw ArgError("checkpoint has trailing bytes");
     }
+    void launch_info(int* step_loop, int* search_lanes, int* clump_batch, int* pair_blocks) override {
+        if (step_loop) {
+            if (opt_.use_graph && !loop_tried_) capture_loop();
+            *step_loop = gexec_loop_ ? 1 : 0;
+        }
+        if (search_lanes) *search_lanes = search_lanes_;
+        if (clump_batch) *clump_batch = clump_batch_;
+        if (pair_blocks) *pair_blocks = pair_bps_;
+    }
     void info(double* bytes, double* ms) override {
         if (bytes) *bytes = mem_.bytes;
         if (ms) *ms = last_ms_;

@@ -42,6 +42,9 @@ class EngineBase {
     virtual void get_intruder(int s, double* pos, double* vel, double* reac, double* tq, int* state) = 0;
     virtual void get_intruder_history(int s, int count, double* out) = 0;
     virtual void info(double* bytes, double* ms) = 0;
+    // launch shapes in use; step_loop: 1 if untimed steps run in a device-side
+    // loop (captured and instantiated), 0 if one step per graph launch
+    virtual void launch_info(int* step_loop, int* search_lanes, int* clump_batch, int* pair_blocks) = 0;
     virtual void set_stop(int s, int nsteps) = 0;
     virtual void timing_enable(int level) = 0;
     virtual void timing_read(double* contact_ms, int* contact_launches, long long* kernel_launches, int* rebuilds) = 0;

@@ -101,7 +101,7 @@ EXPORTED = [
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
     "nbc_timing_phases",
     "nbc_engine_info", "nbc_set_scene_steps", "nbc_cell_sort_noalloc", "nbc_choose_levels",
-    "nbc_checkpoint_write", "nbc_checkpoint_read", "nbc_autotune",
+    "nbc_checkpoint_write", "nbc_checkpoint_read", "nbc_autotune", "nbc_launch_info",
     "nbc_batch_create", "nbc_batch_step", "nbc_batch_engine", "nbc_batch_destroy",
     "nbc_server_create", "nbc_server_submit", "nbc_server_advance", "nbc_server_result",
     "nbc_server_release", "nbc_server_memory", "nbc_server_destroy", "nbc_server_set_cohort",
@@ -349,6 +349,13 @@ class Engine:
         f, c = np.zeros((n, bl, 3)), np.zeros((n, bl, 3))
         _check(lib().nbc_get_chain(self.h, s, bl, _p(f), _p(c)))
         return f, c
+
+    def launch_info(self):
+        """nbc_launch_info: the launch shapes in use and whether untimed steps
+        run in a device-side loop."""
+        v = [C.c_int() for _ in range(4)]
+        _check(lib().nbc_launch_info(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("step_loop",) + TUNED_KEYS, [x.value for x in v]))
 
     def checkpoint(self, path):
         """nbc_checkpoint_write: the exact state after the last step."""
