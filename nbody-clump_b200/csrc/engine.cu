@@ -680,8 +680,7 @@ class EngineT final : public EngineBase {
             blk(h_.L[0].bnbr + o, np * sizeof(int));
             blk(h_.L[0].bpair + o, np * sizeof(int));
             R4<R>* H = (R4<R>*)h_.H[g];
-            blk(H + o, np * sizeof(R4<R>));
-            blk(H + cap + o, np * sizeof(R4<R>));
+            blk(H + 2 * o, 2 * np * sizeof(R4<R>));
             blk((R*)(H + 2 * cap) + o, np * sizeof(R));
             blk(h_.touch[g] + o, np);
             blk(h_.nearf + o, np);
@@ -690,10 +689,8 @@ class EngineT final : public EngineBase {
             blk(h_.nbq + o, nn * sizeof(int));
             R4<R>* fs = (R4<R>*)h_.nfs;
             R4<R>* bs = (R4<R>*)h_.nbs;
-            blk(fs + o, nn * sizeof(R4<R>));
-            blk(fs + cap + o, nn * sizeof(R4<R>));
-            blk(bs + o, nn * sizeof(R4<R>));
-            blk(bs + cap + o, nn * sizeof(R4<R>));
+            blk(fs + 2 * o, 2 * nn * sizeof(R4<R>));
+            blk(bs + 2 * o, 2 * nn * sizeof(R4<R>));
         }
         if (src && off != src->size()) throw ArgError("checkpoint has trailing bytes");
     }

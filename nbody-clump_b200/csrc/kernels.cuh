@@ -38,13 +38,13 @@ __device__ __forceinline__ void slot_sum(const R4<R>* __restrict__ fs, const R4<
     // copies cost the clump pass registers (and warps per SM)
 #pragma unroll 1
     for (int e = rs; e < re; e++) {
-        F = F + xyz<R>(fs[e]);
-        T = T + xyz<R>(fs[cap + e]);
+        F = F + xyz<R>(fs[2 * (size_t)e]);
+        T = T + xyz<R>(fs[2 * (size_t)e + 1]);
     }
 #pragma unroll 1
     for (int e = bs0; e < be; e++) {
-        F = F + xyz<R>(bs[e]);
-        T = T + xyz<R>(bs[cap + e]);
+        F = F + xyz<R>(bs[2 * (size_t)e]);
+        T = T + xyz<R>(bs[2 * (size_t)e + 1]);
     }
 }
 
@@ -294,8 +294,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             __syncwarp();
             // ---- poses of the members, 32 at a time
             double4* __restrict__ kv = (double4*)d.kin;
-            R4<R>* __restrict__ kw = (R4<R>*)(kv + d.N);
-            R4<R>* __restrict__ ka = kw + d.N;
+            R4<R>* __restrict__ kw = (R4<R>*)(kv + d.N);   // angular velocity at 2i, arm at 2i + 1
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
@@ -335,8 +334,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
                     posw[i] = make_double4(p.x, p.y, p.z, o.w);
                     kv[i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
-                    kw[i] = pack<R>(cvt<R>(wk), R(0));
-                    ka[i] = pack<R>(cvt<R>(arm), R(0));
+                    kw[2 * (size_t)i] = pack<R>(cvt<R>(wk), R(0));
+                    kw[2 * (size_t)i + 1] = pack<R>(cvt<R>(arm), R(0));
                     const int sk = s_sc[warp][kk];
                     if (len_floor(cn) > d.par[sk].thresh) {
                         SceneDyn& y = d.dyn[sk];
@@ -728,13 +727,13 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
         ((double4*)d.kin2)[i] = ((const double4*)d.kin)[o];
         const R4<R>* k1 = (const R4<R>*)((const double4*)d.kin + N);
         R4<R>* k2 = (R4<R>*)((double4*)d.kin2 + N);
-        for (int c = 0; c < 2; c++) k2[c * N + i] = k1[c * N + o];
+        for (int c = 0; c < 2; c++) k2[2 * (size_t)i + c] = k1[2 * (size_t)o + c];
         const R4<R>* b1 = (const R4<R>*)d.bhist;
         R4<R>* b2 = (R4<R>*)d.bhist2;
         const uint16_t bits = d.bbits[o];
         for (int sl = 0; sl < NB_SLOTS; sl++) {
             if (!(bits & (1u << sl))) continue;  // only live histories are ever read
-            for (int c = 0; c < 3; c++) b2[((size_t)sl * 3 + c) * N + i] = b1[((size_t)sl * 3 + c) * N + o];
+            for (int c = 0; c < 3; c++) b2[((size_t)sl * N + i) * 3 + c] = b1[((size_t)sl * N + o) * 3 + c];
         }
     }
 }
@@ -1186,9 +1185,9 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p, int s) {
     }
     if (q >= 0 && ti[q]) {
         for (int h = 0; h < 2; h++) {
-            R4<R> v = Hi[h * cap + q];
+            R4<R> v = Hi[2 * (size_t)q + h];
             v.x *= sign; v.y *= sign; v.z *= sign; v.w *= sign;
-            Ho[h * cap + p] = v;
+            Ho[2 * (size_t)p + h] = v;
         }
         const R* h2i = (const R*)(Hi + 2 * cap);
         R* h2o = (R*)(Ho + 2 * cap);
@@ -1238,14 +1237,14 @@ __global__ void k_writeback(const Dev* __restrict__ dp) {
         ((double4*)d.kin)[i] = ((const double4*)d.kin2)[i];
         const R4<R>* k2 = (const R4<R>*)((const double4*)d.kin2 + N);
         R4<R>* k1 = (R4<R>*)((double4*)d.kin + N);
-        for (int c = 0; c < 2; c++) k1[c * N + i] = k2[c * N + i];
+        for (int c = 0; c < 2; c++) k1[2 * (size_t)i + c] = k2[2 * (size_t)i + c];
         const uint16_t bits = d.bbits2[i];
         d.bbits[i] = bits;
         const R4<R>* b2 = (const R4<R>*)d.bhist2;
         R4<R>* b1 = (R4<R>*)d.bhist;
         for (int sl = 0; sl < NB_SLOTS; sl++) {
             if (!(bits & (1u << sl))) continue;
-            for (int c = 0; c < 3; c++) b1[((size_t)sl * 3 + c) * N + i] = b2[((size_t)sl * 3 + c) * N + i];
+            for (int c = 0; c < 3; c++) b1[((size_t)sl * N + i) * 3 + c] = b2[((size_t)sl * N + i) * 3 + c];
         }
         Lc.row[i + s] = Nw.row[i + s];
         Lc.brow[i + s] = Nw.brow[i + s];
@@ -1284,8 +1283,8 @@ __global__ void k_writeback_pairs(const Dev* __restrict__ dp) {
         const uint8_t f = tn[p];
         tc[p] = f;
         if (f) {
-            Hc[p] = Hn[p];
-            Hc[cap + p] = Hn[cap + p];
+            Hc[2 * (size_t)p] = Hn[2 * (size_t)p];
+            Hc[2 * (size_t)p + 1] = Hn[2 * (size_t)p + 1];
             ((R*)(Hc + 2 * cap))[p] = ((const R*)(Hn + 2 * cap))[p];
         }
     }
@@ -1523,8 +1522,8 @@ __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* 
         d.nbq[pn] = onbq[po] + (m.y - m.x);
         d.nbpos[pn] = onear[po] ? onbpos[po] + (m.y - m.x) : -1;
         if (f) {
-            Hn[pn] = Ho[po];
-            Hn[cap + pn] = Ho[oc + po];
+            Hn[2 * (size_t)pn] = Ho[2 * (size_t)po];
+            Hn[2 * (size_t)pn + 1] = Ho[2 * (size_t)po + 1];
             ((R*)(Hn + 2 * cap))[pn] = ((const R*)(Ho + 2 * oc))[po];
         }
     }
@@ -1632,8 +1631,8 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vto
 // bed moving as a whole gives touching subspheres nearly equal velocities,
 // so their difference is taken before rounding to the law's precision), the
 // clump's angular velocity and the subsphere's world arm in the law's
-// precision.  Buffer layout: N double4 (velocity, mass), then N Real4
-// (angular velocity), then N Real4 (arm).
+// precision.  Buffer layout: N double4 (velocity, mass), then per subsphere
+// two adjacent Real4 (angular velocity, arm: one 32-byte record in FP32).
 template <typename R> struct Body {
     double4 p;         // position, radius
     V3<double> v;      // clump velocity
@@ -1645,7 +1644,7 @@ template <typename R>
 __device__ __forceinline__ void load_kin(const void* __restrict__ kin, size_t N, int i, Body<R>& b) {
     const double4 a = ((const double4*)kin)[i];
     const R4<R>* kw = (const R4<R>*)((const double4*)kin + N);
-    const R4<R> w = kw[i], r = kw[N + i];
+    const R4<R> w = kw[2 * (size_t)i], r = kw[2 * (size_t)i + 1];
     b.v = v3(a.x, a.y, a.z);
     b.m = (R)a.w;
     b.w = xyz<R>(w);
@@ -1747,11 +1746,11 @@ __device__ __forceinline__ void boundary_contact(const Law<R>& L, const Body<R>&
     arm_out = Arm;
 }
 
-// pair history layout: R4 (Dv.xyz, Dr.x) at [q], R4 (Dt.xyz, Dr.y) at
-// [cap + q], Dr.z as a scalar after the 2*cap R4s
+// pair history layout: R4 (Dv.xyz, Dr.x) at [2q], R4 (Dt.xyz, Dr.y) at
+// [2q + 1] (one 32-byte record in FP32), Dr.z as a scalar after the 2*cap R4s
 template <typename R>
 __device__ __forceinline__ void hist_read(const R4<R>* H, size_t cap, size_t q, V3<R>& hs, V3<R>& ht, V3<R>& hr) {
-    R4<R> a = H[q], b = H[cap + q];
+    R4<R> a = H[2 * q], b = H[2 * q + 1];
     const R c = ((const R*)(H + 2 * cap))[q];
     hs = v3<R>(a.x, a.y, a.z);
     ht = v3<R>(b.x, b.y, b.z);
@@ -1759,8 +1758,8 @@ __device__ __forceinline__ void hist_read(const R4<R>* H, size_t cap, size_t q, 
 }
 template <typename R>
 __device__ __forceinline__ void hist_write(R4<R>* H, size_t cap, size_t q, V3<R> hs, V3<R> ht, V3<R> hr) {
-    H[q] = pack<R>(hs, hr.x);
-    H[cap + q] = pack<R>(ht, hr.y);
+    H[2 * q] = pack<R>(hs, hr.x);
+    H[2 * q + 1] = pack<R>(ht, hr.y);
     ((R*)(H + 2 * cap))[q] = hr.z;
 }
 
@@ -1950,16 +1949,16 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         const size_t hb = (size_t)slot * 3 * N;
         if (bb_old & (1u << slot)) {
-            R4<R> a = BH[hb + i], b = BH[hb + N + i], c = BH[hb + 2 * N + i];
+            R4<R> a = BH[hb + 3 * i], b = BH[hb + 3 * i + 1], c = BH[hb + 3 * i + 2];
             hs = xyz<R>(a); ht = xyz<R>(b); hr = xyz<R>(c);
         }
         V3<R> f, t, arm;
         LawOut<R> o;
         boundary_contact<R>(L, me, cvt<R>(nd), (R)Apd, (R)Dnd, cvt<R>(RVo), wv, ww, Rij, Mij, csm, hs, hr, ht,
                             f, t, o, arm);
-        BH[hb + i] = pack<R>(o.hs, R(0));
-        BH[hb + N + i] = pack<R>(o.ht, R(0));
-        BH[hb + 2 * N + i] = pack<R>(o.hr, R(0));
+        BH[hb + 3 * i] = pack<R>(o.hs, R(0));
+        BH[hb + 3 * i + 1] = pack<R>(o.ht, R(0));
+        BH[hb + 3 * i + 2] = pack<R>(o.hr, R(0));
         bb_new |= (uint16_t)(1u << slot);
         if (is_intr) {
             iF = iF + f;
@@ -2072,10 +2071,10 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         }
         if (!on) {
             to[p] = 0;
-            fs[ef] = zero;
-            fs[cap + ef] = zero;
-            bs[eb] = zero;
-            bs[cap + eb] = zero;
+            fs[2 * (size_t)ef] = zero;
+            fs[2 * (size_t)ef + 1] = zero;
+            bs[2 * (size_t)eb] = zero;
+            bs[2 * (size_t)eb + 1] = zero;
             continue;
         }
         load_kin<R>(kin, N, i, a);
@@ -2093,10 +2092,10 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         pair_contact2<R>(L, (R)P.cohesion, a, b, hs, hr, ht, fa, ta, tb, o, Ap, nd);
         hist_write<R>(Ho, cap, p, o.hs, o.ht, o.hr);
         to[p] = 1;
-        fs[ef] = pack<R>(fa, R(0));
-        fs[cap + ef] = pack<R>(ta, R(0));
-        bs[eb] = pack<R>(-fa, R(0));
-        bs[cap + eb] = pack<R>(tb, R(0));
+        fs[2 * (size_t)ef] = pack<R>(fa, R(0));
+        fs[2 * (size_t)ef + 1] = pack<R>(ta, R(0));
+        bs[2 * (size_t)eb] = pack<R>(-fa, R(0));
+        bs[2 * (size_t)eb + 1] = pack<R>(tb, R(0));
         if (EXPORT) {
             R4<R>* xf = (R4<R>*)d.xfcn;
             double4* xc = (double4*)d.xcpt;

@@ -123,7 +123,7 @@ struct Dev {
     int* key;         int* key2;         // global cell key at the last rebuild (sorted)
     void* kin;        void* kin2;        // double4 [N] clump velocity + mass, then Real4 [2][N] clump
                                          // angular velocity, world arm (see Body in kernels.cuh)
-    void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][3][N] boundary histories (Dv, Dt, Dr)
+    void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][N][3] boundary histories (Dv, Dt, Dr adjacent)
     uint16_t* bbits;  uint16_t* bbits2;  // [N] boundary slots in contact at the last step
     void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder),
                       // written on request only (getters, export): the clump pass sums the slots itself
@@ -166,14 +166,14 @@ struct Dev {
     // back into the current one), histories ping-pong between steps
     PairList L[2];
     int* lcur;        // index of the current list (0)
-    void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y), Real Dr.z; [2*cap] Real4 then [cap] Real
+    void* H[2];       // per pair: Real4 (Dv.xyz, Dr.x), Real4 (Dt.xyz, Dr.y) adjacent, [2*cap] Real4, then Real Dr.z [cap]
     uint8_t* touch[2];// [cap] pair in contact at the step that wrote H
     // contact slots, one per near row entry (see k_near), written by every
     // contact pass (zero for a pair that does not touch) and summed by the
     // next clump pass in row order: front entries hold the force and torque
     // on the row's subsphere as owner, back entries as partner
-    void* nfs;        // Real4 [2][cap]: force, then torque, per near front entry
-    void* nbs;        // Real4 [2][cap]: force, then torque, per near back entry
+    void* nfs;        // Real4 [cap][2]: force and torque (adjacent) per near front entry
+    void* nbs;        // Real4 [cap][2]: force and torque (adjacent) per near back entry
     int* nbpos;       // [cap] the near back entry of each near pair
     // near rows (the entries that can touch before the next rebuild)
     // (kept in each scene's pair region like the list: rows [N+S] with
