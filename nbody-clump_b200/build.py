@@ -39,6 +39,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "-I", os.path.join(os.path.dirname(HERE), "include")]
+    # extra nvcc flags, e.g. NBC_NVCC_FLAGS="-DNBC_PAIR_MINB=3" for another
+    # launch-bounds choice of the pair kernel
+    common += os.environ.get("NBC_NVCC_FLAGS", "").split()
     for src in SOURCES:
         obj = os.path.join(CSRC, "_obj_" + src.replace(".", "_") + ".o")
         lang = [] if src.endswith(".cu") else ["-x", "cu"] if src.endswith(".cu") else []

@@ -293,8 +293,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             s_cl[warp][12][lane] = q.w;
             __syncwarp();
             // ---- poses of the members, 32 at a time
-            double4* __restrict__ kv = (double4*)d.kin;
-            R4<R>* __restrict__ kw = (R4<R>*)(kv + d.N);   // angular velocity at 2i, arm at 2i + 1
+            double4* __restrict__ kv = (double4*)d.kin;   // per member: velocity + mass, angular velocity, arm
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
@@ -333,9 +332,9 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
                     cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
                     posw[i] = make_double4(p.x, p.y, p.z, o.w);
-                    kv[i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
-                    kw[2 * (size_t)i] = pack<R>(cvt<R>(wk), R(0));
-                    kw[2 * (size_t)i + 1] = pack<R>(cvt<R>(arm), R(0));
+                    kv[3 * (size_t)i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
+                    kv[3 * (size_t)i + 1] = make_double4(wk.x, wk.y, wk.z, 0.0);
+                    kv[3 * (size_t)i + 2] = make_double4(arm.x, arm.y, arm.z, 0.0);
                     const int sk = s_sc[warp][kk];
                     if (len_floor(cn) > d.par[sk].thresh) {
                         SceneDyn& y = d.dyn[sk];
@@ -724,10 +723,7 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
         d.part_fix2[i] = d.part_fix[o];
         d.level2[i] = d.level[o];
         d.bbits2[i] = d.bbits[o];
-        ((double4*)d.kin2)[i] = ((const double4*)d.kin)[o];
-        const R4<R>* k1 = (const R4<R>*)((const double4*)d.kin + N);
-        R4<R>* k2 = (R4<R>*)((double4*)d.kin2 + N);
-        for (int c = 0; c < 2; c++) k2[2 * (size_t)i + c] = k1[2 * (size_t)o + c];
+        for (int c = 0; c < 3; c++) ((double4*)d.kin2)[3 * (size_t)i + c] = ((const double4*)d.kin)[3 * (size_t)o + c];
         const R4<R>* b1 = (const R4<R>*)d.bhist;
         R4<R>* b2 = (R4<R>*)d.bhist2;
         const uint16_t bits = d.bbits[o];
@@ -1234,10 +1230,7 @@ __global__ void k_writeback(const Dev* __restrict__ dp) {
         d.part_fix[i] = d.part_fix2[i];
         d.level[i] = d.level2[i];
         d.key[i] = d.key2[i];
-        ((double4*)d.kin)[i] = ((const double4*)d.kin2)[i];
-        const R4<R>* k2 = (const R4<R>*)((const double4*)d.kin2 + N);
-        R4<R>* k1 = (R4<R>*)((double4*)d.kin + N);
-        for (int c = 0; c < 2; c++) k1[2 * (size_t)i + c] = k2[2 * (size_t)i + c];
+        for (int c = 0; c < 3; c++) ((double4*)d.kin)[3 * (size_t)i + c] = ((const double4*)d.kin2)[3 * (size_t)i + c];
         const uint16_t bits = d.bbits2[i];
         d.bbits[i] = bits;
         const R4<R>* b2 = (const R4<R>*)d.bhist2;
@@ -1557,7 +1550,8 @@ static __global__ void k_shift_rows(const Dev* __restrict__ dp, const int4* __re
 // ===========================================================================
 
 template <typename R> struct Law {
-    R kn_fac, ks_fac, damping, beta, mu, dt;
+    double kn_fac, ks_fac, damping;   // stiffness and damping factors (the normal force is FP64)
+    R beta, mu, dt;
 };
 
 template <typename R> struct LawOut {
@@ -1573,24 +1567,34 @@ template <typename R> struct LawOut {
 // toward this body's contact side, Vtot is this body's contact-point velocity
 // relative to the other's, Dth = dt (w_this - w_other) for walls and the
 // intruder, dt (w_other_side...) as the pair caller passes it.
+//
+// The normal force Kn Dn n + Cn Vnor is evaluated in FP64 whatever R is: on a
+// separating contact its elastic and damping terms nearly cancel (the net
+// force of the contact can be a thousandth of either), so rounding them to
+// FP32 would leave that contact's force with an error of 1e-4 of itself.  The
+// tangential, rolling and twisting parts, the histories and everything after
+// run in R.  With R = double every operation is the reference's, in its order.
 template <typename R>
-__device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vtot, V3<R> Dth, R Rij, R Mij,
-                                       R cs_mult, V3<R> H, V3<R> Mr, V3<R> Mt, LawOut<R>& o) {
-    const R sq = sqrt(Rij * Dn);
-    const R Kn = L.kn_fac * sq;
-    const R Cn = L.damping * sqrt(Kn * Mij);
-    const R Ks = L.ks_fac * sq;
-    const R Cs = cs_mult * L.damping * sqrt(Ks * Mij);
-    const R br = L.beta * Rij;
-    const R Kr = R(0.25) * Kn * br * br;
-    const R Cr = R(0.25) * Cn * br * br;
+__device__ __forceinline__ void hm_law(const Law<R>& L, V3<double> nd, double Dn, V3<double> Vtot, V3<R> Dth,
+                                       double Rij, double Mij, R cs_mult, V3<R> H, V3<R> Mr, V3<R> Mt,
+                                       LawOut<R>& o) {
+    const double sq = sqrt(Rij * Dn);
+    const double Kn = L.kn_fac * sq;
+    const double Cn = L.damping * sqrt(Kn * Mij);
+    const R Ks = (R)(L.ks_fac * sq);
+    const R Cs = cs_mult * (R)L.damping * sqrt(Ks * (R)Mij);
+    const R br = L.beta * (R)Rij;
+    const R Kr = R(0.25) * (R)Kn * br * br;
+    const R Cr = R(0.25) * (R)Cn * br * br;
     const R Kt = R(0.50) * Ks * br * br;
     const R Ct = R(0.50) * Cs * br * br;
-    const R ERR = dot(n, Vtot);
-    const V3<R> Vnor = ERR * n;
-    const V3<R> Vtan = Vtot - Vnor;
-    o.Fn = (Kn * Dn) * n + Cn * Vnor;
-    o.FnL = len_floor(o.Fn);
+    const double ERR = dot(nd, Vtot);
+    const V3<double> Vnor = ERR * nd;
+    const V3<R> Vtan = cvt<R>(Vtot - Vnor);
+    const V3<double> Fn = (Kn * Dn) * nd + Cn * Vnor;
+    const V3<R> n = cvt<R>(nd);
+    o.Fn = cvt<R>(Fn);
+    o.FnL = (R)len_floor(Fn);
     V3<R> Ft = (-Ks) * (L.dt * Vtan) + Cs * Vtan + H;
     const R FtL = len_floor(Ft);
     if (FtL > o.FnL * L.mu) {
@@ -1605,7 +1609,7 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vto
     const V3<R> DthR = Dth - DthT;
     V3<R> rm = Kr * DthR + Mr;
     const R rmL = len_floor(rm);
-    const R rcap = R(0.525) * L.beta * Rij * o.FnL;
+    const R rcap = R(0.525) * L.beta * (R)Rij * o.FnL;
     if (rmL > rcap) {
         rm = (rcap * (R(1) / rmL)) * rm;
         o.hr = rm;
@@ -1615,7 +1619,7 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vto
     }
     V3<R> tm = Kt * DthT + Mt;
     const R tmL = len_floor(tm);
-    const R tcap = R(0.65) * L.mu * L.beta * Rij * o.FnL;
+    const R tcap = R(0.65) * L.mu * L.beta * (R)Rij * o.FnL;
     if (tmL > tcap) {
         tm = (tcap * (R(1) / tmL)) * tm;
         o.ht = tm;
@@ -1627,28 +1631,26 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<R> n, R Dn, V3<R> Vto
     o.Mt = tm;
 }
 
-// The contact kinematics of a subsphere: its clump's velocity in FP64 (a
-// bed moving as a whole gives touching subspheres nearly equal velocities,
-// so their difference is taken before rounding to the law's precision), the
-// clump's angular velocity and the subsphere's world arm in the law's
-// precision.  Buffer layout: N double4 (velocity, mass), then per subsphere
-// two adjacent Real4 (angular velocity, arm: one 32-byte record in FP32).
+// The contact kinematics of a subsphere in FP64 (its clump's velocity and
+// angular velocity, its world arm and mass): a bed moving as a whole gives
+// touching subspheres nearly equal contact-point velocities, so their
+// difference is formed in FP64 before the law rounds anything.  Buffer
+// layout: three adjacent double4 per subsphere (velocity + mass, angular
+// velocity, arm).
 template <typename R> struct Body {
-    double4 p;         // position, radius
-    V3<double> v;      // clump velocity
-    V3<R> w, arm;      // clump angular velocity, world arm
-    R m;
+    double4 p;              // position, radius
+    V3<double> v, w, arm;   // clump velocity, clump angular velocity, world arm
+    double m;
 };
 
 template <typename R>
 __device__ __forceinline__ void load_kin(const void* __restrict__ kin, size_t N, int i, Body<R>& b) {
-    const double4 a = ((const double4*)kin)[i];
-    const R4<R>* kw = (const R4<R>*)((const double4*)kin + N);
-    const R4<R> w = kw[2 * (size_t)i], r = kw[2 * (size_t)i + 1];
+    const double4* k = (const double4*)kin + 3 * (size_t)i;
+    const double4 a = k[0], w = k[1], r = k[2];
     b.v = v3(a.x, a.y, a.z);
-    b.m = (R)a.w;
-    b.w = xyz<R>(w);
-    b.arm = xyz<R>(r);
+    b.m = a.w;
+    b.w = v3(w.x, w.y, w.z);
+    b.arm = v3(r.x, r.y, r.z);
 }
 
 template <typename R>
@@ -1657,44 +1659,14 @@ __device__ __forceinline__ void load_kin(const Dev& d, int i, Body<R>& b) {
 }
 
 
-// Pair contact seen from body a (the pair law of ContactForce_clump_cuk,
-// src/dem_force_clump.cu:3-163, with a in the role of particleI).  Returns
-// false when the pair does not overlap.
-template <typename R>
-__device__ __forceinline__ bool pair_contact(const Law<R>& L, R cohesion, const Body<R>& a, const Body<R>& b,
-                                             V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& fa, V3<R>& ta, LawOut<R>& o,
-                                             double& Ap_out, V3<double>& n_out) {
-    const double dx = b.p.x - a.p.x, dy = b.p.y - a.p.y, dz = b.p.z - a.p.z;
-    const double DistS = dx * dx + dy * dy + dz * dz;
-    const double DistL = sqrt(DistS);
-    const double Dn = a.p.w + b.p.w - DistL;
-    if (!(Dn > 0.0)) return false;
-    const double DistR = 1.0 / DistL;
-    const V3<double> nd = v3(DistR * dx, DistR * dy, DistR * dz);
-    const double Ap = 0.50 * (a.p.w * a.p.w - b.p.w * b.p.w + DistS) * DistR;
-    const double An = DistL - Ap;
-    const V3<R> n = cvt<R>(nd);
-    const R ra = (R)a.p.w, rb = (R)b.p.w;
-    const R Rij = ra * rb / (ra + rb);
-    const R Mij = a.m * b.m / (a.m + b.m);
-    const V3<R> ARMa = a.arm + (R)Ap * n;
-    const V3<R> ARMb = b.arm - (R)An * n;
-    const V3<R> Vtot = cvt<R>(b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
-    const V3<R> Dth = L.dt * (a.w - b.w);
-    hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
-    const R br = L.beta * Rij;
-    fa = (-o.Fn - o.Ft) + (cohesion * br * br) * n;
-    ta = ((-(R)Ap) * cross(n, o.Ft) - o.Mr) - o.Mt;
-    Ap_out = Ap;
-    n_out = nd;
-    return true;
-}
-
-// The pair law evaluated once for both bodies of a touching pair: the force
-// and torque on a (as pair_contact) and on b.  Seen from b every input of the
-// law is exactly negated (normal, relative velocity, rotation increment,
-// negated history), so the law's outputs are negated too: the force on b is
-// -fa and its torque uses b's own lever Ab = (rb^2 - ra^2 + d^2) / 2d.
+// The pair law of ContactForce_clump_cuk (src/dem_force_clump.cu:3-163) with
+// a in the role of particleI, evaluated once for both bodies of a touching
+// pair: the force and torque on a and the torque on b.  Seen from b every
+// input of the law is exactly negated (normal, relative velocity, rotation
+// increment, negated history), so the law's outputs are negated too: the
+// force on b is -fa and its torque uses b's own lever Ab = (rb^2 - ra^2 +
+// d^2) / 2d.  Geometry, lever arms and the contact-point velocity are FP64.
+// Returns false when the pair does not overlap.
 template <typename R>
 __device__ __forceinline__ bool pair_contact2(const Law<R>& L, R cohesion, const Body<R>& a, const Body<R>& b,
                                               V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& fa, V3<R>& ta, V3<R>& tb,
@@ -1709,16 +1681,15 @@ __device__ __forceinline__ bool pair_contact2(const Law<R>& L, R cohesion, const
     const double Ap = 0.50 * (a.p.w * a.p.w - b.p.w * b.p.w + DistS) * DistR;
     const double An = DistL - Ap;
     const double Ab = 0.50 * (b.p.w * b.p.w - a.p.w * a.p.w + DistS) * DistR;
+    const double Rij = a.p.w * b.p.w / (a.p.w + b.p.w);
+    const double Mij = a.m * b.m / (a.m + b.m);
+    const V3<double> ARMa = a.arm + Ap * nd;
+    const V3<double> ARMb = b.arm - An * nd;
+    const V3<double> Vtot = (b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
+    const V3<R> Dth = L.dt * cvt<R>(a.w - b.w);
+    hm_law<R>(L, nd, Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
     const V3<R> n = cvt<R>(nd);
-    const R ra = (R)a.p.w, rb = (R)b.p.w;
-    const R Rij = ra * rb / (ra + rb);
-    const R Mij = a.m * b.m / (a.m + b.m);
-    const V3<R> ARMa = a.arm + (R)Ap * n;
-    const V3<R> ARMb = b.arm - (R)An * n;
-    const V3<R> Vtot = cvt<R>(b.v - a.v) + (cross(b.w, ARMb) - cross(a.w, ARMa));
-    const V3<R> Dth = L.dt * (a.w - b.w);
-    hm_law<R>(L, n, (R)Dn, Vtot, Dth, Rij, Mij, R(1), H, Mr, Mt, o);
-    const R br = L.beta * Rij;
+    const R br = L.beta * (R)Rij;
     fa = (-o.Fn - o.Ft) + (cohesion * br * br) * n;
     const V3<R> nxF = cross(n, o.Ft);
     ta = ((-(R)Ap) * nxF - o.Mr) - o.Mt;
@@ -1729,21 +1700,22 @@ __device__ __forceinline__ bool pair_contact2(const Law<R>& L, R cohesion, const
 }
 
 // a wall or intruder contact: normal n (toward the subsphere), lever Ap,
-// overlap Dn, wall point RVo relative to the wall centre
+// overlap Dn, wall point RVo relative to the wall centre, wall velocity and
+// angular velocity wv, ww (FP64 geometry and velocities, as for pairs)
 template <typename R>
-__device__ __forceinline__ void boundary_contact(const Law<R>& L, const Body<R>& a, V3<R> n, R Ap, R Dn,
-                                                 V3<R> RVo, V3<R> wv, V3<R> ww, R Rij, R Mij, R cs_mult,
-                                                 V3<R> H, V3<R> Mr, V3<R> Mt, V3<R>& f, V3<R>& t,
-                                                 LawOut<R>& o, V3<R>& arm_out) {
-    const V3<R> Arm = (-a.arm) + Ap * n;
-    const V3<R> Vwall = cross(ww, RVo);
-    const V3<R> Vrel = cvt<R>(v3(a.v.x - (double)wv.x, a.v.y - (double)wv.y, a.v.z - (double)wv.z));
-    const V3<R> Vtot = Vrel + (cross(Arm, a.w) - Vwall);
-    const V3<R> Dth = L.dt * (a.w - ww);
-    hm_law<R>(L, n, Dn, Vtot, Dth, Rij, Mij, cs_mult, H, Mr, Mt, o);
+__device__ __forceinline__ void boundary_contact(const Law<R>& L, const Body<R>& a, V3<double> nd, double Ap,
+                                                 double Dn, V3<double> RVo, V3<double> wv, V3<double> ww,
+                                                 double Rij, double Mij, R cs_mult, V3<R> H, V3<R> Mr, V3<R> Mt,
+                                                 V3<R>& f, V3<R>& t, LawOut<R>& o, V3<R>& arm_out) {
+    const V3<double> Arm = (-a.arm) + Ap * nd;
+    const V3<double> Vwall = cross(ww, RVo);
+    const V3<double> Vtot = (a.v - wv) + (cross(Arm, a.w) - Vwall);
+    const V3<R> Dth = L.dt * cvt<R>(a.w - ww);
+    hm_law<R>(L, nd, Dn, Vtot, Dth, Rij, Mij, cs_mult, H, Mr, Mt, o);
+    const V3<R> n = cvt<R>(nd);
     f = o.Fn + o.Ft;
-    t = ((-Ap) * cross(n, o.Ft) - o.Mr) - o.Mt;
-    arm_out = Arm;
+    t = ((-(R)Ap) * cross(n, o.Ft) - o.Mr) - o.Mt;
+    arm_out = cvt<R>(Arm);
 }
 
 // pair history layout: R4 (Dv.xyz, Dr.x) at [2q], R4 (Dt.xyz, Dr.y) at
@@ -1840,7 +1812,7 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
     Body<R> me;
     bool have_kin = false;
     Law<R> L;
-    L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+    L.kn_fac = P.kn_fac; L.ks_fac = P.ks_fac; L.damping = P.damping;
     L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
     const V3<double> RV = v3(pp.x - P.w_c[0], pp.y - P.w_c[1], pp.z - P.w_c[2]);
     // cylinder geometry shared by its three regions
@@ -1860,9 +1832,10 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         double Apd = 0, Dnd = 0;
         V3<double> nd = v3(0.0, 0.0, 0.0), RVo = nd;
         bool on = false;
-        R Rij = (R)r, Mij = R(0), csm = R(2);
-        V3<R> wv = v3<R>((R)P.w_v[0], (R)P.w_v[1], (R)P.w_v[2]);
-        V3<R> ww = v3<R>((R)P.w_w[0], (R)P.w_w[1], (R)P.w_w[2]);
+        double Rij = r, Mij = 0.0;
+        R csm = R(2);
+        V3<double> wv = v3(P.w_v[0], P.w_v[1], P.w_v[2]);
+        V3<double> ww = v3(P.w_w[0], P.w_w[1], P.w_w[2]);
         if (is_wall && P.wall == WALL_CUBE) {
             const int ax = slot >> 1;
             const bool up = (slot & 1) == 0;
@@ -1898,8 +1871,8 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         } else {
             const SceneDyn& y = d.dyn[s];
             const V3<double> RI = v3(pp.x - y.intr_p[0], pp.y - y.intr_p[1], pp.z - y.intr_p[2]);
-            wv = v3<R>((R)y.intr_v[0], (R)y.intr_v[1], (R)y.intr_v[2]);
-            ww = v3<R>((R)P.intr_w[0], (R)P.intr_w[1], (R)P.intr_w[2]);
+            wv = v3(y.intr_v[0], y.intr_v[1], y.intr_v[2]);
+            ww = v3(P.intr_w[0], P.intr_w[1], P.intr_w[2]);
             csm = R(1);
             if (P.intr_shape == 1) {
                 const double cd = len_floor(RI);
@@ -1915,7 +1888,7 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
                 Dnd = r - gap;
                 Apd = gap;
                 on = Dnd > 0.0;
-                Rij = (R)(r * P.intr_R / (r + P.intr_R));
+                Rij = r * P.intr_R / (r + P.intr_R);
             } else {
                 const double LatDx = P.cell[0];
                 const V3<double> pv = v3(P.intr_axis[0], P.intr_axis[1], P.intr_axis[2]);
@@ -1944,7 +1917,7 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
             load_kin<R>(d, i, me);
             have_kin = true;
         }
-        if (is_intr) Mij = P.intr_motion == 1 ? (R)((double)me.m * P.intr_mass / ((double)me.m + P.intr_mass)) : me.m;
+        if (is_intr) Mij = P.intr_motion == 1 ? me.m * P.intr_mass / (me.m + P.intr_mass) : me.m;
         else Mij = me.m;
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         const size_t hb = (size_t)slot * 3 * N;
@@ -1954,7 +1927,7 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         }
         V3<R> f, t, arm;
         LawOut<R> o;
-        boundary_contact<R>(L, me, cvt<R>(nd), (R)Apd, (R)Dnd, cvt<R>(RVo), wv, ww, Rij, Mij, csm, hs, hr, ht,
+        boundary_contact<R>(L, me, nd, Apd, Dnd, RVo, wv, ww, Rij, Mij, csm, hs, hr, ht,
                             f, t, o, arm);
         BH[hb + 3 * i] = pack<R>(o.hs, R(0));
         BH[hb + 3 * i + 1] = pack<R>(o.ht, R(0));
@@ -2027,8 +2000,13 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
 // pending.
 constexpr int PR_THREADS = 256;
 
+// resident blocks of k_pairs per SM: the FP64 contact kinematics of two
+// bodies need up to 128 registers a thread without spilling
+#ifndef NBC_PAIR_MINB
+#define NBC_PAIR_MINB 2
+#endif
 template <typename R, bool EXPORT>
-__global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__ dp) {
+__global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
@@ -2083,7 +2061,7 @@ __global__ void __launch_bounds__(PR_THREADS, 4) k_pairs(const Dev* __restrict__
         if (ti[p]) hist_read<R>(Hi, cap, p, hs, ht, hr);
         const ScenePar& P = d.par[s];
         Law<R> L;
-        L.kn_fac = (R)P.kn_fac; L.ks_fac = (R)P.ks_fac; L.damping = (R)P.damping;
+        L.kn_fac = P.kn_fac; L.ks_fac = P.ks_fac; L.damping = P.damping;
         L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
         V3<R> fa, ta, tb;
         LawOut<R> o;
