@@ -401,8 +401,8 @@ def algorithmic_contact_bytes(N, nnear, ntouch, precision):
     """Unique bytes the contact kernel (k_pairs) must move per step.
 
     Per near pair (the pairs that can touch before the next rebuild, each
-    visited once): its near front slot index, near back slot index, partner
-    and owner 4 B each, the touch flag written 1 B, both subspheres' FP64
+    visited once): its near front record (pair slot, partner, owner and near
+    back slot, 16 B), the touch flag written 1 B, both subspheres' FP64
     position and radius 2 x 32 B, and the four contact slots written (force
     and torque on each side, 4 Real4).  Per touching pair: the previous touch
     flag 1 B, the spring history read and written (2 Real4 + 1 Real each way)

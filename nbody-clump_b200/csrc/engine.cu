@@ -243,6 +243,7 @@ class EngineT final : public EngineBase {
             const int started = read_gstep() - pend_before_;
             launches_ += 3LL * started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
             if (read_int(h_.halt)) {
+                check_scan();
                 // the last step started stopped at its rebuild: finish it on the host path
                 steps_done_ += started - 1;
                 recover_halt();
@@ -296,10 +297,10 @@ class EngineT final : public EngineBase {
         copy_(t.data(), h_.touch[(hg + 1) & 1], (size_t)h_.cap, cudaMemcpyDeviceToHost);
         long long n = 0, c = 0;
         for (int s = 0; s < S_; s++) {
-            std::vector<int> idx(y[s].nnear);
+            std::vector<int4> rec(y[s].nnear);
             if (y[s].nnear)
-                copy_(idx.data(), h_.nfp + y[s].pair_off, (size_t)y[s].nnear * sizeof(int), cudaMemcpyDeviceToHost);
-            for (int p : idx) c += t[p] != 0;
+                copy_(rec.data(), h_.nfr + y[s].pair_off, (size_t)y[s].nnear * sizeof(int4), cudaMemcpyDeviceToHost);
+            for (const int4& e : rec) c += t[e.x] != 0;
             n += y[s].nnear;
         }
         if (nnear) *nnear = n;
@@ -685,7 +686,7 @@ class EngineT final : public EngineBase {
             blk(h_.touch[g] + o, np);
             blk(h_.nearf + o, np);
             blk(h_.nbpos + o, np * sizeof(int));
-            blk(h_.nfp + o, nn * sizeof(int));
+            blk(h_.nfr + o, nn * sizeof(int4));
             blk(h_.nbq + o, nn * sizeof(int));
             R4<R>* fs = (R4<R>*)h_.nfs;
             R4<R>* bs = (R4<R>*)h_.nbs;
@@ -770,7 +771,12 @@ class EngineT final : public EngineBase {
         return n;
     }
     // kernels one rebuild launches (launch_rebuild)
-    int rebuild_launches() const { return 1 + passes_ * 5 + 3 + 2 + 1 + 6 + 1 + (hgrid_ ? 2 : 0) + 4 + 8 + 5; }
+    // kernels of one rebuild in a graph (the eager path adds a k_check_cap):
+    // plan, hash, 3 per radix pass, cellrange, cellstart, reorder, 2 fills,
+    // search, scan, check, (hgrid: fill), compact, (hgrid: xsort), backref,
+    // carry, 2 write-backs, swap, 2 near passes and their scan, commit, 2
+    // boundary-flag passes and their scan, nprefix
+    int rebuild_launches() const { return 24 + 3 * passes_ + (hgrid_ ? 2 : 0); }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -1009,6 +1015,7 @@ class EngineT final : public EngineBase {
             h_.kc_done = flags + 6;
             h_.lstep = flags + 7;
             h_.loop_left = flags + 8;
+            h_.scan_fail = flags + 9;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
             h_.hist = m.take<int>((size_t)256 * rs_blocks_);
             h_.perm = m.take<int>(N);
@@ -1024,7 +1031,10 @@ class EngineT final : public EngineBase {
             h_.cnt_b = m.take<int>(N + 1);
             h_.sfc = m.take<int>(N);
             h_.xcnt = m.take<int>(N);
-            h_.scan_tmp = m.take<int>(std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE)) + 1);
+            const long long scan_tiles = std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE));
+            h_.scan_tmp = m.take<int>(scan_tiles + 1);
+            h_.scan_st = m.take<unsigned long long>(2 * scan_tiles + 2);
+            h_.scan_ctl = m.take<int>(2);
             for (int l = 0; l < 2; l++) {
                 h_.L[l].row = m.take<int>(N + S_);
                 h_.L[l].brow = m.take<int>(N + S_);
@@ -1087,7 +1097,7 @@ class EngineT final : public EngineBase {
             h_.nfs = m.take<R4<R>>(2 * cap);
             h_.nbs = m.take<R4<R>>(2 * cap);
             h_.nbpos = m.take<int>(cap);
-            h_.nfp = m.take<int>(cap);
+            h_.nfr = m.take<int4>(cap);
             h_.nbq = m.take<int>(cap);
             h_.nearf = m.take<uint8_t>(cap);
             h_.xfcn = m.take<R4<R>>(cap);
@@ -1106,7 +1116,7 @@ class EngineT final : public EngineBase {
     // Bytes of the pair buffers per pair slot.
     static double bytes_per_pair() {
         return 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) +
-               3 * sizeof(int) + 1;
+               2 * sizeof(int) + sizeof(int4) + 1;
     }
     // Region capacities for the first lists: slack x each scene's pairs; with
     // the default slack at least the reference's own list capacity, n_sub x
@@ -1181,7 +1191,7 @@ class EngineT final : public EngineBase {
         const int B = 256;
         if (moved > 0)
             k_relayout<R><<<std::min(148 * 8, cdiv(moved, B)), B, 0, stream_>>>(
-                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.nfp, old.nbq, old.nbpos, old.cap,
+                d_, old.L[0], old.H[hg & 1], old.touch[hg & 1], old.nearf, old.nfr, old.nbq, old.nbpos, old.cap,
                 relmap_, moved);
         k_shift_rows<<<std::min(148 * 8, cdiv((long long)N_ + S_, B)), B, 0, stream_>>>(d_, relmap_);
         CK(cudaGetLastError());
@@ -1248,7 +1258,11 @@ class EngineT final : public EngineBase {
         return rd;
     }
 
+    void check_scan() {
+        if (read_int(h_.scan_fail)) throw CudaError("a list-rebuild scan gave up waiting on a tile (step halted)");
+    }
     void check_errors() {
+        check_scan();
         std::vector<SceneDyn> y(S_);
         copy_(y.data(), h_.dyn, S_ * sizeof(SceneDyn), cudaMemcpyDeviceToHost);
         for (int s = 0; s < S_; s++)
@@ -1311,11 +1325,10 @@ class EngineT final : public EngineBase {
     }
     // exclusive scan of a[0, n) (or of a[0, *dn) when dn is given, n then
     // bounds it)
-    void scan(int* a, int n, const int* dn = nullptr) {
-        const int nb = std::min(cdiv(n, SC_TILE), 148 * 8);
-        k_scan_tiles<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp, dn);
-        k_scan_sums<<<1, SC_THREADS, 0, stream_>>>(h_.scan_tmp, cdiv(n, SC_TILE), dn);
-        k_scan_add<<<nb, SC_THREADS, 0, stream_>>>(a, n, h_.scan_tmp, dn);
+    // exclusive scans of a0 (and a1, of the same length) in one launch
+    void scan(int* a0, int* a1, int n, const int* dn = nullptr) {
+        const int nb = std::max(1, cdiv(n, SC_TILE)) * (a1 ? 2 : 1);
+        k_scan1<<<nb, SC_THREADS, 0, stream_>>>(a0, a1, n, dn, h_.scan_st, h_.scan_ctl, h_.halt, h_.scan_fail);
     }
     // The rebuild block of src/dem_simulation_clump.cu:124-176, over the
     // scenes whose rebuild flag is set: every kernel but the near rows walks
@@ -1333,7 +1346,7 @@ class EngineT final : public EngineBase {
         const int gR = std::min(rs_blocks_, 148 * 8);
         for (int p = 0; p < passes_; p++) {
             k_rs_hist<<<gR, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, pl + PL_T);
-            scan(h_.hist, 256 * rs_blocks_, pl + PL_HIST);
+            scan(h_.hist, nullptr, 256 * rs_blocks_, pl + PL_HIST);
             k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T);
             std::swap(ki, ko);
             std::swap(vi, vo);
@@ -1346,13 +1359,13 @@ class EngineT final : public EngineBase {
         if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else k_search<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.cnt_f, N_ + 1, pl + PL_T1);
-        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_f, h_.cnt_b, N_ + 1, pl + PL_T1);
         CK(cudaGetLastError());
         if (eager) {
             // size the regions to the first lists, or grow the ones that overflow
             k_check_cap<<<1, 256, 0, stream_>>>(d_, 0);
             CK(cudaStreamSynchronize(stream_));
+            check_scan();
             std::vector<int> need(S_);
             copy_(need.data(), h_.need, S_ * sizeof(int), cudaMemcpyDeviceToHost);
             std::vector<SceneDyn> y = read_dyn_all();
@@ -1382,13 +1395,12 @@ class EngineT final : public EngineBase {
         // near rows of the rebuilt scenes (counts, scans, rows)
         const int gNr = std::min(cdiv(N_, SEARCH_THREADS / 4), 148 * 16);
         k_near<false, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.cnt_f, N_ + 1, pl + PL_T1);
-        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_f, h_.cnt_b, N_ + 1, pl + PL_T1);
         k_near<true, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
         k_commit<<<std::min(cdiv((long long)K_ + S_ + 1, B), 148 * 8), B, 0, stream_>>>(d_);
         // boundary candidates of the rebuilt scenes (flags, scan, list)
         k_bflag<false><<<std::min(cdiv((long long)N_ + 1, B), 148 * 16), B, 0, stream_>>>(d_);
-        scan(h_.cnt_b, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_b, nullptr, N_ + 1, pl + PL_T1);
         k_bflag<true><<<gN, B, 0, stream_>>>(d_);
         k_nprefix<<<1, SC_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());

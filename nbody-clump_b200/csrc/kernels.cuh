@@ -513,6 +513,106 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict_
     }
 }
 
+// --- exclusive scan of ints in one launch (decoupled look-back) ----------
+// One or two arrays of the same length (n, or *dn) in one launch.  Every
+// block takes one tile from a ticket counter: tickets [0, tiles) are the
+// tiles of the first array, [tiles, 2 tiles) those of the second.  A tile
+// publishes its aggregate, then looks back over its array's earlier tiles
+// (32 at a time, one per lane of warp 0) and sums aggregates until it meets
+// an inclusive prefix, and publishes its own inclusive prefix.  Tickets are
+// taken in the order blocks start, so a tile waits only on tiles held by
+// blocks that are already running: the wait always ends.  Each wait is still
+// bounded (SCAN_SPIN_LIMIT polls); a block that gives up sets *fail and
+// *halt, so every later kernel of the step returns at once and the host
+// reports the failure instead of using the result.  The last block of the
+// grid clears the tile states and the counters for the next scan.
+// ctl: [0] ticket counter, [1] finished blocks.  st: one word per ticket,
+// (state << 32) | value, state 1 = aggregate, 2 = inclusive prefix.
+constexpr unsigned long long SCAN_AGG = 1ull << 32, SCAN_INC = 2ull << 32;
+constexpr int SCAN_SPIN_LIMIT = 1 << 22;
+
+static __global__ void __launch_bounds__(SC_THREADS) k_scan1(int* __restrict__ a0, int* __restrict__ a1, int n,
+                                                            const int* __restrict__ dn,
+                                                            unsigned long long* __restrict__ st, int* __restrict__ ctl,
+                                                            int* __restrict__ halt, int* __restrict__ fail) {
+    __shared__ int sh[SC_THREADS / 32];
+    __shared__ int s_ticket, s_excl, s_last;
+    const int nn = dn ? *dn : n;
+    const int tiles = (nn + SC_TILE - 1) / SC_TILE;
+    const int narr = a1 ? 2 : 1;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl[0], 1);
+    __syncthreads();
+    const int tk = s_ticket;
+    if (tk < narr * tiles) {
+        const int arr = tk >= tiles ? 1 : 0;
+        const int b = tk - arr * tiles;      // tile of its array
+        int* __restrict__ a = arr ? a1 : a0;
+        unsigned long long* __restrict__ sa = st + (size_t)arr * tiles;
+        const int base = b * SC_TILE + threadIdx.x * SC_ITEMS;
+        int v[SC_ITEMS], sum = 0;
+#pragma unroll
+        for (int j = 0; j < SC_ITEMS; j++) { v[j] = base + j < nn ? a[base + j] : 0; sum += v[j]; }
+        int total;
+        int ex = block_excl_scan(sum, sh, total);
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int excl = 0;
+            if (b == 0) {
+                if (lane == 0) atomicExch(&sa[0], SCAN_INC | (unsigned)total);
+            } else {
+                if (lane == 0) atomicExch(&sa[b], SCAN_AGG | (unsigned)total);
+                bool ok = true;
+                for (int j = b - 1;; j -= 32) {
+                    const int t = j - lane;
+                    unsigned long long w = SCAN_INC;   // before the first tile: an inclusive zero
+                    if (t >= 0) {
+                        int polls = 0;
+                        while (((w = *(volatile unsigned long long*)&sa[t]) >> 32) == 0) {
+                            if (++polls > SCAN_SPIN_LIMIT) { ok = false; w = SCAN_INC; break; }
+                            __nanosleep(64);
+                        }
+                    }
+                    const unsigned inc = __ballot_sync(0xffffffffu, (w >> 32) == 2);
+                    const int upto = inc ? __ffs(inc) - 1 : 31;   // the nearest inclusive prefix ends the sum
+                    int c = lane <= upto ? (int)(unsigned)w : 0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+                    excl += c;
+                    if (inc) break;
+                }
+                if (!__all_sync(0xffffffffu, ok) && lane == 0) {
+                    atomicExch(fail, 1);
+                    atomicExch(halt, 1);
+                }
+                if (lane == 0) atomicExch(&sa[b], SCAN_INC | (unsigned)(excl + total));
+            }
+            if (lane == 0) s_excl = excl;
+        }
+        __syncthreads();
+        ex += s_excl;
+#pragma unroll
+        for (int j = 0; j < SC_ITEMS; j++) {
+            if (base + j < nn) a[base + j] = ex;
+            ex += v[j];
+        }
+    }
+    // every block has taken its ticket and is done with the tile states
+    // once the finished count reaches the grid: the last one resets them
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ctl[1], 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int k = threadIdx.x; k < narr * tiles; k += SC_THREADS) st[k] = 0ull;
+        if (threadIdx.x == 0) {
+            ctl[0] = 0;
+            ctl[1] = 0;
+        }
+    }
+}
+
 // --- LSD radix sort, 8-bit digits, stable (the reference sorts with CUB's
 // stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
 constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
@@ -1349,7 +1449,7 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
             const bool nr = k < re && nearf[k];
             if (tother && k < re && !nr) tother[k] = 0;
             const unsigned m = __ballot_sync(gm, nr) >> gshift;
-            if (FILL && nr) d.nfp[rf + nf + __popc(m & lt)] = k;
+            if (FILL && nr) d.nfr[rf + nf + __popc(m & lt)] = make_int4(k, Lc.nbr[k], i, -1);
             nf += __popc(m);
         }
         const int bs = Lc.brow[i + s], be = Lc.brow[i + s + 1];
@@ -1407,7 +1507,10 @@ static __global__ void __launch_bounds__(SC_THREADS) k_nprefix(const Dev* __rest
 // FILL pass lists the candidates in the scene's range of bidx, and
 // k_boundary visits only them.  FILL = false writes the flags into cnt_b of
 // the rebuilt concatenation (free after k_commit); FILL = true writes the
-// list at the scanned offsets and the scene's count.
+// list at the scanned offsets and the scene's count, and completes each
+// rebuilt subsphere's near front records with the near back entry of their
+// pair (k_near's FILL pass writes both rows at once, so a front record
+// cannot take it there).
 template <bool FILL>
 __global__ void k_bflag(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -1423,6 +1526,7 @@ __global__ void k_bflag(const Dev* __restrict__ dp) {
             const int c = d.cnt_b[t] - d.cnt_b[t0];
             if (d.cnt_b[t + 1] - d.cnt_b[t]) d.bidx[P.sub_off + c] = i;
             if (i == P.sub_off + P.nsub - 1) d.dyn[s].nbound = d.cnt_b[t + 1] - d.cnt_b[t0];
+            for (int e = d.nrow[i + s]; e < d.nrow[i + s + 1]; e++) d.nfr[e].w = d.nbpos[d.nfr[e].x];
             continue;
         }
         bool cand = P.has_intr;
@@ -1485,7 +1589,7 @@ static __global__ void k_commit(const Dev* __restrict__ dp) {
 template <typename R>
 __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* __restrict__ oh,
                            const uint8_t* __restrict__ ot, const uint8_t* __restrict__ onear,
-                           const int* __restrict__ onfp, const int* __restrict__ onbq,
+                           const int4* __restrict__ onfr, const int* __restrict__ onbq,
                            const int* __restrict__ onbpos, int ocap,
                            const int4* __restrict__ map, int total) {
     const Dev& d = *dp;
@@ -1511,7 +1615,8 @@ __global__ void k_relayout(const Dev* __restrict__ dp, PairList ol, const void* 
         const uint8_t f = ot[po];
         d.touch[hg & 1][pn] = f;
         d.nearf[pn] = onear[po];
-        d.nfp[pn] = onfp[po] + (m.y - m.x);   // slots past the near count carry nothing
+        const int4 fr = onfr[po];             // slots past the near count carry nothing
+        d.nfr[pn] = make_int4(fr.x + (m.y - m.x), fr.y, fr.z, fr.w + (m.y - m.x));
         d.nbq[pn] = onbq[po] + (m.y - m.x);
         d.nbpos[pn] = onear[po] ? onbpos[po] + (m.y - m.x) : -1;
         if (f) {
@@ -2010,15 +2115,11 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
     const Dev& d = *dp;
     if (*d.halt) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-    const int lc = *d.lcur, hg = *d.hgen;
-    const PairList& Lst = d.L[lc & 1];
+    const int hg = *d.hgen;
     const int S = d.S;
     const int* __restrict__ npre = d.nprefix;
     const int np = npre[S];
-    const int* __restrict__ nfp = d.nfp;
-    const int* __restrict__ nbpos = d.nbpos;
-    const int* __restrict__ nbr = Lst.nbr;
-    const int* __restrict__ own = Lst.own;
+    const int4* __restrict__ nfr = d.nfr;
     const double4* __restrict__ posr = d.posr;
     const void* __restrict__ kin = d.kin;
     const size_t N = (size_t)d.N;
@@ -2036,10 +2137,8 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
         const SceneDyn& ys = d.dyn[s];
         if (d.has_stops && ys.frozen) continue;
         const int ef = ys.pair_off + (w - npre[s]);
-        const int p = nfp[ef];
-        const int eb = nbpos[p];
-        const int jr = nbr[p];
-        const int i = own[p];
+        const int4 rec = nfr[ef];   // pair slot, partner, owner, near back entry: one load
+        const int p = rec.x, jr = rec.y, i = rec.z, eb = rec.w;
         Body<R> a, b;
         bool on = jr >= 0;   // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)
         if (on) {

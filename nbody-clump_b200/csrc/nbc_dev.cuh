@@ -150,6 +150,9 @@ struct Dev {
     int* sfc;                             // [N] same-level front count (hierarchical grid)
     int* xcnt;                            // [N] cross-level entries placed so far (hierarchical grid)
     int* scan_tmp;                        // block sums
+    unsigned long long* scan_st;          // single-launch scan: tile states (zero between scans)
+    int* scan_ctl;                        // single-launch scan: ticket and finished-block counters
+    int* scan_fail;                       // a single-launch scan gave up a wait (the step halted)
     int* any_rebuild;                     // device flag: some scene rebuilds this step
     // rebuild plan (k_plan): the scenes rebuilt at this step in ascending
     // order and prefix sums over them; every rebuild kernel runs over the
@@ -180,7 +183,7 @@ struct Dev {
     // absolute slots, one row array per scene with its end entry)
     int* nrow;        // [N+S] near front offsets
     int* nbrow;       // [N+S] near back offsets
-    int* nfp;         // [cap] near front entries: pair slot
+    int4* nfr;        // [cap] near front entries: pair slot, partner, owner, near back entry
     int* nbq;         // [cap] near back entries: pair slot
     int* nprefix;     // [S+1] prefix over the scenes of their near pairs (the contact pass's work items)
     int* bidx;        // [N] boundary candidates of scene s at [sub_off, sub_off + nbound) (see k_bflag)
