@@ -832,7 +832,8 @@ class EngineT final : public EngineBase {
         hflag_ = g_pinned.get();
         mem_.stream = stream_;
         DevMem::keep_pool(opt_.device);
-        search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
+        search_lanes_ = opt_.search_lanes == 1 || opt_.search_lanes == 16 || opt_.search_lanes == 32
+                            ? opt_.search_lanes : 8;
         clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
         pair_bps_ = opt_.pair_blocks >= 2 && opt_.pair_blocks <= 16 ? opt_.pair_blocks : 12;
         CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
@@ -1337,8 +1338,8 @@ class EngineT final : public EngineBase {
     void launch_rebuild(bool eager) {
         const int B = 128;
         const int gN = std::min(cdiv(N_, B), 148 * 16);         // grid-stride grids
-        const int sl = search_lanes_;
-        const int gS = std::min(cdiv(N_, SEARCH_THREADS / sl), 148 * 16);
+        const int sl = search_lanes_;   // 1: the block-cooperative search (its long rows refilled by 8 lanes)
+        const int gS = std::min(cdiv(N_, SEARCH_THREADS / (sl == 1 ? 8 : sl)), 148 * 16);
         const int* pl = h_.plan;
         k_plan<<<1, SC_THREADS, 0, stream_>>>(d_);
         k_hash<<<gN, B, 0, stream_>>>(d_);
@@ -1356,7 +1357,8 @@ class EngineT final : public EngineBase {
         k_reorder<R><<<gN, B, 0, stream_>>>(d_);
         k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, pl + PL_T1, 0);
         k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, pl + PL_T1, 0);
-        if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        if (sl == 1) k_search_flat<<<std::min(cdiv(N_, SF_G), 148 * 8), SEARCH_THREADS, 0, stream_>>>(d_);
+        else if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else k_search<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         scan(h_.cnt_f, h_.cnt_b, N_ + 1, pl + PL_T1);
