@@ -241,7 +241,7 @@ class EngineT final : public EngineBase {
         if (pend_ > 0) {
             CK(cudaStreamSynchronize(stream_));
             const int started = read_gstep() - pend_before_;
-            launches_ += 3LL * started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
+            launches_ += (1LL + CONTACT_LAUNCHES) * started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
             if (read_int(h_.halt)) {
                 check_scan();
                 // the last step started stopped at its rebuild: finish it on the host path
@@ -1017,6 +1017,7 @@ class EngineT final : public EngineBase {
             h_.lstep = flags + 7;
             h_.loop_left = flags + 8;
             h_.scan_fail = flags + 9;
+            h_.tcount = flags + 10;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
             h_.hist = m.take<int>((size_t)256 * rs_blocks_);
             h_.perm = m.take<int>(N);
@@ -1099,6 +1100,7 @@ class EngineT final : public EngineBase {
             h_.nbs = m.take<R4<R>>(2 * cap);
             h_.nbpos = m.take<int>(cap);
             h_.nfr = m.take<int4>(cap);
+            h_.tlist = m.take<int2>(cap);
             h_.nbq = m.take<int>(cap);
             h_.nearf = m.take<uint8_t>(cap);
             h_.xfcn = m.take<R4<R>>(cap);
@@ -1117,7 +1119,7 @@ class EngineT final : public EngineBase {
     // Bytes of the pair buffers per pair slot.
     static double bytes_per_pair() {
         return 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) +
-               2 * sizeof(int) + sizeof(int4) + 1;
+               2 * sizeof(int) + sizeof(int4) + sizeof(int2) + 1;
     }
     // Region capacities for the first lists: slack x each scene's pairs; with
     // the default slack at least the reference's own list capacity, n_sub x
@@ -1308,12 +1310,18 @@ class EngineT final : public EngineBase {
         // stays valid as the list grows; a small scene gets a small grid so
         // that other scenes' kernels run beside it
         const int pg = std::min(sm_count_ * pair_bps_, cdiv(3LL * N_, PR_THREADS));
+#if NBC_PAIR_SPLIT
+        k_pairs_test<R><<<std::min(sm_count_ * 8, cdiv(3LL * N_, PR_THREADS)), PR_THREADS, 0, stream_>>>(d_);
+        if (exp) k_pairs_law<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
+        else k_pairs_law<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
+#else
         if (exp) k_pairs<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
         else k_pairs<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
+#endif
         CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
         CK(cudaGetLastError());
         mark(6, stream_);
-        if (!capturing_) launches_ += 2;
+        if (!capturing_) launches_ += CONTACT_LAUNCHES;
         // the export step also records the per-subsphere pair part
         if (exp) launch_sum(true);
     }
@@ -1324,9 +1332,8 @@ class EngineT final : public EngineBase {
         else k_sum<R, false><<<cdiv(N_, CT_THREADS), CT_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
-    // exclusive scan of a[0, n) (or of a[0, *dn) when dn is given, n then
-    // bounds it)
-    // exclusive scans of a0 (and a1, of the same length) in one launch
+    // exclusive scans of a0 (and a1, of the same length) over [0, n), or
+    // over [0, *dn) when dn is given (n then bounds it), in one launch
     void scan(int* a0, int* a1, int n, const int* dn = nullptr) {
         const int nb = std::max(1, cdiv(n, SC_TILE)) * (a1 ? 2 : 1);
         k_scan1<<<nb, SC_THREADS, 0, stream_>>>(a0, a1, n, dn, h_.scan_st, h_.scan_ctl, h_.halt, h_.scan_fail);

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
     if (do_pre && blockIdx.x == 0 && threadIdx.x == 0) {
         *d.hgen += 1;
         *d.gstep += 1;
+        *d.tcount = 0;   // the split contact pass's touching list of this step
     }
     // warp-uniform: this warp holds clumps of a scene that moves (a warp whose
     // clumps all belong to scenes standing still skips its work)
@@ -2338,6 +2339,44 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
     return a.w + b.w - sqrt(d2) > 0.0;
 }
 
+// The law of one touching near pair (front entry ef of scene s, pair slot p,
+// owner i, partner jr, near back entry eb; a.p and b.p loaded): kinematics
+// and spring history in, new history, touch flag and the four contact slots
+// out (and the export record).
+template <typename R, bool EXPORT>
+__device__ __forceinline__ void pair_law(const Dev& d, int s, int ef, int p, int i, int jr, int eb, Body<R>& a,
+                                         Body<R>& b) {
+    const int hg = *d.hgen;
+    const size_t cap = (size_t)d.cap;
+    load_kin<R>(d.kin, (size_t)d.N, i, a);
+    load_kin<R>(d.kin, (size_t)d.N, jr, b);
+    V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
+    if (d.touch[hg & 1][p]) hist_read<R>((const R4<R>*)d.H[hg & 1], cap, p, hs, ht, hr);
+    const ScenePar& P = d.par[s];
+    Law<R> L;
+    L.kn_fac = P.kn_fac; L.ks_fac = P.ks_fac; L.damping = P.damping;
+    L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
+    V3<R> fa, ta, tb;
+    LawOut<R> o;
+    double Ap;
+    V3<double> nd;
+    pair_contact2<R>(L, (R)P.cohesion, a, b, hs, hr, ht, fa, ta, tb, o, Ap, nd);
+    hist_write<R>((R4<R>*)d.H[(hg + 1) & 1], cap, p, o.hs, o.ht, o.hr);
+    d.touch[(hg + 1) & 1][p] = 1;
+    R4<R>* fs = (R4<R>*)d.nfs;
+    R4<R>* bs = (R4<R>*)d.nbs;
+    fs[2 * (size_t)ef] = pack<R>(fa, R(0));
+    fs[2 * (size_t)ef + 1] = pack<R>(ta, R(0));
+    bs[2 * (size_t)eb] = pack<R>(-fa, R(0));
+    bs[2 * (size_t)eb + 1] = pack<R>(tb, R(0));
+    if (EXPORT) {
+        R4<R>* xf = (R4<R>*)d.xfcn;
+        double4* xc = (double4*)d.xcpt;
+        xf[p] = pack<R>(-o.Fn, R(0));
+        xc[p] = make_double4(a.p.x + Ap * nd.x, a.p.y + Ap * nd.y, a.p.z + Ap * nd.z, 0.0);
+    }
+}
+
 // Pairs, one thread per near front entry (grid-stride, so a captured launch
 // covers a list that has grown since): the overlap test, and for touching
 // pairs the law once (ContactForce_clump_cuk, src/dem_force_clump.cu:3-163,
@@ -2354,6 +2393,12 @@ constexpr int PR_THREADS = 256;
 #ifndef NBC_PAIR_MINB
 #define NBC_PAIR_MINB 2
 #endif
+// 1: the contact pass as two kernels (overlap test and touching list, then
+// the law over the list); 0: one kernel
+#ifndef NBC_PAIR_SPLIT
+#define NBC_PAIR_SPLIT 0
+#endif
+constexpr int CONTACT_LAUNCHES = NBC_PAIR_SPLIT ? 3 : 2;   // with k_boundary
 template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -2365,12 +2410,6 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
     const int np = npre[S];
     const int4* __restrict__ nfr = d.nfr;
     const double4* __restrict__ posr = d.posr;
-    const void* __restrict__ kin = d.kin;
-    const size_t N = (size_t)d.N;
-    const size_t cap = (size_t)d.cap;
-    const R4<R>* __restrict__ Hi = (const R4<R>*)d.H[hg & 1];
-    R4<R>* __restrict__ Ho = (R4<R>*)d.H[(hg + 1) & 1];
-    const uint8_t* __restrict__ ti = d.touch[hg & 1];
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
     R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
     R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
@@ -2398,31 +2437,76 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
             bs[2 * (size_t)eb + 1] = zero;
             continue;
         }
-        load_kin<R>(kin, N, i, a);
-        load_kin<R>(kin, N, jr, b);
-        V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
-        if (ti[p]) hist_read<R>(Hi, cap, p, hs, ht, hr);
-        const ScenePar& P = d.par[s];
-        Law<R> L;
-        L.kn_fac = P.kn_fac; L.ks_fac = P.ks_fac; L.damping = P.damping;
-        L.beta = (R)P.beta; L.mu = (R)P.mu; L.dt = (R)P.dt;
-        V3<R> fa, ta, tb;
-        LawOut<R> o;
-        double Ap;
-        V3<double> nd;
-        pair_contact2<R>(L, (R)P.cohesion, a, b, hs, hr, ht, fa, ta, tb, o, Ap, nd);
-        hist_write<R>(Ho, cap, p, o.hs, o.ht, o.hr);
-        to[p] = 1;
-        fs[2 * (size_t)ef] = pack<R>(fa, R(0));
-        fs[2 * (size_t)ef + 1] = pack<R>(ta, R(0));
-        bs[2 * (size_t)eb] = pack<R>(-fa, R(0));
-        bs[2 * (size_t)eb + 1] = pack<R>(tb, R(0));
-        if (EXPORT) {
-            R4<R>* xf = (R4<R>*)d.xfcn;
-            double4* xc = (double4*)d.xcpt;
-            xf[p] = pack<R>(-o.Fn, R(0));
-            xc[p] = make_double4(a.p.x + Ap * nd.x, a.p.y + Ap * nd.y, a.p.z + Ap * nd.z, 0.0);
+        pair_law<R, EXPORT>(d, s, ef, p, i, jr, eb, a, b);
+    }
+}
+
+// Split contact pass (NBC_PAIR_SPLIT): k_pairs_test visits every near pair,
+// clears the slots and touch flag of those that do not overlap and appends
+// the others to the step's touching list (warp-aggregated); k_pairs_law then
+// evaluates the law over that list with every lane of a warp on a touching
+// pair.  Each pair writes only its own slots, so the order of the list does
+// not change any result.  The list count is reset by the clump pass.
+template <typename R>
+__global__ void __launch_bounds__(PR_THREADS) k_pairs_test(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
+    const int hg = *d.hgen;
+    const int S = d.S;
+    const int* __restrict__ npre = d.nprefix;
+    const int np = npre[S];
+    const int4* __restrict__ nfr = d.nfr;
+    const double4* __restrict__ posr = d.posr;
+    uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
+    R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
+    R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
+    int2* __restrict__ tl = d.tlist;
+    const R4<R> zero = pack<R>(v3<R>(0, 0, 0), R(0));
+    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
+    for (int w0 = blockIdx.x * blockDim.x; w0 < np; w0 += gridDim.x * blockDim.x) {
+        const int w = w0 + threadIdx.x;   // the whole warp takes every round
+        bool on = false;
+        int s = 0, ef = 0;
+        if (w < np) {
+            s = S == 1 ? 0 : plan_find(npre, S, w);
+            const SceneDyn& ys = d.dyn[s];
+            if (!(d.has_stops && ys.frozen)) {
+                ef = ys.pair_off + (w - npre[s]);
+                const int4 rec = nfr[ef];
+                on = rec.y >= 0 && overlaps(posr[rec.z], posr[rec.y]);
+                if (!on) {
+                    to[rec.x] = 0;
+                    fs[2 * (size_t)ef] = zero;
+                    fs[2 * (size_t)ef + 1] = zero;
+                    bs[2 * (size_t)rec.w] = zero;
+                    bs[2 * (size_t)rec.w + 1] = zero;
+                }
+            }
         }
+        const unsigned m = __ballot_sync(0xffffffffu, on);
+        int base = 0;
+        if ((threadIdx.x & 31) == 0 && m) base = atomicAdd(d.tcount, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (on) tl[base + __popc(m & lt)] = make_int2(ef, s);
+    }
+}
+
+template <typename R, bool EXPORT>
+__global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs_law(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int nt = *d.tcount;
+    const int4* __restrict__ nfr = d.nfr;
+    const double4* __restrict__ posr = d.posr;
+    const int2* __restrict__ tl = d.tlist;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nt; u += gridDim.x * blockDim.x) {
+        const int2 e = tl[u];
+        const int4 rec = nfr[e.x];
+        Body<R> a, b;
+        a.p = posr[rec.z];
+        b.p = posr[rec.y];
+        pair_law<R, EXPORT>(d, e.y, e.x, rec.x, rec.z, rec.y, rec.w, a, b);
     }
 }
 
