@@ -1017,7 +1017,6 @@ class EngineT final : public EngineBase {
             h_.lstep = flags + 7;
             h_.loop_left = flags + 8;
             h_.scan_fail = flags + 9;
-            h_.tcount = flags + 10;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
             h_.hist = m.take<int>((size_t)256 * rs_blocks_);
             h_.perm = m.take<int>(N);
@@ -1100,7 +1099,6 @@ class EngineT final : public EngineBase {
             h_.nbs = m.take<R4<R>>(2 * cap);
             h_.nbpos = m.take<int>(cap);
             h_.nfr = m.take<int4>(cap);
-            h_.tlist = m.take<int2>(cap);
             h_.nbq = m.take<int>(cap);
             h_.nearf = m.take<uint8_t>(cap);
             h_.xfcn = m.take<R4<R>>(cap);
@@ -1119,7 +1117,7 @@ class EngineT final : public EngineBase {
     // Bytes of the pair buffers per pair slot.
     static double bytes_per_pair() {
         return 2.0 * (4 * sizeof(int) + (double)hist_bytes(1) + 1) + 5 * sizeof(R4<R>) + sizeof(double4) +
-               2 * sizeof(int) + sizeof(int4) + sizeof(int2) + 1;
+               2 * sizeof(int) + sizeof(int4) + 1;
     }
     // Region capacities for the first lists: slack x each scene's pairs; with
     // the default slack at least the reference's own list capacity, n_sub x
@@ -1310,14 +1308,8 @@ class EngineT final : public EngineBase {
         // stays valid as the list grows; a small scene gets a small grid so
         // that other scenes' kernels run beside it
         const int pg = std::min(sm_count_ * pair_bps_, cdiv(3LL * N_, PR_THREADS));
-#if NBC_PAIR_SPLIT
-        k_pairs_test<R><<<std::min(sm_count_ * 8, cdiv(3LL * N_, PR_THREADS)), PR_THREADS, 0, stream_>>>(d_);
-        if (exp) k_pairs_law<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
-        else k_pairs_law<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
-#else
         if (exp) k_pairs<R, true><<<pg, PR_THREADS, 0, stream_>>>(d_);
         else k_pairs<R, false><<<pg, PR_THREADS, 0, stream_>>>(d_);
-#endif
         CK(cudaStreamWaitEvent(stream_, ev_join_, 0));
         CK(cudaGetLastError());
         mark(6, stream_);

@@ -112,7 +112,6 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
     if (do_pre && blockIdx.x == 0 && threadIdx.x == 0) {
         *d.hgen += 1;
         *d.gstep += 1;
-        *d.tcount = 0;   // the split contact pass's touching list of this step
     }
     // warp-uniform: this warp holds clumps of a scene that moves (a warp whose
     // clumps all belong to scenes standing still skips its work)
@@ -444,8 +443,12 @@ __device__ __forceinline__ int plan_find(const int* __restrict__ pre, int n, int
 // any length.
 constexpr int SC_THREADS = 256, SC_ITEMS = 4, SC_TILE = SC_THREADS * SC_ITEMS;
 
+// Exclusive scan over a block of NT threads (every thread calls it); sh:
+// NT/32 ints.
+template <int NT = SC_THREADS>
 __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
-    // sh: SC_THREADS/32 ints
+    static_assert(NT % 32 == 0 && NT <= 1024, "whole warps, at most 32");
+    constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int x = v;
     for (int o = 1; o < 32; o <<= 1) {
@@ -455,16 +458,16 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
     if (lane == 31) sh[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < SC_THREADS / 32 ? sh[lane] : 0;
+        int w = lane < NW ? sh[lane] : 0;
         for (int o = 1; o < 32; o <<= 1) {
             int y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
-        if (lane < SC_THREADS / 32) sh[lane] = w;
+        if (lane < NW) sh[lane] = w;
     }
     __syncthreads();
     const int warp_base = warp > 0 ? sh[warp - 1] : 0;
-    total = sh[SC_THREADS / 32 - 1];
+    total = sh[NW - 1];
     __syncthreads();
     return warp_base + x - v;
 }
@@ -1225,7 +1228,7 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
                 acc += n;
             }
             int total;
-            int ex = block_excl_scan(acc, sh.scan, total);
+            int ex = block_excl_scan<SEARCH_THREADS>(acc, sh.scan, total);
             for (int q = q0; q < min(q0 + RPT, SF_ROWS); q++) {
                 const int n = sh.pre[q];
                 sh.pre[q] = ex;
@@ -2393,12 +2396,7 @@ constexpr int PR_THREADS = 256;
 #ifndef NBC_PAIR_MINB
 #define NBC_PAIR_MINB 2
 #endif
-// 1: the contact pass as two kernels (overlap test and touching list, then
-// the law over the list); 0: one kernel
-#ifndef NBC_PAIR_SPLIT
-#define NBC_PAIR_SPLIT 0
-#endif
-constexpr int CONTACT_LAUNCHES = NBC_PAIR_SPLIT ? 3 : 2;   // with k_boundary
+constexpr int CONTACT_LAUNCHES = 2;   // k_pairs and k_boundary
 template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -2438,75 +2436,6 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
             continue;
         }
         pair_law<R, EXPORT>(d, s, ef, p, i, jr, eb, a, b);
-    }
-}
-
-// Split contact pass (NBC_PAIR_SPLIT): k_pairs_test visits every near pair,
-// clears the slots and touch flag of those that do not overlap and appends
-// the others to the step's touching list (warp-aggregated); k_pairs_law then
-// evaluates the law over that list with every lane of a warp on a touching
-// pair.  Each pair writes only its own slots, so the order of the list does
-// not change any result.  The list count is reset by the clump pass.
-template <typename R>
-__global__ void __launch_bounds__(PR_THREADS) k_pairs_test(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
-    const int hg = *d.hgen;
-    const int S = d.S;
-    const int* __restrict__ npre = d.nprefix;
-    const int np = npre[S];
-    const int4* __restrict__ nfr = d.nfr;
-    const double4* __restrict__ posr = d.posr;
-    uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
-    R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
-    R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
-    int2* __restrict__ tl = d.tlist;
-    const R4<R> zero = pack<R>(v3<R>(0, 0, 0), R(0));
-    const unsigned lt = (1u << (threadIdx.x & 31)) - 1u;
-    for (int w0 = blockIdx.x * blockDim.x; w0 < np; w0 += gridDim.x * blockDim.x) {
-        const int w = w0 + threadIdx.x;   // the whole warp takes every round
-        bool on = false;
-        int s = 0, ef = 0;
-        if (w < np) {
-            s = S == 1 ? 0 : plan_find(npre, S, w);
-            const SceneDyn& ys = d.dyn[s];
-            if (!(d.has_stops && ys.frozen)) {
-                ef = ys.pair_off + (w - npre[s]);
-                const int4 rec = nfr[ef];
-                on = rec.y >= 0 && overlaps(posr[rec.z], posr[rec.y]);
-                if (!on) {
-                    to[rec.x] = 0;
-                    fs[2 * (size_t)ef] = zero;
-                    fs[2 * (size_t)ef + 1] = zero;
-                    bs[2 * (size_t)rec.w] = zero;
-                    bs[2 * (size_t)rec.w + 1] = zero;
-                }
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, on);
-        int base = 0;
-        if ((threadIdx.x & 31) == 0 && m) base = atomicAdd(d.tcount, __popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (on) tl[base + __popc(m & lt)] = make_int2(ef, s);
-    }
-}
-
-template <typename R, bool EXPORT>
-__global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs_law(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int nt = *d.tcount;
-    const int4* __restrict__ nfr = d.nfr;
-    const double4* __restrict__ posr = d.posr;
-    const int2* __restrict__ tl = d.tlist;
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nt; u += gridDim.x * blockDim.x) {
-        const int2 e = tl[u];
-        const int4 rec = nfr[e.x];
-        Body<R> a, b;
-        a.p = posr[rec.z];
-        b.p = posr[rec.y];
-        pair_law<R, EXPORT>(d, e.y, e.x, rec.x, rec.z, rec.y, rec.w, a, b);
     }
 }
 

@@ -184,8 +184,6 @@ struct Dev {
     int* nrow;        // [N+S] near front offsets
     int* nbrow;       // [N+S] near back offsets
     int4* nfr;        // [cap] near front entries: pair slot, partner, owner, near back entry
-    int2* tlist;      // [cap] split contact pass: touching near front entries of the step (entry, scene)
-    int* tcount;      // their count
     int* nbq;         // [cap] near back entries: pair slot
     int* nprefix;     // [S+1] prefix over the scenes of their near pairs (the contact pass's work items)
     int* bidx;        // [N] boundary candidates of scene s at [sub_off, sub_off + nbound) (see k_bflag)
