@@ -835,6 +835,10 @@ class EngineT final : public EngineBase {
         search_lanes_ = opt_.search_lanes == 1 || opt_.search_lanes == 16 || opt_.search_lanes == 32
                             ? opt_.search_lanes : 8;
         clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
+        // the clump pass's staged contact records (dynamic shared memory past the 48 KB default)
+        CK(cudaFuncSetAttribute(k_clump<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 2>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 4>()));
         pair_bps_ = opt_.pair_blocks >= 2 && opt_.pair_blocks <= 16 ? opt_.pair_blocks : 12;
         CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
         S_ = (int)sc.size();
@@ -1274,9 +1278,12 @@ class EngineT final : public EngineBase {
     void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0,
                       cudaGraphConditionalHandle loop = 0, int use_loop = 0) {
         const int g = cdiv(K_ + S_, CL_THREADS);
-        if (clump_batch_ == 1) k_clump<R, 1><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
-        else if (clump_batch_ == 4) k_clump<R, 4><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
-        else k_clump<R, 2><<<g, CL_THREADS, 0, stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        if (clump_batch_ == 1)
+            k_clump<R, 1><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        else if (clump_batch_ == 4)
+            k_clump<R, 4><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        else
+            k_clump<R, 2><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         CK(cudaGetLastError());
         if (!capturing_) launches_ += 1;
     }

@@ -52,6 +52,28 @@ __device__ __forceinline__ void slot_sum(const R4<R>* __restrict__ fs, const R4<
 // clump pass
 // ===========================================================================
 
+// 16-byte asynchronous copy global -> shared (no register holds the data in
+// flight, so one thread can have many outstanding), and the wait for all of
+// the calling thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+// a contact record staged for the clump pass: force and torque (two Real4)
+template <typename R> struct SlotRec {
+    R4<R> f, t;
+};
+template <typename R>
+__device__ __forceinline__ void stage_rec(SlotRec<R>* dst, const R4<R>* f, const R4<R>* t) {
+    for (int k = 0; k < (int)sizeof(R4<R>) / 16; k++) {
+        cp_async16((char*)&dst->f + 16 * k, (const char*)f + 16 * k);
+        cp_async16((char*)&dst->t + 16 * k, (const char*)t + 16 * k);
+    }
+}
+
 // Integrate_Before_clump_cuk / Attitude_clump_cuk / Integrate_After_clump_cuk
 // (src/dem_integrate_clumpsphere.cu:3-141), UpdatePos_cuk (src/dem_clump.cu:
 // 113-138), ComputeTorqueFromWorldPos_Kernel + reduce_by_key
@@ -83,6 +105,14 @@ __device__ __forceinline__ bool scene_post(const SceneDyn& y, int post, int L) {
 }
 constexpr int CL_THREADS = 128;
 constexpr int CL_WARPS = CL_THREADS / 32;
+// staged contact records per warp: CL_STAGE per member of a chunk on
+// average; a lane whose members would overflow the warp's records sums from
+// global memory directly (same order, same result).  Dynamic shared memory.
+constexpr int CL_STAGE = 4;
+template <typename R, int J>
+constexpr size_t clump_dyn_smem() {
+    return (size_t)CL_WARPS * CL_STAGE * 32 * J * sizeof(SlotRec<R>);
+}
 // J: members each lane keeps in flight per batch of loads (a launch shape
 // the autotuner picks; results do not depend on it); a warp stages 32 J
 // members in shared memory at a time.  J <= 2 fits 128 registers (4 blocks,
@@ -97,6 +127,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
     __shared__ int s_ms[CL_WARPS][33];               // member-list offsets of the warp's clumps
     __shared__ int s_sc[CL_WARPS][32];               // scene of each of the warp's clumps
     __shared__ int s_pre[CL_WARPS][32];              // the clump's scene takes this step
+    extern __shared__ __align__(16) unsigned char cl_dsm[];   // staged contact records
     const Dev& d = *dp;
     if (*d.halt) {
         // a rebuild ran out of pair capacity: the host finishes that step, so
@@ -164,6 +195,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const int* __restrict__ nbrow = d.nbrow;
             const uint16_t* __restrict__ bbits = d.bbits;
             const size_t N = (size_t)d.N, cap = (size_t)d.cap;
+            SlotRec<R>* stage = (SlotRec<R>*)cl_dsm + (size_t)warp * CL_STAGE * CL_CHUNK;
             F = v3(0.0, 0.0, 0.0);
             T = F;
             for (int c0 = M0; c0 < M1; c0 += CL_CHUNK) {
@@ -188,15 +220,60 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     q1[j] = nbrow[ro + 1];
                     bb[j] = bbits[i];
                 }
+                // stage every contact record of the lane's members (front
+                // slots, back slots, the boundary force) with asynchronous
+                // copies: one wait for all of them instead of one per slot
+                int nrec = 0;
+#pragma unroll
+                for (int j = 0; j < J; j++)
+                    if (idx[j] >= 0) nrec += (r1[j] - r0[j]) + (q1[j] - q0[j]) + (bb[j] ? 1 : 0);
+                int rbase = nrec;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, rbase, o);
+                    if (lane >= o) rbase += y;
+                }
+                rbase -= nrec;
+                const bool staged = rbase + nrec <= CL_STAGE * CL_CHUNK;
+                SlotRec<R>* st = stage + rbase;
+                if (staged) {
+                    int o = 0;
+#pragma unroll
+                    for (int j = 0; j < J; j++) {
+                        if (idx[j] < 0) continue;
+                        for (int e = r0[j]; e < r1[j]; e++, o++) stage_rec<R>(st + o, fsl + 2 * (size_t)e, fsl + 2 * (size_t)e + 1);
+                        for (int e = q0[j]; e < q1[j]; e++, o++) stage_rec<R>(st + o, bsl + 2 * (size_t)e, bsl + 2 * (size_t)e + 1);
+                        if (bb[j]) { stage_rec<R>(st + o, fbd + idx[j], fbd + N + idx[j]); o++; }
+                    }
+                    cp_async_wait_all();
+                }
+                int o = 0;
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     if (idx[j] < 0) continue;
                     const int kk = own[j];
                     V3<R> fr, tr;
-                    slot_sum<R>(fsl, bsl, cap, r0[j], r1[j], q0[j], q1[j], fr, tr);
-                    if (bb[j]) {
-                        fr = fr + xyz<R>(fbd[idx[j]]);
-                        tr = tr + xyz<R>(fbd[N + idx[j]]);
+                    if (staged) {
+                        // the order of slot_sum: front slots, back slots, then the boundary force
+                        fr = v3<R>(0, 0, 0);
+                        tr = fr;
+                        const int ns = (r1[j] - r0[j]) + (q1[j] - q0[j]);
+#pragma unroll 1
+                        for (int e = 0; e < ns; e++, o++) {
+                            fr = fr + xyz<R>(st[o].f);
+                            tr = tr + xyz<R>(st[o].t);
+                        }
+                        if (bb[j]) {
+                            fr = fr + xyz<R>(st[o].f);
+                            tr = tr + xyz<R>(st[o].t);
+                            o++;
+                        }
+                    } else {
+                        slot_sum<R>(fsl, bsl, cap, r0[j], r1[j], q0[j], q1[j], fr, tr);
+                        if (bb[j]) {
+                            fr = fr + xyz<R>(fbd[idx[j]]);
+                            tr = tr + xyz<R>(fbd[N + idx[j]]);
+                        }
                     }
                     const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
                                             ps[j].z - s_cl[warp][2][kk]);
