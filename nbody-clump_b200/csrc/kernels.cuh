@@ -979,10 +979,19 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     const int nrows = 9 * (my + 1);
     // ---- ranges of the stencil rows: lane k resolves rows [k C, k C + C)
     {
+        constexpr int MAXC = (MAX_ROWS + SL - 1) / SL;
         const int C = (nrows + SL - 1) / SL;
         const int r0 = min(lane * C, nrows), r1 = min(r0 + C, nrows);
-        int acc = 0, lc = -1, gx = 0, gy = 0, gz = 0, base = 0, cx0 = 0, cy0 = 0, cz0 = 0;
-        for (int r = r0; r < r1; r++) {
+        // the cells of the lane's rows first, then all their cstart loads at
+        // once (the rows are independent), then the lengths
+        int ca[MAXC], cb[MAXC];
+        int lc = -1, gx = 0, gy = 0, gz = 0, base = 0, cx0 = 0, cy0 = 0, cz0 = 0;
+#pragma unroll
+        for (int k = 0; k < MAXC; k++) {
+            const int r = r0 + k;
+            ca[k] = -1;
+            cb[k] = -1;
+            if (r >= r1) continue;
             const int l = my - r / 9, rr = r % 9;
             if (l != lc) {
                 lc = l;
@@ -1003,12 +1012,25 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
             }
             const int z = cz0 + rr / 3 - 1, y = cy0 + rr % 3 - 1;
             const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
-            int s = 0, n = 0;
             if (xa <= xb && z >= 0 && z < gz && y >= 0 && y < gy) {
                 const int c0 = base + (z * gy + y) * gx;
-                s = cstart[c0 + xa];
-                n = cstart[c0 + xb + 1] - s;
+                ca[k] = c0 + xa;
+                cb[k] = c0 + xb + 1;
             }
+        }
+#pragma unroll
+        for (int k = 0; k < MAXC; k++) {
+            if (ca[k] >= 0) {
+                ca[k] = cstart[ca[k]];
+                cb[k] = cstart[cb[k]];
+            }
+        }
+        int acc = 0;
+#pragma unroll
+        for (int k = 0; k < MAXC; k++) {
+            const int r = r0 + k;
+            if (r >= r1) continue;
+            const int s = ca[k] >= 0 ? ca[k] : 0, n = ca[k] >= 0 ? cb[k] - ca[k] : 0;
             rs[r] = s;
             pre[r] = acc;
             acc += n;
@@ -1034,16 +1056,18 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     int* __restrict__ scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
     int* __restrict__ scr_b = scr_f + SCR_CAP;
     int r = 0;
-    int jn = -1, rn = 0;
+    // the next candidate's position and clump are loaded a batch ahead
+    int jn = -1, rn = 0, cn = 0;
     double4 pn = make_double4(0, 0, 0, 0);
     if (lane < total) {
         while (pre[r + 1] <= lane) r++;
         jn = rs[r] + (lane - pre[r]);
         rn = r;
         pn = posr[jn];
+        cn = cid[jn];
     }
     for (int b0 = 0; b0 < total; b0 += SL) {
-        const int j = jn, rj = rn;
+        const int j = jn, rj = rn, cj = cn;
         const double4 pj = pn;
         const int f = b0 + SL + lane;
         jn = -1;
@@ -1052,6 +1076,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
             jn = rs[r] + (f - pre[r]);
             rn = r;
             pn = posr[jn];
+            cn = cid[jn];
         }
         const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
         const double d2 = dx * dx + dy * dy + dz * dz;
@@ -1064,7 +1089,7 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
         const unsigned fm = __ballot_sync(gm, front) >> gshift;
         const unsigned bm = __ballot_sync(gm, back) >> gshift;
         if (hit) {
-            const int flag = cid[j] == ci ? INTRA : 0;
+            const int flag = cj == ci ? INTRA : 0;
             if (FILL) {
                 if (front) {
                     const int q = rf + nf + __popc(fm & lt);
