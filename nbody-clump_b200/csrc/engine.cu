@@ -772,11 +772,11 @@ class EngineT final : public EngineBase {
     }
     // kernels one rebuild launches (launch_rebuild)
     // kernels of one rebuild in a graph (the eager path adds a k_check_cap):
-    // plan, hash, 3 per radix pass, cellrange, cellstart, reorder, 2 fills,
-    // search, scan, check, (hgrid: fill), compact, (hgrid: xsort), backref,
-    // carry, 2 write-backs, swap, 2 near passes and their scan, commit, 2
-    // boundary-flag passes and their scan, nprefix
-    int rebuild_launches() const { return 24 + 3 * passes_ + (hgrid_ ? 2 : 0); }
+    // plan, hash, 3 per radix pass, cellrange, cellstart, reorder, search,
+    // scan, check, compact, (hgrid: xsort), backref, carry, write-back, 2
+    // near passes and their scan, commit, 2 boundary-flag passes and their
+    // scan, nprefix
+    int rebuild_launches() const { return 19 + 3 * passes_ + (hgrid_ ? 1 : 0); }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -1361,8 +1361,6 @@ class EngineT final : public EngineBase {
         k_cellrange<<<gN, B, 0, stream_>>>(d_, ki, vi);
         k_cellstart<<<std::min(cdiv(h_.cells + S_, 256), 148 * 16), 256, 0, stream_>>>(d_);
         k_reorder<R><<<gN, B, 0, stream_>>>(d_);
-        k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_f, pl + PL_T1, 0);
-        k_fill_n<<<std::min(cdiv(N_ + 1, 256), 148 * 16), 256, 0, stream_>>>(h_.cnt_b, pl + PL_T1, 0);
         if (sl == 1) k_search_flat<<<std::min(cdiv(N_, SF_G), 148 * 8), SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
@@ -1389,7 +1387,6 @@ class EngineT final : public EngineBase {
             }
         }
         k_check_cap<<<1, 256, 0, stream_>>>(d_, 1);
-        if (hgrid_) k_fill_n<<<std::min(cdiv(N_, 256), 148 * 16), 256, 0, stream_>>>(h_.xcnt, pl + PL_T, 0);
         if (sl == 16) k_compact<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_compact<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else k_compact<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
@@ -1397,9 +1394,7 @@ class EngineT final : public EngineBase {
         k_backref<<<gN, B, 0, stream_>>>(d_);
         const int gP = std::min(148 * 8, cdiv(8LL * N_, 256));
         k_carry<R><<<gP, 256, 0, stream_>>>(d_);
-        k_writeback<R><<<gN, B, 0, stream_>>>(d_);
-        k_writeback_pairs<R><<<gP, 256, 0, stream_>>>(d_);
-        k_swap<<<1, 1, 0, stream_>>>(d_);
+        k_writeback<R><<<gP, 256, 0, stream_>>>(d_);
         // near rows of the rebuilt scenes (counts, scans, rows)
         const int gNr = std::min(cdiv(N_, SEARCH_THREADS / 4), 148 * 16);
         k_near<false, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);

@@ -893,7 +893,12 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
     if (*d.halt) return;
     const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const size_t N = (size_t)d.N;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
     NBC_GRID_STRIDE(t, T) {
+        // the search's counters start at zero
+        d.cnt_f[t] = 0;
+        d.cnt_b[t] = 0;
+        d.xcnt[t] = 0;
         const int k = plan_find(d.psub, ns, t);
         const int i = d.par[d.pscene[k]].sub_off + (t - d.psub[k]);
         const int o = d.perm[i];
@@ -1659,14 +1664,33 @@ __global__ void k_carry(const Dev* __restrict__ dp) {
     }
 }
 
-// The rebuilt scenes' gathered per-subsphere state and new rows, written
-// back into the current buffers.
+// Commits a rebuild.  When every scene was rebuilt (always for a single
+// scene) the gathered buffers, the build list and the carried history
+// generation become the current ones by exchanging pointers in the table
+// (one thread); k_near then clears the other touch generation for the pairs
+// that are not near (it still holds the flags of the previous list).
+// Otherwise the rebuilt scenes' gathered per-subsphere state, new rows, list
+// entries, carried histories and touch flags are written back into the
+// current buffers and the generation the next contact pass reads (both
+// generations then agree on the region).
 template <typename R>
-__global__ void k_writeback(const Dev* __restrict__ dp) {
+__global__ void k_writeback(Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
-    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
-    if (ns == d.S) return;  // every scene rebuilt: k_swap exchanges the buffers instead
+    const int ns = d.plan[PL_NS];
+    if (ns == d.S) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            Dev& w = *dp;
+#define NBC_SWAP(a, b) { auto tmp_ = w.a; w.a = w.b; w.b = tmp_; }
+            NBC_SWAP(posr, posr2) NBC_SWAP(lom, lom2) NBC_SWAP(cum, cum2) NBC_SWAP(clump_id, clump_id2)
+            NBC_SWAP(part_fix, part_fix2) NBC_SWAP(level, level2) NBC_SWAP(key, key2) NBC_SWAP(kin, kin2)
+            NBC_SWAP(bhist, bhist2) NBC_SWAP(bbits, bbits2)
+            NBC_SWAP(L[0], L[1]) NBC_SWAP(H[0], H[1]) NBC_SWAP(touch[0], touch[1])
+#undef NBC_SWAP
+        }
+        return;
+    }
+    const int T = d.plan[PL_T];
     const size_t N = (size_t)d.N;
     const PairList& Lc = d.L[0];
     const PairList& Nw = d.L[1];
@@ -1696,22 +1720,9 @@ __global__ void k_writeback(const Dev* __restrict__ dp) {
             Lc.brow[i + s + 1] = Nw.brow[i + s + 1];
         }
     }
-}
-
-// the rebuilt scenes' new list entries, carried histories and touch flags,
-// written back into the current list and the generation the next contact
-// pass reads (both generations then agree on the region)
-template <typename R>
-__global__ void k_writeback_pairs(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int ns = d.plan[PL_NS];
-    if (ns == d.S) return;
     const int np = d.ppair[ns];
     const int hg = *d.hgen;
     const size_t cap = (size_t)d.cap;
-    const PairList& Lc = d.L[0];
-    const PairList& Nw = d.L[1];
     R4<R>* Hc = (R4<R>*)d.H[hg & 1];
     const R4<R>* Hn = (const R4<R>*)d.H[(hg + 1) & 1];
     uint8_t* tc = d.touch[hg & 1];
@@ -1731,22 +1742,6 @@ __global__ void k_writeback_pairs(const Dev* __restrict__ dp) {
             ((R*)(Hc + 2 * cap))[p] = ((const R*)(Hn + 2 * cap))[p];
         }
     }
-}
-
-// When every scene was rebuilt (always for a single scene) the gathered
-// buffers, the build list and the carried history generation become the
-// current ones by exchanging pointers in the table instead of copying back;
-// k_near then clears the other touch generation for the pairs that are not
-// near (it still holds the flags of the previous list).
-static __global__ void k_swap(Dev* __restrict__ dp) {
-    Dev& d = *dp;
-    if (*d.halt || d.plan[PL_NS] != d.S) return;
-#define NBC_SWAP(a, b) { auto tmp_ = d.a; d.a = d.b; d.b = tmp_; }
-    NBC_SWAP(posr, posr2) NBC_SWAP(lom, lom2) NBC_SWAP(cum, cum2) NBC_SWAP(clump_id, clump_id2)
-    NBC_SWAP(part_fix, part_fix2) NBC_SWAP(level, level2) NBC_SWAP(key, key2) NBC_SWAP(kin, kin2)
-    NBC_SWAP(bhist, bhist2) NBC_SWAP(bbits, bbits2)
-    NBC_SWAP(L[0], L[1]) NBC_SWAP(H[0], H[1]) NBC_SWAP(touch[0], touch[1])
-#undef NBC_SWAP
 }
 
 // Near rows.  Between two rebuilds of a scene every subsphere stays within
@@ -1772,7 +1767,8 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     const PairList& Lc = d.L[0];
     const uint8_t* __restrict__ nearf = d.nearf;
     const int* __restrict__ bpair = Lc.bpair;
-    // after k_swap: the other touch generation still holds the old list's flags
+    // after the pointer exchange of k_writeback: the other touch generation
+    // still holds the old list's flags
     uint8_t* __restrict__ tother = !FILL && ns == d.S ? d.touch[(*d.hgen + 1) & 1] : nullptr;
     if (!FILL && blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
     for (int t = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL; t < T;
