@@ -774,9 +774,8 @@ class EngineT final : public EngineBase {
     // kernels of one rebuild in a graph (the eager path adds a k_check_cap):
     // plan, hash, 3 per radix pass, cellrange, cellstart, reorder, search,
     // scan, check, compact, (hgrid: xsort), backref, carry, write-back, 2
-    // near passes and their scan, commit, 2 boundary-flag passes and their
-    // scan, nprefix
-    int rebuild_launches() const { return 19 + 3 * passes_ + (hgrid_ ? 1 : 0); }
+    // near-row passes and their scan, the finishing pass
+    int rebuild_launches() const { return 15 + 3 * passes_ + (hgrid_ ? 1 : 0); }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -1035,10 +1034,10 @@ class EngineT final : public EngineBase {
             h_.bprefix = m.take<int>(S_ + 1);
             h_.cnt_b = m.take<int>(N + 1);
             h_.sfc = m.take<int>(N);
-            h_.xcnt = m.take<int>(N);
+            h_.xcnt = m.take<int>(N + 1);
             const long long scan_tiles = std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE));
             h_.scan_tmp = m.take<int>(scan_tiles + 1);
-            h_.scan_st = m.take<unsigned long long>(2 * scan_tiles + 2);
+            h_.scan_st = m.take<unsigned long long>(3 * scan_tiles + 3);
             h_.scan_ctl = m.take<int>(2);
             for (int l = 0; l < 2; l++) {
                 h_.L[l].row = m.take<int>(N + S_);
@@ -1331,11 +1330,11 @@ class EngineT final : public EngineBase {
         else k_sum<R, false><<<cdiv(N_, CT_THREADS), CT_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
-    // exclusive scans of a0 (and a1, of the same length) over [0, n), or
+    // exclusive scans of a0 (and a1, a2, of the same length) over [0, n), or
     // over [0, *dn) when dn is given (n then bounds it), in one launch
-    void scan(int* a0, int* a1, int n, const int* dn = nullptr) {
-        const int nb = std::max(1, cdiv(n, SC_TILE)) * (a1 ? 2 : 1);
-        k_scan1<<<nb, SC_THREADS, 0, stream_>>>(a0, a1, n, dn, h_.scan_st, h_.scan_ctl, h_.halt, h_.scan_fail);
+    void scan(int* a0, int* a1, int* a2, int n, const int* dn = nullptr) {
+        const int nb = std::max(1, cdiv(n, SC_TILE)) * (a2 ? 3 : (a1 ? 2 : 1));
+        k_scan1<<<nb, SC_THREADS, 0, stream_>>>(a0, a1, a2, n, dn, h_.scan_st, h_.scan_ctl, h_.halt, h_.scan_fail);
     }
     // The rebuild block of src/dem_simulation_clump.cu:124-176, over the
     // scenes whose rebuild flag is set: every kernel but the near rows walks
@@ -1353,7 +1352,7 @@ class EngineT final : public EngineBase {
         const int gR = std::min(rs_blocks_, 148 * 8);
         for (int p = 0; p < passes_; p++) {
             k_rs_hist<<<gR, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, pl + PL_T);
-            scan(h_.hist, nullptr, 256 * rs_blocks_, pl + PL_HIST);
+            scan(h_.hist, nullptr, nullptr, 256 * rs_blocks_, pl + PL_HIST);
             k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T);
             std::swap(ki, ko);
             std::swap(vi, vo);
@@ -1365,7 +1364,7 @@ class EngineT final : public EngineBase {
         else if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else k_search<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.cnt_f, h_.cnt_b, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_f, h_.cnt_b, nullptr, N_ + 1, pl + PL_T1);
         CK(cudaGetLastError());
         if (eager) {
             // size the regions to the first lists, or grow the ones that overflow
@@ -1395,17 +1394,14 @@ class EngineT final : public EngineBase {
         const int gP = std::min(148 * 8, cdiv(8LL * N_, 256));
         k_carry<R><<<gP, 256, 0, stream_>>>(d_);
         k_writeback<R><<<gP, 256, 0, stream_>>>(d_);
-        // near rows of the rebuilt scenes (counts, scans, rows)
+        // near rows and boundary candidates of the rebuilt scenes (counts and
+        // flags, their scans, rows and list with the rebuild's bookkeeping),
+        // then the work-item prefixes over the scenes
         const int gNr = std::min(cdiv(N_, SEARCH_THREADS / 4), 148 * 16);
         k_near<false, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
-        scan(h_.cnt_f, h_.cnt_b, N_ + 1, pl + PL_T1);
+        scan(h_.cnt_f, h_.cnt_b, h_.xcnt, N_ + 1, pl + PL_T1);
         k_near<true, 4><<<gNr, SEARCH_THREADS, 0, stream_>>>(d_);
-        k_commit<<<std::min(cdiv((long long)K_ + S_ + 1, B), 148 * 8), B, 0, stream_>>>(d_);
-        // boundary candidates of the rebuilt scenes (flags, scan, list)
-        k_bflag<false><<<std::min(cdiv((long long)N_ + 1, B), 148 * 16), B, 0, stream_>>>(d_);
-        scan(h_.cnt_b, nullptr, N_ + 1, pl + PL_T1);
-        k_bflag<true><<<gN, B, 0, stream_>>>(d_);
-        k_nprefix<<<1, SC_THREADS, 0, stream_>>>(d_);
+        k_near_finish<<<std::min(cdiv(N_, SC_THREADS), 148 * 8), SC_THREADS, 0, stream_>>>(d_);
         CK(cudaGetLastError());
     }
 

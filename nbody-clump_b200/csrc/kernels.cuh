@@ -595,9 +595,9 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict_
 }
 
 // --- exclusive scan of ints in one launch (decoupled look-back) ----------
-// One or two arrays of the same length (n, or *dn) in one launch.  Every
+// One to three arrays of the same length (n, or *dn) in one launch.  Every
 // block takes one tile from a ticket counter: tickets [0, tiles) are the
-// tiles of the first array, [tiles, 2 tiles) those of the second.  A tile
+// tiles of the first array, [tiles, 2 tiles) those of the second, and so on.  A tile
 // publishes its aggregate, then looks back over its array's earlier tiles
 // (32 at a time, one per lane of warp 0) and sums aggregates until it meets
 // an inclusive prefix, and publishes its own inclusive prefix.  Tickets are
@@ -612,22 +612,22 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict_
 constexpr unsigned long long SCAN_AGG = 1ull << 32, SCAN_INC = 2ull << 32;
 constexpr int SCAN_SPIN_LIMIT = 1 << 22;
 
-static __global__ void __launch_bounds__(SC_THREADS) k_scan1(int* __restrict__ a0, int* __restrict__ a1, int n,
-                                                            const int* __restrict__ dn,
+static __global__ void __launch_bounds__(SC_THREADS) k_scan1(int* __restrict__ a0, int* __restrict__ a1,
+                                                            int* __restrict__ a2, int n, const int* __restrict__ dn,
                                                             unsigned long long* __restrict__ st, int* __restrict__ ctl,
                                                             int* __restrict__ halt, int* __restrict__ fail) {
     __shared__ int sh[SC_THREADS / 32];
     __shared__ int s_ticket, s_excl, s_last;
     const int nn = dn ? *dn : n;
     const int tiles = (nn + SC_TILE - 1) / SC_TILE;
-    const int narr = a1 ? 2 : 1;
+    const int narr = a2 ? 3 : (a1 ? 2 : 1);
     if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl[0], 1);
     __syncthreads();
     const int tk = s_ticket;
     if (tk < narr * tiles) {
-        const int arr = tk >= tiles ? 1 : 0;
+        const int arr = tk / tiles;
         const int b = tk - arr * tiles;      // tile of its array
-        int* __restrict__ a = arr ? a1 : a0;
+        int* __restrict__ a = arr == 0 ? a0 : (arr == 1 ? a1 : a2);
         unsigned long long* __restrict__ sa = st + (size_t)arr * tiles;
         const int base = b * SC_TILE + threadIdx.x * SC_ITEMS;
         int v[SC_ITEMS], sum = 0;
@@ -1631,8 +1631,17 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p, int s) {
             ot = io < jo ? jo : io;
         }
         sign = oo == io ? R(1) : R(-1);
-        for (int r = O.row[oo + s]; r < O.row[oo + s + 1]; r++)
-            if ((O.nbr[r] & IDX_MASK) == ot) { q = r; break; }
+        // the first entry of the old owner row with partner ot, four
+        // entries loaded at a time
+        const int rb = O.row[oo + s], re = O.row[oo + s + 1];
+        for (int r = rb; r < re && q < 0; r += 4) {
+            int v[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] = r + k < re ? (O.nbr[r + k] & IDX_MASK) : -1;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (q < 0 && v[k] == ot) q = r + k;
+        }
     }
     if (q >= 0 && ti[q]) {
         for (int h = 0; h < 2; h++) {
@@ -1744,6 +1753,36 @@ __global__ void k_writeback(Dev* __restrict__ dp) {
     }
 }
 
+// Boundary candidates.  Walls do not move (their velocity enters only the
+// contact law), and between two rebuilds of a scene every subsphere stays
+// within Thresh of where it was at the rebuild, so a subsphere farther than
+// 2 Thresh from every wall region at a rebuild cannot touch a wall before
+// the next one.  At each rebuild the near-row count pass flags, per rebuilt
+// subsphere (new order), whether it is within that margin of a wall --
+// every subsphere of a scene with an intruder is a candidate, the intruder
+// moves -- and clears the wall contact bits of the others (they are not in
+// contact now); the fill pass lists the candidates in the scene's range of
+// bidx, and k_boundary visits only them.
+__device__ __forceinline__ bool bound_candidate(const Dev& d, const ScenePar& P, int i) {
+    bool cand = P.has_intr;
+    if (!cand && P.wall != WALL_NONE) {
+        const double4 pp = d.posr[i];
+        const double m = 2.0 * P.thresh * (1.0 + 1e-6) + 1e-12;
+        const double r = pp.w + m;
+        const double ex = pp.x - P.w_c[0], ey = pp.y - P.w_c[1], ez = pp.z - P.w_c[2];
+        if (P.wall == WALL_CUBE) {
+            cand = fabs(ex) + r >= P.w_half[0] * (1 - 1e-9) || fabs(ey) + r >= P.w_half[1] * (1 - 1e-9) ||
+                   fabs(ez) + r >= P.w_half[2] * (1 - 1e-9);
+        } else {
+            const double ax = ex * P.cyl_axis[0] + ey * P.cyl_axis[1] + ez * P.cyl_axis[2];
+            const double rr = ex * ex + ey * ey + ez * ez - ax * ax;
+            const double in = P.cyl_R - r;
+            cand = fabs(ax) + r >= P.cyl_H * (1 - 1e-9) || in <= 0 || rr >= in * in * (1 - 1e-9);
+        }
+    }
+    return cand;
+}
+
 // Near rows.  Between two rebuilds of a scene every subsphere stays within
 // Thresh of where it was at the rebuild (a larger displacement triggers the
 // next one), so a pair whose distance at a rebuild is at least ri + rj +
@@ -1753,8 +1792,12 @@ __global__ void k_writeback(Dev* __restrict__ dp) {
 // near entries in its pair region (front: pair slot in row order, back: the
 // pair slot of each near back entry) and the contact pass visits only them,
 // with the same results as visiting the whole list.  FILL = false counts
-// them into cnt_f / cnt_b of the rebuilt concatenation; FILL = true writes
-// the rows at the scanned offsets.
+// them into cnt_f / cnt_b of the rebuilt concatenation and flags the
+// boundary candidates into xcnt; FILL = true writes the rows and the
+// candidate list at the scanned offsets, and finishes the rebuild's
+// bookkeeping: per-clump member lists of the rebuilt scenes in ascending
+// subsphere order (the order thrust::sort_by_key gives reduce_by_key,
+// src/dem_clumpsphere.cu:123-147), the scenes' pair and near counts.
 template <bool FILL, int SL>
 __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -1770,7 +1813,7 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
     // after the pointer exchange of k_writeback: the other touch generation
     // still holds the old list's flags
     uint8_t* __restrict__ tother = !FILL && ns == d.S ? d.touch[(*d.hgen + 1) & 1] : nullptr;
-    if (!FILL && blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
+    if (!FILL && blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; d.xcnt[T] = 0; }
     for (int t = blockIdx.x * (SEARCH_THREADS / SL) + threadIdx.x / SL; t < T;
          t += gridDim.x * (SEARCH_THREADS / SL)) {
         const PlanItem it = plan_item(d, ns, t);
@@ -1815,115 +1858,75 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
         if (!FILL && lane == 0) {
             d.cnt_f[t] = nf;
             d.cnt_b[t] = nb;
+            const bool cand = bound_candidate(d, d.par[s], i);
+            if (!cand) d.bbits[i] = 0;
+            d.xcnt[t] = cand ? 1 : 0;
+        }
+        if (FILL && lane == 0) {
+            const ScenePar& P = d.par[s];
+            const int t0 = d.psub[it.k];
+            if (d.xcnt[t + 1] - d.xcnt[t]) d.bidx[P.sub_off + d.xcnt[t] - d.xcnt[t0]] = i;
+            if (i == P.sub_off + P.nsub - 1) d.dyn[s].nbound = d.xcnt[t + 1] - d.xcnt[t0];
+        }
+    }
+    if (FILL) {
+        const int TK = d.plan[PL_TK];
+        NBC_GRID_STRIDE(u, TK + ns + 1) {
+            if (u < TK) {
+                const int k = plan_find(d.pclump, ns, u);
+                const int c = d.par[d.pscene[k]].clump_off + (u - d.pclump[k]);
+                const int mb = d.mem_start[c], me = d.mem_start[c + 1];
+                for (int m = mb; m < me; m++) d.mem_idx[m] = d.inv[d.mem_idx[m]];
+                for (int m = mb + 1; m < me; m++) {
+                    int v = d.mem_idx[m], q = m - 1;
+                    while (q >= mb && d.mem_idx[q] > v) { d.mem_idx[q + 1] = d.mem_idx[q]; q--; }
+                    d.mem_idx[q + 1] = v;
+                }
+            } else if (u < TK + ns) {
+                const int k = u - TK;
+                SceneDyn& y = d.dyn[d.pscene[k]];
+                y.npairs = d.ppair[k + 1] - d.ppair[k];
+                y.nnear = d.cnt_f[d.psub[k + 1]] - d.cnt_f[d.psub[k]];
+                y.nrebuild++;
+                y.rebuild = 0;
+            } else {
+                *d.any_rebuild = 0;
+            }
         }
     }
 }
 
-// the contact pass's work items: near pairs of every scene, scene by scene
-// (one block)
-static __global__ void __launch_bounds__(SC_THREADS) k_nprefix(const Dev* __restrict__ dp) {
+// The last pass of a rebuild: the contact pass's work items (near pairs) and
+// the boundary candidates of every scene as prefixes over the scenes (block
+// 0), and each rebuilt subsphere's near front records completed with the
+// near back entry of their pair (the near-row fill pass writes both rows at
+// once, so a front record cannot take it there).
+static __global__ void __launch_bounds__(SC_THREADS) k_near_finish(const Dev* __restrict__ dp) {
     __shared__ int sh[SC_THREADS / 32];
     const Dev& d = *dp;
     if (*d.halt) return;
-    int run = 0, brun = 0;
-    for (int b = 0; b < d.S; b += SC_THREADS) {
-        const int s = b + threadIdx.x;
-        int tot;
-        const int ex = block_excl_scan(s < d.S ? d.dyn[s].nnear : 0, sh, tot);
-        if (s < d.S) d.nprefix[s] = run + ex;
-        run += tot;
-        const int bx = block_excl_scan(s < d.S ? d.dyn[s].nbound : 0, sh, tot);
-        if (s < d.S) d.bprefix[s] = brun + bx;
-        brun += tot;
+    if (blockIdx.x == 0) {
+        int run = 0, brun = 0;
+        for (int b = 0; b < d.S; b += SC_THREADS) {
+            const int s = b + threadIdx.x;
+            int tot;
+            const int ex = block_excl_scan(s < d.S ? d.dyn[s].nnear : 0, sh, tot);
+            if (s < d.S) d.nprefix[s] = run + ex;
+            run += tot;
+            const int bx = block_excl_scan(s < d.S ? d.dyn[s].nbound : 0, sh, tot);
+            if (s < d.S) d.bprefix[s] = brun + bx;
+            brun += tot;
+        }
+        if (threadIdx.x == 0) {
+            d.nprefix[d.S] = run;
+            d.bprefix[d.S] = brun;
+        }
     }
-    if (threadIdx.x == 0) {
-        d.nprefix[d.S] = run;
-        d.bprefix[d.S] = brun;
-    }
-}
-
-// Boundary candidates.  Walls do not move (their velocity enters only the
-// contact law), and between two rebuilds of a scene every subsphere stays
-// within Thresh of where it was at the rebuild, so a subsphere farther than
-// 2 Thresh from every wall region at a rebuild cannot touch a wall before
-// the next one.  At each rebuild k_bflag flags, per rebuilt subsphere (new
-// order), whether it is within that margin of a wall -- every subsphere of a
-// scene with an intruder is a candidate, the intruder moves -- and clears
-// the wall contact bits of the others (they are not in contact now); the
-// FILL pass lists the candidates in the scene's range of bidx, and
-// k_boundary visits only them.  FILL = false writes the flags into cnt_b of
-// the rebuilt concatenation (free after k_commit); FILL = true writes the
-// list at the scanned offsets and the scene's count, and completes each
-// rebuilt subsphere's near front records with the near back entry of their
-// pair (k_near's FILL pass writes both rows at once, so a front record
-// cannot take it there).
-template <bool FILL>
-__global__ void k_bflag(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
     const int T = d.plan[PL_T], ns = d.plan[PL_NS];
-    NBC_GRID_STRIDE(t, T + (FILL ? 0 : 1)) {
-        if (!FILL && t == T) { d.cnt_b[T] = 0; continue; }
+    NBC_GRID_STRIDE(t, T) {
         const PlanItem it = plan_item(d, ns, t);
         const int i = it.i, s = it.s;
-        const ScenePar& P = d.par[s];
-        if (FILL) {
-            const int t0 = d.psub[it.k];
-            const int c = d.cnt_b[t] - d.cnt_b[t0];
-            if (d.cnt_b[t + 1] - d.cnt_b[t]) d.bidx[P.sub_off + c] = i;
-            if (i == P.sub_off + P.nsub - 1) d.dyn[s].nbound = d.cnt_b[t + 1] - d.cnt_b[t0];
-            for (int e = d.nrow[i + s]; e < d.nrow[i + s + 1]; e++) d.nfr[e].w = d.nbpos[d.nfr[e].x];
-            continue;
-        }
-        bool cand = P.has_intr;
-        if (!cand && P.wall != WALL_NONE) {
-            const double4 pp = d.posr[i];
-            const double m = 2.0 * P.thresh * (1.0 + 1e-6) + 1e-12;
-            const double r = pp.w + m;
-            const double ex = pp.x - P.w_c[0], ey = pp.y - P.w_c[1], ez = pp.z - P.w_c[2];
-            if (P.wall == WALL_CUBE) {
-                cand = fabs(ex) + r >= P.w_half[0] * (1 - 1e-9) || fabs(ey) + r >= P.w_half[1] * (1 - 1e-9) ||
-                       fabs(ez) + r >= P.w_half[2] * (1 - 1e-9);
-            } else {
-                const double ax = ex * P.cyl_axis[0] + ey * P.cyl_axis[1] + ez * P.cyl_axis[2];
-                const double rr = ex * ex + ey * ey + ez * ez - ax * ax;
-                const double in = P.cyl_R - r;
-                cand = fabs(ax) + r >= P.cyl_H * (1 - 1e-9) || in <= 0 || rr >= in * in * (1 - 1e-9);
-            }
-        }
-        if (!cand) d.bbits[i] = 0;
-        d.cnt_b[t] = cand ? 1 : 0;
-    }
-}
-
-// Finishes a rebuild: per-clump member lists of the rebuilt scenes in
-// ascending subsphere order (the order thrust::sort_by_key gives
-// reduce_by_key, src/dem_clumpsphere.cu:123-147) and the scene bookkeeping.
-static __global__ void k_commit(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int ns = d.plan[PL_NS], TK = d.plan[PL_TK];
-    NBC_GRID_STRIDE(u, TK + ns + 1) {
-        if (u < TK) {
-            const int k = plan_find(d.pclump, ns, u);
-            const int c = d.par[d.pscene[k]].clump_off + (u - d.pclump[k]);
-            const int mb = d.mem_start[c], me = d.mem_start[c + 1];
-            for (int m = mb; m < me; m++) d.mem_idx[m] = d.inv[d.mem_idx[m]];
-            for (int m = mb + 1; m < me; m++) {
-                int v = d.mem_idx[m], q = m - 1;
-                while (q >= mb && d.mem_idx[q] > v) { d.mem_idx[q + 1] = d.mem_idx[q]; q--; }
-                d.mem_idx[q + 1] = v;
-            }
-        } else if (u < TK + ns) {
-            const int k = u - TK;
-            SceneDyn& y = d.dyn[d.pscene[k]];
-            y.npairs = d.ppair[k + 1] - d.ppair[k];
-            y.nnear = d.cnt_f[d.psub[k + 1]] - d.cnt_f[d.psub[k]];
-            y.nrebuild++;
-            y.rebuild = 0;
-        } else {
-            *d.any_rebuild = 0;
-        }
+        for (int e = d.nrow[i + s]; e < d.nrow[i + s + 1]; e++) d.nfr[e].w = d.nbpos[d.nfr[e].x];
     }
 }
 
