@@ -1211,42 +1211,35 @@ __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search(const Dev* __restr
 // (consecutive in the sorted order, so mostly of one grid level) and
 //   1. finds each one's cell on its own level and every coarser one (three
 //      divisions per subsphere and level);
-//   2. resolves every stencil row of the chunk (one thread per row slot,
-//      MAX_ROWS slots per subsphere, unused ones empty) and scans their
-//      lengths over the whole chunk: the chunk's candidates are then one flat
-//      range, each subsphere's in its discovery order;
-//   3. tests the candidates 32 per thread (one bitmap word each), walking the
-//      row prefix as it goes -- every lane busy whatever a subsphere's row
-//      lengths;
+//   2. resolves every stencil row of the chunk (MAX_ROWS row slots per
+//      subsphere, unused ones empty): first the cell ranges, then their
+//      cstart loads several at a time, then a scan of the lengths over the
+//      whole chunk, so the chunk's candidates are one flat range, each
+//      subsphere's in its discovery order;
+//   3. per window of SF_CAP candidates, maps every candidate to its row slot
+//      (each row writes its own range), then tests the candidates a warp
+//      word at a time (a lane per candidate, the word by ballot) -- every
+//      lane busy whatever the row lengths;
 //   4. emits the hits: one warp per subsphere, a lane per bitmap word, ballot
 //      prefixes for the front and back positions, so each row keeps the
 //      discovery order.
-// Windows of SF_CAP candidates bound the bitmap; hits of a subsphere that
-// spans windows are appended in window order.
+// Hits of a subsphere that spans windows are appended in window order.
 constexpr int SF_G = 32;
 constexpr int SF_ROWS = SF_G * MAX_ROWS;
-constexpr int SF_CAP = 16384;
+constexpr int SF_CAP = 8192;
+constexpr int SF_RPT = (SF_ROWS + SEARCH_THREADS - 1) / SEARCH_THREADS;   // row slots per thread
 struct SearchFlatShared {
     double4 pi[SF_G];
     int ii[SF_G], tt[SF_G], ci[SF_G], scene[SF_G], nrows[SF_G], nf[SF_G], nb[SF_G];
     int cc[SF_G][MAX_LEVELS][3];   // cell of the subsphere on the k-th level it searches (own level first)
     int rs[SF_ROWS];               // first sorted slot of each row slot
     int pre[SF_ROWS + 1];          // exclusive prefix of the row lengths over the chunk
+    unsigned short rowid[SF_CAP];  // row slot of each candidate of the current window
     unsigned bits[SF_CAP / 32];    // hits of the current window
     int scan[SEARCH_THREADS / 32];
     int claim;
 };
-
-// the row slot in [q0, q0 + n) holding flat candidate f (pre[q0] <= f < pre[q0 + n])
-__device__ __forceinline__ int sf_row(const int* __restrict__ pre, int q0, int n, int f) {
-    int lo = q0, hi = q0 + n - 1;
-    while (lo < hi) {
-        const int m = (lo + hi + 1) >> 1;
-        if (pre[m] <= f) lo = m;
-        else hi = m - 1;
-    }
-    return lo;
-}
+static_assert(SF_ROWS < 65536, "row slots fit 16 bits");
 
 static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const Dev* __restrict__ dp) {
     __shared__ SearchFlatShared sh;
@@ -1254,6 +1247,7 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
     if (*d.halt) return;
     const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = SEARCH_THREADS / 32;
     const double4* __restrict__ posr = d.posr2;
     const int* __restrict__ cid = d.clump_id2;
     const int* __restrict__ cstart = d.cstart;
@@ -1302,41 +1296,63 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
             sh.cc[s][k][2] = cz;
         }
         __syncthreads();
-        // ---- 2. stencil rows (a run of consecutive slots per thread) and their prefix
-        {
-            constexpr int RPT = (SF_ROWS + SEARCH_THREADS - 1) / SEARCH_THREADS;
-            const int q0 = tid * RPT;
-            int acc = 0;
-            for (int q = q0; q < min(q0 + RPT, SF_ROWS); q++) {
+        // ---- 2. stencil rows: the cell range of each row slot (thread-strided
+        // slots), the cstart loads of SF_RB slots issued together, then the lengths
+        constexpr int SF_RB = 7;
+#pragma unroll 1
+        for (int k0 = 0; k0 < SF_RPT; k0 += SF_RB) {
+            int ca[SF_RB], cb[SF_RB];
+#pragma unroll
+            for (int k = 0; k < SF_RB; k++) {
+                const int q = tid + (k0 + k) * SEARCH_THREADS;
+                ca[k] = -1;
+                cb[k] = -1;
+                if (q >= SF_ROWS) continue;
                 const int s = q / MAX_ROWS, r = q % MAX_ROWS;
-                int st = 0, n = 0;
-                if (s < G && r < sh.nrows[s]) {
-                    const ScenePar& P = d.par[sh.scene[s]];
-                    const int k = r / 9, rr = r % 9, l = sh.nrows[s] / 9 - 1 - k;
-                    int gx, gy, gz, base;
-                    if (P.levels <= 1) {
-                        gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
-                        base = P.cell_off;
-                    } else {
-                        gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
-                        base = P.cell_off + P.loff[l];
-                    }
-                    const int cx0 = sh.cc[s][k][0], cy0 = sh.cc[s][k][1], cz0 = sh.cc[s][k][2];
-                    const int z = cz0 + rr / 3 - 1, y = cy0 + rr % 3 - 1;
-                    const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
-                    if (xa <= xb && z >= 0 && z < gz && y >= 0 && y < gy) {
-                        const int cb = base + (z * gy + y) * gx;
-                        st = cstart[cb + xa];
-                        n = cstart[cb + xb + 1] - st;
-                    }
+                if (s >= G || r >= sh.nrows[s]) continue;
+                const ScenePar& P = d.par[sh.scene[s]];
+                const int kl = r / 9, rr = r % 9, l = sh.nrows[s] / 9 - 1 - kl;
+                int gx, gy, gz, base;
+                if (P.levels <= 1) {
+                    gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
+                    base = P.cell_off;
+                } else {
+                    gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
+                    base = P.cell_off + P.loff[l];
                 }
-                sh.rs[q] = st;
-                sh.pre[q] = n;
-                acc += n;
+                const int cx0 = sh.cc[s][kl][0], cy0 = sh.cc[s][kl][1], cz0 = sh.cc[s][kl][2];
+                const int z = cz0 + rr / 3 - 1, y = cy0 + rr % 3 - 1;
+                const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
+                if (xa <= xb && z >= 0 && z < gz && y >= 0 && y < gy) {
+                    const int cb0 = base + (z * gy + y) * gx;
+                    ca[k] = cb0 + xa;
+                    cb[k] = cb0 + xb + 1;
+                }
             }
+#pragma unroll
+            for (int k = 0; k < SF_RB; k++) {
+                if (ca[k] >= 0) {
+                    ca[k] = cstart[ca[k]];
+                    cb[k] = cstart[cb[k]];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < SF_RB; k++) {
+                const int q = tid + (k0 + k) * SEARCH_THREADS;
+                if (q >= SF_ROWS) continue;
+                sh.rs[q] = ca[k] >= 0 ? ca[k] : 0;
+                sh.pre[q] = ca[k] >= 0 ? cb[k] - ca[k] : 0;
+            }
+        }
+        __syncthreads();
+        {
+            // exclusive prefix of the lengths: a run of consecutive slots per thread
+            const int q0 = tid * SF_RPT;
+            int acc = 0;
+            for (int q = q0; q < min(q0 + SF_RPT, SF_ROWS); q++) acc += sh.pre[q];
             int total;
             int ex = block_excl_scan<SEARCH_THREADS>(acc, sh.scan, total);
-            for (int q = q0; q < min(q0 + RPT, SF_ROWS); q++) {
+            for (int q = q0; q < min(q0 + SF_RPT, SF_ROWS); q++) {
                 const int n = sh.pre[q];
                 sh.pre[q] = ex;
                 ex += n;
@@ -1348,39 +1364,44 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
         for (int w0 = 0; w0 < F; w0 += SF_CAP) {
             const int wend = min(F, w0 + SF_CAP);
             const int nwords = (wend - w0 + 31) >> 5;
-            // ---- 3. tests, 32 consecutive candidates per thread
-            for (int wd = tid; wd < nwords; wd += SEARCH_THREADS) {
-                const int f0 = w0 + 32 * wd, fe = min(f0 + 32, wend);
-                int q = sf_row(sh.pre, 0, SF_ROWS, f0);
-                int s = q / MAX_ROWS;
-                double4 pi = sh.pi[s];
-                int i = sh.ii[s];
-                int nxt = sh.pre[q + 1], jo = sh.rs[q] - sh.pre[q];
-                unsigned word = 0;
-                for (int f = f0; f < fe; f++) {
-                    while (f >= nxt) {
-                        q++;
-                        nxt = sh.pre[q + 1];
-                        jo = sh.rs[q] - sh.pre[q];
+            // ---- 3a. the row slot of every candidate of the window
+            for (int q = tid; q < SF_ROWS; q += SEARCH_THREADS) {
+                const int a = max(sh.pre[q], w0), b = min(sh.pre[q + 1], wend);
+                for (int f = a; f < b; f++) sh.rowid[f - w0] = (unsigned short)q;
+            }
+            __syncthreads();
+            // ---- 3b. tests, a warp word (32 candidates) at a time, two words in flight
+            for (int wd = warp; wd < nwords; wd += 2 * NW) {
+                bool hit[2] = {false, false};
+                int jj[2] = {-1, -1}, ss[2] = {0, 0};
+                double4 pj[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int f = w0 + 32 * (wd + u * NW) + lane;
+                    if (wd + u * NW < nwords && f < wend) {
+                        const int q = sh.rowid[f - w0];
+                        ss[u] = q / MAX_ROWS;
+                        jj[u] = sh.rs[q] + (f - sh.pre[q]);
+                        pj[u] = posr[jj[u]];
                     }
-                    if (q / MAX_ROWS != s) {
-                        s = q / MAX_ROWS;
-                        pi = sh.pi[s];
-                        i = sh.ii[s];
-                    }
-                    const int j = jo + f;
-                    const double4 pj = posr[j];
-                    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    const double d2 = dx * dx + dy * dy + dz * dz;
-                    const double lim = 1.50 * (pi.w + pj.w);
-                    if (j != i && d2 < lim * lim) word |= 1u << (f - f0);
                 }
-                sh.bits[wd] = word;
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    if (jj[u] >= 0) {
+                        const double4 pi = sh.pi[ss[u]];
+                        const double dx = pi.x - pj[u].x, dy = pi.y - pj[u].y, dz = pi.z - pj[u].z;
+                        const double d2 = dx * dx + dy * dy + dz * dz;
+                        const double lim = 1.50 * (pi.w + pj[u].w);
+                        hit[u] = jj[u] != sh.ii[ss[u]] && d2 < lim * lim;
+                    }
+                    const unsigned word = __ballot_sync(0xffffffffu, hit[u]);
+                    if (lane == 0 && wd + u * NW < nwords) sh.bits[wd + u * NW] = word;
+                }
             }
             __syncthreads();
             // ---- 4. hits in discovery order, a warp per subsphere
-            for (int s = warp; s < G; s += SEARCH_THREADS / 32) {
-                const int qs = s * MAX_ROWS, nr = sh.nrows[s];
+            for (int s = warp; s < G; s += NW) {
+                const int qs = s * MAX_ROWS;
                 const int a = max(sh.pre[qs], w0), b = min(sh.pre[qs + MAX_ROWS], wend);
                 if (a >= b) continue;
                 const int i = sh.ii[s], tb = sh.tt[s] - i, ci = sh.ci[s];
@@ -1400,7 +1421,7 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
                     unsigned fm = 0;   // front hits among m
                     for (unsigned mm = m; mm; mm &= mm - 1) {
                         const int bit = __ffs(mm) - 1;
-                        const int q = sf_row(sh.pre, qs, nr, f0 + bit);
+                        const int q = sh.rowid[f0 + bit - w0];
                         const int j = sh.rs[q] + (f0 + bit - sh.pre[q]);
                         if (q - qs < 9 && i < j) fm |= 1u << bit;
                     }
@@ -1415,7 +1436,7 @@ static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const 
                     int pf = nf + xf - cf, pb = nb + xb - cb;
                     for (unsigned mm = m; mm; mm &= mm - 1) {
                         const int bit = __ffs(mm) - 1;
-                        const int q = sf_row(sh.pre, qs, nr, f0 + bit);
+                        const int q = sh.rowid[f0 + bit - w0];
                         const int j = sh.rs[q] + (f0 + bit - sh.pre[q]);
                         const int flag = cid[j] == ci ? INTRA : 0;
                         if (fm & (1u << bit)) {
