@@ -380,7 +380,7 @@ nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n, nbc_options*
         best.pair_blocks = 12;
         best.use_graph = 1;
         double tb = trial(best);
-        const int lanes[] = {1, 16, 32}, batch[] = {1, 4}, blocks[] = {4, 8, 16};
+        const int lanes[] = {16, 32}, batch[] = {1, 4}, blocks[] = {4, 8, 16};
         for (int x : lanes) {
             nbc_options o = best;
             o.search_lanes = x;

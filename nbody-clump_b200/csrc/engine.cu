@@ -831,8 +831,7 @@ class EngineT final : public EngineBase {
         hflag_ = g_pinned.get();
         mem_.stream = stream_;
         DevMem::keep_pool(opt_.device);
-        search_lanes_ = opt_.search_lanes == 1 || opt_.search_lanes == 16 || opt_.search_lanes == 32
-                            ? opt_.search_lanes : 8;
+        search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
         clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
         // the clump pass's staged contact records (dynamic shared memory past the 48 KB default)
         CK(cudaFuncSetAttribute(k_clump<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
@@ -1343,8 +1342,8 @@ class EngineT final : public EngineBase {
     void launch_rebuild(bool eager) {
         const int B = 128;
         const int gN = std::min(cdiv(N_, B), 148 * 16);         // grid-stride grids
-        const int sl = search_lanes_;   // 1: the block-cooperative search (its long rows refilled by 8 lanes)
-        const int gS = std::min(cdiv(N_, SEARCH_THREADS / (sl == 1 ? 8 : sl)), 148 * 16);
+        const int sl = search_lanes_;
+        const int gS = std::min(cdiv(N_, SEARCH_THREADS / sl), 148 * 16);
         const int* pl = h_.plan;
         k_plan<<<1, SC_THREADS, 0, stream_>>>(d_);
         k_hash<<<gN, B, 0, stream_>>>(d_);
@@ -1360,8 +1359,7 @@ class EngineT final : public EngineBase {
         k_cellrange<<<gN, B, 0, stream_>>>(d_, ki, vi);
         k_cellstart<<<std::min(cdiv(h_.cells + S_, 256), 148 * 16), 256, 0, stream_>>>(d_);
         k_reorder<R><<<gN, B, 0, stream_>>>(d_);
-        if (sl == 1) k_search_flat<<<std::min(cdiv(N_, SF_G), 148 * 8), SEARCH_THREADS, 0, stream_>>>(d_);
-        else if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
+        if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else k_search<8><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         scan(h_.cnt_f, h_.cnt_b, nullptr, N_ + 1, pl + PL_T1);

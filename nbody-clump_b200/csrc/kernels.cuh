@@ -1205,271 +1205,6 @@ __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search(const Dev* __restr
     }
 }
 
-// The fused search, block-cooperative: the same counts, scratch rows and
-// cross-level counts as k_search, from a flat walk over a chunk's candidates.
-// A block claims SF_G consecutive subspheres of the rebuilt concatenation
-// (consecutive in the sorted order, so mostly of one grid level) and
-//   1. finds each one's cell on its own level and every coarser one (three
-//      divisions per subsphere and level);
-//   2. resolves every stencil row of the chunk (MAX_ROWS row slots per
-//      subsphere, unused ones empty): first the cell ranges, then their
-//      cstart loads several at a time, then a scan of the lengths over the
-//      whole chunk, so the chunk's candidates are one flat range, each
-//      subsphere's in its discovery order;
-//   3. per window of SF_CAP candidates, maps every candidate to its row slot
-//      (each row writes its own range), then tests the candidates a warp
-//      word at a time (a lane per candidate, the word by ballot) -- every
-//      lane busy whatever the row lengths;
-//   4. emits the hits: one warp per subsphere, a lane per bitmap word, ballot
-//      prefixes for the front and back positions, so each row keeps the
-//      discovery order.
-// Hits of a subsphere that spans windows are appended in window order.
-constexpr int SF_G = 32;
-constexpr int SF_ROWS = SF_G * MAX_ROWS;
-constexpr int SF_CAP = 8192;
-constexpr int SF_RPT = (SF_ROWS + SEARCH_THREADS - 1) / SEARCH_THREADS;   // row slots per thread
-struct SearchFlatShared {
-    double4 pi[SF_G];
-    int ii[SF_G], tt[SF_G], ci[SF_G], scene[SF_G], nrows[SF_G], nf[SF_G], nb[SF_G];
-    int cc[SF_G][MAX_LEVELS][3];   // cell of the subsphere on the k-th level it searches (own level first)
-    int rs[SF_ROWS];               // first sorted slot of each row slot
-    int pre[SF_ROWS + 1];          // exclusive prefix of the row lengths over the chunk
-    unsigned short rowid[SF_CAP];  // row slot of each candidate of the current window
-    unsigned bits[SF_CAP / 32];    // hits of the current window
-    int scan[SEARCH_THREADS / 32];
-    int claim;
-};
-static_assert(SF_ROWS < 65536, "row slots fit 16 bits");
-
-static __global__ void __launch_bounds__(SEARCH_THREADS, 8) k_search_flat(const Dev* __restrict__ dp) {
-    __shared__ SearchFlatShared sh;
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = SEARCH_THREADS / 32;
-    const double4* __restrict__ posr = d.posr2;
-    const int* __restrict__ cid = d.clump_id2;
-    const int* __restrict__ cstart = d.cstart;
-    int* __restrict__ cnt_f = d.cnt_f;
-    for (;;) {
-        const int c0 = claim_chunk(d.plan + PL_CS, SF_G, &sh.claim);
-        if (c0 >= T) break;
-        const int G = min(SF_G, T - c0);
-        if (tid < SF_G) {
-            int nr = 0;
-            if (tid < G) {
-                const PlanItem it = plan_item(d, ns, c0 + tid);
-                const ScenePar& P = d.par[it.s];
-                sh.ii[tid] = it.i;
-                sh.tt[tid] = c0 + tid;
-                sh.scene[tid] = it.s;
-                sh.pi[tid] = posr[it.i];
-                sh.ci[tid] = cid[it.i];
-                // out-of-box subspheres do not search
-                if (d.key2[it.i] != P.cell_off + P.cellnum - 1) nr = 9 * ((P.levels > 1 ? d.level2[it.i] : 0) + 1);
-            }
-            sh.nrows[tid] = nr;
-            sh.nf[tid] = 0;
-            sh.nb[tid] = 0;
-        }
-        __syncthreads();
-        // ---- 1. cells on the levels searched
-        for (int q = tid; q < G * MAX_LEVELS; q += SEARCH_THREADS) {
-            const int s = q / MAX_LEVELS, k = q % MAX_LEVELS;
-            if (9 * k >= sh.nrows[s]) continue;
-            const ScenePar& P = d.par[sh.scene[s]];
-            const double4 pi = sh.pi[s];
-            int cx, cy, cz;
-            if (P.levels <= 1) {
-                cx = (int)floor((pi.x - P.origin[0]) * P.icell[0]);
-                cy = (int)floor((pi.y - P.origin[1]) * P.icell[1]);
-                cz = (int)floor((pi.z - P.origin[2]) * P.icell[2]);
-            } else {
-                const double c = P.lcell[sh.nrows[s] / 9 - 1 - k];
-                cx = (int)floor((pi.x - P.origin[0]) / c);
-                cy = (int)floor((pi.y - P.origin[1]) / c);
-                cz = (int)floor((pi.z - P.origin[2]) / c);
-            }
-            sh.cc[s][k][0] = cx;
-            sh.cc[s][k][1] = cy;
-            sh.cc[s][k][2] = cz;
-        }
-        __syncthreads();
-        // ---- 2. stencil rows: the cell range of each row slot (thread-strided
-        // slots), the cstart loads of SF_RB slots issued together, then the lengths
-        constexpr int SF_RB = 7;
-#pragma unroll 1
-        for (int k0 = 0; k0 < SF_RPT; k0 += SF_RB) {
-            int ca[SF_RB], cb[SF_RB];
-#pragma unroll
-            for (int k = 0; k < SF_RB; k++) {
-                const int q = tid + (k0 + k) * SEARCH_THREADS;
-                ca[k] = -1;
-                cb[k] = -1;
-                if (q >= SF_ROWS) continue;
-                const int s = q / MAX_ROWS, r = q % MAX_ROWS;
-                if (s >= G || r >= sh.nrows[s]) continue;
-                const ScenePar& P = d.par[sh.scene[s]];
-                const int kl = r / 9, rr = r % 9, l = sh.nrows[s] / 9 - 1 - kl;
-                int gx, gy, gz, base;
-                if (P.levels <= 1) {
-                    gx = P.gdim[0]; gy = P.gdim[1]; gz = P.gdim[2];
-                    base = P.cell_off;
-                } else {
-                    gx = P.ldim[l][0]; gy = P.ldim[l][1]; gz = P.ldim[l][2];
-                    base = P.cell_off + P.loff[l];
-                }
-                const int cx0 = sh.cc[s][kl][0], cy0 = sh.cc[s][kl][1], cz0 = sh.cc[s][kl][2];
-                const int z = cz0 + rr / 3 - 1, y = cy0 + rr % 3 - 1;
-                const int xa = max(cx0 - 1, 0), xb = min(cx0 + 1, gx - 1);
-                if (xa <= xb && z >= 0 && z < gz && y >= 0 && y < gy) {
-                    const int cb0 = base + (z * gy + y) * gx;
-                    ca[k] = cb0 + xa;
-                    cb[k] = cb0 + xb + 1;
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < SF_RB; k++) {
-                if (ca[k] >= 0) {
-                    ca[k] = cstart[ca[k]];
-                    cb[k] = cstart[cb[k]];
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < SF_RB; k++) {
-                const int q = tid + (k0 + k) * SEARCH_THREADS;
-                if (q >= SF_ROWS) continue;
-                sh.rs[q] = ca[k] >= 0 ? ca[k] : 0;
-                sh.pre[q] = ca[k] >= 0 ? cb[k] - ca[k] : 0;
-            }
-        }
-        __syncthreads();
-        {
-            // exclusive prefix of the lengths: a run of consecutive slots per thread
-            const int q0 = tid * SF_RPT;
-            int acc = 0;
-            for (int q = q0; q < min(q0 + SF_RPT, SF_ROWS); q++) acc += sh.pre[q];
-            int total;
-            int ex = block_excl_scan<SEARCH_THREADS>(acc, sh.scan, total);
-            for (int q = q0; q < min(q0 + SF_RPT, SF_ROWS); q++) {
-                const int n = sh.pre[q];
-                sh.pre[q] = ex;
-                ex += n;
-            }
-            if (tid == 0) sh.pre[SF_ROWS] = total;
-        }
-        __syncthreads();
-        const int F = sh.pre[SF_ROWS];
-        for (int w0 = 0; w0 < F; w0 += SF_CAP) {
-            const int wend = min(F, w0 + SF_CAP);
-            const int nwords = (wend - w0 + 31) >> 5;
-            // ---- 3a. the row slot of every candidate of the window
-            for (int q = tid; q < SF_ROWS; q += SEARCH_THREADS) {
-                const int a = max(sh.pre[q], w0), b = min(sh.pre[q + 1], wend);
-                for (int f = a; f < b; f++) sh.rowid[f - w0] = (unsigned short)q;
-            }
-            __syncthreads();
-            // ---- 3b. tests, a warp word (32 candidates) at a time, two words in flight
-            for (int wd = warp; wd < nwords; wd += 2 * NW) {
-                bool hit[2] = {false, false};
-                int jj[2] = {-1, -1}, ss[2] = {0, 0};
-                double4 pj[2];
-#pragma unroll
-                for (int u = 0; u < 2; u++) {
-                    const int f = w0 + 32 * (wd + u * NW) + lane;
-                    if (wd + u * NW < nwords && f < wend) {
-                        const int q = sh.rowid[f - w0];
-                        ss[u] = q / MAX_ROWS;
-                        jj[u] = sh.rs[q] + (f - sh.pre[q]);
-                        pj[u] = posr[jj[u]];
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 2; u++) {
-                    if (jj[u] >= 0) {
-                        const double4 pi = sh.pi[ss[u]];
-                        const double dx = pi.x - pj[u].x, dy = pi.y - pj[u].y, dz = pi.z - pj[u].z;
-                        const double d2 = dx * dx + dy * dy + dz * dz;
-                        const double lim = 1.50 * (pi.w + pj[u].w);
-                        hit[u] = jj[u] != sh.ii[ss[u]] && d2 < lim * lim;
-                    }
-                    const unsigned word = __ballot_sync(0xffffffffu, hit[u]);
-                    if (lane == 0 && wd + u * NW < nwords) sh.bits[wd + u * NW] = word;
-                }
-            }
-            __syncthreads();
-            // ---- 4. hits in discovery order, a warp per subsphere
-            for (int s = warp; s < G; s += NW) {
-                const int qs = s * MAX_ROWS;
-                const int a = max(sh.pre[qs], w0), b = min(sh.pre[qs + MAX_ROWS], wend);
-                if (a >= b) continue;
-                const int i = sh.ii[s], tb = sh.tt[s] - i, ci = sh.ci[s];
-                int* __restrict__ scr_f = d.scr + (size_t)i * (2 * SCR_CAP);
-                int* __restrict__ scr_b = scr_f + SCR_CAP;
-                int nf = sh.nf[s], nb = sh.nb[s];
-                const int wa = (a - w0) >> 5, wb = (b - 1 - w0) >> 5;
-                for (int wbase = wa; wbase <= wb; wbase += 32) {
-                    const int wd = wbase + lane;
-                    const int f0 = w0 + 32 * wd;
-                    unsigned m = 0;
-                    if (wd <= wb) {
-                        m = sh.bits[wd];
-                        if (f0 < a) m &= ~0u << (a - f0);
-                        if (b - f0 < 32) m &= (1u << (b - f0)) - 1u;
-                    }
-                    unsigned fm = 0;   // front hits among m
-                    for (unsigned mm = m; mm; mm &= mm - 1) {
-                        const int bit = __ffs(mm) - 1;
-                        const int q = sh.rowid[f0 + bit - w0];
-                        const int j = sh.rs[q] + (f0 + bit - sh.pre[q]);
-                        if (q - qs < 9 && i < j) fm |= 1u << bit;
-                    }
-                    const int cf = __popc(fm), cb = __popc(m) - cf;
-                    int xf = cf, xb = cb;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int yf = __shfl_up_sync(0xffffffffu, xf, o);
-                        const int yb = __shfl_up_sync(0xffffffffu, xb, o);
-                        if (lane >= o) { xf += yf; xb += yb; }
-                    }
-                    int pf = nf + xf - cf, pb = nb + xb - cb;
-                    for (unsigned mm = m; mm; mm &= mm - 1) {
-                        const int bit = __ffs(mm) - 1;
-                        const int q = sh.rowid[f0 + bit - w0];
-                        const int j = sh.rs[q] + (f0 + bit - sh.pre[q]);
-                        const int flag = cid[j] == ci ? INTRA : 0;
-                        if (fm & (1u << bit)) {
-                            if (pf < SCR_CAP) scr_f[pf] = j | flag;
-                            pf++;
-                        } else {
-                            const bool cross = q - qs >= 9;
-                            if (pb < SCR_CAP) scr_b[pb] = j | flag | (cross ? CROSS_TAG : 0);
-                            pb++;
-                            if (cross) atomicAdd(&cnt_f[j + tb], 1);
-                        }
-                    }
-                    nf += __shfl_sync(0xffffffffu, xf, 31);
-                    nb += __shfl_sync(0xffffffffu, xb, 31);
-                }
-                if (lane == 0) {
-                    sh.nf[s] = nf;
-                    sh.nb[s] = nb;
-                }
-            }
-            __syncthreads();
-        }
-        if (tid < G) {
-            const int s = sh.scene[tid], t = sh.tt[tid], nf = sh.nf[tid], nb = sh.nb[tid];
-            atomicAdd(&cnt_f[t], nf);
-            d.cnt_b[t] = nb;
-            d.sfc[t] = nf;
-            const int bl = d.par[s].bl;
-            if (nf > bl / 2 || nb > bl / 2) atomicOr(&d.dyn[s].err, ERR_ROW_OVERFLOW);
-        }
-    }
-}
-
 // After the scans: the pairs of each rebuilt scene's new list (front and
 // back entries are equally many: every pair is one owner entry and one
 // partner entry) into need[s], their prefix over the rebuilt scenes into
