@@ -658,6 +658,8 @@ class EngineT final : public EngineBase {
         blk(h_.cw, K_ * sizeof(double4));
         blk(h_.cq, K_ * sizeof(double4));
         blk(h_.cprop, K_ * sizeof(double4));
+        blk(h_.cinv, K_ * sizeof(double4));
+        blk(h_.mem_cl, N * sizeof(int));
         blk(h_.cF, K_ * sizeof(double4));
         blk(h_.cT, K_ * sizeof(double4));
         blk(h_.mem_start, (K_ + 1) * sizeof(int));
@@ -1005,6 +1007,8 @@ class EngineT final : public EngineBase {
             h_.fbnd = m.take<R4<R>>(2 * N);
             h_.cpos = m.take<double4>(K_); h_.cvel = m.take<double4>(K_); h_.cw = m.take<double4>(K_);
             h_.cq = m.take<double4>(K_); h_.cprop = m.take<double4>(K_);
+            h_.cinv = m.take<double4>(K_);
+            h_.mem_cl = m.take<int>(N);
             h_.cF = m.take<double4>(K_); h_.cT = m.take<double4>(K_);
             h_.mem_start = m.take<int>(K_ + 1);
             h_.mem_idx = m.take<int>(N);
@@ -1077,6 +1081,17 @@ class EngineT final : public EngineBase {
         copy_(h_.cw, cw.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
         copy_(h_.cq, cq.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
         copy_(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        {
+            // the clump pass's reciprocals: IEEE divisions, bitwise those it formed each step
+            std::vector<double4> cinv(K_);
+            for (int k = 0; k < K_; k++)
+                cinv[k] = make_double4(1.0 / cprop[k].x, 1.0 / cprop[k].y, 1.0 / cprop[k].z, 1.0 / cprop[k].w);
+            copy_(h_.cinv, cinv.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+            std::vector<int> mcl(N);
+            for (int k = 0; k < K_; k++)
+                for (int m = mstart[k]; m < mstart[k + 1]; m++) mcl[m] = k;
+            copy_(h_.mem_cl, mcl.data(), N * sizeof(int), cudaMemcpyHostToDevice);
+        }
         copy_(h_.mem_start, mstart.data(), (K_ + 1) * sizeof(int), cudaMemcpyHostToDevice);
         copy_(h_.mem_idx, midx.data(), N * sizeof(int), cudaMemcpyHostToDevice);
         // the first list is empty: rows of zeros (the slab is zeroed)

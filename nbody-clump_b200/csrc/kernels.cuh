@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
         s_ms[warp][lane] = mem_start[k0 + min(lane, nk)];
         if (lane == 0) s_ms[warp][32] = mem_start[k0 + nk];
         const int sc = d.csid[k];
-        double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cprop[k];
+        double4 cp = d.cpos[k], cv = d.cvel[k], cw = d.cw[k], cq = d.cq[k], pr = d.cinv[k];
         const bool pre_k = stops ? scene_pre(d.dyn[sc], do_pre, L) : do_pre != 0;
         const bool post_k = stops ? scene_post(d.dyn[sc], post, L) : post != 0;
         s_sc[warp][lane] = sc;
@@ -172,15 +172,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
         __syncwarp();
         const int M0 = s_ms[warp][0], M1 = s_ms[warp][nk];
         const int mb = s_ms[warp][isc ? lane : nk - 1], me = s_ms[warp][isc ? lane + 1 : nk];
-        // the warp-local clump holding member slot m (members are grouped by clump)
-        auto owner = [&](int m) {
-            int lo = 0, hi = nk - 1;
-            while (lo < hi) {
-                const int h = (lo + hi + 1) >> 1;
-                if (s_ms[warp][h] <= m) lo = h; else hi = h - 1;
-            }
-            return lo;
-        };
+        // the warp-local clump of member slot m: mem_cl[m] - k0
+        const int* __restrict__ mem_cl = d.mem_cl;
         const ScenePar& P = d.par[sc];
         const double Dt = P.dt;
         V3<double> F, T;
@@ -204,7 +197,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                 for (int j = 0; j < J; j++) {
                     const int m = c0 + 32 * j + lane;
                     idx[j] = m < M1 ? mem_idx[m] : -1;
-                    own[j] = m < M1 ? owner(m) : 0;
+                    own[j] = m < M1 ? mem_cl[m] - k0 : 0;
                 }
                 double4 ps[J];
                 int r0[J], r1[J], q0[J], q1[J];
@@ -312,9 +305,9 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                 }
             }
             if (post_k) {
-                V3<double> ac = (1.0 / pr.w) * F;
+                V3<double> ac = pr.w * F;   // pr: the reciprocals 1/I, 1/M
                 ac.z = ac.z + P.gravity;
-                V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
+                V3<double> al = v3(pr.x * T.x, pr.y * T.y, pr.z * T.z);
                 cv.x += (0.5 * Dt) * ac.x; cv.y += (0.5 * Dt) * ac.y; cv.z += (0.5 * Dt) * ac.z;
                 cw.x += (0.5 * Dt) * al.x; cw.y += (0.5 * Dt) * al.y; cw.z += (0.5 * Dt) * al.z;
             }
@@ -324,9 +317,9 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
         }
         if (do_pre) {
             const double4 cp_old = cp;
-            V3<double> ac = (1.0 / pr.w) * F;
+            V3<double> ac = pr.w * F;   // pr: the reciprocals 1/I, 1/M
             ac.z = ac.z + P.gravity;
-            V3<double> al = v3((1.0 / pr.x) * T.x, (1.0 / pr.y) * T.y, (1.0 / pr.z) * T.z);
+            V3<double> al = v3(pr.x * T.x, pr.y * T.y, pr.z * T.z);
             V3<double> v = xyzd(cv), w = xyzd(cw);
             V3<double> dist = Dt * v + (0.5 * Dt * Dt) * ac;
             cp.x += dist.x; cp.y += dist.y; cp.z += dist.z;
@@ -378,11 +371,12 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             // records, in flight together
             constexpr int JP = J;
             for (int c0 = M0; c0 < M1; c0 += 32 * JP) {
-                int idx[JP];
+                int idx[JP], own[JP];
 #pragma unroll
                 for (int j = 0; j < JP; j++) {
                     const int m = c0 + 32 * j + lane;
                     idx[j] = m < M1 ? mem_idx[m] : -1;
+                    own[j] = m < M1 ? mem_cl[m] - k0 : 0;
                 }
                 double4 lo[JP], old[JP], cu[JP];
 #pragma unroll
@@ -396,7 +390,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                 for (int j = 0; j < JP; j++) {
                     if (idx[j] < 0) continue;
                     const int i = idx[j];
-                    const int kk = owner(c0 + 32 * j + lane);
+                    const int kk = own[j];
                     if (!s_pre[warp][kk]) continue;
                     const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
                                                     s_cl[warp][12][kk]);

@@ -134,6 +134,8 @@ struct Dev {
     double4* cw;
     double4* cq;      // x y z w
     double4* cprop;   // Ixx Iyy Izz M
+    int* mem_cl;      // [N] clump of each member slot (fixed: members stay in their clump's range)
+    double4* cinv;    // 1/Ixx 1/Iyy 1/Izz 1/M (correctly rounded divisions, computed once)
     double4* cF;      // force on clump from the last force pass
     double4* cT;
     int* mem_start;   // [K+1]
