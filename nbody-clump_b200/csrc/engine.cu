@@ -241,7 +241,7 @@ class EngineT final : public EngineBase {
         if (pend_ > 0) {
             CK(cudaStreamSynchronize(stream_));
             const int started = read_gstep() - pend_before_;
-            launches_ += (CLUMP_LAUNCHES + CONTACT_LAUNCHES) * (long long)started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
+            launches_ += (1LL + CONTACT_LAUNCHES) * started + (timing_ == 0 && gexec_loop_ ? 1 : 0);
             if (read_int(h_.halt)) {
                 check_scan();
                 // the last step started stopped at its rebuild: finish it on the host path
@@ -1292,17 +1292,13 @@ class EngineT final : public EngineBase {
                       cudaGraphConditionalHandle loop = 0, int use_loop = 0) {
         const int g = cdiv(K_ + S_, CL_THREADS);
         if (clump_batch_ == 1)
-            k_clump<R, 1><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre);
+            k_clump<R, 1><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         else if (clump_batch_ == 4)
-            k_clump<R, 4><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre);
+            k_clump<R, 4><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         else
-            k_clump<R, 2><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre);
-        // the member poses and the step's rebuild test (a step only)
-        if (do_pre)
-            k_pose<<<std::min(cdiv(N_, PS_THREADS), sm_count_ * 8), PS_THREADS, 0, stream_>>>(d_, cond, use_cond,
-                                                                                              loop, use_loop);
+            k_clump<R, 2><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         CK(cudaGetLastError());
-        if (!capturing_) launches_ += do_pre ? CLUMP_LAUNCHES : 1;
+        if (!capturing_) launches_ += 1;
     }
     bool capturing_ = false;
     // the contact pass: k_pairs, with k_boundary beside it on the second

@@ -75,7 +75,8 @@ __device__ __forceinline__ void stage_rec(SlotRec<R>* dst, const R4<R>* f, const
 }
 
 // Integrate_Before_clump_cuk / Attitude_clump_cuk / Integrate_After_clump_cuk
-// (src/dem_integrate_clumpsphere.cu:3-141), ComputeTorqueFromWorldPos_Kernel + reduce_by_key
+// (src/dem_integrate_clumpsphere.cu:3-141), UpdatePos_cuk (src/dem_clump.cu:
+// 113-138), ComputeTorqueFromWorldPos_Kernel + reduce_by_key
 // (src/dem_clumpsphere.cu:86-151), IntegratePene_Before_cuk and
 // Integrate_After_cuk (src/dem_integrate_penetrator.cu:3-113).
 //
@@ -85,14 +86,13 @@ __device__ __forceinline__ void stage_rec(SlotRec<R>* dst, const R4<R>* f, const
 // all member records (every load of the chunk in flight at once), each
 // member's force and lever-arm torque go to shared memory, and each lane then
 // sums its own clump's members in ascending order (the reduce_by_key order)
-// and integrates its clump once.  The lanes after the last clump hold one
-// thread per scene for the intruder.  The member poses of a step follow in
-// k_pose, one thread per member (a wave of member-parallel memory traffic
-// that 32 clumps per warp would serialise).
+// and integrates its clump once.  The new poses are shared the same way and
+// the lanes pose the members 32 at a time.  The lanes after the last clump
+// hold one thread per scene for the intruder.
 //
 // A step (do_pre) also advances the spring-history generation so the next
 // contact pass reads what the previous one wrote, and counts itself; the last
-// block of k_pose sets the graph's rebuild condition (when given a handle)
+// block to finish sets the graph's rebuild condition (when given a handle)
 // and counts the step in lstep.  A scene with a stop s takes the steps started
 // at lstep = 0 .. s-1 and closes the last one at lstep = s; afterwards it
 // stands still (frozen) while the other scenes go on, so its state is
@@ -118,15 +118,23 @@ constexpr size_t clump_dyn_smem() {
 // members in shared memory at a time.  J <= 2 fits 128 registers (4 blocks,
 // 16 warps per SM) with a few bytes of spill; J = 4 keeps 3 blocks per SM.
 template <typename R, int J>
-__global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev* __restrict__ dp, int do_pre) {
+__global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev* __restrict__ dp, int do_pre,
+                                                      cudaGraphConditionalHandle cond, int use_cond,
+                                                      cudaGraphConditionalHandle loop, int use_loop) {
     constexpr int CL_CHUNK = 32 * J;
     __shared__ double s_mf[CL_WARPS][6][CL_CHUNK];   // member force xyz, torque xyz
-    __shared__ double s_cl[CL_WARPS][3][32];         // clump position at the start of the step
+    __shared__ double s_cl[CL_WARPS][13][32];        // clump position, velocity, angular velocity, quaternion
     __shared__ int s_ms[CL_WARPS][33];               // member-list offsets of the warp's clumps
     __shared__ int s_sc[CL_WARPS][32];               // scene of each of the warp's clumps
+    __shared__ int s_pre[CL_WARPS][32];              // the clump's scene takes this step
     extern __shared__ __align__(16) unsigned char cl_dsm[];   // staged contact records
     const Dev& d = *dp;
-    if (*d.halt) return;   // a rebuild ran out of pair capacity: the host finishes that step
+    if (*d.halt) {
+        // a rebuild ran out of pair capacity: the host finishes that step, so
+        // a device-side step loop ends here
+        if (use_loop && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(loop, 0u);
+        return;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k0 = (blockIdx.x * CL_WARPS + warp) * 32;
     const int t = k0 + lane;
@@ -159,6 +167,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
         const bool pre_k = stops ? scene_pre(d.dyn[sc], do_pre, L) : do_pre != 0;
         const bool post_k = stops ? scene_post(d.dyn[sc], post, L) : post != 0;
         s_sc[warp][lane] = sc;
+        s_pre[warp][lane] = isc && pre_k;
         s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
         __syncwarp();
         const int M0 = s_ms[warp][0], M1 = s_ms[warp][nk];
@@ -346,6 +355,65 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                 d.cw[k] = make_double4(w.x, w.y, w.z, 0.0);
                 d.cq[k] = q;
             }
+            __syncwarp();   // the old positions in s_cl are no longer read
+            s_cl[warp][0][lane] = cp.x; s_cl[warp][1][lane] = cp.y; s_cl[warp][2][lane] = cp.z;
+            s_cl[warp][3][lane] = v.x; s_cl[warp][4][lane] = v.y; s_cl[warp][5][lane] = v.z;
+            s_cl[warp][6][lane] = w.x; s_cl[warp][7][lane] = w.y; s_cl[warp][8][lane] = w.z;
+            s_cl[warp][9][lane] = q.x; s_cl[warp][10][lane] = q.y; s_cl[warp][11][lane] = q.z;
+            s_cl[warp][12][lane] = q.w;
+            __syncwarp();
+            // ---- poses of the members, 32 at a time
+            double4* __restrict__ kv = (double4*)d.kin;   // per member: velocity + mass, angular velocity, arm
+            const double4* __restrict__ lom = d.lom;
+            double4* __restrict__ cum = d.cum;
+            double4* __restrict__ posw = d.posr;
+            // J members per lane at a time: all indices, then all member
+            // records, in flight together
+            constexpr int JP = J;
+            for (int c0 = M0; c0 < M1; c0 += 32 * JP) {
+                int idx[JP], own[JP];
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    const int m = c0 + 32 * j + lane;
+                    idx[j] = m < M1 ? mem_idx[m] : -1;
+                    own[j] = m < M1 ? mem_cl[m] - k0 : 0;
+                }
+                double4 lo[JP], old[JP], cu[JP];
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    const int i = idx[j] < 0 ? 0 : idx[j];
+                    lo[j] = lom[i];
+                    old[j] = posw[i];
+                    cu[j] = cum[i];
+                }
+#pragma unroll
+                for (int j = 0; j < JP; j++) {
+                    if (idx[j] < 0) continue;
+                    const int i = idx[j];
+                    const int kk = own[j];
+                    if (!s_pre[warp][kk]) continue;
+                    const double4 qk = make_double4(s_cl[warp][9][kk], s_cl[warp][10][kk], s_cl[warp][11][kk],
+                                                    s_cl[warp][12][kk]);
+                    const V3<double> arm = rot_b2w(qk, v3(lo[j].x, lo[j].y, lo[j].z));
+                    const V3<double> p = v3(s_cl[warp][0][kk] + arm.x, s_cl[warp][1][kk] + arm.y,
+                                            s_cl[warp][2][kk] + arm.z);
+                    const double4 c = cu[j], o = old[j];
+                    const V3<double> cn = v3((c.x + p.x) - o.x, (c.y + p.y) - o.y, (c.z + p.z) - o.z);
+                    const V3<double> vk = v3(s_cl[warp][3][kk], s_cl[warp][4][kk], s_cl[warp][5][kk]);
+                    const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
+                    cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
+                    posw[i] = make_double4(p.x, p.y, p.z, o.w);
+                    kv[3 * (size_t)i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
+                    kv[3 * (size_t)i + 1] = make_double4(wk.x, wk.y, wk.z, 0.0);
+                    kv[3 * (size_t)i + 2] = make_double4(arm.x, arm.y, arm.z, 0.0);
+                    const int sk = s_sc[warp][kk];
+                    if (len_floor(cn) > d.par[sk].thresh) {
+                        SceneDyn& y = d.dyn[sk];
+                        if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
+                        if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
+                    }
+                }
+            }
         }
         if (isc && post_k && !pre_k) {   // closing half-kick only (sync, or the scene's last step)
             d.cvel[k] = cv;
@@ -395,61 +463,12 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             }
         }
     }
-}
-
-// The member poses of a step (UpdatePos_cuk, src/dem_clump.cu:113-138), one
-// thread per member slot after the clump pass: the clump's new position,
-// attitude, velocity and angular velocity (just written by the clump pass)
-// give the subsphere's world lever arm and position, its displacement since
-// the last rebuild (the rebuild test) and its contact kinematics.  Members of
-// a scene past its stop stand still.  The last block to finish sets the
-// graph's rebuild condition (when given a handle), counts the step in lstep
-// and counts a device-side step loop down (ending it at zero, or at once when
-// a rebuild has run out of pair capacity).
-constexpr int PS_THREADS = 256;
-static __global__ void __launch_bounds__(PS_THREADS) k_pose(const Dev* __restrict__ dp,
-                                                            cudaGraphConditionalHandle cond, int use_cond,
-                                                            cudaGraphConditionalHandle loop, int use_loop) {
-    const Dev& d = *dp;
-    if (*d.halt) {
-        // the host finishes that step, so a device-side step loop ends here
-        if (use_loop && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(loop, 0u);
-        return;
-    }
-    const int L = *d.lstep;   // written only by the last block, after every block has read it
-    const bool stops = d.has_stops;
-    const int* __restrict__ mem_cl = d.mem_cl;
-    const int* __restrict__ mem_idx = d.mem_idx;
-    const double4* __restrict__ lom = d.lom;
-    double4* __restrict__ cum = d.cum;
-    double4* __restrict__ posw = d.posr;
-    double4* __restrict__ kv = (double4*)d.kin;   // per member: velocity + mass, angular velocity, arm
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < d.N; m += gridDim.x * blockDim.x) {
-        const int k = mem_cl[m], i = mem_idx[m];
-        const int sk = d.csid[k];
-        if (stops && !scene_pre(d.dyn[sk], 1, L)) continue;
-        const double4 cp = d.cpos[k], qk = d.cq[k], vk = d.cvel[k], wk = d.cw[k];
-        const double4 lo = lom[i], o = posw[i], c = cum[i];
-        const V3<double> arm = rot_b2w(qk, v3(lo.x, lo.y, lo.z));
-        const V3<double> p = v3(cp.x + arm.x, cp.y + arm.y, cp.z + arm.z);
-        const V3<double> cn = v3((c.x + p.x) - o.x, (c.y + p.y) - o.y, (c.z + p.z) - o.z);
-        cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
-        posw[i] = make_double4(p.x, p.y, p.z, o.w);
-        kv[3 * (size_t)i] = make_double4(vk.x, vk.y, vk.z, lo.w);
-        kv[3 * (size_t)i + 1] = make_double4(wk.x, wk.y, wk.z, 0.0);
-        kv[3 * (size_t)i + 2] = make_double4(arm.x, arm.y, arm.z, 0.0);
-        if (len_floor(cn) > d.par[sk].thresh) {
-            SceneDyn& y = d.dyn[sk];
-            if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
-            if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
-        }
-    }
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(d.kc_done, 1) == (int)gridDim.x - 1) {
             *d.kc_done = 0;
-            *d.lstep = L + 1;
+            if (do_pre) *d.lstep = L + 1;
             if (use_cond) cudaGraphSetConditional(cond, atomicAdd(d.any_rebuild, 0) ? 1u : 0u);
             if (use_loop) {
                 const int left = *d.loop_left - 1;
@@ -2229,7 +2248,6 @@ constexpr int PR_THREADS = 256;
 #define NBC_PAIR_MINB 2
 #endif
 constexpr int CONTACT_LAUNCHES = 2;   // k_pairs and k_boundary
-constexpr int CLUMP_LAUNCHES = 2;     // k_clump and k_pose
 template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
