@@ -402,15 +402,16 @@ def algorithmic_contact_bytes(N, nnear, ntouch, precision):
 
     Per near pair (the pairs that can touch before the next rebuild, each
     visited once): its near front record (pair slot, partner, owner and near
-    back slot, 16 B), the touch flag written 1 B, both subspheres' FP64
+    back slot, 16 B), both clump ids 8 B, the touch flag written 1 B, both subspheres' FP64
     position and radius 2 x 32 B, and the four contact slots written (force
     and torque on each side, 4 Real4).  Per touching pair: the previous touch
     flag 1 B, the spring history read and written (2 Real4 + 1 Real each way)
-    and both subspheres' FP64 contact kinematics (3 x 32 B each).  N is unused: the
+    and both subspheres' FP64 contact kinematics (3 x 32 B each: the
+    subsphere's arm and mass, its clump's velocity and angular velocity).  N is unused: the
     per-subsphere sums are part of the clump pass."""
     r = 4 if precision == "mixed" else 8
     r4 = 4 * r
-    per_near = 4 * 4 + 1 + 2 * 32 + 4 * r4
+    per_near = 4 * 4 + 2 * 4 + 1 + 2 * 32 + 4 * r4
     per_touch = 1 + 2 * (2 * r4 + r) + 2 * 3 * 32
     return per_near * nnear + per_touch * ntouch
 
@@ -422,11 +423,11 @@ def algorithmic_clump_bytes(N, K, nnear, precision):
     torque written (6 x 32 B) plus its member offset 4 B; per member its index
     4 B, FP64 position read and written 2 x 32 B, body offset and mass 32 B,
     displacement since the rebuild read and written 2 x 32 B, contact
-    kinematics written 3 x 32 B, near-row offsets 16 B and boundary bits 2 B;
+    kinematics (arm, mass) written 32 B, near-row offsets 16 B and boundary bits 2 B;
     per near pair its two contact-slot pairs read (4 Real4)."""
     r4 = 16 if precision == "mixed" else 32
     per_clump = 5 * 32 + 6 * 32 + 4
-    per_sub = 4 + 2 * 32 + 32 + 2 * 32 + 3 * 32 + 16 + 2
+    per_sub = 4 + 2 * 32 + 32 + 2 * 32 + 32 + 16 + 2
     return per_clump * K + per_sub * N + 4 * r4 * nnear
 
 

@@ -647,7 +647,7 @@ class EngineT final : public EngineBase {
         blk(h_.part_fix, N * sizeof(int));
         blk(h_.level, N * sizeof(int));
         blk(h_.key, N * sizeof(int));
-        blk(h_.kin, 3 * N * sizeof(double4));
+        blk(h_.kin, N * sizeof(double4));
         blk(h_.bhist, (size_t)NB_SLOTS * 3 * N * sizeof(R4<R>));
         blk(h_.bbits, N * sizeof(uint16_t));
         blk(h_.fbnd, 2 * N * sizeof(R4<R>));
@@ -997,10 +997,10 @@ class EngineT final : public EngineBase {
             h_.part_fix = m.take<int>(N); h_.part_fix2 = m.take<int>(N);
             h_.level = m.take<int>(N); h_.level2 = m.take<int>(N);
             h_.key = m.take<int>(N); h_.key2 = m.take<int>(N);
-            // contact kinematics: velocity and mass, angular velocity and lever
-            // arm, all FP64, three double4 per subsphere
-            h_.kin = m.take<char>(3 * N * sizeof(double4));
-            h_.kin2 = m.take<char>(3 * N * sizeof(double4));
+            // contact kinematics: world lever arm and mass, one FP64 double4 per
+            // subsphere (the velocities are read from the clump's records)
+            h_.kin = m.take<char>(N * sizeof(double4));
+            h_.kin2 = m.take<char>(N * sizeof(double4));
             h_.bhist = m.take<R4<R>>((size_t)NB_SLOTS * 3 * N); h_.bhist2 = m.take<R4<R>>((size_t)NB_SLOTS * 3 * N);
             h_.bbits = m.take<uint16_t>(N); h_.bbits2 = m.take<uint16_t>(N);
             h_.fsum = m.take<R4<R>>(2 * N);

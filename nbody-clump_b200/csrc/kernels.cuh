@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             s_cl[warp][12][lane] = q.w;
             __syncwarp();
             // ---- poses of the members, 32 at a time
-            double4* __restrict__ kv = (double4*)d.kin;   // per member: velocity + mass, angular velocity, arm
+            double4* __restrict__ kv = (double4*)d.kin;   // per member: world arm, mass
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
@@ -403,9 +403,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     const V3<double> wk = v3(s_cl[warp][6][kk], s_cl[warp][7][kk], s_cl[warp][8][kk]);
                     cum[i] = make_double4(cn.x, cn.y, cn.z, 0.0);
                     posw[i] = make_double4(p.x, p.y, p.z, o.w);
-                    kv[3 * (size_t)i] = make_double4(vk.x, vk.y, vk.z, lo[j].w);
-                    kv[3 * (size_t)i + 1] = make_double4(wk.x, wk.y, wk.z, 0.0);
-                    kv[3 * (size_t)i + 2] = make_double4(arm.x, arm.y, arm.z, 0.0);
+                    kv[i] = make_double4(arm.x, arm.y, arm.z, lo[j].w);
                     const int sk = s_sc[warp][kk];
                     if (len_floor(cn) > d.par[sk].thresh) {
                         SceneDyn& y = d.dyn[sk];
@@ -903,7 +901,7 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
         d.part_fix2[i] = d.part_fix[o];
         d.level2[i] = d.level[o];
         d.bbits2[i] = d.bbits[o];
-        for (int c = 0; c < 3; c++) ((double4*)d.kin2)[3 * (size_t)i + c] = ((const double4*)d.kin)[3 * (size_t)o + c];
+        ((double4*)d.kin2)[i] = ((const double4*)d.kin)[o];
         const R4<R>* b1 = (const R4<R>*)d.bhist;
         R4<R>* b2 = (R4<R>*)d.bhist2;
         const uint16_t bits = d.bbits[o];
@@ -1463,7 +1461,7 @@ __global__ void k_writeback(Dev* __restrict__ dp) {
         d.part_fix[i] = d.part_fix2[i];
         d.level[i] = d.level2[i];
         d.key[i] = d.key2[i];
-        for (int c = 0; c < 3; c++) ((double4*)d.kin)[3 * (size_t)i + c] = ((const double4*)d.kin2)[3 * (size_t)i + c];
+        ((double4*)d.kin)[i] = ((const double4*)d.kin2)[i];
         const uint16_t bits = d.bbits2[i];
         d.bbits[i] = bits;
         const R4<R>* b2 = (const R4<R>*)d.bhist2;
@@ -1838,9 +1836,11 @@ __device__ __forceinline__ void hm_law(const Law<R>& L, V3<double> nd, double Dn
 // The contact kinematics of a subsphere in FP64 (its clump's velocity and
 // angular velocity, its world arm and mass): a bed moving as a whole gives
 // touching subspheres nearly equal contact-point velocities, so their
-// difference is formed in FP64 before the law rounds anything.  Buffer
-// layout: three adjacent double4 per subsphere (velocity + mass, angular
-// velocity, arm).
+// difference is formed in FP64 before the law rounds anything.  The
+// subsphere's own record is one double4 (world arm, mass) written by the
+// pose pass; the velocities are read from its clump's records (the values the
+// clump pass wrote with the same half-kick), so a clump's velocity is stored
+// once rather than once per member.
 template <typename R> struct Body {
     double4 p;              // position, radius
     V3<double> v, w, arm;   // clump velocity, clump angular velocity, world arm
@@ -1848,20 +1848,13 @@ template <typename R> struct Body {
 };
 
 template <typename R>
-__device__ __forceinline__ void load_kin(const void* __restrict__ kin, size_t N, int i, Body<R>& b) {
-    const double4* k = (const double4*)kin + 3 * (size_t)i;
-    const double4 a = k[0], w = k[1], r = k[2];
-    b.v = v3(a.x, a.y, a.z);
-    b.m = a.w;
-    b.w = v3(w.x, w.y, w.z);
+__device__ __forceinline__ void load_kin(const Dev& d, int i, int c, Body<R>& b) {
+    const double4 r = ((const double4*)d.kin)[i], v = d.cvel[c], w = d.cw[c];
     b.arm = v3(r.x, r.y, r.z);
+    b.m = r.w;
+    b.v = v3(v.x, v.y, v.z);
+    b.w = v3(w.x, w.y, w.z);
 }
-
-template <typename R>
-__device__ __forceinline__ void load_kin(const Dev& d, int i, Body<R>& b) {
-    load_kin<R>(d.kin, (size_t)d.N, i, b);
-}
-
 
 // The pair law of ContactForce_clump_cuk (src/dem_force_clump.cu:3-163) with
 // a in the role of particleI, evaluated once for both bodies of a touching
@@ -2118,7 +2111,7 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         if (!on) continue;
         if (!have_kin) {
             me.p = pp;
-            load_kin<R>(d, i, me);
+            load_kin<R>(d, i, d.clump_id[i], me);
             have_kin = true;
         }
         if (is_intr) Mij = P.intr_motion == 1 ? me.m * P.intr_mass / (me.m + P.intr_mass) : me.m;
@@ -2194,16 +2187,16 @@ __device__ __forceinline__ bool overlaps(double4 a, double4 b) {
 }
 
 // The law of one touching near pair (front entry ef of scene s, pair slot p,
-// owner i, partner jr, near back entry eb; a.p and b.p loaded): kinematics
-// and spring history in, new history, touch flag and the four contact slots
-// out (and the export record).
+// owner i of clump ci, partner jr of clump cj, near back entry eb; a.p and b.p
+// loaded): kinematics and spring history in, new history, touch flag and the
+// four contact slots out (and the export record).
 template <typename R, bool EXPORT>
-__device__ __forceinline__ void pair_law(const Dev& d, int s, int ef, int p, int i, int jr, int eb, Body<R>& a,
-                                         Body<R>& b) {
+__device__ __forceinline__ void pair_law(const Dev& d, int s, int ef, int p, int i, int jr, int ci, int cj, int eb,
+                                         Body<R>& a, Body<R>& b) {
     const int hg = *d.hgen;
     const size_t cap = (size_t)d.cap;
-    load_kin<R>(d.kin, (size_t)d.N, i, a);
-    load_kin<R>(d.kin, (size_t)d.N, jr, b);
+    load_kin<R>(d, i, ci, a);
+    load_kin<R>(d, jr, cj, b);
     V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
     if (d.touch[hg & 1][p]) hist_read<R>((const R4<R>*)d.H[hg & 1], cap, p, hs, ht, hr);
     const ScenePar& P = d.par[s];
@@ -2259,6 +2252,7 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
     const int np = npre[S];
     const int4* __restrict__ nfr = d.nfr;
     const double4* __restrict__ posr = d.posr;
+    const int* __restrict__ cid = d.clump_id;
     uint8_t* __restrict__ to = d.touch[(hg + 1) & 1];
     R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
     R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
@@ -2273,9 +2267,12 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
         const int p = rec.x, jr = rec.y, i = rec.z, eb = rec.w;
         Body<R> a, b;
         bool on = jr >= 0;   // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)
+        int ci = 0, cj = 0;
         if (on) {
             a.p = posr[i];
             b.p = posr[jr];
+            ci = cid[i];      // with the positions, for the kinematics of a touching pair
+            cj = cid[jr];
             on = overlaps(a.p, b.p);
         }
         if (!on) {
@@ -2286,7 +2283,7 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
             bs[2 * (size_t)eb + 1] = zero;
             continue;
         }
-        pair_law<R, EXPORT>(d, s, ef, p, i, jr, eb, a, b);
+        pair_law<R, EXPORT>(d, s, ef, p, i, jr, ci, cj, eb, a, b);
     }
 }
 

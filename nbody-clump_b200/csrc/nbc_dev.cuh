@@ -121,8 +121,8 @@ struct Dev {
     int* part_fix;    int* part_fix2;    // original index (ParticleID)
     int* level;       int* level2;       // hgrid level (0 = coarsest)
     int* key;         int* key2;         // global cell key at the last rebuild (sorted)
-    void* kin;        void* kin2;        // double4 [N][3]: clump velocity + mass, clump angular
-                                         // velocity, world arm (see Body in kernels.cuh)
+    void* kin;        void* kin2;        // double4 [N]: world arm, mass (the velocities are the
+                                         // clump's; see Body in kernels.cuh)
     void* bhist;      void* bhist2;      // Real4 [NB_SLOTS][N][3] boundary histories (Dv, Dt, Dr adjacent)
     uint16_t* bbits;  uint16_t* bbits2;  // [N] boundary slots in contact at the last step
     void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder),
