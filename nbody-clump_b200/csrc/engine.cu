@@ -667,8 +667,7 @@ class EngineT final : public EngineBase {
         // rows and work-item prefixes
         blk(h_.L[0].row, (N + S_) * sizeof(int));
         blk(h_.L[0].brow, (N + S_) * sizeof(int));
-        blk(h_.nrow, (N + S_) * sizeof(int));
-        blk(h_.nbrow, (N + S_) * sizeof(int));
+        blk(h_.nrb, (N + S_) * sizeof(int2));
         blk(h_.nprefix, (S_ + 1) * sizeof(int));
         blk(h_.bprefix, (S_ + 1) * sizeof(int));
         blk(h_.ring, (size_t)S_ * ring_len_ * 6 * sizeof(double));
@@ -1030,8 +1029,7 @@ class EngineT final : public EngineBase {
             h_.cstart = m.take<int>(cells + 1);
             h_.scr = m.take<int>((size_t)N * 2 * SCR_CAP);
             h_.cnt_f = m.take<int>(N + 1);
-            h_.nrow = m.take<int>(N + S_);
-            h_.nbrow = m.take<int>(N + S_);
+            h_.nrb = m.take<int2>(N + S_);
             h_.nprefix = m.take<int>(S_ + 1);
             h_.bidx = m.take<int>(N);
             h_.bprefix = m.take<int>(S_ + 1);

@@ -184,8 +184,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const R4<R>* __restrict__ fsl = (const R4<R>*)d.nfs;
             const R4<R>* __restrict__ bsl = (const R4<R>*)d.nbs;
             const R4<R>* __restrict__ fbd = (const R4<R>*)d.fbnd;
-            const int* __restrict__ nrow = d.nrow;
-            const int* __restrict__ nbrow = d.nbrow;
+            const int2* __restrict__ nrb = d.nrb;
             const uint16_t* __restrict__ bbits = d.bbits;
             const size_t N = (size_t)d.N, cap = (size_t)d.cap;
             SlotRec<R>* stage = (SlotRec<R>*)cl_dsm + (size_t)warp * CL_STAGE * CL_CHUNK;
@@ -207,10 +206,11 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     const int i = idx[j] < 0 ? 0 : idx[j];
                     const int ro = i + s_sc[warp][own[j]];
                     ps[j] = posr[i];
-                    r0[j] = nrow[ro];
-                    r1[j] = nrow[ro + 1];
-                    q0[j] = nbrow[ro];
-                    q1[j] = nbrow[ro + 1];
+                    const int2 ra = nrb[ro], rb = nrb[ro + 1];
+                    r0[j] = ra.x;
+                    r1[j] = rb.x;
+                    q0[j] = ra.y;
+                    q1[j] = rb.y;
                     bb[j] = bbits[i];
                 }
                 // stage every contact record of the lane's members (front
@@ -1572,11 +1572,9 @@ __global__ void __launch_bounds__(SEARCH_THREADS) k_near(const Dev* __restrict__
             rf = base + d.cnt_f[t] - d.cnt_f[t0];
             rb = base + d.cnt_b[t] - d.cnt_b[t0];
             if (lane == 0) {
-                d.nrow[i + s] = rf;
-                d.nbrow[i + s] = rb;
+                d.nrb[i + s] = make_int2(rf, rb);
                 if (i == d.par[s].sub_off + d.par[s].nsub - 1) {
-                    d.nrow[i + s + 1] = base + d.cnt_f[t + 1] - d.cnt_f[t0];
-                    d.nbrow[i + s + 1] = base + d.cnt_b[t + 1] - d.cnt_b[t0];
+                    d.nrb[i + s + 1] = make_int2(base + d.cnt_f[t + 1] - d.cnt_f[t0], base + d.cnt_b[t + 1] - d.cnt_b[t0]);
                 }
             }
         }
@@ -1674,7 +1672,7 @@ static __global__ void __launch_bounds__(SC_THREADS) k_near_finish(const Dev* __
     NBC_GRID_STRIDE(t, T) {
         const PlanItem it = plan_item(d, ns, t);
         const int i = it.i, s = it.s;
-        for (int e = d.nrow[i + s]; e < d.nrow[i + s + 1]; e++) d.nfr[e].w = d.nbpos[d.nfr[e].x];
+        for (int e = d.nrb[i + s].x; e < d.nrb[i + s + 1].x; e++) d.nfr[e].w = d.nbpos[d.nfr[e].x];
     }
 }
 
@@ -1742,8 +1740,8 @@ static __global__ void k_shift_rows(const Dev* __restrict__ dp, const int4* __re
         const int delta = map[s].y - map[s].x;
         Lc.row[r] += delta;
         Lc.brow[r] += delta;
-        d.nrow[r] += delta;
-        d.nbrow[r] += delta;
+        d.nrb[r].x += delta;
+        d.nrb[r].y += delta;
     }
 }
 
@@ -2295,8 +2293,8 @@ template <typename R>
 __device__ __forceinline__ void contact_sum(const Dev& d, int i, int s, V3<R>& F, V3<R>& T, V3<R>* pairF = nullptr,
                                             V3<R>* pairT = nullptr) {
     const size_t N = (size_t)d.N;
-    slot_sum<R>((const R4<R>*)d.nfs, (const R4<R>*)d.nbs, (size_t)d.cap, d.nrow[i + s], d.nrow[i + s + 1],
-                d.nbrow[i + s], d.nbrow[i + s + 1], F, T);
+    const int2 ra = d.nrb[i + s], rb = d.nrb[i + s + 1];
+    slot_sum<R>((const R4<R>*)d.nfs, (const R4<R>*)d.nbs, (size_t)d.cap, ra.x, rb.x, ra.y, rb.y, F, T);
     if (pairF) { *pairF = F; *pairT = T; }
     if (d.bbits[i]) {
         const R4<R>* fb = (const R4<R>*)d.fbnd;

@@ -183,8 +183,7 @@ struct Dev {
     // near rows (the entries that can touch before the next rebuild)
     // (kept in each scene's pair region like the list: rows [N+S] with
     // absolute slots, one row array per scene with its end entry)
-    int* nrow;        // [N+S] near front offsets
-    int* nbrow;       // [N+S] near back offsets
+    int2* nrb;        // [N+S] near row offsets (front, back), one record per subsphere
     int4* nfr;        // [cap] near front entries: pair slot, partner, owner, near back entry
     int* nbq;         // [cap] near back entries: pair slot
     int* nprefix;     // [S+1] prefix over the scenes of their near pairs (the contact pass's work items)
