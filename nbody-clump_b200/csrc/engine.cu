@@ -773,10 +773,10 @@ class EngineT final : public EngineBase {
     }
     // kernels one rebuild launches (launch_rebuild)
     // kernels of one rebuild in a graph (the eager path adds a k_check_cap):
-    // plan, hash, 3 per radix pass, cellrange, cellstart, reorder, search,
+    // plan, hash, 3 per radix pass, reorder with the cell table, search,
     // scan, check, compact, (hgrid: xsort), backref, carry, write-back, 2
     // near-row passes and their scan, the finishing pass
-    int rebuild_launches() const { return 15 + 3 * passes_ + (hgrid_ ? 1 : 0); }
+    int rebuild_launches() const { return 13 + 3 * passes_ + (hgrid_ ? 1 : 0); }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -1365,12 +1365,12 @@ class EngineT final : public EngineBase {
         for (int p = 0; p < passes_; p++) {
             k_rs_hist<<<gR, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, pl + PL_T);
             scan(h_.hist, nullptr, nullptr, 256 * rs_blocks_, pl + PL_HIST);
-            k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T);
+            // the last pass writes the permutation, its inverse and the sorted keys
+            k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T,
+                                                         p == passes_ - 1 ? d_ : nullptr);
             std::swap(ki, ko);
             std::swap(vi, vo);
         }
-        k_cellrange<<<gN, B, 0, stream_>>>(d_, ki, vi);
-        k_cellstart<<<std::min(cdiv(h_.cells + S_, 256), 148 * 16), 256, 0, stream_>>>(d_);
         k_reorder<R><<<gN, B, 0, stream_>>>(d_);
         if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);

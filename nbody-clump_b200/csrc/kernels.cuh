@@ -810,10 +810,15 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __rest
     }
 }
 
+// The scatter of one pass.  With fin (the last pass of a rebuild's sort),
+// the sorted order goes straight into the engine's tables instead of the
+// output arrays: the permutation, its inverse and the sorted keys (key2) at
+// the subsphere slots of the rebuilt scenes (the cell table is built from
+// key2; FindBegEndInCell_cuk, src/dem_grid.cu:105-153).
 static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
                                                            int* __restrict__ kout, int* __restrict__ vout, int n,
                                                            int shift, const int* __restrict__ hist,
-                                                           const int* __restrict__ dn) {
+                                                           const int* __restrict__ dn, const Dev* __restrict__ fin = nullptr) {
     __shared__ int base[256];
     __shared__ int wcnt[RS_THREADS / 32][257];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -835,8 +840,18 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __r
             if (valid) {
                 int off = base[dig] + rank;
                 for (int w = 0; w < warp; w++) off += wcnt[w][dig];
-                kout[off] = k;
-                vout[off] = vin[idx];
+                if (fin) {
+                    const Dev& d = *fin;
+                    const int ks = plan_find(d.psub, d.plan[PL_NS], off);
+                    const int i = d.par[d.pscene[ks]].sub_off + (off - d.psub[ks]);
+                    const int o = vin[idx];
+                    d.inv[o] = i;
+                    d.perm[i] = o;
+                    d.key2[i] = k;
+                } else {
+                    kout[off] = k;
+                    vout[off] = vin[idx];
+                }
             }
             __syncthreads();
             int add = 0;
@@ -847,44 +862,36 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __r
     }
 }
 
-// --- cell ranges, reorder ------------------------------------------------
-static __global__ void k_fill_i(int* __restrict__ a, int n, int v) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
-}
-// a[0, *dn) = v
-static __global__ void k_fill_n(int* __restrict__ a, const int* __restrict__ dn, int v) {
-    const int n = *dn;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = v;
-}
-
-// The permutation of the sort, its inverse and the sorted keys (into key2),
-// at the subsphere slots of the rebuilt scenes.  The cell table is built
-// from key2 by k_cellstart (FindBegEndInCell_cuk, src/dem_grid.cu:105-153, as
-// one start offset per cell: cell c holds the sorted slots
-// [cstart[c], cstart[c + 1])).
-static __global__ void k_cellrange(const Dev* __restrict__ dp, const int* __restrict__ skey, const int* __restrict__ perm) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int T = d.plan[PL_T], ns = d.plan[PL_NS];
-    NBC_GRID_STRIDE(t, T) {
-        const int k = plan_find(d.psub, ns, t);
-        const int i = d.par[d.pscene[k]].sub_off + (t - d.psub[k]);
-        const int o = perm[t];
-        d.inv[o] = i;
-        d.perm[i] = o;
-        d.key2[i] = skey[t];
-    }
-}
-
+// --- reorder and cell table ---------------------------------------------
 // SortArray_*_cuk (src/dem_grid.cu:336-437) for every persistent per-subsphere
 // array at once, into the alternate buffers (written back by k_writeback).
 // The displacement accumulator restarts at zero (src/dem_simulation_clump.cu:172).
+// The same launch builds the cell table: cstart[c] = first sorted slot whose
+// cell key is >= c, for the cells of the rebuilt scenes and the entry after
+// each one's last cell (the next scene's first slot, which every writer of
+// that entry agrees on).
 template <typename R>
 __global__ void k_reorder(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
     const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const size_t N = (size_t)d.N;
+    {
+        const int TC = d.plan[PL_TC];
+        const int* __restrict__ key = d.key2;
+        NBC_GRID_STRIDE(u, TC) {
+            const int k = plan_find(d.pcell, ns, u);
+            const ScenePar& P = d.par[d.pscene[k]];
+            const int c = P.cell_off + (u - d.pcell[k]);
+            int lo = P.sub_off, len = P.nsub;
+            while (len > 0) {
+                const int h = len >> 1;
+                if (key[lo + h] < c) { lo += h + 1; len -= h + 1; }
+                else len = h;
+            }
+            d.cstart[c] = lo;
+        }
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
     NBC_GRID_STRIDE(t, T) {
         // the search's counters start at zero
@@ -1118,28 +1125,6 @@ __device__ __forceinline__ void group_search(const Dev& d, const ScenePar& P, co
     }
     nf_out = nf;
     nb_out = nb;
-}
-
-// cstart[c] = first sorted slot whose cell key is >= c, for the cells of the
-// rebuilt scenes and the entry after each one's last cell (the next scene's
-// first slot, which every writer of that entry agrees on)
-static __global__ void k_cellstart(const Dev* __restrict__ dp) {
-    const Dev& d = *dp;
-    if (*d.halt) return;
-    const int TC = d.plan[PL_TC], ns = d.plan[PL_NS];
-    const int* __restrict__ key = d.key2;
-    NBC_GRID_STRIDE(u, TC) {
-        const int k = plan_find(d.pcell, ns, u);
-        const ScenePar& P = d.par[d.pscene[k]];
-        const int c = P.cell_off + (u - d.pcell[k]);
-        int lo = P.sub_off, len = P.nsub;
-        while (len > 0) {
-            const int h = len >> 1;
-            if (key[lo + h] < c) { lo += h + 1; len -= h + 1; }
-            else len = h;
-        }
-        d.cstart[c] = lo;
-    }
 }
 
 // the subsphere of element t of the rebuilt concatenation and its scene
