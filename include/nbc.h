@@ -284,6 +284,18 @@ nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n_scenes, nbc_o
 #define NBC_MAX_LEVELS 6
 int nbc_choose_levels(const double* radius, int n, int max_levels, int* level, double* level_cell);
 
+/* Mass properties of clump templates (replaces the Monte Carlo integration of
+ * the reference's template builder, make_clump_template_lambda.m:172-209, for
+ * many clumps at once): for clump k, members clump_start[k] ..
+ * clump_start[k+1]-1 with centres[3 m] (clump frame) and radii[m], the union
+ * of the spheres (overlap counted once) integrated over its bounding box
+ * with `samples` points of a deterministic low-discrepancy sequence.
+ * out[10 k ..]: volume, centroid xyz, and the second central moments per
+ * unit volume xx yy zz xy xz yz (inertia = density * volume * (trace * I -
+ * moments)).  Host arrays; runs on `device` and returns when done. */
+nbc_status nbc_union_mass(const double* centres, const double* radii, const int* clump_start, int nclumps,
+                          int samples, double* out, int device);
+
 /* --- allocation-free cell sort ------------------------------------------
  * No counterpart in the reference (its sort allocates CUB scratch with
  * cudaMalloc on first use, src/dem_grid.cu:278-305).  For callers that

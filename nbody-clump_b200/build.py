@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libnbc.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "capi.cpp", "io.cpp", "noalloc.cu", "tune.cpp", "serve.cpp"]
+SOURCES = ["engine.cu", "capi.cpp", "io.cpp", "noalloc.cu", "tune.cpp", "serve.cpp", "generate.cu"]
 HEADERS = ["kernels.cuh", "nbc_dev.cuh", "nbc_math.cuh", "engine.h", "io.h", "handle.h", "dem_clump_main.h",
            "dem_clump_main.cpp", "main.cpp"]
 

@@ -77,6 +77,26 @@ def choose_levels(radius, max_levels=6):
     return lv, cell[:L].copy()
 
 
+def union_mass(centres, radii, clump_start, samples=1 << 16, device=0):
+    """Union volume, centroid and second central moments of clump templates
+    (nbc_union_mass): centres [M][3] and radii [M] of all members, clump k
+    owning members clump_start[k] .. clump_start[k+1]-1.  Returns
+    (volume[K], centroid[K][3], moments[K][3][3])."""
+    c = np.ascontiguousarray(centres, dtype=np.float64).reshape(-1, 3)
+    r = np.ascontiguousarray(radii, dtype=np.float64)
+    st = np.ascontiguousarray(clump_start, dtype=np.int32)
+    K = len(st) - 1
+    out = np.zeros((max(K, 1), 10))
+    _check(lib().nbc_union_mass(_p(c), _p(r), _p(st, P_I), K, int(samples), _p(out), int(device)))
+    out = out[:K]
+    m = np.empty((K, 3, 3))
+    m[:, 0, 0], m[:, 1, 1], m[:, 2, 2] = out[:, 4], out[:, 5], out[:, 6]
+    m[:, 0, 1] = m[:, 1, 0] = out[:, 7]
+    m[:, 0, 2] = m[:, 2, 0] = out[:, 8]
+    m[:, 1, 2] = m[:, 2, 1] = out[:, 9]
+    return out[:, 0].copy(), out[:, 1:4].copy(), m
+
+
 def with_levels(scene: dict, max_levels=6) -> dict:
     """The scene with a hierarchical grid chosen by nbc_choose_levels (or
     unchanged when one level is best)."""
@@ -100,7 +120,7 @@ EXPORTED = [
     "nbc_get_intruder",
     "nbc_get_intruder_diag", "nbc_get_intruder_history", "nbc_timing_enable", "nbc_timing_read",
     "nbc_timing_phases",
-    "nbc_engine_info", "nbc_set_scene_steps", "nbc_cell_sort_noalloc", "nbc_choose_levels",
+    "nbc_engine_info", "nbc_set_scene_steps", "nbc_cell_sort_noalloc", "nbc_choose_levels", "nbc_union_mass",
     "nbc_checkpoint_write", "nbc_checkpoint_read", "nbc_autotune", "nbc_launch_info",
     "nbc_batch_create", "nbc_batch_step", "nbc_batch_engine", "nbc_batch_destroy",
     "nbc_server_create", "nbc_server_submit", "nbc_server_advance", "nbc_server_result",

@@ -409,7 +409,8 @@ def _poly_members(rng, n_clumps, rmin, rmax, max_members, rho):
     """Clumps of 1..max_members subspheres (uniform): a clump size r_c
     log-uniform in [rmin, rmax], member radii r_c x U(0.8, 1), centres at
     0.6 r_c in random directions; mass 0.8 x the spheres' and inertia
-    0.4 M r_c^2 (a filled-clump approximation)."""
+    0.4 M r_c^2 (a filled-clump approximation: the small test scenes use it,
+    it needs no GPU)."""
     m = rng.integers(1, max_members + 1, n_clumps)
     rc = np.exp(rng.uniform(np.log(rmin), np.log(rmax), n_clumps))
     locals_, radii, masses, props, ext = [], [], [], [], np.zeros(n_clumps)
@@ -430,6 +431,54 @@ def _poly_members(rng, n_clumps, rmin, rmax, max_members, rho):
         props.append([I, I, I, M])
         ext[k] = 2.0 * (np.linalg.norm(cen, axis=1).max() + rr.max())
     return locals_, radii, masses, np.array(props), ext
+
+
+
+def _poly_templates(rng, n_clumps, rmin, rmax, max_members, rho, lam=0.5, samples=1 << 16):
+    """The cfg2 / cfg4 clump templates: clumps of 1..max_members subspheres
+    (uniform), every subsphere's radius log-uniform in [rmin, rmax]; member n
+    attached to a random earlier member j in a uniformly random direction at
+    centre distance |r_n - r_j| + 2 lam min(r_n, r_j): the reference's
+    template builder (make_clump_template_lambda.m) places equal spheres at
+    2 r lambda, and for unequal ones this keeps the smaller sphere sticking
+    out of the larger by the same fraction of its diameter.  Mass, centre of mass
+    and inertia of each union (overlap counted once) come from
+    nbc.union_mass (the builder's Monte Carlo integration, on the GPU for all
+    clumps at once); members are re-expressed in the clump's principal frame
+    and the clump mass is split equally among them, as the builder does."""
+    import nbc
+    m = rng.integers(1, max_members + 1, n_clumps)
+    start = np.concatenate([[0], np.cumsum(m)]).astype(np.int32)
+    M = int(start[-1])
+    r_all = np.exp(rng.uniform(np.log(rmin), np.log(rmax), M))
+    d = rng.normal(size=(M, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    u = rng.random(M)
+    cen = np.zeros((M, 3))
+    for k in range(n_clumps):
+        b = start[k]
+        for n in range(1, m[k]):
+            j = b + int(u[b + n] * n)
+            ra, rb = r_all[b + n], r_all[j]
+            cen[b + n] = cen[j] + (abs(ra - rb) + 2.0 * lam * min(ra, rb)) * d[b + n]
+    vol, com, mom = nbc.union_mass(cen, r_all, start, samples=samples)
+    mass = rho * vol
+    inertia = (rho * vol)[:, None, None] * (np.trace(mom, axis1=1, axis2=2)[:, None, None] * np.eye(3) - mom)
+    w, V = np.linalg.eigh(inertia)
+    flip = np.linalg.det(V) < 0
+    V[flip, :, 0] = -V[flip, :, 0]
+    owner = np.repeat(np.arange(n_clumps), m)
+    local = np.einsum("mi,mij->mj", cen - com[owner], V[owner])
+    props = np.column_stack([w[:, 0], w[:, 1], w[:, 2], mass])
+    locals_, radii, masses = [], [], []
+    ext = np.zeros(n_clumps)
+    for k in range(n_clumps):
+        sl = slice(start[k], start[k + 1])
+        locals_.append(local[sl])
+        radii.append(r_all[sl])
+        masses.append(np.full(m[k], mass[k] / m[k]))
+        ext[k] = 2.0 * (np.linalg.norm(local[sl], axis=1) + r_all[sl]).max()
+    return locals_, radii, masses, props, ext
 
 
 def layered_packing_box(rng, diam, hx, hy, z0, jitter=0.02):
@@ -462,7 +511,7 @@ def make_poly_bed(n_sub, seed, half_xy, rmin=0.5e-3, rmax=5e-3, max_members=8, m
     rng = np.random.default_rng(seed)
     rho = MATERIAL["rho"]
     k = max(1, int(round(n_sub / (0.5 * (1 + max_members)))))
-    locals_, radii, masses, props, ext = _poly_members(rng, k, rmin, rmax, max_members, rho)
+    locals_, radii, masses, props, ext = _poly_templates(rng, k, rmin, rmax, max_members, rho)
     pts = layered_packing_box(rng, ext, half_xy, half_xy, 0.0)
     top = float(pts[:, 2].max() + ext.max())
     H = 0.75 * top
