@@ -2226,8 +2226,6 @@ constexpr int PR_THREADS = 256;
 constexpr int CONTACT_LAUNCHES = 2;   // k_pairs and k_boundary
 template <typename R, bool EXPORT>
 __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* __restrict__ dp) {
-    // each warp's queue of touching pairs (front entry, scene) awaiting the law
-    __shared__ int2 s_q[PR_THREADS / 32][64];
     const Dev& d = *dp;
     if (*d.halt) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) *d.post_pending = 1;
@@ -2242,56 +2240,34 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
     R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
     R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
     const R4<R> zero = pack<R>(v3<R>(0, 0, 0), R(0));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    int2* __restrict__ q = s_q[warp];
-    // the law of a queued touching pair (its record and positions are reread:
-    // they were just loaded, so they come from L1)
-    auto law = [&](int2 e) {
-        const int4 rec = nfr[e.x];
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
+        // work item w: near front entry w - nprefix[s] of scene s
+        const int s = S == 1 ? 0 : plan_find(npre, S, w);
+        const SceneDyn& ys = d.dyn[s];
+        if (d.has_stops && ys.frozen) continue;
+        const int ef = ys.pair_off + (w - npre[s]);
+        const int4 rec = nfr[ef];   // pair slot, partner, owner, near back entry: one load
+        const int p = rec.x, jr = rec.y, i = rec.z, eb = rec.w;
         Body<R> a, b;
-        a.p = posr[rec.z];
-        b.p = posr[rec.y];
-        pair_law<R, EXPORT>(d, e.y, e.x, rec.x, rec.z, rec.y, cid[rec.z], cid[rec.y], rec.w, a, b);
-    };
-    int qn = 0;   // queued pairs (warp-uniform, below 32 between rounds)
-    // warp-strided chunks of 32 work items: the overlap test for every near
-    // pair, then the law 32 touching pairs at a time, so that the law runs on
-    // full warps whatever the mix of touching and separated pairs
-    for (int base = blockIdx.x * blockDim.x + warp * 32; base < np; base += gridDim.x * blockDim.x) {
-        const int w = base + lane;   // work item w: near front entry w - nprefix[s] of scene s
-        bool on = false;
-        int s = 0, ef = 0;
-        if (w < np) {
-            s = S == 1 ? 0 : plan_find(npre, S, w);
-            const SceneDyn& ys = d.dyn[s];
-            if (!(d.has_stops && ys.frozen)) {
-                ef = ys.pair_off + (w - npre[s]);
-                const int4 rec = nfr[ef];   // pair slot, partner, owner, near back entry: one load
-                // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)
-                on = rec.y >= 0 && overlaps(posr[rec.z], posr[rec.y]);
-                if (!on) {
-                    to[rec.x] = 0;
-                    fs[2 * (size_t)ef] = zero;
-                    fs[2 * (size_t)ef + 1] = zero;
-                    bs[2 * (size_t)rec.w] = zero;
-                    bs[2 * (size_t)rec.w + 1] = zero;
-                }
-            }
+        bool on = jr >= 0;   // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)
+        int ci = 0, cj = 0;
+        if (on) {
+            a.p = posr[i];
+            b.p = posr[jr];
+            ci = cid[i];      // with the positions, for the kinematics of a touching pair
+            cj = cid[jr];
+            on = overlaps(a.p, b.p);
         }
-        const unsigned m = __ballot_sync(0xffffffffu, on);
-        if (on) q[qn + __popc(m & lt)] = make_int2(ef, s);
-        qn += __popc(m);
-        __syncwarp();
-        if (qn >= 32) {
-            const int2 e = q[qn - 32 + lane];
-            __syncwarp();   // every lane has its entry before the queue is refilled
-            qn -= 32;
-            law(e);
+        if (!on) {
+            to[p] = 0;
+            fs[2 * (size_t)ef] = zero;
+            fs[2 * (size_t)ef + 1] = zero;
+            bs[2 * (size_t)eb] = zero;
+            bs[2 * (size_t)eb + 1] = zero;
+            continue;
         }
+        pair_law<R, EXPORT>(d, s, ef, p, i, jr, ci, cj, eb, a, b);
     }
-    __syncwarp();
-    if (lane < qn) law(q[lane]);
 }
 
 // The contact force and torque on subsphere i: its contact slots, then the
