@@ -5,9 +5,10 @@
 // overlapping spheres by deterministic Monte Carlo integration over the
 // clump's bounding box, counting overlap once.  nbc_union_mass does that for
 // many clumps at once: one block per clump, the points of a Kronecker
-// low-discrepancy sequence (the "R3" sequence: coordinates frac(0.5 + n a_d),
-// a_d = 1/g^d with g the real root of g^3 = g + 1), so the result is the same
-// on every run and converges faster than random points.  The host turns the
+// low-discrepancy sequence (the three-dimensional R sequence: coordinates
+// frac(0.5 + n a_d), a_d = 1/g^d with g the positive root of g^4 = g + 1, so
+// that 1, a_1, a_2, a_3 are rationally independent), so the result is the
+// same on every run and converges faster than random points.  The host turns the
 // moments into mass, centre of mass and inertia (scenegen.py) and rotates
 // the template into its principal frame.
 #include <cuda_runtime.h>
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(UM_THREADS) k_union_mass(const double* __restr
     __shared__ double4 s_m[UM_MAX_MEMBERS];
     __shared__ double s_box[6];
     __shared__ double sh[UM_THREADS / 32];
-    const double g = 1.32471795724474602596;   // g^3 = g + 1
+    const double g = 1.22074408460575947536;   // g^4 = g + 1
     const double a1 = 1.0 / g, a2 = 1.0 / (g * g), a3 = 1.0 / (g * g * g);
     for (int k = blockIdx.x; k < K; k += gridDim.x) {
         const int m0 = start[k], nm = start[k + 1] - start[k];
