@@ -2240,13 +2240,27 @@ __global__ void __launch_bounds__(PR_THREADS, NBC_PAIR_MINB) k_pairs(const Dev* 
     R4<R>* __restrict__ fs = (R4<R>*)d.nfs;
     R4<R>* __restrict__ bs = (R4<R>*)d.nbs;
     const R4<R> zero = pack<R>(v3<R>(0, 0, 0), R(0));
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
-        // work item w: near front entry w - nprefix[s] of scene s
-        const int s = S == 1 ? 0 : plan_find(npre, S, w);
+    // work item w: near front entry w - nprefix[s] of scene s; its record
+    // (pair slot, partner, owner, near back entry) is loaded one item ahead
+    auto fetch = [&](int w, int4& rec, int& s, int& ef) {
+        if (w >= np) return false;
+        s = S == 1 ? 0 : plan_find(npre, S, w);
         const SceneDyn& ys = d.dyn[s];
-        if (d.has_stops && ys.frozen) continue;
-        const int ef = ys.pair_off + (w - npre[s]);
-        const int4 rec = nfr[ef];   // pair slot, partner, owner, near back entry: one load
+        if (d.has_stops && ys.frozen) return false;
+        ef = ys.pair_off + (w - npre[s]);
+        rec = nfr[ef];
+        return true;
+    };
+    const int stride = gridDim.x * blockDim.x;
+    int4 recn = make_int4(0, 0, 0, 0);
+    int sn = 0, efn = 0;
+    bool liven = fetch(blockIdx.x * blockDim.x + threadIdx.x, recn, sn, efn);
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += stride) {
+        const int4 rec = recn;
+        const int s = sn, ef = efn;
+        const bool live = liven;
+        liven = fetch(w + stride, recn, sn, efn);
+        if (!live) continue;
         const int p = rec.x, jr = rec.y, i = rec.z, eb = rec.w;
         Body<R> a, b;
         bool on = jr >= 0;   // pairs inside one clump have no force (src/dem_force_clump.cu:18-19)

@@ -77,7 +77,7 @@ def choose_levels(radius, max_levels=6):
     return lv, cell[:L].copy()
 
 
-def union_mass(centres, radii, clump_start, samples=1 << 16, device=0):
+def union_mass(centres, radii, clump_start, samples=1 << 18, device=0):
     """Union volume, centroid and second central moments of clump templates
     (nbc_union_mass): centres [M][3] and radii [M] of all members, clump k
     owning members clump_start[k] .. clump_start[k+1]-1.  Returns

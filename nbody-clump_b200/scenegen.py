@@ -434,7 +434,7 @@ def _poly_members(rng, n_clumps, rmin, rmax, max_members, rho):
 
 
 
-def _poly_templates(rng, n_clumps, rmin, rmax, max_members, rho, lam=0.5, samples=1 << 16):
+def _poly_templates(rng, n_clumps, rmin, rmax, max_members, rho, lam=0.5, samples=1 << 18):
     """The cfg2 / cfg4 clump templates: clumps of 1..max_members subspheres
     (uniform), every subsphere's radius log-uniform in [rmin, rmax]; member n
     attached to a random earlier member j in a uniformly random direction at
