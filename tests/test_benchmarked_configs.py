@@ -168,7 +168,12 @@ def test_force_depth_curve_mixed_against_f64():
     import nbc
     st = _poly_bed_settled()
     Ri, v = 8e-3, 0.2
-    sc = sg.with_sphere_intruder(st, Ri, v)
+    # above the highest subsphere within 2 cm of the axis, so that the
+    # intruder meets the bed at once whatever its surface looks like
+    pos = st["sub"]["pos"]
+    near = np.hypot(pos[:, 0], pos[:, 1]) < 0.02
+    top = pos[near][np.argmax(pos[near][:, 2])]
+    sc = sg.with_sphere_intruder(st, Ri, v, xy=(float(top[0]), float(top[1])))
     dt = float(sc["params"]["StepSize"])
     sample = max(1, int(round(0.02 * Ri / (v * dt))))
     max_samples = 200   # 4 R_I of travel at most
