@@ -567,7 +567,7 @@ def serve_requests(args):
         n = np.exp(rng.uniform(np.log(1000), np.log(200_000)))
         bed = bank[int(np.argmin(np.abs(np.log(sizes) - np.log(n))))]
         r_i, v, mu = rng.uniform(5e-3, 20e-3), rng.uniform(0.05, 0.5), rng.uniform(0.2, 0.8)
-        sc = sg.with_sphere_intruder(bed, r_i, v, mu=mu)
+        sc = sg.with_sphere_intruder(bed, r_i, v, mu=mu, surface=98)
         nsteps = int(math.ceil(args.depth_ratio * r_i / (v * sc["params"]["StepSize"])))
         reqs.append((t_arr[k], sc, nsteps))
     return sizes, reqs
@@ -625,7 +625,7 @@ def run_cfg2(args):
     hi[2] = top - 3 * rmax
     phi = bulk_packing_fraction(settled["sub"]["pos"], settled["sub"]["radius"], lo, hi)
     e.close()
-    sc = sg.with_sphere_intruder(settled, 0.02, 0.1)
+    sc = sg.with_sphere_intruder(settled, 0.02, 0.1, surface=98)
     dt = float(sc["params"]["StepSize"])
     total = int(round(0.5 / dt))
     nchunk = 100

@@ -526,16 +526,24 @@ def make_poly_bed(n_sub, seed, half_xy, rmin=0.5e-3, rmax=5e-3, max_members=8, m
                     props, locals_, radii, masses, cube=make_cube((half_xy, half_xy, H), (0, 0, H)))
 
 
-def with_sphere_intruder(scene, radius, speed, mu=None, xy=(0.0, 0.0), gap=0.0, mass=1.0):
+def with_sphere_intruder(scene, radius, speed, mu=None, xy=(0.0, 0.0), gap=0.0, mass=1.0, surface=None):
     """The scene with a sphere intruder of this radius above xy, its lowest
     point `gap` above the highest subsphere under it, driven down at a
-    constant speed (the reference's constant_velocity motion)."""
+    constant speed (the reference's constant_velocity motion).  With
+    surface=q (a percentile) its lowest point rests that far above the q-th
+    percentile of the subsphere tops under it instead: a settled bed keeps a
+    few subspheres thrown up by the impacts of its fall, and the intruder
+    should meet the bed, not them."""
     out = dict(scene)
     out["params"] = dict(scene["params"])
     if mu is not None:
         out["params"]["Frcoe"] = float(mu)
     pos, rad = scene["sub"]["pos"], scene["sub"]["radius"]
-    z = _place_intruder_on_bed(pos, rad, xy, "sphere", radius, radius, -gap)
+    if surface is None:
+        z = _place_intruder_on_bed(pos, rad, xy, "sphere", radius, radius, -gap)
+    else:
+        under = np.hypot(pos[:, 0] - xy[0], pos[:, 1] - xy[1]) < radius + rad.max()
+        z = float(np.percentile(pos[under, 2] + rad[under], surface)) + gap + radius
     I = 0.4 * mass * radius ** 2
     out["intruder"] = make_intruder("sphere", radius, (xy[0], xy[1], z), (0, 0, -float(speed)),
                                     prop=(I, I, I, mass), motion="constant_velocity")

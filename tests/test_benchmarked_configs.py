@@ -168,15 +168,8 @@ def test_force_depth_curve_mixed_against_f64():
     import nbc
     st = _poly_bed_settled()
     Ri, v = 8e-3, 0.2
-    sc = sg.with_sphere_intruder(st, Ri, v)
-    # the settled bed still has a few subspheres thrown up by the impacts of
-    # its fall: rest the intruder on the bed's surface under it (the 98th
-    # percentile of the subsphere tops there), not on those
-    pos, rad = st["sub"]["pos"], st["sub"]["radius"]
-    under = np.hypot(pos[:, 0], pos[:, 1]) < Ri + 5e-3
-    surface = float(np.percentile(pos[under, 2] + rad[under], 98))
-    sc["intruder"] = dict(sc["intruder"])
-    sc["intruder"]["pos"] = np.array([0.0, 0.0, surface + Ri])
+    # on the bed's surface, not on the few subspheres its fall threw up
+    sc = sg.with_sphere_intruder(st, Ri, v, surface=98)
     dt = float(sc["params"]["StepSize"])
     sample = max(1, int(round(0.02 * Ri / (v * dt))))
     max_samples = 200   # 4 R_I of travel at most
