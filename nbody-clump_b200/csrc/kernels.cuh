@@ -109,9 +109,12 @@ constexpr int CL_WARPS = CL_THREADS / 32;
 // average; a lane whose members would overflow the warp's records sums from
 // global memory directly (same order, same result).  Dynamic shared memory.
 constexpr int CL_STAGE = 4;
+// member positions kept from the member sums for the poses (the first
+// CL_POS members of a warp's range; later ones are read again)
+constexpr int CL_POS = 128;
 template <typename R, int J>
 constexpr size_t clump_dyn_smem() {
-    return (size_t)CL_WARPS * CL_STAGE * 32 * J * sizeof(SlotRec<R>);
+    return (size_t)CL_WARPS * CL_STAGE * 32 * J * sizeof(SlotRec<R>) + (size_t)CL_WARPS * CL_POS * sizeof(double4);
 }
 // J: members each lane keeps in flight per batch of loads (a launch shape
 // the autotuner picks; results do not depend on it); a warp stages 32 J
@@ -188,6 +191,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const uint16_t* __restrict__ bbits = d.bbits;
             const size_t N = (size_t)d.N, cap = (size_t)d.cap;
             SlotRec<R>* stage = (SlotRec<R>*)cl_dsm + (size_t)warp * CL_STAGE * CL_CHUNK;
+            double4* spos = (double4*)(cl_dsm + (size_t)CL_WARPS * CL_STAGE * CL_CHUNK * sizeof(SlotRec<R>)) +
+                            (size_t)warp * CL_POS;
             F = v3(0.0, 0.0, 0.0);
             T = F;
             for (int c0 = M0; c0 < M1; c0 += CL_CHUNK) {
@@ -268,6 +273,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                             tr = tr + xyz<R>(fbd[N + idx[j]]);
                         }
                     }
+                    const int mr = c0 + 32 * j + lane - M0;
+                    if (mr < CL_POS) spos[mr] = ps[j];   // for the poses below
                     const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
                                             ps[j].z - s_cl[warp][2][kk]);
                     const V3<double> f = v3((double)fr.x, (double)fr.y, (double)fr.z);
@@ -367,6 +374,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
+            const double4* spos = (const double4*)(cl_dsm + (size_t)CL_WARPS * CL_STAGE * CL_CHUNK * sizeof(SlotRec<R>)) +
+                                  (size_t)warp * CL_POS;
             // J members per lane at a time: all indices, then all member
             // records, in flight together
             constexpr int JP = J;
@@ -382,8 +391,10 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
 #pragma unroll
                 for (int j = 0; j < JP; j++) {
                     const int i = idx[j] < 0 ? 0 : idx[j];
+                    const int mr = c0 + 32 * j + lane - M0;
                     lo[j] = lom[i];
-                    old[j] = posw[i];
+                    // the member sums of this step kept the position
+                    old[j] = post && mr < CL_POS ? spos[mr] : posw[i];
                     cu[j] = cum[i];
                 }
 #pragma unroll
