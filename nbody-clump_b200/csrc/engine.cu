@@ -721,7 +721,7 @@ class EngineT final : public EngineBase {
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     Dev h_{};            // host copy of the device table
     Dev* d_ = nullptr;   // device table
-    int S_ = 0, N_ = 0, K_ = 0, passes_ = 0, rs_blocks_ = 0;
+    int S_ = 0, N_ = 0, K_ = 0;
     bool hgrid_ = false;
     bool first_list_ = true;
     int search_lanes_ = 8;
@@ -773,10 +773,10 @@ class EngineT final : public EngineBase {
     }
     // kernels one rebuild launches (launch_rebuild)
     // kernels of one rebuild in a graph (the eager path adds a k_check_cap):
-    // plan, hash, 3 per radix pass, reorder with the cell table, search,
-    // scan, check, compact, (hgrid: xsort), backref, carry, write-back, 2
-    // near-row passes and their scan, the finishing pass
-    int rebuild_launches() const { return 13 + 3 * passes_ + (hgrid_ ? 1 : 0); }
+    // plan, hash, the cell counts' scan, scatter, per-cell order and table,
+    // reorder, search, scan, check, compact, (hgrid: xsort), backref, carry,
+    // write-back, 2 near-row passes and their scan, the finishing pass
+    int rebuild_launches() const { return 17 + (hgrid_ ? 1 : 0); }
     cudaEvent_t* next_record() {
         if ((size_t)(NMARK * (ev_used_ + 1)) > ev_.size()) {
             for (int k = 0; k < 64 * NMARK; k++) {
@@ -936,11 +936,6 @@ class EngineT final : public EngineBase {
         if ((long long)N_ >= (1LL << 30)) throw ArgError("more than 2^30 subspheres in one engine");
         h_.S = S_; h_.N = N_; h_.K = K_;
         h_.cells = cells;
-        int bits = 1;
-        while ((1LL << bits) < (long long)cells) bits++;
-        h_.sort_bits = bits;
-        passes_ = cdiv(bits, 8);
-        rs_blocks_ = cdiv(N_, RS_TILE);
 
         // host arrays in the input order
         std::vector<double4> posr(N_), lom(N_);
@@ -1023,7 +1018,8 @@ class EngineT final : public EngineBase {
             h_.loop_left = flags + 8;
             h_.scan_fail = flags + 9;
             h_.kA = m.take<int>(N); h_.vA = m.take<int>(N); h_.kB = m.take<int>(N); h_.vB = m.take<int>(N);
-            h_.hist = m.take<int>((size_t)256 * rs_blocks_);
+            h_.ccnt = m.take<int>((size_t)cells + S_ + 1);
+            h_.ccur = m.take<int>((size_t)cells + S_ + 1);
             h_.perm = m.take<int>(N);
             h_.inv = m.take<int>(N);
             h_.cstart = m.take<int>(cells + 1);
@@ -1036,7 +1032,7 @@ class EngineT final : public EngineBase {
             h_.cnt_b = m.take<int>(N + 1);
             h_.sfc = m.take<int>(N);
             h_.xcnt = m.take<int>(N + 1);
-            const long long scan_tiles = std::max(cdiv(N + 1, SC_TILE), cdiv((long long)256 * rs_blocks_, SC_TILE));
+            const long long scan_tiles = std::max(cdiv(N + 1, SC_TILE), cdiv((long long)cells + S_ + 1, SC_TILE));
             h_.scan_tmp = m.take<int>(scan_tiles + 1);
             h_.scan_st = m.take<unsigned long long>(3 * scan_tiles + 3);
             h_.scan_ctl = m.take<int>(2);
@@ -1360,17 +1356,11 @@ class EngineT final : public EngineBase {
         const int* pl = h_.plan;
         k_plan<<<1, SC_THREADS, 0, stream_>>>(d_);
         k_hash<<<gN, B, 0, stream_>>>(d_);
-        int *ki = h_.kA, *vi = h_.vA, *ko = h_.kB, *vo = h_.vB;
-        const int gR = std::min(rs_blocks_, 148 * 8);
-        for (int p = 0; p < passes_; p++) {
-            k_rs_hist<<<gR, RS_THREADS, 0, stream_>>>(ki, N_, 8 * p, h_.hist, pl + PL_T);
-            scan(h_.hist, nullptr, nullptr, 256 * rs_blocks_, pl + PL_HIST);
-            // the last pass writes the permutation, its inverse and the sorted keys
-            k_rs_scatter<<<gR, RS_THREADS, 0, stream_>>>(ki, vi, ko, vo, N_, 8 * p, h_.hist, pl + PL_T,
-                                                         p == passes_ - 1 ? d_ : nullptr);
-            std::swap(ki, ko);
-            std::swap(vi, vo);
-        }
+        // counting sort by cell: the counts' scan, the scatter, each cell's
+        // range in subsphere order with the permutation and the cell table
+        scan(h_.ccnt, nullptr, nullptr, h_.cells + S_ + 1, pl + PL_TC1);
+        k_cscatter<<<gN, B, 0, stream_>>>(d_);
+        k_cellfix<<<std::min(cdiv(h_.cells + S_, 256), 148 * 16), 256, 0, stream_>>>(d_);
         k_reorder<R><<<gN, B, 0, stream_>>>(d_);
         if (sl == 16) k_search<16><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);
         else if (sl == 32) k_search<32><<<gS, SEARCH_THREADS, 0, stream_>>>(d_);

@@ -745,10 +745,10 @@ static __global__ void __launch_bounds__(SC_THREADS) k_plan(const Dev* __restric
         d.plan[PL_T] = nsub;
         d.plan[PL_TC] = ncell;
         d.plan[PL_T1] = nsub + 1;
-        d.plan[PL_HIST] = 256 * ((nsub + RS_TILE - 1) / RS_TILE);
         d.plan[PL_TK] = nclump;
         d.plan[PL_CS] = 0;
         d.plan[PL_CC] = 0;
+        d.plan[PL_TC1] = ncell + 1;
     }
 }
 
@@ -757,7 +757,16 @@ static __global__ void __launch_bounds__(SC_THREADS) k_plan(const Dev* __restric
 // GetParticleCellIndex_cuk (src/dem_grid.cu:155-202); hierarchical variant
 // GetParticleCellIndex_hGrid_cuk (src/dem_hgrid.cu:205-242) with the
 // out-of-box bucket kept inside the scene's cell range.  Element t of the
-// rebuilt concatenation: key kA[t], value vA[t] = its subsphere.
+// rebuilt concatenation: kA[t] = its cell's index u in the rebuilt scenes'
+// cell table (pcell[k] + local cell), vA[t] = its subsphere; ccnt[u] counts
+// the cell's subspheres.
+//
+// The stable sort by cell (the reference sorts with CUB's stable radix
+// sort, src/dem_grid.cu:278-305) is a counting sort: the scan of ccnt gives
+// each cell's first sorted slot, k_cscatter drops every element into its
+// cell's range, and k_cellfix puts each cell's range back in ascending
+// subsphere order -- the order a stable sort keeps -- and writes the
+// permutation, its inverse, the sorted keys and the cell table.
 static __global__ void k_hash(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
@@ -796,7 +805,68 @@ static __global__ void k_hash(const Dev* __restrict__ dp) {
                 local = P.loff[lv] + (cz * P.ldim[lv][1] * P.ldim[lv][0] + cy * P.ldim[lv][0] + cx);
             }
         }
-        d.kA[t] = P.cell_off + local;
+        // the cell's index in the rebuilt scenes' cell table, and its count
+        const int u = d.pcell[k] + local;
+        d.kA[t] = u;
+        atomicAdd(&d.ccnt[u], 1);
+    }
+}
+
+// every element into its cell's range (in any order within the cell)
+static __global__ void k_cscatter(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int T = d.plan[PL_T];
+    NBC_GRID_STRIDE(t, T) {
+        const int u = d.kA[t];
+        d.vB[d.ccnt[u] + atomicAdd(&d.ccur[u], 1)] = d.vA[t];
+    }
+}
+
+// Per cell of the rebuilt scenes: its range of the sorted order in
+// ascending subsphere order (insertion sort; ranges longer than 32 -- the
+// out-of-box bucket of a scene that has lost subspheres -- by Shell sort),
+// then the permutation, its inverse and the sorted keys (key2) at the
+// range's subsphere slots and the cell's start in the cell table (the entry
+// after a scene's last cell is the next scene's first slot).  The cursors
+// go back to zero for the next rebuild.
+static __global__ void k_cellfix(const Dev* __restrict__ dp) {
+    const Dev& d = *dp;
+    if (*d.halt) return;
+    const int TC = d.plan[PL_TC], ns = d.plan[PL_NS];
+    int* __restrict__ v = d.vB;
+    NBC_GRID_STRIDE(u, TC) {
+        const int k = plan_find(d.pcell, ns, u);
+        const ScenePar& P = d.par[d.pscene[k]];
+        const int c = P.cell_off + (u - d.pcell[k]);
+        const int a = d.ccnt[u], b = d.ccnt[u + 1];
+        const int base = P.sub_off - d.psub[k];   // subsphere slot of sorted position t: base + t
+        d.cstart[c] = base + a;
+        d.ccur[u] = 0;
+        if (b - a <= 32) {
+            for (int x = a + 1; x < b; x++) {
+                const int w = v[x];
+                int y = x - 1;
+                while (y >= a && v[y] > w) { v[y + 1] = v[y]; y--; }
+                v[y + 1] = w;
+            }
+        } else {
+            int gap = 1;
+            while (gap < (b - a) / 3) gap = 3 * gap + 1;
+            for (; gap > 0; gap /= 3)
+                for (int x = a + gap; x < b; x++) {
+                    const int w = v[x];
+                    int y = x - gap;
+                    while (y >= a && v[y] > w) { v[y + gap] = v[y]; y -= gap; }
+                    v[y + gap] = w;
+                }
+        }
+        for (int t = a; t < b; t++) {
+            const int i = base + t, o = v[t];
+            d.inv[o] = i;
+            d.perm[i] = o;
+            d.key2[i] = c;
+        }
     }
 }
 
@@ -821,15 +891,10 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const int* __rest
     }
 }
 
-// The scatter of one pass.  With fin (the last pass of a rebuild's sort),
-// the sorted order goes straight into the engine's tables instead of the
-// output arrays: the permutation, its inverse and the sorted keys (key2) at
-// the subsphere slots of the rebuilt scenes (the cell table is built from
-// key2; FindBegEndInCell_cuk, src/dem_grid.cu:105-153).
 static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin,
                                                            int* __restrict__ kout, int* __restrict__ vout, int n,
                                                            int shift, const int* __restrict__ hist,
-                                                           const int* __restrict__ dn, const Dev* __restrict__ fin = nullptr) {
+                                                           const int* __restrict__ dn) {
     __shared__ int base[256];
     __shared__ int wcnt[RS_THREADS / 32][257];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -851,18 +916,8 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __r
             if (valid) {
                 int off = base[dig] + rank;
                 for (int w = 0; w < warp; w++) off += wcnt[w][dig];
-                if (fin) {
-                    const Dev& d = *fin;
-                    const int ks = plan_find(d.psub, d.plan[PL_NS], off);
-                    const int i = d.par[d.pscene[ks]].sub_off + (off - d.psub[ks]);
-                    const int o = vin[idx];
-                    d.inv[o] = i;
-                    d.perm[i] = o;
-                    d.key2[i] = k;
-                } else {
-                    kout[off] = k;
-                    vout[off] = vin[idx];
-                }
+                kout[off] = k;
+                vout[off] = vin[idx];
             }
             __syncthreads();
             int add = 0;
@@ -877,10 +932,6 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const int* __r
 // SortArray_*_cuk (src/dem_grid.cu:336-437) for every persistent per-subsphere
 // array at once, into the alternate buffers (written back by k_writeback).
 // The displacement accumulator restarts at zero (src/dem_simulation_clump.cu:172).
-// The same launch builds the cell table: cstart[c] = first sorted slot whose
-// cell key is >= c, for the cells of the rebuilt scenes and the entry after
-// each one's last cell (the next scene's first slot, which every writer of
-// that entry agrees on).
 template <typename R>
 __global__ void k_reorder(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
@@ -888,20 +939,9 @@ __global__ void k_reorder(const Dev* __restrict__ dp) {
     const int T = d.plan[PL_T], ns = d.plan[PL_NS];
     const size_t N = (size_t)d.N;
     {
-        const int TC = d.plan[PL_TC];
-        const int* __restrict__ key = d.key2;
-        NBC_GRID_STRIDE(u, TC) {
-            const int k = plan_find(d.pcell, ns, u);
-            const ScenePar& P = d.par[d.pscene[k]];
-            const int c = P.cell_off + (u - d.pcell[k]);
-            int lo = P.sub_off, len = P.nsub;
-            while (len > 0) {
-                const int h = len >> 1;
-                if (key[lo + h] < c) { lo += h + 1; len -= h + 1; }
-                else len = h;
-            }
-            d.cstart[c] = lo;
-        }
+        // the sort's cell counts back to zero for the next rebuild
+        const int TC1 = d.plan[PL_TC1];
+        NBC_GRID_STRIDE(u, TC1) d.ccnt[u] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) { d.cnt_f[T] = 0; d.cnt_b[T] = 0; }
     NBC_GRID_STRIDE(t, T) {

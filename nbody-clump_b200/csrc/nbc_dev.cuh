@@ -94,17 +94,16 @@ constexpr int PL_NS = 0;     // rebuilt scenes
 constexpr int PL_T = 1;      // their subspheres
 constexpr int PL_TC = 2;     // their cell-table entries
 constexpr int PL_T1 = 3;     // PL_T + 1 (scan length of the counts)
-constexpr int PL_HIST = 4;   // radix histogram entries (256 per tile)
-constexpr int PL_TK = 5;     // their clumps
-constexpr int PL_CS = 6;     // work counter of k_search (subspheres claimed)
-constexpr int PL_CC = 7;     // work counter of k_compact
+constexpr int PL_TK = 4;     // their clumps
+constexpr int PL_CS = 5;     // work counter of k_search (subspheres claimed)
+constexpr int PL_CC = 6;     // work counter of k_compact
+constexpr int PL_TC1 = 7;    // PL_TC + 1 (scan length of the cell counts)
 constexpr int PL_SIZE = 8;
 
 struct Dev {
     int S, N, K;
     int cap;          // pair capacity of each list buffer
     int cells;        // total global cells (sum over scenes)
-    int sort_bits;    // key bits for the radix sort
     int has_stops;    // some scene has a step limit (nbc_set_scene_steps): the kernels check for frozen scenes
     ScenePar* par;
     SceneDyn* dyn;
@@ -143,7 +142,6 @@ struct Dev {
     int* post_pending;// device flag: a force pass has run whose half-kick is pending
     // broad phase scratch
     int* kA; int* vA; int* kB; int* vB;   // radix sort ping-pong
-    int* hist;        // radix histograms
     int* perm;        // [N] old index of new slot i (part_idx_pre)
     int* inv;         // [N] new slot of old index
     int* cstart;                          // [cells+1] first sorted slot of each cell
@@ -160,6 +158,8 @@ struct Dev {
     // order and prefix sums over them; every rebuild kernel runs over the
     // concatenation of the rebuilt scenes only
     int* plan;        // [PL_SIZE] counts, see PL_*
+    int* ccnt;        // [cells + S + 1] subspheres per cell of the rebuilt scenes (the sort's counts; zero at rest)
+    int* ccur;        // [cells + S + 1] fill cursors of the sort's scatter (zero at rest)
     int* pscene;      // [S] rebuilt scenes
     int* psub;        // [S+1] prefix of their subsphere counts
     int* pcell;       // [S+1] prefix of their cell-table entries (cellnum + 1)
