@@ -436,12 +436,14 @@ def _poly_members(rng, n_clumps, rmin, rmax, max_members, rho):
 
 def _poly_templates(rng, n_clumps, rmin, rmax, max_members, rho, lam=0.5, samples=1 << 18):
     """The cfg2 / cfg4 clump templates: clumps of 1..max_members subspheres
-    (uniform), every subsphere's radius log-uniform in [rmin, rmax]; member n
-    attached to a random earlier member j in a uniformly random direction at
-    centre distance |r_n - r_j| + 2 lam min(r_n, r_j): the reference's
-    template builder (make_clump_template_lambda.m) places equal spheres at
-    2 r lambda, and for unequal ones this keeps the smaller sphere sticking
-    out of the larger by the same fraction of its diameter.  Mass, centre of mass
+    (uniform), every subsphere's radius log-uniform in [rmin, rmax]; the
+    largest is the core and each other member sits on it in a uniformly
+    random direction at centre distance |r_n - r_core| + 2 lam min(r_n,
+    r_core): the reference's template builder (make_clump_template_lambda.m)
+    places equal spheres at 2 r lambda, and for unequal ones this keeps the
+    smaller sphere sticking out of the larger by the same fraction of its
+    diameter (a compact clump, like the builder's ball and cross families,
+    rather than a chain).  Mass, centre of mass
     and inertia of each union (overlap counted once) come from
     nbc.union_mass (the builder's Monte Carlo integration, on the GPU for all
     clumps at once); members are re-expressed in the clump's principal frame
@@ -453,14 +455,14 @@ def _poly_templates(rng, n_clumps, rmin, rmax, max_members, rho, lam=0.5, sample
     r_all = np.exp(rng.uniform(np.log(rmin), np.log(rmax), M))
     d = rng.normal(size=(M, 3))
     d /= np.linalg.norm(d, axis=1)[:, None]
-    u = rng.random(M)
     cen = np.zeros((M, 3))
     for k in range(n_clumps):
-        b = start[k]
-        for n in range(1, m[k]):
-            j = b + int(u[b + n] * n)
-            ra, rb = r_all[b + n], r_all[j]
-            cen[b + n] = cen[j] + (abs(ra - rb) + 2.0 * lam * min(ra, rb)) * d[b + n]
+        b, e = start[k], start[k + 1]
+        core = b + int(np.argmax(r_all[b:e]))
+        rc, rr = r_all[core], r_all[b:e]
+        dist = np.abs(rr - rc) + 2.0 * lam * np.minimum(rr, rc)
+        cen[b:e] = dist[:, None] * d[b:e]
+        cen[core] = 0.0
     vol, com, mom = nbc.union_mass(cen, r_all, start, samples=samples)
     mass = rho * vol
     inertia = (rho * vol)[:, None, None] * (np.trace(mom, axis1=1, axis2=2)[:, None, None] * np.eye(3) - mom)
