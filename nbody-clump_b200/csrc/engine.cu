@@ -1341,7 +1341,10 @@ class EngineT final : public EngineBase {
     // exclusive scans of a0 (and a1, a2, of the same length) over [0, n), or
     // over [0, *dn) when dn is given (n then bounds it), in one launch
     void scan(int* a0, int* a1, int* a2, int n, const int* dn = nullptr) {
-        const int nb = std::max(1, cdiv(n, SC_TILE)) * (a2 ? 3 : (a1 ? 2 : 1));
+        // a grid of at most a few blocks per SM takes the tiles; a grid sized
+        // for the largest length would start tens of thousands of blocks that
+        // find nothing to do when few scenes are rebuilt
+        const int nb = std::min(std::max(1, cdiv(n, SC_TILE)) * (a2 ? 3 : (a1 ? 2 : 1)), sm_count_ * 4);
         k_scan1<<<nb, SC_THREADS, 0, stream_>>>(a0, a1, a2, n, dn, h_.scan_st, h_.scan_ctl, h_.halt, h_.scan_fail);
     }
     // The rebuild block of src/dem_simulation_clump.cu:124-176, over the

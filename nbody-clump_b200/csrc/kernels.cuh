@@ -598,14 +598,15 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan_add(int* __restrict_
 }
 
 // --- exclusive scan of ints in one launch (decoupled look-back) ----------
-// One to three arrays of the same length (n, or *dn) in one launch.  Every
-// block takes one tile from a ticket counter: tickets [0, tiles) are the
-// tiles of the first array, [tiles, 2 tiles) those of the second, and so on.  A tile
+// One to three arrays of the same length (n, or *dn) in one launch.  Blocks
+// take tiles from a ticket counter until none is left: tickets [0, tiles)
+// are the tiles of the first array, [tiles, 2 tiles) those of the second,
+// and so on.  A tile
 // publishes its aggregate, then looks back over its array's earlier tiles
 // (32 at a time, one per lane of warp 0) and sums aggregates until it meets
-// an inclusive prefix, and publishes its own inclusive prefix.  Tickets are
-// taken in the order blocks start, so a tile waits only on tiles held by
-// blocks that are already running: the wait always ends.  Each wait is still
+// an inclusive prefix, and publishes its own inclusive prefix.  A block
+// takes its next ticket only after finishing its tile, so a tile waits only
+// on tiles held by blocks that are running: the wait always ends.  Each wait is still
 // bounded (SCAN_SPIN_LIMIT polls); a block that gives up sets *fail and
 // *halt, so every later kernel of the step returns at once and the host
 // reports the failure instead of using the result.  The last block of the
@@ -624,10 +625,14 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan1(int* __restrict__ a
     const int nn = dn ? *dn : n;
     const int tiles = (nn + SC_TILE - 1) / SC_TILE;
     const int narr = a2 ? 3 : (a1 ? 2 : 1);
-    if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl[0], 1);
-    __syncthreads();
-    const int tk = s_ticket;
-    if (tk < narr * tiles) {
+    // a fixed grid takes tiles until none is left (the grid is set when the
+    // launch is captured; the tile count is known only on the device)
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = atomicAdd(&ctl[0], 1);
+        __syncthreads();
+        const int tk = s_ticket;
+        __syncthreads();
+        if (tk >= narr * tiles) break;
         const int arr = tk / tiles;
         const int b = tk - arr * tiles;      // tile of its array
         int* __restrict__ a = arr == 0 ? a0 : (arr == 1 ? a1 : a2);
