@@ -301,7 +301,8 @@ nbc_status nbc_union_mass(const double* centres, const double* radii, const int*
  * cudaMalloc on first use, src/dem_grid.cu:278-305).  For callers that
  * cannot call cudaMalloc -- device memory owned by another framework's pool,
  * or a run whose memory budget is fixed at start-up: the cell hash of a
- * list rebuild plus the engine's stable radix sort, with the caller's
+ * list rebuild plus a stable radix sort by cell (the order of the engine's
+ * sort), with the caller's
  * buffers and one scratch array compiled into the library (NBC_NOALLOC_MAX_N
  * elements, about 2.2 MB per GPU that loads the library, kept until exit).
  *   pos_dev   device array [n][3] of positions (caller-owned)

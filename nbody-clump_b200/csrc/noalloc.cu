@@ -3,9 +3,9 @@
 // Some callers cannot call cudaMalloc: a host program whose device memory
 // is owned by another framework's pool, or code running where allocation is
 // forbidden once a run has started (a memory budget fixed at start-up).
-// nbc_cell_sort_noalloc gives them the engine's cell hash and stable radix
-// sort (the first half of a list rebuild) using only buffers the caller
-// passes plus one scratch array compiled into this library.
+// nbc_cell_sort_noalloc gives them the engine's cell hash and a stable radix
+// sort by cell (the order of the first half of a list rebuild) using only
+// buffers the caller passes plus one scratch array compiled into this library.
 //
 // Scratch: `g_sort_scratch` below, NBC_NOALLOC_MAX_N elements of key/value
 // ping-pong plus the radix histograms, about 2.2 MB, held on every GPU that
