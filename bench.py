@@ -735,6 +735,14 @@ def run_serve(args):
         fin = max(arr, fin) + sv
         ttr_plain.append(fin - arr)
     q = lambda v, p: float(np.percentile(v, p))
+    # the error of a served result against FP64: the first request's first
+    # step against the oracle from the same state (pair list and per-contact
+    # normal force), and the oracle's speed on it
+    ex = nbc.Engine([reqs[0][1]], precision=args.precision, use_graph=False)
+    ex.step_export(1)
+    first = {"pairs": ex.pairs(), "fcn": ex.pair_forces()}
+    ex.close()
+    cpu = None if args.no_cpu_baseline else cpu_baseline(args, reqs[0][1], first)
     line = {"metric": "time-to-result p50/p99 and throughput, served vs plain (cfg4)",
             "workload": f"cfg4: {len(reqs)} penetration requests, Poisson rate {args.rate}/s, "
                         f"subspheres log-uniform in [1k, 200k] (bank of {len(sizes)} pre-settled beds), "
@@ -747,6 +755,7 @@ def run_serve(args):
             "throughput_ratio": (work / makespan) / (work / sum(svc)),
             "failed": failed, "failed_plain": failed_plain,
             "slots": args.slots, "cohort": args.cohort, "budget_gb": args.budget_gb,
+            "request0_vs_fp64": cpu,
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy beds settled by the engine)"}
     print(json.dumps(line), flush=True)
