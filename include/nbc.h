@@ -49,6 +49,30 @@ typedef int nbc_status;
 #define NBC_MOTION_GRAVITY 1
 #define NBC_MOTION_GRAVITY_AFTER_CONTACT 2
 
+/* nbc_scene_desc.sphere_mode: the behaviour of the reference's sphere-only
+ * drivers (class DEMmain, src/dem.h:31-99) where it differs from the clump
+ * path.  0 = the clump path.  The bits need one-sphere clumps whose member
+ * sits at the clump centre (LocalPos = 0). */
+#define NBC_SPHERE_KINEMATICS 1   /* first half-kick and attitude without the
+                                     intruder's force and torque (src/dem_integrate.cu:
+                                     20-21,72); cohesion in the penetrator law
+                                     (src/dem_force_penetrator.cu:119-123) */
+#define NBC_SPHERE_CUBE_WALL 2    /* the sphere cube wall: tangential force
+                                     without history, no rolling or twisting
+                                     moment (src/dem_force_cube_wall.cu:70-141) */
+#define NBC_SPHERE_RESET_HISTORY 4 /* pair spring histories restart from zero at
+                                     every rebuild: the driver exchanges the history
+                                     pointers once more after the list build has
+                                     carried them and cleared the other buffer
+                                     (src/dem_simulation_cylind.cu:141 after
+                                     src/dem_grid.cu:687-749) */
+
+/* DEMmain drivers for nbc_open_sphere */
+#define NBC_DRIVER_CYLINDER 0     /* DEMmain::RunSimulation, src/dem_simulation_cylind.cu:3-211 */
+#define NBC_DRIVER_CUBE 1         /* DEMmain::RunSimulation2, src/dem_simulation_cube.cu:3-226 */
+#define NBC_DRIVER_SPLIT 2        /* DEMmain::RunSimulation_Split, src/dem_simulation_split.cu:3-211 */
+#define NBC_DRIVER_HGRID 3        /* DEMmain::RunSimulation_HGrid, src/dem_simulation_hgrid.cu:3-201 */
+
 /* One scene: the contents of world.par, ph/ch .bt and Rocks/ files.
  * Replaces Parameters/GlobalFlg (src/dem_parameters.h:7-79) plus the arrays
  * loaded by DEMSubSphereIo::LoadPhase (src/dem_subsphere_io.cu:151-193) and
@@ -84,6 +108,11 @@ typedef struct {
     int levels;
     const int* level;                        /* [n_sub], 0 = coarsest */
     const double* level_cell;                /* [levels] cell size per level */
+    int sphere_mode;                         /* NBC_SPHERE_* bits, 0 = the clump path */
+    /* split driver (NBC_DRIVER_SPLIT) body kinds per clump, or NULL: 0 free,
+     * 1 moved at the prescribed velocity (-0.2 y, -0.2 x, 0), 2 fixed
+     * (src/dem_integrate_withglue.cu:3-60) */
+    const int* body_kind;
 } nbc_scene_desc;
 
 typedef struct {
@@ -111,6 +140,19 @@ nbc_status nbc_open(const char* workdir, const nbc_options* opt, nbc_engine** ou
 /* Run StartStep..EndStep with the reference's outputs into workdir
  * (OutPart, OutClump, OutForce, OutCnt; src/dem_simulation_clump.cu:74-259). */
 nbc_status nbc_run(nbc_engine* e);
+
+/* --- drop-in entry points: the sphere-only drivers of class DEMmain ------
+ * (src/dem.h:31-99; RunSimulation, RunSimulation2, RunSimulation_Split and
+ * RunSimulation_HGrid, selected by NBC_DRIVER_*).  Reads world.par, the
+ * 21-column ph file named by IniConFile (src/dem_io.cu:155-202), the
+ * driver's wall (Rocks/CylindWall.bt, or Rocks/CubeWall.bt for
+ * NBC_DRIVER_CUBE), Rocks/Penetrator.bt and, for NBC_DRIVER_HGRID, grid.bt
+ * (src/dem_io.cu:204-248).  Each sphere becomes a one-sphere clump and the
+ * scene runs with the driver's NBC_SPHERE_* behaviour; nbc_run then writes
+ * the drivers' outputs (OutPart/ph.N.bin in the sphere layout, with an
+ * intruder OutPart/intruder.N.bin and OutForce/fc.N.bin, and OutCnt for the
+ * cube driver with an intruder). */
+nbc_status nbc_open_sphere(const char* workdir, int driver, const nbc_options* opt, nbc_engine** out);
 
 /* --- scene-level calls ---------------------------------------------------- */
 nbc_status nbc_create(const nbc_scene_desc* const* scenes, int n_scenes, const nbc_options* opt,

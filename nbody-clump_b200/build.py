@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "capi.cpp", "io.cpp", "noalloc.cu", "tune.cpp", "serve.cpp", "generate.cu"]
 HEADERS = ["kernels.cuh", "nbc_dev.cuh", "nbc_math.cuh", "engine.h", "io.h", "handle.h", "dem_clump_main.h",
-           "dem_clump_main.cpp", "main.cpp"]
+           "dem_clump_main.cpp", "main.cpp", "dem_main.h", "dem_main.cpp", "sphere_main.cpp"]
 
 
 def _stale() -> bool:
@@ -64,15 +64,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("link failed")
     for o in objs:
         os.remove(o)
-    # the drop-in executable: the reference's main() on DEMClumpMain
-    exe = os.path.join(HERE, "nbody_clump_b200")
-    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(HERE), "include"),
-           os.path.join(CSRC, "main.cpp"), os.path.join(CSRC, "dem_clump_main.cpp"), "-L", HERE, "-lnbc",
-           "-Wl,-rpath,$ORIGIN", "-o", exe]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("drop-in executable failed to link")
+    # the drop-in executables: the reference's main() on DEMClumpMain, and
+    # the sphere-only drivers on DEMmain
+    for name, srcs in (("nbody_clump_b200", ["main.cpp", "dem_clump_main.cpp"]),
+                       ("nbody_sphere_b200", ["sphere_main.cpp", "dem_main.cpp"])):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(HERE), "include"),
+               *[os.path.join(CSRC, f) for f in srcs], "-L", HERE, "-lnbc", "-Wl,-rpath,$ORIGIN",
+               "-o", os.path.join(HERE, name)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"drop-in executable {name} failed to link")
     return OUT
 
 

@@ -202,9 +202,128 @@ nbc_status nbc_open(const char* workdir, const nbc_options* opt, nbc_engine** ou
     return NBC_OK;
 }
 
+nbc_status nbc_open_sphere(const char* workdir, int driver, const nbc_options* opt, nbc_engine** out) {
+    if (!workdir || !out) return fail(NBC_ERR_ARG, "nbc_open_sphere: bad arguments");
+    *out = nullptr;
+    if (driver < NBC_DRIVER_CYLINDER || driver > NBC_DRIVER_HGRID)
+        return fail(NBC_ERR_ARG, "nbc_open_sphere: unknown driver");
+    std::unique_ptr<nbc::Workdir> wd(new nbc::Workdir());
+    std::string err;
+    if (!nbc::load_sphere_workdir(workdir, driver, *wd, err)) return fail(NBC_ERR_IO, err);
+    nbc_options o;
+    if (opt) o = *opt;
+    else { nbc_default_options(&o); o.precision = NBC_PREC_F64; }
+    const nbc_scene_desc* d = &wd->desc;
+    nbc_engine* e = nullptr;
+    nbc_status st = nbc_create(&d, 1, &o, &e);
+    if (st != NBC_OK) return st;
+    e->wd = std::move(wd);
+    *out = e;
+    return NBC_OK;
+}
+
+// The sphere drivers' loop with their outputs (src/dem_simulation_cylind.cu:
+// 62-209 and its cube, split and hgrid variants): OutPart/ph.N.bin in the
+// sphere layout every OutputInterval steps, with an intruder also
+// OutPart/intruder.N.bin and OutForce/fc.N.bin (src/dem_io.cu:331-342); the
+// cube driver with an intruder also OutCnt every 2 OutputInterval steps
+// (src/dem_simulation_cube.cu:212-223).
+static nbc_status run_sphere(nbc_engine* e) {
+    nbc::Workdir& w = *e->wd;
+    const nbc_scene_desc& D = w.desc;
+    const std::string dir = w.dir;
+    const bool intr = w.is_intruder;
+    const bool cnt = intr && w.driver == NBC_DRIVER_CUBE;
+    if (!nbc::make_dirs(dir + "/OutPart/")) return fail(NBC_ERR_IO, "cannot create OutPart");
+    if (cnt && !nbc::make_dirs(dir + "/OutCnt/")) return fail(NBC_ERR_IO, "cannot create OutCnt");
+    if (intr && !nbc::make_dirs(dir + "/OutForce/")) return fail(NBC_ERR_IO, "cannot create OutForce");
+    const int n = D.n_sub, bl = D.branch_len, oi = D.output_interval;
+    std::vector<int> fix(n), cid(n), ident(n), type(n), nei;
+    std::vector<double> pos(3 * (size_t)n), rad(n), vel(3 * (size_t)n), quat(4 * (size_t)n), angv(3 * (size_t)n),
+        prop(4 * (size_t)n);
+    std::vector<double> cp(3 * (size_t)n), cv(3 * (size_t)n), cq(4 * (size_t)n), cw(3 * (size_t)n),
+        cpr(4 * (size_t)n);
+    std::vector<double> hist, fcn, cpt;
+    for (int i = 0; i < n; i++) ident[i] = i;
+    int count = 0, count2 = 0;
+    for (int ii = D.start_step; ii < D.end_step;) {
+        const int to_out = oi - count;
+        const int to_cnt = cnt ? 2 * oi - count2 : to_out;
+        const int chunk = std::min(std::min(to_out, to_cnt), D.end_step - ii);
+        const bool exp = cnt && chunk == to_cnt;
+        nbc_status st = exp ? nbc_step_export(e, chunk) : nbc_step(e, chunk);
+        if (st != NBC_OK) return st;
+        ii += chunk;
+        count += chunk;
+        if (cnt) count2 += chunk;
+        if (count == oi || (cnt && count2 == 2 * oi)) {
+            st = nbc_sync(e);
+            if (st != NBC_OK) return st;
+        }
+        if (count == oi) {
+            std::printf("StepSize = %d\n", ii);
+            st = guard([&] {
+                e->eng->get_subspheres(0, fix.data(), cid.data(), pos.data(), rad.data());
+                e->eng->get_clumps(0, cp.data(), cv.data(), cq.data(), cw.data(), nullptr, nullptr);
+                e->eng->get_clump_prop(0, cpr.data());
+            });
+            if (st != NBC_OK) return st;
+            // the drivers sort every per-sphere array (src/dem_simulation_cylind.cu:102-108):
+            // sphere i of the sorted order is clump cid[i]
+            for (int i = 0; i < n; i++) {
+                const size_t k = (size_t)cid[i];
+                type[i] = w.type[k];
+                for (int c = 0; c < 3; c++) {
+                    vel[3 * (size_t)i + c] = cv[3 * k + c];
+                    angv[3 * (size_t)i + c] = cw[3 * k + c];
+                }
+                for (int c = 0; c < 4; c++) {
+                    quat[4 * (size_t)i + c] = cq[4 * k + c];
+                    prop[4 * (size_t)i + c] = cpr[4 * k + c];
+                }
+            }
+            if (!nbc::write_sphere_ph(nbc::bin_name(dir + "/OutPart", "ph", ii), n, ident.data(), fix.data(),
+                                      type.data(), pos.data(), vel.data(), quat.data(), angv.data(), prop.data(),
+                                      rad.data()))
+                return fail(NBC_ERR_IO, "cannot write OutPart");
+            if (intr) {
+                double ip[3], iv[3], re[3], tq[3];
+                int state;
+                hist.resize(6 * (size_t)oi);
+                st = guard([&] {
+                    e->eng->get_intruder(0, ip, iv, re, tq, &state);
+                    e->eng->get_intruder_history(0, oi, hist.data());
+                });
+                if (st != NBC_OK) return st;
+                double iw[3] = {D.intr_angvel[0], D.intr_angvel[1], D.intr_angvel[2]};
+                bool ok = nbc::write_ch(nbc::bin_name(dir + "/OutPart", "intruder", ii), 0, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr, ip, iv, w.intr_quat, iw);
+                ok = ok && nbc::write_fc(nbc::bin_name(dir + "/OutForce", "fc", ii), oi, hist.data());
+                if (!ok) return fail(NBC_ERR_IO, "cannot write the intruder files");
+            }
+            count = 0;
+        }
+        if (cnt && count2 == 2 * oi) {
+            nei.resize((size_t)n * bl);
+            fcn.resize((size_t)n * bl * 3);
+            cpt.resize((size_t)n * bl * 3);
+            st = guard([&] {
+                e->eng->get_rows(0, bl, nei.data(), nullptr, nullptr);
+                e->eng->get_chain(0, bl, fcn.data(), cpt.data());
+            });
+            if (st != NBC_OK) return st;
+            if (!nbc::write_cnt(dir + "/OutCnt", ii, n, bl, nei.data(), fcn.data(), cpt.data()))
+                return fail(NBC_ERR_IO, "cannot write OutCnt");
+            count2 = 0;
+        }
+    }
+    return nbc_sync(e);
+}
+
 // RunSimulationClump's loop with its outputs (src/dem_simulation_clump.cu:74-259)
 nbc_status nbc_run(nbc_engine* e) {
     if (!e || !e->eng || !e->wd) return fail(NBC_ERR_STATE, "nbc_run: engine not opened from a working directory");
+    if (e->wd->driver >= 0) return run_sphere(e);
     nbc::Workdir& w = *e->wd;
     const nbc_scene_desc& D = w.desc;
     const std::string dir = w.dir;

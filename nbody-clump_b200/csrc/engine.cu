@@ -651,6 +651,7 @@ class EngineT final : public EngineBase {
         blk(h_.bhist, (size_t)NB_SLOTS * 3 * N * sizeof(R4<R>));
         blk(h_.bbits, N * sizeof(uint16_t));
         blk(h_.fbnd, 2 * N * sizeof(R4<R>));
+        if (h_.fint) blk(h_.fint, 2 * N * sizeof(R4<R>));
         blk(h_.bidx, N * sizeof(int));
         // clumps
         blk(h_.cpos, K_ * sizeof(double4));
@@ -723,6 +724,9 @@ class EngineT final : public EngineBase {
     Dev* d_ = nullptr;   // device table
     int S_ = 0, N_ = 0, K_ = 0;
     bool hgrid_ = false;
+    bool sphere_any_ = false;   // some scene runs a sphere driver's behaviour (the clump pass's SPH build)
+    bool sphere_kin_ = false;   // some scene runs the sphere drivers' kinematics (Dev::fint)
+    bool has_kinds_ = false;    // some scene has split-driver body kinds (Dev::kind)
     bool first_list_ = true;
     int search_lanes_ = 8;
     int clump_batch_ = 2;    // members per lane per load batch of the clump pass
@@ -835,9 +839,12 @@ class EngineT final : public EngineBase {
         search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
         clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
         // the clump pass's staged contact records (dynamic shared memory past the 48 KB default)
-        CK(cudaFuncSetAttribute(k_clump<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
-        CK(cudaFuncSetAttribute(k_clump<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 2>()));
-        CK(cudaFuncSetAttribute(k_clump<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 4>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 2>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 4>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 2>()));
+        CK(cudaFuncSetAttribute(k_clump<R, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 4>()));
         pair_bps_ = opt_.pair_blocks >= 2 && opt_.pair_blocks <= 16 ? opt_.pair_blocks : 12;
         CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
         S_ = (int)sc.size();
@@ -928,6 +935,37 @@ class EngineT final : public EngineBase {
                 }
                 P.intr_mass = D.intr_prop[3];
             }
+            // the reference's sphere-only drivers (class DEMmain)
+            if (D.sphere_mode & ~(NBC_SPHERE_KINEMATICS | NBC_SPHERE_CUBE_WALL | NBC_SPHERE_RESET_HISTORY))
+                throw ArgError("scene " + std::to_string(s) + ": unknown sphere_mode bits");
+            P.sphere = D.sphere_mode | (D.body_kind ? SPH_KINDS : 0);
+            if (P.sphere) {
+                // one-sphere clumps with the member at the centre: the clump
+                // kinematics are then the sphere kinematics
+                if (D.n_sub != D.n_clump)
+                    throw ArgError("scene " + std::to_string(s) + ": sphere drivers need one subsphere per clump");
+                std::vector<char> seen(D.n_clump, 0);
+                for (int i = 0; i < D.n_sub; i++) {
+                    const int c = D.clump_id[i];
+                    if (c < 0 || c >= D.n_clump || seen[c] || D.local[3 * i] != 0.0 || D.local[3 * i + 1] != 0.0 ||
+                        D.local[3 * i + 2] != 0.0)
+                        throw ArgError("scene " + std::to_string(s) +
+                                       ": sphere drivers need one subsphere per clump at its centre (LocalPos = 0)");
+                    seen[c] = 1;
+                }
+            }
+            if (P.sphere) sphere_any_ = true;
+            if (P.sphere & SPH_KIN) sphere_kin_ = true;
+            if (P.sphere & SPH_KINDS) {
+                for (int k = 0; k < D.n_clump; k++)
+                    if (D.body_kind[k] < 0 || D.body_kind[k] > 2)
+                        throw ArgError("scene " + std::to_string(s) + ": body kind out of range at clump " +
+                                       std::to_string(k));
+                has_kinds_ = true;
+                // bodies of kind 1 move without triggering a rebuild: every
+                // listed pair stays in the contact pass (near margin unbounded)
+                P.thresh = 1e100;
+            }
             start_step_[s] = D.start_step;
             ring_len_ = std::max(ring_len_, std::max(1, D.output_interval));
         }
@@ -941,6 +979,7 @@ class EngineT final : public EngineBase {
         std::vector<double4> posr(N_), lom(N_);
         std::vector<int> cid(N_), fix(N_), lev(N_, 0), sid(N_), csid(K_), mstart(K_ + 1, 0), midx(N_);
         std::vector<double4> cpos(K_), cvel(K_), cw(K_), cq(K_), cprop(K_);
+        std::vector<int> kind(has_kinds_ ? K_ : 0, 0);
         for (int s = 0; s < S_; s++) {
             const nbc_scene_desc& D = *sc[s];
             const ScenePar& P = hpar_[s];
@@ -968,6 +1007,10 @@ class EngineT final : public EngineBase {
                 cw[g] = make_double4(D.clump_angvel[3 * k], D.clump_angvel[3 * k + 1], D.clump_angvel[3 * k + 2], 0);
                 cq[g] = make_double4(D.clump_quat[4 * k], D.clump_quat[4 * k + 1], D.clump_quat[4 * k + 2], D.clump_quat[4 * k + 3]);
                 cprop[g] = make_double4(D.clump_prop[4 * k], D.clump_prop[4 * k + 1], D.clump_prop[4 * k + 2], D.clump_prop[4 * k + 3]);
+                // bits 0-1: Type; bits 2-3: the kind the split driver's first
+                // half-kick sees, the body's original index (0, 1, 2, or 3 for
+                // any larger index; see k_clump)
+                if (has_kinds_ && D.body_kind) kind[g] = D.body_kind[k] | (std::min(k, 3) << 2);
             }
         }
         for (int k = 0; k < K_; k++) mstart[k + 1] += mstart[k];
@@ -999,6 +1042,8 @@ class EngineT final : public EngineBase {
             h_.bbits = m.take<uint16_t>(N); h_.bbits2 = m.take<uint16_t>(N);
             h_.fsum = m.take<R4<R>>(2 * N);
             h_.fbnd = m.take<R4<R>>(2 * N);
+            h_.fint = sphere_kin_ ? m.take<R4<R>>(2 * N) : nullptr;
+            h_.kind = has_kinds_ ? m.take<int>(K_) : nullptr;
             h_.cpos = m.take<double4>(K_); h_.cvel = m.take<double4>(K_); h_.cw = m.take<double4>(K_);
             h_.cq = m.take<double4>(K_); h_.cprop = m.take<double4>(K_);
             h_.cinv = m.take<double4>(K_);
@@ -1075,6 +1120,7 @@ class EngineT final : public EngineBase {
         copy_(h_.cw, cw.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
         copy_(h_.cq, cq.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
         copy_(h_.cprop, cprop.data(), K_ * sizeof(double4), cudaMemcpyHostToDevice);
+        if (h_.kind) copy_(h_.kind, kind.data(), K_ * sizeof(int), cudaMemcpyHostToDevice);
         {
             // the clump pass's reciprocals: IEEE divisions, bitwise those it formed each step
             std::vector<double4> cinv(K_);
@@ -1285,12 +1331,19 @@ class EngineT final : public EngineBase {
     void launch_clump(int do_pre, cudaGraphConditionalHandle cond = 0, int use_cond = 0,
                       cudaGraphConditionalHandle loop = 0, int use_loop = 0) {
         const int g = cdiv(K_ + S_, CL_THREADS);
-        if (clump_batch_ == 1)
-            k_clump<R, 1><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        if (sphere_any_) {
+            if (clump_batch_ == 1)
+                k_clump<R, 1, true><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+            else if (clump_batch_ == 4)
+                k_clump<R, 4, true><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+            else
+                k_clump<R, 2, true><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+        } else if (clump_batch_ == 1)
+            k_clump<R, 1, false><<<g, CL_THREADS, clump_dyn_smem<R, 1>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         else if (clump_batch_ == 4)
-            k_clump<R, 4><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+            k_clump<R, 4, false><<<g, CL_THREADS, clump_dyn_smem<R, 4>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         else
-            k_clump<R, 2><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
+            k_clump<R, 2, false><<<g, CL_THREADS, clump_dyn_smem<R, 2>(), stream_>>>(d_, do_pre, cond, use_cond, loop, use_loop);
         CK(cudaGetLastError());
         if (!capturing_) launches_ += 1;
     }
@@ -1314,8 +1367,11 @@ class EngineT final : public EngineBase {
         mark(3, stream2_);
         // grid-stride over the boundary candidates (a device count)
         const int bg = std::min(sm_count_ * 8, cdiv(N_, BD_THREADS));
-        if (exp) k_boundary<R, true><<<bg, BD_THREADS, 0, stream2_>>>(d_);
-        else k_boundary<R, false><<<bg, BD_THREADS, 0, stream2_>>>(d_);
+        if (sphere_any_) {
+            if (exp) k_boundary<R, true, true><<<bg, BD_THREADS, 0, stream2_>>>(d_);
+            else k_boundary<R, false, true><<<bg, BD_THREADS, 0, stream2_>>>(d_);
+        } else if (exp) k_boundary<R, true, false><<<bg, BD_THREADS, 0, stream2_>>>(d_);
+        else k_boundary<R, false, false><<<bg, BD_THREADS, 0, stream2_>>>(d_);
         mark(4, stream2_);
         CK(cudaEventRecord(ev_join_, stream2_));
         // grid-stride over the near pairs (a device count), so a fixed grid

@@ -5,8 +5,10 @@
 // (src/dem_subsphere_io.cu:151-193, src/dem_clumpsphere_io.cu:24-62),
 // Rocks/CubeWall.bt (src/dem_cube_wall_io.cu:21-53), Rocks/Penetrator.bt
 // (src/dem_penetrator_io.cu:21-116) and Rocks/CylindWall.bt
-// (src/dem_cylind_wall_io.cu:20-55).  Writers: the field-block .bin files of
-// src/dem_binary_io.h:17-181.  Errors are returned, never exit().
+// (src/dem_cylind_wall_io.cu:20-55); the sphere drivers' 21-column ph file
+// and grid.bt (src/dem_io.cu:155-248).  Writers: the field-block .bin files
+// of src/dem_binary_io.h:17-181 and src/dem_io.cu:313-329.  Errors are
+// returned, never exit().
 #include "io.h"
 
 #include <sys/stat.h>
@@ -81,9 +83,8 @@ static bool load_par(const std::string& path, Workdir& w, std::string& err) {
 
 static double pd(const Workdir& w, const char* k) { return std::atof(w.par.at(k).c_str()); }
 
-bool load_workdir(const std::string& dir, Workdir& w, std::string& err) {
-    w.dir = dir;
-    if (!load_par(dir + "/world.par", w, err)) return false;
+// the scalars of world.par both paths read
+static bool par_scalars(Workdir& w, std::string& err) {
     nbc_scene_desc& D = w.desc;
     memset(&D, 0, sizeof(D));
     D.n_sub = (int)pd(w, "NumberBody");
@@ -105,8 +106,118 @@ bool load_workdir(const std::string& dir, Workdir& w, std::string& err) {
     }
     D.is_wall_force = pd(w, "isWallForce") != 0;
     w.is_intruder = pd(w, "isIntruder") != 0;
-    if (D.n_sub <= 0 || D.n_clump <= 0) { err = "NumberBody and ClumpNum must be positive"; return false; }
+    if (D.n_sub <= 0) { err = "NumberBody must be positive"; return false; }
     if (D.output_interval <= 0) { err = "OutputInterval must be positive"; return false; }
+    D.levels = 1;
+    return true;
+}
+
+// Rocks/CubeWall.bt (src/dem_cube_wall_io.cu:21-53)
+static bool read_cube(const std::string& path, nbc_scene_desc& D, std::string& err) {
+    std::ifstream f(path);
+    if (!f) { err = "Error! Cannot open " + path + "!"; return false; }
+    double v[16];
+    for (int k = 0; k < 16; k++)
+        if (!(f >> v[k])) { err = "Rocks/CubeWall.bt: malformed"; return false; }
+    D.wall = NBC_WALL_CUBE;
+    for (int a = 0; a < 3; a++) {
+        D.cube_half[a] = v[a]; D.cube_centre[a] = v[3 + a]; D.cube_vel[a] = v[6 + a]; D.cube_angvel[a] = v[13 + a];
+    }
+    return true;
+}
+
+// Rocks/CylindWall.bt (src/dem_cylind_wall_io.cu:20-55)
+static bool read_cyl(const std::string& path, nbc_scene_desc& D, std::string& err) {
+    std::ifstream f(path);
+    if (!f) { err = "Error! Cannot open " + path + "!"; return false; }
+    double v[22];
+    for (int k = 0; k < 22; k++)
+        if (!(f >> v[k])) { err = "Rocks/CylindWall.bt: malformed"; return false; }
+    D.wall = NBC_WALL_CYLINDER;
+    D.cyl_radius = v[0]; D.cyl_half_height = v[1];
+    for (int a = 0; a < 3; a++) {
+        D.cyl_axis[a] = v[2 + a]; D.cyl_centre[a] = v[9 + a]; D.cyl_vel[a] = v[12 + a]; D.cyl_angvel[a] = v[19 + a];
+    }
+    return true;
+}
+
+// Rocks/Penetrator.bt (src/dem_penetrator_io.cu:21-116); `use` sets the
+// scene's intruder, otherwise the file is only checked
+static bool read_penetrator(const std::string& dir, Workdir& w, bool use, std::string& err) {
+    nbc_scene_desc& D = w.desc;
+    const std::string pp = dir + "/Rocks/Penetrator.bt";
+    std::ifstream f(pp);
+    if (!f) { err = "Error! Cannot open " + pp + "!"; return false; }
+    nbc_scene_desc T;
+    memset(&T, 0, sizeof(T));
+    std::string tok;
+    f >> tok;
+    std::string lt = lower(tok);
+    if (lt == "sphere") {
+        T.intruder = NBC_INTR_SPHERE;
+        f >> T.intr_radius;
+        T.intr_half_height = T.intr_radius;
+        T.intr_axis[2] = 1.0;
+    } else if (lt == "cylinder") {
+        T.intruder = NBC_INTR_CYLINDER;
+        f >> T.intr_radius >> T.intr_half_height >> T.intr_axis[0] >> T.intr_axis[1] >> T.intr_axis[2];
+    } else {
+        char* end = nullptr;
+        T.intr_radius = std::strtod(tok.c_str(), &end);
+        if (end == tok.c_str() || *end != '\0') { err = "Error! Unknown penetrator shape '" + tok + "'"; return false; }
+        T.intruder = NBC_INTR_CYLINDER;
+        f >> T.intr_half_height >> T.intr_axis[0] >> T.intr_axis[1] >> T.intr_axis[2];
+    }
+    double q[4];
+    f >> T.intr_prop[0] >> T.intr_prop[1] >> T.intr_prop[2] >> T.intr_prop[3];
+    f >> T.intr_pos[0] >> T.intr_pos[1] >> T.intr_pos[2];
+    f >> T.intr_vel[0] >> T.intr_vel[1] >> T.intr_vel[2];
+    f >> q[0] >> q[1] >> q[2] >> q[3];
+    f >> T.intr_angvel[0] >> T.intr_angvel[1] >> T.intr_angvel[2];
+    if (!f || T.intr_radius <= 0.0 || T.intr_prop[3] <= 0.0) { err = "Error! Invalid penetrator data in " + pp; return false; }
+    T.intr_motion = NBC_MOTION_CONSTANT_VELOCITY;
+    std::string opt;
+    if (f >> opt) {
+        if (lower(opt) != "motion") { err = "Error! Unknown penetrator option '" + opt + "'"; return false; }
+        std::string m;
+        f >> m;
+        m = lower(m);
+        if (m == "constant_velocity" || m == "constant" || m == "kinematic") T.intr_motion = NBC_MOTION_CONSTANT_VELOCITY;
+        else if (m == "gravity" || m == "dynamic") T.intr_motion = NBC_MOTION_GRAVITY;
+        else if (m == "gravity_after_contact") T.intr_motion = NBC_MOTION_GRAVITY_AFTER_CONTACT;
+        else { err = "Error! Unknown penetrator motion mode '" + m + "'"; return false; }
+    }
+    if (!use) return true;
+    D.intruder = T.intruder;
+    D.intr_motion = T.intr_motion;
+    D.intr_radius = T.intr_radius;
+    D.intr_half_height = T.intr_half_height;
+    for (int a = 0; a < 3; a++) {
+        D.intr_axis[a] = T.intr_axis[a]; D.intr_pos[a] = T.intr_pos[a]; D.intr_vel[a] = T.intr_vel[a];
+        D.intr_angvel[a] = T.intr_angvel[a];
+    }
+    for (int c = 0; c < 4; c++) { D.intr_prop[c] = T.intr_prop[c]; w.intr_quat[c] = q[c]; }
+    return true;
+}
+
+static void point_desc(Workdir& w) {
+    nbc_scene_desc& D = w.desc;
+    D.clump_id = w.cid.data(); D.pos = w.pos.data(); D.local = w.local.data(); D.mass = w.mass.data();
+    D.radius = w.radius.data();
+    D.clump_pos = w.cpos.data(); D.clump_vel = w.cvel.data(); D.clump_quat = w.cquat.data();
+    D.clump_angvel = w.cw.data(); D.clump_prop = w.cprop.data();
+    D.level = w.level.empty() ? nullptr : w.level.data();
+    D.level_cell = w.lcell.empty() ? nullptr : w.lcell.data();
+    D.body_kind = w.kind.empty() ? nullptr : w.kind.data();
+}
+
+bool load_workdir(const std::string& dir, Workdir& w, std::string& err) {
+    w.dir = dir;
+    w.driver = -1;
+    if (!load_par(dir + "/world.par", w, err)) return false;
+    if (!par_scalars(w, err)) return false;
+    nbc_scene_desc& D = w.desc;
+    if (D.n_clump <= 0) { err = "NumberBody and ClumpNum must be positive"; return false; }
 
     // ph (src/dem_subsphere_io.cu:151-193)
     std::string ini = w.par["IniConFile"];
@@ -136,10 +247,7 @@ bool load_workdir(const std::string& dir, Workdir& w, std::string& err) {
             w.cprop[4 * k + 2] >> w.cprop[4 * k + 3];
         if (!ch) { err = "ch.00000000.bt: short or malformed at row " + std::to_string(k); return false; }
     }
-    D.clump_id = w.cid.data(); D.pos = w.pos.data(); D.local = w.local.data(); D.mass = w.mass.data();
-    D.radius = w.radius.data();
-    D.clump_pos = w.cpos.data(); D.clump_vel = w.cvel.data(); D.clump_quat = w.cquat.data();
-    D.clump_angvel = w.cw.data(); D.clump_prop = w.cprop.data();
+    point_desc(w);
     for (int i = 0; i < D.n_sub; i++)
         if (w.cid[i] < 0 || w.cid[i] >= D.n_clump) { err = "clump id out of range in " + ini; return false; }
 
@@ -147,77 +255,99 @@ bool load_workdir(const std::string& dir, Workdir& w, std::string& err) {
     // closed cylinder when only Rocks/CylindWall.bt is present
     const std::string cube = dir + "/Rocks/CubeWall.bt", cyl = dir + "/Rocks/CylindWall.bt";
     if (file_exists(cube)) {
-        std::ifstream f(cube);
-        double v[16];
-        for (int k = 0; k < 16; k++)
-            if (!(f >> v[k])) { err = "Rocks/CubeWall.bt: malformed"; return false; }
-        D.wall = NBC_WALL_CUBE;
-        for (int a = 0; a < 3; a++) {
-            D.cube_half[a] = v[a]; D.cube_centre[a] = v[3 + a]; D.cube_vel[a] = v[6 + a]; D.cube_angvel[a] = v[13 + a];
-        }
+        if (!read_cube(cube, D, err)) return false;
     } else if (file_exists(cyl)) {
-        std::ifstream f(cyl);
-        double v[22];
-        for (int k = 0; k < 22; k++)
-            if (!(f >> v[k])) { err = "Rocks/CylindWall.bt: malformed"; return false; }
-        D.wall = NBC_WALL_CYLINDER;
-        D.cyl_radius = v[0]; D.cyl_half_height = v[1];
-        for (int a = 0; a < 3; a++) {
-            D.cyl_axis[a] = v[2 + a]; D.cyl_centre[a] = v[9 + a]; D.cyl_vel[a] = v[12 + a]; D.cyl_angvel[a] = v[19 + a];
-        }
+        if (!read_cyl(cyl, D, err)) return false;
     } else if (D.is_wall_force) {
         err = "isWallForce set but neither Rocks/CubeWall.bt nor Rocks/CylindWall.bt exists";
         return false;
     }
-
     // intruder (src/dem_penetrator_io.cu:21-116)
     D.intruder = NBC_INTR_NONE;
-    if (w.is_intruder) {
-        const std::string pp = dir + "/Rocks/Penetrator.bt";
-        std::ifstream f(pp);
-        if (!f) { err = "Error! Cannot open " + pp + "!"; return false; }
-        std::string tok;
-        f >> tok;
-        std::string lt = lower(tok);
-        if (lt == "sphere") {
-            D.intruder = NBC_INTR_SPHERE;
-            f >> D.intr_radius;
-            D.intr_half_height = D.intr_radius;
-            D.intr_axis[2] = 1.0;
-        } else if (lt == "cylinder") {
-            D.intruder = NBC_INTR_CYLINDER;
-            f >> D.intr_radius >> D.intr_half_height >> D.intr_axis[0] >> D.intr_axis[1] >> D.intr_axis[2];
-        } else {
-            char* end = nullptr;
-            D.intr_radius = std::strtod(tok.c_str(), &end);
-            if (end == tok.c_str() || *end != '\0') { err = "Error! Unknown penetrator shape '" + tok + "'"; return false; }
-            D.intruder = NBC_INTR_CYLINDER;
-            f >> D.intr_half_height >> D.intr_axis[0] >> D.intr_axis[1] >> D.intr_axis[2];
-        }
-        double q[4];
-        f >> D.intr_prop[0] >> D.intr_prop[1] >> D.intr_prop[2] >> D.intr_prop[3];
-        f >> D.intr_pos[0] >> D.intr_pos[1] >> D.intr_pos[2];
-        f >> D.intr_vel[0] >> D.intr_vel[1] >> D.intr_vel[2];
-        f >> q[0] >> q[1] >> q[2] >> q[3];
-        f >> D.intr_angvel[0] >> D.intr_angvel[1] >> D.intr_angvel[2];
-        for (int c = 0; c < 4; c++) w.intr_quat[c] = q[c];
-        if (!f || D.intr_radius <= 0.0 || D.intr_prop[3] <= 0.0) { err = "Error! Invalid penetrator data in " + pp; return false; }
-        D.intr_motion = NBC_MOTION_CONSTANT_VELOCITY;
-        std::string opt;
-        if (f >> opt) {
-            if (lower(opt) != "motion") { err = "Error! Unknown penetrator option '" + opt + "'"; return false; }
-            std::string m;
-            f >> m;
-            m = lower(m);
-            if (m == "constant_velocity" || m == "constant" || m == "kinematic") D.intr_motion = NBC_MOTION_CONSTANT_VELOCITY;
-            else if (m == "gravity" || m == "dynamic") D.intr_motion = NBC_MOTION_GRAVITY;
-            else if (m == "gravity_after_contact") D.intr_motion = NBC_MOTION_GRAVITY_AFTER_CONTACT;
-            else { err = "Error! Unknown penetrator motion mode '" + m + "'"; return false; }
-        }
-    }
-    D.levels = 1;
+    if (w.is_intruder && !read_penetrator(dir, w, true, err)) return false;
     return true;
 }
+
+// The sphere-only drivers' working directory (class DEMmain): world.par with
+// the same 38 keys, the 21-column ph file named by IniConFile
+// (DEMSphereIo::LoadPhase, src/dem_io.cu:155-202: id, id, Type, Pos, Vel,
+// Quat, AngSpd, Property = Ixx Iyy Izz M, Radius), the driver's wall file (read
+// whatever isWallForce says: the drivers apply the wall unconditionally,
+// src/dem_simulation_cylind.cu:157), Rocks/Penetrator.bt (always read,
+// src/dem_simulation_cylind.cu:54-60) and, for the hgrid driver, grid.bt
+// (DEMSphereIo::LoadGridLevels, src/dem_io.cu:204-248: per level "id
+// cellSize nx ny nz offset id", GridLevels rows; Type is the sphere's level,
+// 0 the coarsest).  Sphere k becomes clump k with one member at its centre.
+bool load_sphere_workdir(const std::string& dir, int driver, Workdir& w, std::string& err) {
+    w.dir = dir;
+    w.driver = driver;
+    if (driver < NBC_DRIVER_CYLINDER || driver > NBC_DRIVER_HGRID) { err = "unknown DEMmain driver"; return false; }
+    if (!load_par(dir + "/world.par", w, err)) return false;
+    if (!par_scalars(w, err)) return false;
+    nbc_scene_desc& D = w.desc;
+    const int n = D.n_sub;
+    D.n_clump = n;
+    std::string ini = w.par["IniConFile"];
+    std::ifstream ph(dir + "/" + ini);
+    if (!ph) { err = "Error! Cannot open " + ini + "!"; return false; }
+    w.cid.resize(n); w.type.resize(n);
+    w.pos.resize(3 * (size_t)n); w.local.assign(3 * (size_t)n, 0.0);
+    w.mass.resize(n); w.radius.resize(n);
+    w.cpos.resize(3 * (size_t)n); w.cvel.resize(3 * (size_t)n); w.cquat.resize(4 * (size_t)n);
+    w.cw.resize(3 * (size_t)n); w.cprop.resize(4 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        double t0, t1;
+        double* p = &w.cpos[3 * (size_t)i];
+        double* v = &w.cvel[3 * (size_t)i];
+        double* q = &w.cquat[4 * (size_t)i];
+        double* a = &w.cw[3 * (size_t)i];
+        double* pr = &w.cprop[4 * (size_t)i];
+        ph >> t0 >> t1 >> w.type[i] >> p[0] >> p[1] >> p[2] >> v[0] >> v[1] >> v[2] >> q[0] >> q[1] >> q[2] >> q[3] >>
+            a[0] >> a[1] >> a[2] >> pr[0] >> pr[1] >> pr[2] >> pr[3] >> w.radius[i];
+        if (!ph) { err = ini + ": short or malformed at row " + std::to_string(i); return false; }
+        w.cid[i] = i;
+        for (int c = 0; c < 3; c++) w.pos[3 * (size_t)i + c] = p[c];
+        w.mass[i] = pr[3];
+    }
+    D.is_wall_force = 1;
+    D.sphere_mode = NBC_SPHERE_KINEMATICS;
+    if (driver == NBC_DRIVER_CUBE) {
+        if (!read_cube(dir + "/Rocks/CubeWall.bt", D, err)) return false;
+        D.sphere_mode |= NBC_SPHERE_CUBE_WALL;
+    } else {
+        if (!read_cyl(dir + "/Rocks/CylindWall.bt", D, err)) return false;
+        if (driver != NBC_DRIVER_HGRID) D.sphere_mode |= NBC_SPHERE_RESET_HISTORY;
+    }
+    if (driver == NBC_DRIVER_SPLIT) {
+        for (int i = 0; i < n; i++)
+            if (w.type[i] < 0 || w.type[i] > 2) { err = ini + ": Type must be 0, 1 or 2 at row " + std::to_string(i); return false; }
+        w.kind = w.type;
+    }
+    if (driver == NBC_DRIVER_HGRID) {
+        const int L = (int)pd(w, "GridLevels");
+        if (L < 1 || L > 6) { err = "GridLevels must be 1 .. 6"; return false; }
+        std::ifstream g(dir + "/grid.bt");
+        if (!g) { err = "Error! Cannot open grid.bt!"; return false; }
+        std::vector<double> cell(L);
+        for (int l = 0; l < L; l++) {
+            int id, nx, ny, nz, off, id2;
+            g >> id >> cell[l] >> nx >> ny >> nz >> off >> id2;
+            if (!g || !(cell[l] > 0)) { err = "grid.bt: short or malformed at level " + std::to_string(l); return false; }
+        }
+        for (int i = 0; i < n; i++)
+            if (w.type[i] < 0 || w.type[i] >= L) { err = ini + ": Type is not a grid level at row " + std::to_string(i); return false; }
+        if (L > 1) {
+            D.levels = L;
+            w.level = w.type;
+            w.lcell = cell;
+        }
+    }
+    D.intruder = NBC_INTR_NONE;
+    if (!read_penetrator(dir, w, w.is_intruder, err)) return false;
+    point_desc(w);
+    return true;
+}
+
 
 // ---------------------------------------------------------------------------
 // writers (src/dem_binary_io.h)
@@ -247,6 +377,24 @@ bool write_ph(const std::string& path, int n, const int* sorted_id, const int* p
     w.raw(pos, 24 * (size_t)n);
     w.raw(local, 24 * (size_t)n);
     w.raw(mass, 8 * (size_t)n);
+    w.raw(radius, 8 * (size_t)n);
+    return w.ok;
+}
+
+// SaveParticles_Bin of the sphere drivers (src/dem_io.cu:313-329)
+bool write_sphere_ph(const std::string& path, int n, const int* sorted_id, const int* part_fix, const int* type,
+                     const double* pos, const double* vel, const double* quat, const double* angvel,
+                     const double* prop, const double* radius) {
+    BinWriter w(path);
+    w.i32(n);
+    w.raw(sorted_id, 4 * (size_t)n);
+    w.raw(part_fix, 4 * (size_t)n);
+    w.raw(type, 4 * (size_t)n);
+    w.raw(pos, 24 * (size_t)n);
+    w.raw(vel, 24 * (size_t)n);
+    w.raw(quat, 32 * (size_t)n);
+    w.raw(angvel, 24 * (size_t)n);
+    w.raw(prop, 32 * (size_t)n);
     w.raw(radius, 8 * (size_t)n);
     return w.ok;
 }

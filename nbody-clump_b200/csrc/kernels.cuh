@@ -120,7 +120,34 @@ constexpr size_t clump_dyn_smem() {
 // the autotuner picks; results do not depend on it); a warp stages 32 J
 // members in shared memory at a time.  J <= 2 fits 128 registers (4 blocks,
 // 16 warps per SM) with a few bytes of spill; J = 4 keeps 3 blocks per SM.
-template <typename R, int J>
+// One attitude step (Attitude_clump_cuk, src/dem_integrate_clumpsphere.cu:
+// 45-90, the expressions of k_clump's own update): the split driver's bodies
+// that turn without their first half-kick use it.
+__device__ __forceinline__ double4 quat_step(double4 q, V3<double> w, V3<double> al, double Dt) {
+    const V3<double> Wb = rot_w2b(q, w), Wdb = rot_w2b(q, al);
+    double4 qd, qdd;
+    qd.x = 0.50 * (Wb.x * q.w - Wb.y * q.z + Wb.z * q.y);
+    qd.y = 0.50 * (Wb.x * q.z + Wb.y * q.w - Wb.z * q.x);
+    qd.z = 0.50 * (-Wb.x * q.y + Wb.y * q.x + Wb.z * q.w);
+    qd.w = 0.50 * (-Wb.x * q.x - Wb.y * q.y - Wb.z * q.z);
+    qdd.x = (Wdb.x * q.w - Wdb.y * q.z + Wdb.z * q.y) * 0.50 + (Wb.x * qd.w - Wb.y * qd.z + Wb.z * qd.y) * 0.50;
+    qdd.y = (Wdb.x * q.z + Wdb.y * q.w - Wdb.z * q.x) * 0.50 + (Wb.x * qd.z + Wb.y * qd.w - Wb.z * qd.x) * 0.50;
+    qdd.z = (-Wdb.x * q.y + Wdb.y * q.x + Wdb.z * q.w) * 0.50 + (-Wb.x * qd.y + Wb.y * qd.x + Wb.z * qd.w) * 0.50;
+    qdd.w = (-Wdb.x * q.x - Wdb.y * q.y - Wdb.z * q.z) * 0.50 + (-Wb.x * qd.x - Wb.y * qd.y - Wb.z * qd.z) * 0.50;
+    const double h2 = 0.5 * Dt * Dt;
+    double4 r;
+    r.x = (q.x + Dt * qd.x) + h2 * qdd.x;
+    r.y = (q.y + Dt * qd.y) + h2 * qdd.y;
+    r.z = (q.z + Dt * qd.z) + h2 * qdd.z;
+    r.w = (q.w + Dt * qd.w) + h2 * qdd.w;
+    const double inv = 1.0 / sqrt(r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w);
+    r.x *= inv; r.y *= inv; r.z *= inv; r.w *= inv;
+    return r;
+}
+
+// SPH: the build for batches with a sphere-driver scene (ScenePar::sphere);
+// the clump path's build carries none of that code.
+template <typename R, int J, bool SPH>
 __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev* __restrict__ dp, int do_pre,
                                                       cudaGraphConditionalHandle cond, int use_cond,
                                                       cudaGraphConditionalHandle loop, int use_loop) {
@@ -311,7 +338,9 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     T = xyzd(d.cT[k]);
                 }
             }
-            if (post_k) {
+            // split driver: only Type 0 takes the closing half-kick
+            // (src/dem_integrate_withglue.cu:140)
+            if (post_k && !(SPH && (P.sphere & SPH_KINDS) && (d.kind[k] & 3) != 0)) {
                 V3<double> ac = pr.w * F;   // pr: the reciprocals 1/I, 1/M
                 ac.z = ac.z + P.gravity;
                 V3<double> al = v3(pr.x * T.x, pr.y * T.y, pr.z * T.z);
@@ -324,6 +353,17 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
         }
         if (do_pre) {
             const double4 cp_old = cp;
+            if (SPH && (P.sphere & SPH_KIN) && mb < me) {
+                // the sphere drivers' first half-kick and attitude leave the
+                // intruder out (src/dem_integrate.cu:20-21,72); one member
+                const int i0 = mem_idx[mb];
+                if ((d.bbits[i0] >> SLOT_INTR) & 1) {
+                    const R4<R>* __restrict__ fi = (const R4<R>*)d.fint;
+                    const R4<R> a = fi[i0], b = fi[(size_t)d.N + i0];
+                    F = F - v3((double)a.x, (double)a.y, (double)a.z);
+                    T = T - v3((double)b.x, (double)b.y, (double)b.z);
+                }
+            }
             V3<double> ac = pr.w * F;   // pr: the reciprocals 1/I, 1/M
             ac.z = ac.z + P.gravity;
             V3<double> al = v3(pr.x * T.x, pr.y * T.y, pr.z * T.z);
@@ -350,6 +390,27 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             q.w = (q.w + Dt * qd.w) + h2 * qdd.w;
             const double inv = 1.0 / sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
             q.x *= inv; q.y *= inv; q.z *= inv; q.w *= inv;
+            if (SPH && (P.sphere & SPH_KINDS)) {
+                // split driver (src/dem_integrate_withglue.cu:3-110).  Its call
+                // passes the original index where the first half-kick expects
+                // Type (src/dem_simulation_split.cu:84-85 against
+                // src/dem_integrate_withglue.cu:113-114), so the kick and the
+                // move go by the body's original index (bits 2-3: 0 free, 1
+                // driven at (-0.2 y, -0.2 x, 0), 2 or more still) and the
+                // attitude by its Type (bits 0-1: turns only for Type 0)
+                const int kd = d.kind[k], ka = kd & 3, kb = (kd >> 2) & 3;
+                if (kb != 0) {
+                    cp = cp_old;
+                    w = xyzd(cw);
+                    v = xyzd(cv);
+                    if (kb == 1) {
+                        v = v3(-0.2 * cp_old.y, -0.2 * cp_old.x, 0.0);
+                        cp.x += Dt * v.x; cp.y += Dt * v.y; cp.z += Dt * v.z;
+                    }
+                    if (ka == 0) q = quat_step(cq, w, al, Dt);
+                }
+                if (ka != 0) q = cq;
+            }
             if (!pre_k) {   // the scene stands still: keep the clump as it is
                 cp = cp_old;
                 v = xyzd(cv);
@@ -416,7 +477,11 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     posw[i] = make_double4(p.x, p.y, p.z, o.w);
                     kv[i] = make_double4(arm.x, arm.y, arm.z, lo[j].w);
                     const int sk = s_sc[warp][kk];
-                    if (len_floor(cn) > d.par[sk].thresh) {
+                    double thr = d.par[sk].thresh;
+                    if (SPH && (d.par[sk].sphere & SPH_KINDS))   // split driver: the free body of the first
+                        thr = ((d.kind[k0 + kk] >> 2) & 3) == 0 ? 0.10 * o.w : INFINITY;   // half-kick at 0.1 r
+                                                                  // (src/dem_integrate_withglue.cu:41)
+                    if (len_floor(cn) > thr) {
                         SceneDyn& y = d.dyn[sk];
                         if (!*(volatile int*)&y.rebuild) atomicExch(&y.rebuild, 1);
                         if (!*(volatile int*)d.any_rebuild) atomicExch(d.any_rebuild, 1);
@@ -1408,7 +1473,13 @@ __device__ __forceinline__ void carry_one(const Dev& d, int p, int s) {
     }
     int q = -1;
     R sign = R(1);
-    {
+    if (P.sphere & SPH_RESET) {
+        // DEMmain::RunSimulation and _Split exchange the history pointers
+        // once more after the list build has carried the histories and
+        // cleared the other buffer (src/dem_simulation_cylind.cu:141,
+        // src/dem_grid.cu:687-749): after a rebuild every pair starts from zero
+        q = -1;
+    } else {
         const int io = d.perm[i], jo = d.perm[j];
         int oo, ot;
         if (P.levels > 1 && d.level2[i] != d.level2[j]) {
@@ -1981,11 +2052,13 @@ constexpr int BD_THREADS = 128;
 // ForcePene_clump_cuk (src/dem_contact_penetrator.cu:8-84,
 // src/dem_sphere_intruder.cuh:20-51, src/dem_force_penetrator_clump.cu:4-182).
 // Writes the summed boundary force/torque where some slot is in contact and
-// the slot mask; the intruder totals go to fixed-point accumulators.
-template <typename R, bool EXPORT>
+// the slot mask; the intruder totals go to fixed-point accumulators.  SPH:
+// the build for batches with a sphere-driver scene (ScenePar::sphere); the
+// clump path's build carries none of that code.
+template <typename R, bool EXPORT, bool SPH>
 __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s);
 
-template <typename R, bool EXPORT>
+template <typename R, bool EXPORT, bool SPH>
 __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__ dp) {
     const Dev& d = *dp;
     if (*d.halt) return;
@@ -1996,11 +2069,11 @@ __global__ void __launch_bounds__(BD_THREADS) k_boundary(const Dev* __restrict__
         // work item w: boundary candidate w - bprefix[s] of scene s
         const int s = S == 1 ? 0 : plan_find(bpre, S, w);
         const int i = d.bidx[d.par[s].sub_off + (w - bpre[s])];
-        boundary_one<R, EXPORT>(d, i, s);
+        boundary_one<R, EXPORT, SPH>(d, i, s);
     }
 }
 
-template <typename R, bool EXPORT>
+template <typename R, bool EXPORT, bool SPH>
 __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
     const double4 pp = d.posr[i];   // issued before the scene's flag is known
     const uint16_t bb_old = d.bbits[i];
@@ -2157,7 +2230,9 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         else Mij = me.m;
         V3<R> hs = v3<R>(0, 0, 0), ht = hs, hr = hs;
         const size_t hb = (size_t)slot * 3 * N;
-        if (bb_old & (1u << slot)) {
+        // the sphere driver's cube wall keeps no history
+        const bool memless = SPH && is_wall && P.wall == WALL_CUBE && (P.sphere & SPH_CUBE);
+        if (!memless && (bb_old & (1u << slot))) {
             R4<R> a = BH[hb + 3 * i], b = BH[hb + 3 * i + 1], c = BH[hb + 3 * i + 2];
             hs = xyz<R>(a); ht = xyz<R>(b); hr = xyz<R>(c);
         }
@@ -2165,9 +2240,21 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         LawOut<R> o;
         boundary_contact<R>(L, me, nd, Apd, Dnd, RVo, wv, ww, Rij, Mij, csm, hs, hr, ht,
                             f, t, o, arm);
-        BH[hb + 3 * i] = pack<R>(o.hs, R(0));
-        BH[hb + 3 * i + 1] = pack<R>(o.ht, R(0));
-        BH[hb + 3 * i + 2] = pack<R>(o.hr, R(0));
+        if (SPH && memless) {
+            // tangential torque only: the moments and the history writes
+            // are commented out there (src/dem_force_cube_wall.cu:86-87,137-141)
+            t = (-(R)Apd) * cross(cvt<R>(nd), o.Ft);
+        } else {
+            BH[hb + 3 * i] = pack<R>(o.hs, R(0));
+            BH[hb + 3 * i + 1] = pack<R>(o.ht, R(0));
+            BH[hb + 3 * i + 2] = pack<R>(o.hr, R(0));
+        }
+        if (SPH && is_intr && (P.sphere & SPH_KIN)) {
+            // the sphere driver's penetrator law adds cohesion
+            // (src/dem_force_penetrator.cu:119-123)
+            const double cf = ((-P.cohesion) * (P.beta * Rij)) * (P.beta * Rij);
+            f = f + cvt<R>(cf * nd);
+        }
         bb_new |= (uint16_t)(1u << slot);
         if (is_intr) {
             iF = iF + f;
@@ -2198,6 +2285,11 @@ __device__ __forceinline__ void boundary_one(const Dev& d, int i, int s) {
         R4<R>* fb = (R4<R>*)d.fbnd;
         fb[i] = pack<R>(wF + iF, R(0));
         fb[N + i] = pack<R>(wT + iT, R(0));
+        if (SPH && (P.sphere & SPH_KIN) && (bb_new & (1u << SLOT_INTR))) {
+            R4<R>* fi = (R4<R>*)d.fint;
+            fi[i] = pack<R>(iF, R(0));
+            fi[N + i] = pack<R>(iT, R(0));
+        }
     }
     if (EXPORT) {
         R4<R>* xp = (R4<R>*)d.xparts;

@@ -31,6 +31,13 @@ constexpr int ERR_NONFINITE = 2;       // non-finite wall input/output (src/dem_
 constexpr int ERR_BAD_CLUMP = 4;       // clump id out of range
 constexpr int ERR_ROW_OVERFLOW = 8;    // a row exceeded BranchLmtLen/2 (reference semantics, export only)
 
+// ScenePar::sphere: the reference's sphere-only drivers where they differ
+// from the clump path (bits 1, 2, 4 are NBC_SPHERE_* of the C ABI)
+constexpr int SPH_KIN = 1;      // first half-kick and attitude without the intruder; penetrator cohesion
+constexpr int SPH_CUBE = 2;     // cube wall without history and without rolling or twisting moment
+constexpr int SPH_RESET = 4;    // pair histories restart from zero at every rebuild
+constexpr int SPH_KINDS = 8;    // body kinds of the split driver (Dev::kind)
+
 struct ScenePar {
     // integration and contact law (world.par, src/dem_parameters.h:49-66)
     double dt, E, nu, mu, damping, gravity, beta, cohesion, thresh;
@@ -55,6 +62,7 @@ struct ScenePar {
     // intruder
     int has_intr, intr_shape, intr_motion, intr_wait;  // shape 0 cylinder 1 sphere; motion 0 kinematic 1 gravity
     double intr_R, intr_H, intr_axis[3], intr_mass, intr_w[3];
+    int sphere;     // SPH_* bits, 0 = the clump path
 };
 
 struct SceneDyn {
@@ -127,6 +135,8 @@ struct Dev {
     void* fsum;       // Real4 [2][N]: force and torque on each subsphere (pairs + walls + intruder),
                       // written on request only (getters, export): the clump pass sums the slots itself
     void* fbnd;       // Real4 [2][N]: wall + intruder force and torque, valid where bbits != 0
+    void* fint;       // Real4 [2][N]: intruder force and torque alone, valid where the intruder bit of
+                      // bbits is set, in SPH_KIN scenes (null when there are none)
     // clumps
     double4* cpos;    // xyz
     double4* cvel;
@@ -135,6 +145,8 @@ struct Dev {
     double4* cprop;   // Ixx Iyy Izz M
     int* mem_cl;      // [N] clump of each member slot (fixed: members stay in their clump's range)
     double4* cinv;    // 1/Ixx 1/Iyy 1/Izz 1/M (correctly rounded divisions, computed once)
+    int* kind;        // [K] body kind of the split driver (0 free, 1 prescribed velocity, 2 fixed),
+                      // read in SPH_KINDS scenes only (null when there are none)
     double4* cF;      // force on clump from the last force pass
     double4* cT;
     int* mem_start;   // [K+1]

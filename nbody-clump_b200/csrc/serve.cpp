@@ -90,7 +90,7 @@ namespace {
 // a scene descriptor with its own copies of every array
 struct SceneCopy {
     nbc_scene_desc d{};
-    std::vector<int> cid, level;
+    std::vector<int> cid, level, kind;
     std::vector<double> pos, local, mass, radius, cpos, cvel, cquat, cw, cprop, lcell;
     explicit SceneCopy(const nbc_scene_desc& s) : d(s) {
         const size_t n = (size_t)s.n_sub, k = (size_t)s.n_clump;
@@ -110,6 +110,7 @@ struct SceneCopy {
         d.clump_prop = cp(s.clump_prop, 4 * k, cprop);
         d.level = s.levels > 1 ? cp(s.level, n, level) : nullptr;
         d.level_cell = s.levels > 1 ? cp(s.level_cell, (size_t)s.levels, lcell) : nullptr;
+        d.body_kind = cp(s.body_kind, k, kind);
     }
 };
 

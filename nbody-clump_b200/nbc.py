@@ -24,6 +24,9 @@ STATUS = {-1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_IO", -4: "ERR_NONFINITE", -5: 
           -6: "ERR_MEMORY", -7: "ERR_STATE"}
 PREC = {"f64": 0, "mixed": 1}
 WALL = {None: 0, "cube": 1, "cylinder": 2}
+# DEMmain drivers of nbc_open_sphere (NBC_DRIVER_*) and the NBC_SPHERE_* bits
+SPHERE_DRIVERS = {"cylinder": 0, "cube": 1, "split": 2, "hgrid": 3}
+SPHERE_KINEMATICS, SPHERE_CUBE_WALL, SPHERE_RESET_HISTORY = 1, 2, 4
 MOTION = {"constant_velocity": 0, "gravity": 1, "gravity_after_contact": 2}
 
 D3 = C.c_double * 3
@@ -52,6 +55,7 @@ class SceneDesc(C.Structure):
         ("intr_radius", C.c_double), ("intr_half_height", C.c_double), ("intr_axis", D3),
         ("intr_prop", D4), ("intr_pos", D3), ("intr_vel", D3), ("intr_angvel", D3),
         ("levels", C.c_int), ("level", P_I), ("level_cell", P_D),
+        ("sphere_mode", C.c_int), ("body_kind", P_I),
     ]
 
 
@@ -113,7 +117,7 @@ class Options(C.Structure):
 
 
 EXPORTED = [
-    "nbc_last_error", "nbc_default_options", "nbc_open", "nbc_run", "nbc_create", "nbc_destroy",
+    "nbc_last_error", "nbc_default_options", "nbc_open", "nbc_open_sphere", "nbc_run", "nbc_create", "nbc_destroy",
     "nbc_step", "nbc_step_export", "nbc_sync", "nbc_num_scenes", "nbc_scene_stats", "nbc_contact_counts",
     "nbc_get_subspheres", "nbc_get_subsphere_body", "nbc_get_clumps", "nbc_get_sub_forces",
     "nbc_get_force_parts", "nbc_get_pairs", "nbc_get_rows", "nbc_get_chain", "nbc_get_pair_forces",
@@ -222,6 +226,11 @@ def scene_desc(scene: dict):
         keep["level_cell"] = np.ascontiguousarray(lv["cell"], dtype=np.float64)
         d.levels = len(keep["level_cell"])
         d.level, d.level_cell = _p(keep["level"], P_I), _p(keep["level_cell"])
+    # the sphere-only drivers' behaviour (NBC_SPHERE_* bits) and split-driver body kinds
+    d.sphere_mode = int(scene.get("sphere_mode", 0))
+    if scene.get("body_kind") is not None:
+        keep["body_kind"] = np.ascontiguousarray(scene["body_kind"], dtype=np.int32)
+        d.body_kind = _p(keep["body_kind"], P_I)
     return d, keep
 
 
@@ -251,6 +260,21 @@ class Engine:
         o.precision, o.use_graph = PREC[precision], int(use_graph)
         h = C.c_void_p()
         _check(L.nbc_open(workdir.encode(), C.byref(o), C.byref(h)))
+        self.h = h
+        self._descs = []
+        return self
+
+    @classmethod
+    def open_sphere(cls, workdir: str, driver: str, precision="f64", use_graph=True):
+        """The sphere-only drivers' drop-in path (DEMmain): driver is one of
+        SPHERE_DRIVERS."""
+        self = cls.__new__(cls)
+        L = lib()
+        o = Options()
+        L.nbc_default_options(C.byref(o))
+        o.precision, o.use_graph = PREC[precision], int(use_graph)
+        h = C.c_void_p()
+        _check(L.nbc_open_sphere(workdir.encode(), SPHERE_DRIVERS[driver], C.byref(o), C.byref(h)))
         self.h = h
         self._descs = []
         return self

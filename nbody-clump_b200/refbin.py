@@ -16,6 +16,15 @@ completed step number (``src/dem_binary_io.h:47-55``).
                        (src/dem_subsphere_io.cu:279-303)
     OutCnt/{Nei,Fcn,Cpt}.N.bin  int32 n; int32 bl; then n x bl int32 / f64x3
                        rows (src/dem_binary_io.h:100-121)
+
+The sphere-only drivers (class DEMmain) write their own particle file:
+
+    OutPart/ph.N.bin   int32 n; int32[n] sorted id; int32[n] original id;
+                       int32[n] Type; f64[n,3] pos; f64[n,3] vel; f64[n,4] quat;
+                       f64[n,3] angvel; f64[n,4] property; f64[n] radius
+                       (src/dem_io.cu:313-329)
+    OutPart/intruder.N.bin  the OutClump/ch layout with the intruder alone
+                       (src/dem_io.cu:331-342)
 """
 from __future__ import annotations
 
@@ -58,6 +67,17 @@ def read_ph(path):
            "clump_id": c.take("<i4", n), "pos": c.take("<f8", 3 * n, (n, 3)),
            "local": c.take("<f8", 3 * n, (n, 3)), "mass": c.take("<f8", n),
            "radius": c.take("<f8", n)}
+    assert c.done(), path
+    return out
+
+
+def read_sphere_ph(path):
+    c = _Cursor(path)
+    n = int(c.take("<i4", 1)[0])
+    out = {"sorted_id": c.take("<i4", n), "part_fix": c.take("<i4", n), "type": c.take("<i4", n),
+           "pos": c.take("<f8", 3 * n, (n, 3)), "vel": c.take("<f8", 3 * n, (n, 3)),
+           "quat": c.take("<f8", 4 * n, (n, 4)), "angvel": c.take("<f8", 3 * n, (n, 3)),
+           "prop": c.take("<f8", 4 * n, (n, 4)), "radius": c.take("<f8", n)}
     assert c.done(), path
     return out
 

@@ -628,6 +628,66 @@ def make_test_spheres(n=400, seed=1, r=1e-3, overlap=0.02, vel=0.5, angvel=200.0
                     cube=cube, cylinder=cyl, intruder=intr)
 
 
+def make_test_sphere_levels(n_side=6, seed=43, R=1.5e-3, ratio=0.40, overlap=0.02, vel=0.5, angvel=200.0,
+                            thresh_ratio=0.0003, dt=2e-7, steps=24, bl=64):
+    """Spheres of two sizes on two grid levels, every sphere in contact: a
+    compressed cubic lattice of radius-R spheres (neighbours overlap by about
+    2 `overlap` R) and, in each lattice layer, a sphere of radius `ratio` R
+    at the centre of every square of four, overlapping those four; a closed
+    cylinder around the lattice whose caps and side press on the outer
+    spheres.  The level table (coarse level 0 for the large spheres, cells
+    of three radii) goes in scene["levels"]."""
+    rng = np.random.default_rng(seed)
+    rho = MATERIAL["rho"]
+    a = 2 * R * (1 - overlap)
+    g = np.arange(n_side) * a
+    big = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    h = (g[:-1] + 0.5 * a)
+    small = np.stack(np.meshgrid(h, h, g, indexing="ij"), -1).reshape(-1, 3)
+    pts = np.concatenate([big, small]) + R
+    rad = np.concatenate([np.full(len(big), R), np.full(len(small), ratio * R)])
+    pts = pts + rng.uniform(-0.02 * overlap * R, 0.02 * overlap * R, pts.shape)
+    K = len(pts)
+    m = rho * 4 / 3 * math.pi * rad ** 3
+    I = 0.4 * m * rad * rad
+    centre = 0.5 * (pts.min(0) + pts.max(0))
+    half_diag = math.sqrt(2) * 0.5 * (n_side - 1) * a
+    cyl = make_cylinder(half_diag + R * (1 - overlap), 0.5 * (n_side - 1) * a + R * (1 - overlap), centre)
+    params = default_params(StepSize=dt, EndStep=steps, OutputInterval=1, Thresh=thresh_ratio * ratio * R,
+                            BranchLmtLen=bl)
+    lo, hi = centre - (half_diag + 2 * R), centre + (half_diag + 2 * R)
+    set_world_box(params, lo, hi)
+    sc = assemble(params, pts, random_unit_quaternions(rng, K), rng.uniform(-vel, vel, (K, 3)),
+                  rng.uniform(-angvel, angvel, (K, 3)), np.stack([I, I, I, m], 1),
+                  [np.zeros((1, 3))] * K, [np.array([x]) for x in rad], [np.array([x]) for x in m],
+                  cylinder=cyl)
+    sc["levels"] = {"level": (rad < R).astype(np.int32), "cell": np.array([3 * R, 3 * ratio * R])}
+    return sc
+
+
+def make_test_split(n=343, seed=44, r=1e-3, offset=(0.05, 0.08), vel=3.0, angvel=200.0, dt=5e-6, steps=24,
+                    kinds=(0.7, 0.15, 0.15), bl=64):
+    """A compressed lattice of one-sphere clumps in a closed cylinder, away
+    from the z axis (so that driven spheres move), with body kinds of the
+    split driver drawn per sphere: free, driven at the prescribed velocity,
+    fixed (scene["body_kind"]).  Free spheres move fast enough to pass a
+    tenth of their radius within a few steps."""
+    sc = make_test_spheres(n=n, seed=seed, r=r, vel=vel, angvel=angvel, intruder=None, dt=dt, steps=steps,
+                           wall="cylinder", bl=bl)
+    shift = np.array([offset[0], offset[1], 0.0])
+    sc["sub"]["pos"] = sc["sub"]["pos"] + shift
+    sc["clump"]["pos"] = sc["clump"]["pos"] + shift
+    sc["cylinder"]["centre"] = sc["cylinder"]["centre"] + shift
+    p = sc["params"]
+    for a, k in enumerate("xyz"):
+        p["WorldOrigin_" + k] += shift[a]
+        p["BoxLowLmt_" + k] += shift[a]
+        p["BoxUpLmt_" + k] += shift[a]
+    rng = np.random.default_rng(seed + 1000)
+    sc["body_kind"] = rng.choice(3, size=len(sc["clump"]["pos"]), p=list(kinds)).astype(np.int32)
+    return sc
+
+
 def make_test_tetra(n_clumps=120, seed=2, r=1e-3, squeeze=0.8, vel=0.5, angvel=200.0,
                     intruder="cylinder", motion="constant_velocity", thresh_ratio=0.0003,
                     dt=2e-7, steps=30, wall="cube", bl=96, sigma=0.15):
@@ -759,6 +819,61 @@ def write_reference_inputs(scene: dict, d: str):
         f.write(f"motion {it['motion']}\n")
 
 
+SPHERE_DRIVER_MODE = {"cylinder": 1 | 4, "cube": 1 | 2, "split": 1 | 4, "hgrid": 1}
+
+
+def as_sphere_driver(scene: dict, driver: str) -> dict:
+    """The scene as the sphere-only driver `driver` runs it (nbc.SPHERE_DRIVERS):
+    the driver's NBC_SPHERE_* bits, its wall, and the split driver's body kinds
+    (scene["body_kind"]) or the hgrid driver's level table (scene["levels"])."""
+    sc = dict(scene)
+    sc["sphere_mode"] = SPHERE_DRIVER_MODE[driver]
+    sc["params"] = dict(scene["params"], isWallForce=1)
+    if driver != "split":
+        sc.pop("body_kind", None)
+    if driver != "hgrid":
+        sc.pop("levels", None)
+    return sc
+
+
+def write_sphere_inputs(scene: dict, d: str, driver: str = "cylinder"):
+    """A working directory for the reference's sphere-only drivers (class
+    DEMmain): world.par, the 21-column ph file (id, id, Type, pos, vel, quat,
+    angular velocity, Ixx Iyy Izz M, radius; src/dem_io.cu:183-185), Rocks/
+    (the driver's wall file and Penetrator.bt, which every driver reads) and,
+    for the hgrid driver, grid.bt (id, cell size, cells per axis, first cell,
+    id per level; src/dem_io.cu:204-248).  The scene holds one-sphere clumps
+    at their centres with sphere k = clump k; Type is the grid level (hgrid),
+    the body kind (split) or 0."""
+    s, c = scene["sub"], scene["clump"]
+    K = len(c["pos"])
+    if len(s["radius"]) != K or np.abs(s["local"]).max() != 0.0 or np.any(s["clump_id"] != np.arange(K)):
+        raise ValueError("the sphere drivers take one-sphere clumps at their centres, sphere k = clump k")
+    p = dict(scene["params"])
+    typ = np.zeros(K, dtype=np.int64)
+    lv = scene.get("levels")
+    cells = [3.0 * float(np.max(s["radius"]))]
+    if driver == "hgrid" and lv is not None:
+        typ = np.asarray(lv["level"], dtype=np.int64)
+        cells = [float(x) for x in lv["cell"]]
+    if driver == "split":
+        typ = np.asarray(scene["body_kind"], dtype=np.int64)
+    p["GridLevels"] = len(cells) if driver == "hgrid" else p.get("GridLevels", 1)
+    write_reference_inputs(dict(scene, params=p), d)
+    with open(os.path.join(d, p["IniConFile"]), "w") as f:
+        for k in range(K):
+            cols = np.concatenate([c["pos"][k], c["vel"][k], c["quat"][k], c["angvel"][k], c["prop"][k],
+                                   [s["radius"][k]]])
+            f.write("%d %d %d %s\n" % (k, k, typ[k], " ".join(_g(v) for v in cols)))
+    if driver == "hgrid":
+        with open(os.path.join(d, "grid.bt"), "w") as f:
+            off = 0
+            for l, cell in enumerate(cells):
+                n = [int(math.ceil(p["WorldSize_" + a] / cell)) for a in "xyz"]
+                f.write("%d %s %d %d %d %d %d\n" % (l, _g(cell), n[0], n[1], n[2], off, l))
+                off += n[0] * n[1] * n[2]
+
+
 def read_reference_inputs(d: str) -> dict:
     """Read a reference working directory (world.par, ph/ch .bt, Rocks/) into
     a scene dict; the inverse of write_reference_inputs."""
@@ -827,10 +942,13 @@ def scene_to_npz(scene: dict, path: str):
     for grp in ("sub", "clump"):
         for k, v in scene[grp].items():
             flat[f"{grp}/{k}"] = np.asarray(v)
-    for grp in ("cube", "cylinder", "intruder"):
+    for grp in ("cube", "cylinder", "intruder", "levels"):
         if scene.get(grp) is not None:
             for k, v in scene[grp].items():
                 flat[f"{grp}/{k}"] = np.asarray(v)
+    for k in ("sphere_mode", "body_kind"):
+        if scene.get(k) is not None:
+            flat["extra/" + k] = np.asarray(scene[k])
     np.savez_compressed(path, **flat)
 
 
@@ -850,6 +968,8 @@ def scene_from_npz(path: str) -> dict:
             elif isinstance(v, (np.str_, str)):
                 v = str(v)
             scene["params"][k] = v
+        elif grp == "extra":
+            scene[k] = v.item() if v.shape == () else v
         else:
             if scene.get(grp) is None:
                 scene[grp] = {}

@@ -18,14 +18,18 @@ Two phases:
     ``OutForce/*.bin``; layouts of ``src/dem_binary_io.h``) and stores a
     compact ``<case>.ref.npz`` in ``--out``.
 
-Cases in SPHERE_PATH run the reference's sphere-only driver instead
-(``oracle/_ref/nbody_sphere_ref``: ``DEMmain::RunSimulation``,
-``src/dem_simulation_cylind.cu:3-211``, the only driver of the reference
-with a closed cylinder wall).  Their scenes are one-sphere clumps with
-LocalPos = 0, written in the sphere format (``ph`` with 21 columns,
-``src/dem_io.cu:155-193``) plus ``Rocks/CylindWall.bt``; the sphere
-driver's ``OutPart/ph.*.bin`` (``src/dem_io.cu:313-329``) gives positions,
-velocities, quaternions and angular velocities at every step.
+Cases in SPHERE_PATH run one of the reference's sphere-only drivers instead
+(``oracle/_ref/nbody_sphere_ref <driver>``: ``DEMmain::RunSimulation``
+(cylinder), ``RunSimulation2`` (cube), ``RunSimulation_Split`` and
+``RunSimulation_HGrid``, ``src/dem_simulation_{cylind,cube,split,hgrid}.cu``).
+Their scenes are one-sphere clumps with LocalPos = 0, written by
+``scenegen.write_sphere_inputs`` in the sphere format (``ph`` with 21
+columns, ``src/dem_io.cu:155-193``, the driver's wall file, and ``grid.bt``
+for the hgrid driver); the driver's ``OutPart/ph.*.bin``
+(``src/dem_io.cu:313-329``) gives positions, velocities, quaternions and
+angular velocities at every step, and with an intruder
+``OutPart/intruder.*.bin`` and ``OutForce/fc.*.bin`` its position and force
+history (and ``OutCnt`` for the cube driver).
 
 The ``.ref.npz`` files are committed next to this script and read by
 ``tests/test_oracle_golden.py`` and the GPU parity tests.
@@ -62,8 +66,20 @@ CASES = {
                                                 steps=24),
     "cfg0_settle": None,
     "cyl_spheres": lambda: sg.make_test_cyl("spheres", seed=31, steps=24, thresh_ratio=1e-3),
+    "sph_cube": lambda: _cohesive(sg.make_test_spheres(n=343, seed=41, intruder="sphere", wall="cube",
+                                                       steps=24), 5e3),
+    "sph_cyl": lambda: sg.make_test_spheres(n=343, seed=42, intruder="cylinder", wall="cylinder", steps=24),
+    "sph_hgrid": lambda: sg.make_test_sphere_levels(seed=43, steps=24),
+    "sph_split": lambda: sg.make_test_split(seed=44, steps=24),
 }
-SPHERE_PATH = {"cyl_spheres"}
+# cases run by the reference's sphere-only driver (oracle/_ref/nbody_sphere_ref <driver>)
+SPHERE_PATH = {"cyl_spheres": "cylinder", "sph_cube": "cube", "sph_cyl": "cylinder", "sph_hgrid": "hgrid",
+               "sph_split": "split"}
+
+
+def _cohesive(sc, c):
+    sc["params"]["Cohesion"] = c
+    return sc
 STEPS = 24
 FORCE_STEPS = (2, 12, 24)
 
@@ -91,50 +107,14 @@ def prepare(ref_dir: str | None, names):
         print("wrote", path, sc["params"]["NumberBody"], "subspheres")
 
 
-def write_sphere_inputs(scene: dict, d: str):
-    """The sphere driver's inputs for a scene of one-sphere clumps: world.par
-    (the same 38 keys), the 21-column ph file (id, id, Type, pos, vel, quat,
-    angular velocity, Ixx Iyy Izz M, radius; src/dem_io.cu:183-185) and
-    Rocks/ (CylindWall.bt, src/dem_cylind_wall_io.cu:41-49; an inert
-    Penetrator.bt, which the driver always reads)."""
-    s, c = scene["sub"], scene["clump"]
-    if len(s["radius"]) != len(c["pos"]) or np.abs(s["local"]).max() != 0.0:
-        raise ValueError("the sphere driver takes one-sphere clumps with LocalPos = 0")
-    if np.any(s["clump_id"] != np.arange(len(c["pos"]))):
-        raise ValueError("sphere k must be clump k")
-    sg.write_reference_inputs(scene, d)   # world.par and Rocks/, as for the clump path
-    with open(os.path.join(d, scene["params"]["IniConFile"]), "w") as f:
-        for k in range(len(c["pos"])):
-            cols = np.concatenate([c["pos"][k], c["vel"][k], c["quat"][k], c["angvel"][k], c["prop"][k],
-                                   [s["radius"][k]]])
-            f.write("%d %d 0 %s\n" % (k, k, " ".join(sg._g(v) for v in cols)))
-
-
-def read_sphere_ph(path: str) -> dict:
-    """OutPart/ph.N.bin of the sphere driver (src/dem_io.cu:313-329): int32 n,
-    int32 sortedParticleID[n], ParticleID[n], Type[n], then double3 Pos, Vel,
-    double4 Quat, double3 AngSpd, double4 Property, double Radius."""
-    b = open(path, "rb").read()
-    n = int(np.frombuffer(b, np.int32, 1, 0)[0])
-    o = 4
-    out = {}
-    for key, dt, w in (("sorted_id", np.int32, 1), ("part_fix", np.int32, 1), ("type", np.int32, 1),
-                       ("pos", np.float64, 3), ("vel", np.float64, 3), ("quat", np.float64, 4),
-                       ("angvel", np.float64, 3), ("prop", np.float64, 4), ("radius", np.float64, 1)):
-        a = np.frombuffer(b, dt, n * w, o)
-        o += a.nbytes
-        out[key] = a.reshape(n, w) if w > 1 else a.copy()
-    if o != len(b):
-        raise ValueError(f"{path}: {len(b) - o} trailing bytes")
-    return out
-
-
 def run_sphere_case(binary: str, name: str, out: str, keep: bool):
     sc = sg.scene_from_npz(os.path.join(HERE, f"{name}.scene.npz"))
     work = tempfile.mkdtemp(prefix=f"ref_{name}_")
-    write_sphere_inputs(sc, work)
+    driver = SPHERE_PATH[name]
+    sg.write_sphere_inputs(sc, work, driver)
     t0 = time.time()
-    r = subprocess.run([binary], cwd=work, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, timeout=900)
+    r = subprocess.run([binary, driver], cwd=work, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       timeout=900)
     wall = time.time() - t0
     if r.returncode != 0:
         print(r.stdout.decode(errors="replace")[-3000:])
@@ -143,9 +123,21 @@ def run_sphere_case(binary: str, name: str, out: str, keep: bool):
     steps = p["EndStep"] - p["StartStep"]
     res = {"wall_s": np.array(wall), "steps": np.array(steps)}
     for s in range(p["OutputInterval"], steps + 1, p["OutputInterval"]):
-        ph = read_sphere_ph(os.path.join(work, "OutPart", "ph.%08d.bin" % s))
+        ph = refbin.read_sphere_ph(os.path.join(work, "OutPart", "ph.%08d.bin" % s))
         for k in ("part_fix", "pos", "vel", "quat", "angvel"):
             res[f"s{s}/{k}"] = ph[k]
+        if p["isIntruder"]:
+            it = refbin.read_ch(os.path.join(work, "OutPart", "intruder.%08d.bin" % s))
+            fc = refbin.read_fc(os.path.join(work, "OutForce", "fc.%08d.bin" % s))
+            res[f"s{s}/intr_pos"] = it["pos"][0]
+            res[f"s{s}/intr_force"] = fc["force"]
+    if p["isIntruder"] and driver == "cube":
+        for s in range(2 * p["OutputInterval"], steps + 1, 2 * p["OutputInterval"]):
+            nei = refbin.read_cnt(os.path.join(work, "OutCnt", "Nei.%08d.bin" % s), np.int32)
+            rows, slots = np.nonzero(nei >= 0)
+            res[f"c{s}/rows"] = rows.astype(np.int32)
+            res[f"c{s}/slots"] = slots.astype(np.int16)
+            res[f"c{s}/nei"] = nei[rows, slots].astype(np.int32)
     np.savez_compressed(os.path.join(out, f"{name}.ref.npz"), **res)
     print(f"{name}: {steps} steps in {wall:.2f} s wall (reference sphere driver, incl. file IO)")
     if not keep:
