@@ -506,25 +506,27 @@ def run_batch(args):
     w.close()
     # launch shapes for the batch measured on it (untimed); the plain arm keeps the defaults
     tuned = nbc.autotune(scenes, precision=args.precision, trial_steps=100) if args.autotune else None
-    t0 = time.perf_counter()
-    b = nbc.Batch(scenes, tuned=tuned, **opts)
-    t1 = time.perf_counter()
-    b.step(args.steps)
-    b.sync()
-    t2 = time.perf_counter()
+    with ClockSampler(0) as clk_b:
+        t0 = time.perf_counter()
+        b = nbc.Batch(scenes, tuned=tuned, **opts)
+        t1 = time.perf_counter()
+        b.step(args.steps)
+        b.sync()
+        t2 = time.perf_counter()
     last = b.engines[0].clumps()
     b.close()
     bc, bs = t1 - t0, t2 - t1
     pc = ps = 0.0
-    for sc in scenes:
-        t0 = time.perf_counter()
-        e = nbc.Engine([sc], **opts)
-        t1 = time.perf_counter()
-        e.step(args.steps)
-        e.sync()
-        ps += time.perf_counter() - t1
-        pc += t1 - t0
-        e.close()
+    with ClockSampler(0) as clk_p:
+        for sc in scenes:
+            t0 = time.perf_counter()
+            e = nbc.Engine([sc], **opts)
+            t1 = time.perf_counter()
+            e.step(args.steps)
+            e.sync()
+            ps += time.perf_counter() - t1
+            pc += t1 - t0
+            e.close()
     work = n_sub * args.steps
     arm = lambda c, st: {"create_s": c, "step_s": st, "scenes_per_s": args.scenes / (c + st),
                          "subsphere_steps_per_s": work / st}
@@ -542,6 +544,7 @@ def run_batch(args):
             "scene0_after": {"mean_height_m": float(last["pos"][:, 2].mean()),
                              "mean_speed_m_s": float(np.linalg.norm(last["vel"], axis=1).mean())},
             "cpu_baseline_scene0": cpu,
+            "clocks": {"batched": clk_b.summary(), "plain": clk_p.summary()},
             "dtype": "f32 contact law, f64 positions/quaternions" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded numpy beds)"}
     print(json.dumps(line), flush=True)

@@ -123,7 +123,7 @@ typedef struct {
     double pair_slack;  /* pair capacity = slack * pairs of the first list; 0 = 1.6 and at least
                            the reference's own n_sub * BranchLmtLen/2 as far as 30% of free memory allows */
     int search_lanes;   /* lanes per subsphere in the neighbour search: 8, 16 or 32 (0 = 8) */
-    int clump_batch;    /* members each lane of the clump pass loads at a time: 1, 2 or 4 (0 = 2) */
+    int clump_batch;    /* members each lane of the clump pass loads at a time: 1, 2 or 4 (0 = 1) */
     int pair_blocks;    /* blocks per SM of the pair kernel's grid: 2 .. 16 (0 = 12) */
 } nbc_options;
 

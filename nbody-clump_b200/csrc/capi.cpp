@@ -495,11 +495,11 @@ nbc_status nbc_autotune(const nbc_scene_desc* const* scenes, int n, nbc_options*
         };
         nbc_options best = *opt;
         best.search_lanes = 8;
-        best.clump_batch = 2;
+        best.clump_batch = 1;
         best.pair_blocks = 12;
         best.use_graph = 1;
         double tb = trial(best);
-        const int lanes[] = {16, 32}, batch[] = {1, 4}, blocks[] = {4, 8, 16};
+        const int lanes[] = {16, 32}, batch[] = {2, 4}, blocks[] = {4, 8, 16};
         for (int x : lanes) {
             nbc_options o = best;
             o.search_lanes = x;

@@ -729,7 +729,7 @@ class EngineT final : public EngineBase {
     bool has_kinds_ = false;    // some scene has split-driver body kinds (Dev::kind)
     bool first_list_ = true;
     int search_lanes_ = 8;
-    int clump_batch_ = 2;    // members per lane per load batch of the clump pass
+    int clump_batch_ = 1;    // members per lane per load batch of the clump pass
     int pair_bps_ = 12;      // blocks per SM of the pair kernel's grid
     int sm_count_ = 148;
     int ring_len_ = 1;
@@ -837,7 +837,7 @@ class EngineT final : public EngineBase {
         mem_.stream = stream_;
         DevMem::keep_pool(opt_.device);
         search_lanes_ = opt_.search_lanes == 16 || opt_.search_lanes == 32 ? opt_.search_lanes : 8;
-        clump_batch_ = opt_.clump_batch == 1 || opt_.clump_batch == 4 ? opt_.clump_batch : 2;
+        clump_batch_ = opt_.clump_batch == 2 || opt_.clump_batch == 4 ? opt_.clump_batch : 1;
         // the clump pass's staged contact records (dynamic shared memory past the 48 KB default)
         CK(cudaFuncSetAttribute(k_clump<R, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 1>()));
         CK(cudaFuncSetAttribute(k_clump<R, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)clump_dyn_smem<R, 2>()));

@@ -6,10 +6,12 @@
 //                pose of every member subsphere (+ rebuild test); one extra
 //                thread per scene advances the intruder.
 //   [rebuild]    only when some scene's subsphere moved more than Thresh
-//                since that scene's last rebuild: hash, radix sort, cell
-//                ranges, reorder, count/scan/fill of the half pair list in
-//                the reference's traversal order, back references, history
-//                carry, clump member lists.
+//                since that scene's last rebuild: hash with cell counts,
+//                counting sort by cell (each cell's range in subsphere
+//                order: the reference's stable sort), reorder and cell
+//                table, count/scan/fill of the half pair list in the
+//                reference's traversal order, back references, history
+//                carry, near rows, clump member lists.
 //   k_pairs      per near pair: overlap test, the law once for both
 //                subspheres of a touching pair, the new spring history, the
 //                force and torque on each side into its near-row slot
@@ -105,21 +107,27 @@ __device__ __forceinline__ bool scene_post(const SceneDyn& y, int post, int L) {
 }
 constexpr int CL_THREADS = 128;
 constexpr int CL_WARPS = CL_THREADS / 32;
-// staged contact records per warp: CL_STAGE per member of a chunk on
+// staged contact records per warp: cl_stage<J>() per member of a chunk on
 // average; a lane whose members would overflow the warp's records sums from
 // global memory directly (same order, same result).  Dynamic shared memory.
-constexpr int CL_STAGE = 4;
-// member positions kept from the member sums for the poses (the first
-// CL_POS members of a warp's range; later ones are read again)
-constexpr int CL_POS = 128;
+// Four records per member at J <= 2 (a shallower stage at J = 2 sends more
+// lanes to the unstaged sums: 46.6 against 35.9 µs per cfg1 step); two at
+// J = 4, whose 168 registers allow 3 blocks per SM that four records' 104 KB
+// per block would cut to 2.
+template <int J>
+__host__ __device__ constexpr int cl_stage() {
+    return J == 4 ? 2 : 4;
+}
 template <typename R, int J>
 constexpr size_t clump_dyn_smem() {
-    return (size_t)CL_WARPS * CL_STAGE * 32 * J * sizeof(SlotRec<R>) + (size_t)CL_WARPS * CL_POS * sizeof(double4);
+    return (size_t)CL_WARPS * cl_stage<J>() * 32 * J * sizeof(SlotRec<R>);
 }
 // J: members each lane keeps in flight per batch of loads (a launch shape
 // the autotuner picks; results do not depend on it); a warp stages 32 J
 // members in shared memory at a time.  J <= 2 fits 128 registers (4 blocks,
-// 16 warps per SM) with a few bytes of spill; J = 4 keeps 3 blocks per SM.
+// 16 warps per SM, of which J = 2's 60 KB of shared memory leaves 3) with a
+// few bytes of spill; J = 4 keeps 3 blocks per SM.  J = 1 is the default
+// (the fastest on the cfg1 and cfg3 states).
 // One attitude step (Attitude_clump_cuk, src/dem_integrate_clumpsphere.cu:
 // 45-90, the expressions of k_clump's own update): the split driver's bodies
 // that turn without their first half-kick use it.
@@ -217,9 +225,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const int2* __restrict__ nrb = d.nrb;
             const uint16_t* __restrict__ bbits = d.bbits;
             const size_t N = (size_t)d.N, cap = (size_t)d.cap;
-            SlotRec<R>* stage = (SlotRec<R>*)cl_dsm + (size_t)warp * CL_STAGE * CL_CHUNK;
-            double4* spos = (double4*)(cl_dsm + (size_t)CL_WARPS * CL_STAGE * CL_CHUNK * sizeof(SlotRec<R>)) +
-                            (size_t)warp * CL_POS;
+            SlotRec<R>* stage = (SlotRec<R>*)cl_dsm + (size_t)warp * cl_stage<J>() * CL_CHUNK;
             F = v3(0.0, 0.0, 0.0);
             T = F;
             for (int c0 = M0; c0 < M1; c0 += CL_CHUNK) {
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                     if (lane >= o) rbase += y;
                 }
                 rbase -= nrec;
-                const bool staged = rbase + nrec <= CL_STAGE * CL_CHUNK;
+                const bool staged = rbase + nrec <= cl_stage<J>() * CL_CHUNK;
                 SlotRec<R>* st = stage + rbase;
                 if (staged) {
                     int o = 0;
@@ -300,8 +306,6 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
                             tr = tr + xyz<R>(fbd[N + idx[j]]);
                         }
                     }
-                    const int mr = c0 + 32 * j + lane - M0;
-                    if (mr < CL_POS) spos[mr] = ps[j];   // for the poses below
                     const V3<double> r = v3(ps[j].x - s_cl[warp][0][kk], ps[j].y - s_cl[warp][1][kk],
                                             ps[j].z - s_cl[warp][2][kk]);
                     const V3<double> f = v3((double)fr.x, (double)fr.y, (double)fr.z);
@@ -435,8 +439,6 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
             const double4* __restrict__ lom = d.lom;
             double4* __restrict__ cum = d.cum;
             double4* __restrict__ posw = d.posr;
-            const double4* spos = (const double4*)(cl_dsm + (size_t)CL_WARPS * CL_STAGE * CL_CHUNK * sizeof(SlotRec<R>)) +
-                                  (size_t)warp * CL_POS;
             // J members per lane at a time: all indices, then all member
             // records, in flight together
             constexpr int JP = J;
@@ -452,10 +454,8 @@ __global__ void __launch_bounds__(CL_THREADS, J <= 2 ? 4 : 3) k_clump(const Dev*
 #pragma unroll
                 for (int j = 0; j < JP; j++) {
                     const int i = idx[j] < 0 ? 0 : idx[j];
-                    const int mr = c0 + 32 * j + lane - M0;
                     lo[j] = lom[i];
-                    // the member sums of this step kept the position
-                    old[j] = post && mr < CL_POS ? spos[mr] : posw[i];
+                    old[j] = posw[i];
                     cu[j] = cum[i];
                 }
 #pragma unroll
@@ -768,7 +768,8 @@ static __global__ void __launch_bounds__(SC_THREADS) k_scan1(int* __restrict__ a
 }
 
 // --- LSD radix sort, 8-bit digits, stable (the reference sorts with CUB's
-// stable DeviceRadixSort, src/dem_grid.cu:278-305) ------------------------
+// stable DeviceRadixSort, src/dem_grid.cu:278-305); the allocation-free
+// sort (noalloc.cu) uses it, the engine's rebuild sorts by counting --------
 constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
 
 // The plan of a rebuild (one block).  Rebuilt scenes are listed in ascending

@@ -18,7 +18,7 @@ def test_every_launch_shape_gives_the_same_results():
     clump states and lists for every value the autotuner tries."""
     sc = nbc.with_levels(sg.make_test_poly(n_clumps=150, seed=5))
     ref = None
-    for shape in ({}, {"search_lanes": 16}, {"search_lanes": 32}, {"clump_batch": 1}, {"clump_batch": 4},
+    for shape in ({}, {"search_lanes": 16}, {"search_lanes": 32}, {"clump_batch": 2}, {"clump_batch": 4},
                   {"pair_blocks": 4}, {"pair_blocks": 16}):
         e = nbc.Engine([sc], precision="mixed", tuned=shape)
         e.step(24)
