@@ -135,7 +135,12 @@ struct nbo_scene {
     double* lcell;         /* [levels] */
     int (*ldim)[3];        /* [levels] */
     int* loff;             /* [levels] */
+    /* sphere-only drivers */
+    int sphere;            /* SPH_* bits */
+    int* kind;             /* [K] split driver Type per sphere (= clump) */
+    d3* scum;              /* [K] CumPos of the sphere drivers */
 };
+enum { SPH_KIN = 1, SPH_CUBE = 2, SPH_RESET = 4 };
 
 static int g_threads = 1;
 void nbo_set_threads(int n) { g_threads = n > 0 ? n : 1; }
@@ -308,6 +313,12 @@ nbo_scene* nbo_create(const nbo_desc* d) {
     }
     s->mem_order = (int*)xcalloc(N, sizeof(int));
     s->mem_start = (int*)xcalloc(K + 1, sizeof(int));
+    s->sphere = d->sphere_mode;
+    if (s->sphere) s->scum = (d3*)xcalloc(K, sizeof(d3));
+    if (d->body_kind) {
+        s->kind = (int*)xcalloc(K, sizeof(int));
+        memcpy(s->kind, d->body_kind, K * sizeof(int));
+    }
     return s;
 }
 
@@ -322,7 +333,7 @@ void nbo_destroy(nbo_scene* s) {
                     s->RVn_i, s->pe_Dv, s->pe_Dv_pre, s->pe_Dt, s->pe_Dt_pre, s->pe_Dr,
                     s->pe_Dr_pre, s->LcFlg, s->totF, s->totT, s->cpos, s->cvel, s->cw, s->cFc,
                     s->cTc, s->cq, s->cprop, s->mem_order, s->mem_start, s->level, s->lcell,
-                    s->ldim, s->loff};
+                    s->ldim, s->loff, s->kind, s->scum};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     for (int f = 0; f < 6; f++)
         for (int h = 0; h < 3; h++) { free(s->wc_hist[f][h]); free(s->wc_hist_pre[f][h]); }
@@ -396,6 +407,96 @@ static void clump_integrate_after(nbo_scene* s) {
         T.z = (1.0 / P.z) * T.z;
         s->cvel[i] = add3(s->cvel[i], mul3(0.5 * Dt, F));
         s->cw[i] = add3(s->cw[i], mul3(0.5 * Dt, T));
+    }
+}
+
+/* The sphere drivers' integrator, one sphere per clump (sphere i of the
+ * sorted order is clump c = clump_id[i], LocalPos = 0):
+ * Integrate_Before_cuk + Attitude_cuk (src/dem_integrate.cu:3-100): the
+ * first half-kick and the attitude from the contact and wall force and
+ * torque only, the displacement accumulated in CumPos.  The split driver
+ * (src/dem_integrate_withglue.cu:3-110) is called with the original index
+ * where its first half-kick expects Type (src/dem_simulation_split.cu:84-85):
+ * its kick and move go by original index (0 free with the 0.1 r rebuild
+ * test, 1 driven at (-0.2 y, -0.2 x, 0), 2 and above still), its attitude
+ * by Type (turns only for Type 0). */
+static void sphere_quat(nbo_scene* s, int c, d3 W, d3 T) {
+    double Dt = s->dt;
+    d4 q = s->cq[c], qd, qdd;
+    double m[3][3];
+    quat2dcm(q, m);
+    d3 Wb = map3(m, W), Wdb = map3(m, T);
+    qd.x = 0.50 * (Wb.x * q.w - Wb.y * q.z + Wb.z * q.y);
+    qd.y = 0.50 * (Wb.x * q.z + Wb.y * q.w - Wb.z * q.x);
+    qd.z = 0.50 * (-Wb.x * q.y + Wb.y * q.x + Wb.z * q.w);
+    qd.w = 0.50 * (-Wb.x * q.x - Wb.y * q.y - Wb.z * q.z);
+    qdd.x = (Wdb.x * q.w - Wdb.y * q.z + Wdb.z * q.y) * 0.50 + (Wb.x * qd.w - Wb.y * qd.z + Wb.z * qd.y) * 0.50;
+    qdd.y = (Wdb.x * q.z + Wdb.y * q.w - Wdb.z * q.x) * 0.50 + (Wb.x * qd.z + Wb.y * qd.w - Wb.z * qd.x) * 0.50;
+    qdd.z = (-Wdb.x * q.y + Wdb.y * q.x + Wdb.z * q.w) * 0.50 + (-Wb.x * qd.y + Wb.y * qd.x + Wb.z * qd.w) * 0.50;
+    qdd.w = (-Wdb.x * q.x - Wdb.y * q.y - Wdb.z * q.z) * 0.50 + (-Wb.x * qd.x - Wb.y * qd.y - Wb.z * qd.z) * 0.50;
+    q = add4(add4(q, mul4(Dt, qd)), mul4(0.5 * Dt * Dt, qdd));
+    double nrm = sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    s->cq[c] = mul4(1.0 / nrm, q);
+}
+
+static d3 scale_inertia(d4 P, d3 T) {
+    T.x = (1.0 / P.x) * T.x;
+    T.y = (1.0 / P.y) * T.y;
+    T.z = (1.0 / P.z) * T.z;
+    return T;
+}
+
+static void sphere_integrate_before(nbo_scene* s) {
+    double Dt = s->dt;
+    int flag = 0;
+    for (int i = 0; i < s->N; i++) {
+        int c = s->clump_id[i];
+        int kb = s->kind ? (c < 3 ? c : 3) : 0;
+        d4 P = s->cprop[c];
+        if (kb == 0) {
+            d3 F = add3(s->Fc[i], s->Fw[i]);
+            d3 T = scale_inertia(P, add3(s->Tc[i], s->Tw[i]));
+            F = mul3(1.0 / P.w, F);
+            F.z = F.z + s->gravity;
+            d3 dist = add3(mul3(Dt, s->cvel[c]), mul3(0.5 * Dt * Dt, F));
+            s->scum[c] = add3(s->scum[c], dist);
+            s->cpos[c] = add3(s->cpos[c], dist);
+            s->cvel[c] = add3(s->cvel[c], mul3(0.5 * Dt, F));
+            s->cw[c] = add3(s->cw[c], mul3(0.5 * Dt, T));
+            double thr = s->kind ? 0.10 * s->radius[i] : s->thresh;
+            if (length3(s->scum[c]) > thr) flag = 1;
+        } else if (kb == 1) {
+            d3 p = s->cpos[c];
+            d3 v = mk3(-0.2 * p.y, -0.2 * p.x, 0.0);
+            d3 dist = mul3(Dt, v);
+            s->scum[c] = add3(s->scum[c], dist);
+            s->cpos[c] = add3(p, dist);
+            s->cvel[c] = v;
+        }
+        s->pos[i] = s->cpos[c];
+    }
+    if (flag && s->update == 0) s->update = 1;
+    for (int i = 0; i < s->N; i++) {
+        int c = s->clump_id[i];
+        if (s->kind && s->kind[c] != 0) continue;
+        sphere_quat(s, c, s->cw[c], scale_inertia(s->cprop[c], add3(s->Tc[i], s->Tw[i])));
+    }
+}
+
+/* Integrate_After_cuk (src/dem_integrate.cu:104-146; the split driver's only
+ * for Type 0, src/dem_integrate_withglue.cu:136-160) */
+static void sphere_integrate_after(nbo_scene* s) {
+    double Dt = s->dt;
+    for (int i = 0; i < s->N; i++) {
+        int c = s->clump_id[i];
+        if (s->kind && s->kind[c] != 0) continue;
+        d4 P = s->cprop[c];
+        d3 F = add3(add3(s->Fc[i], s->Fw[i]), s->Fi[i]);
+        d3 T = scale_inertia(P, add3(add3(s->Tc[i], s->Tw[i]), s->Ti[i]));
+        F = mul3(1.0 / P.w, F);
+        F.z = F.z + s->gravity;
+        s->cvel[c] = add3(s->cvel[c], mul3(0.5 * Dt, F));
+        s->cw[c] = add3(s->cw[c], mul3(0.5 * Dt, T));
     }
 }
 
@@ -828,6 +929,8 @@ static void pair_force(nbo_scene* s) {
         ARMj = sub3(ARMj, mul3(An, DistU));
         d3 Vrel = sub3(s->cvel[cJ], s->cvel[cI]);
         d3 Vrot = sub3(cross3(s->cw[cJ], ARMj), cross3(s->cw[cI], ARMi));
+        if (s->sphere & SPH_KIN)   /* ContactForce_cuk, src/dem_force_particle.cu:87-89 */
+            Vrot = add3(mul3(An, cross3(DistU, s->cw[cJ])), mul3(Ap, cross3(DistU, s->cw[cI])));
         d3 Vtot = add3(Vrel, Vrot);
         double ERR = dot3(DistU, Vtot);
         d3 Vnor = mul3(ERR, DistU);
@@ -905,10 +1008,11 @@ static void sum_cont_force(nbo_scene* s) {
  * 16-183).  The cylinder wall uses the same law (ForceWall_cuk,
  * src/dem_force_cylind_wall.cu:3-139) with DistU = RVn/|RVn| and Ap = |RVn|. */
 static void wall_law(nbo_scene* s, int i, d3 RVo, d3 DistU, double Ap, double Dn, d3 Wv, d3 Ww,
-                     d3* Dv_pre, d3* Dt_pre, d3* Dr_pre, d3* Dv, d3* Dt, d3* Dr) {
+                     d3* Dv_pre, d3* Dt_pre, d3* Dr_pre, d3* Dv, d3* Dt, d3* Dr, int memless) {
     double dt = s->dt;
     int c = s->clump_id[i];
     d3 H = Dv_pre[i], Mr = Dr_pre[i], Mt = Dt_pre[i];
+    if (memless) H = Mr = Mt = mk3(0, 0, 0);
     double Rij = s->radius[i], Mij = s->mass[i];
     double Kn = 2.0 * s->E * sqrt(Rij * Dn) / (3.0 * (1.0 - s->nu * s->nu));
     double Cn = s->damping * sqrt(Kn * Mij);
@@ -926,6 +1030,8 @@ static void wall_law(nbo_scene* s, int i, d3 RVo, d3 DistU, double Ap, double Dn
     d3 Vwall = cross3(Ww, RVo);
     d3 Vrel = sub3(s->cvel[c], Wv);
     d3 Vrot = sub3(cross3(Arm, s->cw[c]), Vwall);
+    if (s->sphere & SPH_KIN)   /* the sphere walls, src/dem_force_cylind_wall.cu:55, dem_force_cube_wall.cu:55 */
+        Vrot = sub3(mul3(Ap, cross3(DistU, s->cw[c])), Vwall);
     d3 Vtot = add3(Vrel, Vrot);
     double ERR = dot3(DistU, Vtot);
     d3 Vnor = mul3(ERR, DistU);
@@ -944,6 +1050,9 @@ static void wall_law(nbo_scene* s, int i, d3 RVo, d3 DistU, double Ap, double Dn
     }
     s->Fw[i] = add3(add3(s->Fw[i], nf), tf);
     s->Tw[i] = sub3(s->Tw[i], mul3(Ap, cross3(DistU, tf)));
+    /* the sphere cube wall stops here: its moment update and history
+     * writes are commented out (src/dem_force_cube_wall.cu:137-141) */
+    if (memless) return;
     d3 Dth = mul3(dt, sub3(s->cw[c], Ww));
     double DthL = dot3(Dth, DistU);
     d3 DthT = mul3(DthL, DistU);
@@ -1007,10 +1116,21 @@ static int cube_wall(nbo_scene* s) {
             d3 RVn = sub3(RV, f[k].RVo);
             double Ap = dot3(RVn, f[k].n);
             double Dn = r - Ap;
+            d3 n = f[k].n;
+            int memless = (s->sphere & SPH_CUBE) != 0;
+            if (memless) {
+                /* CubeWallInteraction_cuk / ForceWall_Cube_cuk
+                 * (src/dem_force_cube_wall.cu:24-40,175-296): the normal and
+                 * lever from RVn itself */
+                Dn = r - length3(RVn);
+                double DistL = sqrt(RVn.x * RVn.x + RVn.y * RVn.y + RVn.z * RVn.z);
+                n = mul3(1.0 / DistL, RVn);
+                Ap = DistL;
+            }
             if (Dn <= 0.0) continue;
-            wall_law(s, i, f[k].RVo, f[k].n, Ap, Dn, s->cube_v, s->cube_w,
+            wall_law(s, i, f[k].RVo, n, Ap, Dn, s->cube_v, s->cube_w,
                      s->wc_hist_pre[k][0], s->wc_hist_pre[k][1], s->wc_hist_pre[k][2],
-                     s->wc_hist[k][0], s->wc_hist[k][1], s->wc_hist[k][2]);
+                     s->wc_hist[k][0], s->wc_hist[k][1], s->wc_hist[k][2], memless);
         }
         if (!finite3(s->Fw[i]) || !finite3(s->Tw[i])) bad = 1;
     }
@@ -1044,7 +1164,7 @@ static void cylinder_wall(nbo_scene* s) {
             d3 DistU = mul3(1.0 / DistL, RVn);
             wall_law(s, i, RVo, DistU, DistL, Dn, s->cyl_v, s->cyl_w,
                      s->cy_hist_pre[k][0], s->cy_hist_pre[k][1], s->cy_hist_pre[k][2],
-                     s->cy_hist[k][0], s->cy_hist[k][1], s->cy_hist[k][2]);
+                     s->cy_hist[k][0], s->cy_hist[k][1], s->cy_hist[k][2], 0);
         }
     }
 }
@@ -1161,6 +1281,8 @@ static void pene_force(nbo_scene* s) {
         d3 Vwall = cross3(s->intr_w, s->RVo_i[i]);
         d3 Vrel = sub3(s->cvel[c], s->intr_v);
         d3 Vrot = sub3(cross3(Arm, s->cw[c]), Vwall);
+        if (s->sphere & SPH_KIN)   /* ForcePene_cuk, src/dem_force_penetrator.cu:83-84 */
+            Vrot = sub3(mul3(Ap, cross3(DistU, s->cw[c])), Vwall);
         d3 Vtot = add3(Vrel, Vrot);
         double ERR = dot3(DistU, Vtot);
         d3 Vnor = mul3(ERR, DistU);
@@ -1177,9 +1299,12 @@ static void pene_force(nbo_scene* s) {
         } else {
             th = sub3(tf, mul3(Cs, Vtan));
         }
-        s->Fi[i] = add3(nf, tf);
+        /* the clump law has no cohesion here; the sphere driver's adds
+         * -Cohesion (beta R*)^2 n (src/dem_force_penetrator.cu:119-123) */
+        d3 coh = (s->sphere & SPH_KIN) ? mul3(((-s->cohesion) * br) * br, DistU) : mk3(0, 0, 0);
+        s->Fi[i] = (s->sphere & SPH_KIN) ? add3(add3(nf, tf), coh) : add3(nf, tf);
         s->Ti[i] = mul3(-Ap, cross3(DistU, tf));
-        s->peneTc[i] = mul3(-1.0, cross3(s->RVo_i[i], add3(add3(nf, tf), mk3(0, 0, 0))));
+        s->peneTc[i] = mul3(-1.0, cross3(s->RVo_i[i], add3(add3(nf, tf), coh)));
         s->Fcn_i[i] = nf;
         s->Fct_i[i] = tf;
         d3 Dth = mul3(dt, sub3(s->cw[c], s->intr_w));
@@ -1315,13 +1440,23 @@ static void exchange_walls(nbo_scene* s) {
 
 int nbo_step(nbo_scene* s, int nsteps) {
     for (int it = 0; it < nsteps; it++) {
-        clump_integrate_before(s);
-        update_pos(s);
+        if (s->sphere) {
+            sphere_integrate_before(s);
+        } else {
+            clump_integrate_before(s);
+            update_pos(s);
+        }
         if (s->is_intruder) pene_integrate_before(s);
-        if (s->update != 0 || s->step == s->start_step) {
+        int rebuilt = s->update != 0 || s->step == s->start_step;
+        if (rebuilt) {
             int rc = rebuild(s);
             if (rc) return rc;
-        } else {
+            if (s->sphere) memset(s->scum, 0, s->K * sizeof(d3));
+        }
+        /* the cylinder and split drivers exchange the pair histories on
+         * every step, after a rebuild too (src/dem_simulation_cylind.cu:141):
+         * the carried histories are cleared */
+        if (!rebuilt || (s->sphere & SPH_RESET)) {
             /* DEMForce::ForceExchange, src/dem_force.cu:88-98 */
             swap_d3(&s->Dv, &s->Dv_pre);
             swap_d3(&s->Dt, &s->Dt_pre);
@@ -1374,7 +1509,8 @@ int nbo_step(nbo_scene* s, int nsteps) {
             s->totT[i] = add3(add3(s->Tc[i], s->Tw[i]), s->Ti[i]);
         }
         sum_force_on_clump(s);
-        clump_integrate_after(s);
+        if (s->sphere) sphere_integrate_after(s);
+        else clump_integrate_after(s);
         s->step++;
     }
     return 0;

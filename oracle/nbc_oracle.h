@@ -17,7 +17,14 @@
  *
  * Additions that the reference has only on its sphere path are restated with
  * clump kinematics: the closed cylinder wall (src/dem_force_cylind_wall.cu:
- * 3-237) and the hierarchical grid (src/dem_hgrid_contlist.cu:57-248).
+ * 3-237) and the hierarchical grid (src/dem_hgrid_contlist.cu:57-248), the
+ * latter race-free (the reference's cross-level appends race with its
+ * same-level ones).  With nbo_desc.sphere_mode it restates the sphere-only
+ * drivers themselves (class DEMmain: src/dem_integrate.cu,
+ * src/dem_integrate_withglue.cu, src/dem_force_particle.cu:3-182,
+ * src/dem_force_cube_wall.cu, src/dem_force_penetrator.cu:8-187 and the
+ * drivers' history exchange, src/dem_simulation_{cylind,cube,split}.cu),
+ * pinned to the reference's own runs of those drivers.
  */
 #ifndef NBC_ORACLE_H
 #define NBC_ORACLE_H
@@ -61,6 +68,14 @@ typedef struct {
     int levels;
     const int* level;          /* [N] 0 = coarsest */
     const double* level_cell;  /* [levels] cell size per level */
+    /* the reference's sphere-only drivers (class DEMmain): bits 1 sphere
+     * kinematics (first half-kick and attitude without the intruder, the
+     * sphere laws' lever arms, penetrator cohesion), 2 the sphere cube wall
+     * (no history, no rolling or twisting moment), 4 pair histories reset at
+     * every rebuild; body_kind (or NULL) the split driver's Type per sphere.
+     * One-sphere clumps with LocalPos = 0, sphere k = clump k. */
+    int sphere_mode;
+    const int* body_kind;
 } nbo_desc;
 
 typedef struct nbo_scene nbo_scene;

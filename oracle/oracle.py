@@ -43,6 +43,7 @@ class Desc(C.Structure):
         ("intr_prop", D4), ("intr_pos", D3), ("intr_vel", D3), ("intr_quat", D4),
         ("intr_angvel", D3),
         ("levels", C.c_int), ("level", P_I), ("level_cell", P_D),
+        ("sphere_mode", C.c_int), ("body_kind", P_I),
     ]
 
 
@@ -145,6 +146,11 @@ class OracleScene:
             d.levels = len(keep["level_cell"])
             d.level = _p(keep["level"], P_I)
             d.level_cell = _p(keep["level_cell"])
+        # the reference's sphere-only drivers (scenegen.as_sphere_driver)
+        d.sphere_mode = int(scene.get("sphere_mode", 0))
+        if scene.get("body_kind") is not None:
+            keep["body_kind"] = np.ascontiguousarray(scene["body_kind"], dtype=np.int32)
+            d.body_kind = _p(keep["body_kind"], P_I)
         self._desc = d
         self.h = L.nbo_create(C.byref(d))
 

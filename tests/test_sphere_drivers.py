@@ -110,6 +110,33 @@ def test_sphere_fixtures_exercise_their_driver(golden_dir):
     assert (np.abs(vel[rest & (k == 0)] - v0[rest & (k == 0)]).max(1) > 0).all()
 
 
+@pytest.mark.parametrize("name", REF_PINNED)
+def test_oracle_matches_reference_sphere_driver(golden_dir, name):
+    """The oracle's restatement of the sphere drivers (integrator, sphere
+    laws, memoryless cube wall, penetrator cohesion, history reset, the split
+    driver's kinds) against the reference's own run of the driver, every one
+    of 24 steps (CPU): sort order bit-exact, states to 1e-13, the intruder's
+    position exact and its reaction to 1e-13 of its scale."""
+    import oracle
+    driver = CASES[name]
+    sc = _scene(golden_dir, name)
+    g = np.load(os.path.join(golden_dir, f"{name}.ref.npz"))
+    o = oracle.OracleScene(sg.as_sphere_driver(sc, driver))
+    for s in range(1, int(g["steps"]) + 1):
+        o.step(1)
+        pf = g[f"s{s}/part_fix"]
+        assert np.array_equal(o.sub()["part_fix"], pf), f"step {s}: sort order"
+        c = o.clumps()
+        for k in ("pos", "vel", "angvel", "quat"):
+            assert _rel(c[k], _by_original(pf, g[f"s{s}/{k}"])) < 1e-13, (s, k)
+        if f"s{s}/intr_force" in g:
+            it = o.intruder()
+            assert np.array_equal(it["pos"], g[f"s{s}/intr_pos"]), s
+            ref = g[f"s{s}/intr_force"][0]
+            assert np.abs(it["reaction"] - ref).max() <= 1e-13 * max(1e-3, np.abs(ref).max()), s
+    assert o.rebuilds >= 2
+
+
 def test_reference_hgrid_driver_breaks_action_reaction(golden_dir):
     """The reference's hgrid list build races: a large sphere's thread
     appends its same-level partners with a plain read-modify-write of its
@@ -200,10 +227,11 @@ def test_dropin_hgrid_driver_matches_oracle(golden_dir):
     """RunSimulation_HGrid on two sphere sizes and two levels of grid.bt
     against the oracle's race-free hierarchical grid, every step: sort order
     and states to rounding (no intruder, so the driver's kinematics are the
-    clump path's)."""
+    clump path's except for the sphere laws' lever arms, which the oracle
+    restates too)."""
     import oracle
     sc = _scene(golden_dir, "sph_hgrid")
-    orc = oracle.OracleScene(sc)
+    orc = oracle.OracleScene(sg.as_sphere_driver(sc, "hgrid"))
     with tempfile.TemporaryDirectory() as d:
         _run(sc, "hgrid", d)
         for s in range(1, 25):
