@@ -179,6 +179,83 @@ def test_write_sphere_inputs_layout(golden_dir, driver):
             assert grid[1, 5] == n[0]
 
 
+def _open_sphere_status(d, driver):
+    import ctypes as C
+    h = C.c_void_p()
+    rc = nbc.lib().nbc_open_sphere(d.encode(), nbc.SPHERE_DRIVERS[driver] if isinstance(driver, str) else driver,
+                                   None, C.byref(h))
+    if rc == 0:
+        nbc.lib().nbc_destroy(h)
+    return rc, nbc.lib().nbc_last_error().decode()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_open_sphere_parses_every_driver(golden_dir, name):
+    """nbc_open_sphere reads each driver's working directory (world.par, the
+    21-column ph, the driver's wall, Penetrator.bt, grid.bt); the engine then
+    needs a CUDA device (no CPU fallback)."""
+    from conftest import cuda_available
+    sc = _scene(golden_dir, name)
+    with tempfile.TemporaryDirectory() as d:
+        sg.write_sphere_inputs(sc, d, CASES[name])
+        rc, msg = _open_sphere_status(d, CASES[name])
+        assert rc == (0 if cuda_available() else -5), msg
+
+
+def _remove(rel):
+    def f(d):
+        os.remove(os.path.join(d, rel))
+    return f
+
+
+def _edit(rel, fn):
+    def f(d):
+        p = os.path.join(d, rel)
+        open(p, "w").write(fn(open(p).read()))
+    return f
+
+
+def _ph_type(value):
+    def f(d):
+        p = os.path.join(d, "ph.00000000.bt")
+        lines = open(p).read().splitlines()
+        cols = lines[3].split()
+        cols[2] = str(value)
+        lines[3] = " ".join(cols)
+        open(p, "w").write("\n".join(lines) + "\n")
+    return f
+
+
+@pytest.mark.parametrize("name,driver,mutate,needle", [
+    ("sph_cube", "cube", _remove("Rocks/CubeWall.bt"), "CubeWall.bt"),
+    ("sph_cyl", "cylinder", _remove("Rocks/CylindWall.bt"), "CylindWall.bt"),
+    ("sph_cyl", "cylinder", _remove("Rocks/Penetrator.bt"), "Penetrator.bt"),
+    ("sph_hgrid", "hgrid", _remove("grid.bt"), "grid.bt"),
+    ("sph_hgrid", "hgrid", _ph_type(2), "not a grid level"),
+    ("sph_split", "split", _ph_type(5), "Type must be 0, 1 or 2"),
+    ("sph_cube", "cube", _edit("ph.00000000.bt", lambda t: "\n".join(t.splitlines()[:-3]) + "\n"),
+     "short or malformed"),
+])
+def test_open_sphere_rejects_bad_inputs(golden_dir, name, driver, mutate, needle):
+    """Missing or malformed inputs come back as NBC_ERR_IO with the file
+    named (the reference exits, src/dem_io.cu:196-199,
+    src/dem_penetrator_io.cu:21-27), before any device work."""
+    sc = _scene(golden_dir, name)
+    with tempfile.TemporaryDirectory() as d:
+        sg.write_sphere_inputs(sc, d, driver)
+        mutate(d)
+        rc, msg = _open_sphere_status(d, driver)
+        assert rc == -3 and needle in msg, (rc, msg)
+
+
+def test_open_sphere_rejects_unknown_driver(golden_dir):
+    sc = _scene(golden_dir, "sph_cyl")
+    with tempfile.TemporaryDirectory() as d:
+        sg.write_sphere_inputs(sc, d, "cylinder")
+        rc, msg = _open_sphere_status(d, 7)
+        assert rc == -1 and "driver" in msg
+
+
 # --------------------------------------------------------------------------
 # GPU: the drop-in executable against the reference's drivers
 # --------------------------------------------------------------------------
