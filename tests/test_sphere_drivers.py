@@ -155,6 +155,14 @@ def test_reference_hgrid_driver_breaks_action_reaction(golden_dir):
     gz = np.array([0.0, 0.0, sc["params"]["Gravity"]])
     F = (v1 - sc["clump"]["vel"] - dt * gz) * m[:, None] / (0.5 * dt)
     assert np.abs(F.sum(0)).max() > 1.0
+    # the oracle's race-free list on the same scene: the pair forces cancel,
+    # what is left is the wall's force
+    import oracle
+    o = oracle.OracleScene(sg.as_sphere_driver(sc, "hgrid"))
+    o.step(1)
+    Fo = (o.clumps()["vel"] - sc["clump"]["vel"] - dt * gz) * m[:, None] / (0.5 * dt)
+    fw = o.sub_forces()["fw"].sum(0)
+    assert np.abs(Fo.sum(0) - fw).max() < 1e-9 * np.abs(Fo).max()
 
 
 @pytest.mark.parametrize("driver", ["cylinder", "cube", "split", "hgrid"])
